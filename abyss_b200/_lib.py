@@ -1,0 +1,98 @@
+"""ctypes binding of libabyss_reg.so (include/abyss_reg.h, include/abyss_reg_compat.h).
+
+The library is built in-tree by ``abyss_b200/csrc/Makefile``; importing this
+module never builds or falls back: if the shared object is missing, ``lib()``
+raises, so nothing can run the path without the CUDA code.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libabyss_reg.so")
+
+ABYSS_OK = 0
+ABYSS_WARN_OVERFLOW = 1
+ABYSS_ERR_ARG = -1
+ABYSS_ERR_CUDA = -2
+ABYSS_ERR_OOM = -3
+ABYSS_ERR_TIMEOUT = -4
+ABYSS_ERR_STATE = -5
+ABYSS_ERR_NODEVICE = -6
+
+_dp = C.POINTER(C.c_double)
+_fp = C.POINTER(C.c_float)
+_ip = C.POINTER(C.c_int)
+_vp = C.c_void_p
+
+
+class Tuning(C.Structure):
+    """abyss_tuning: launch shape (zero = automatic)."""
+
+    _fields_ = [("kernel", C.c_int), ("mode", C.c_int), ("threads", C.c_int), ("ipt", C.c_int),
+                ("j_split", C.c_int), ("grid", C.c_int)]
+
+    def as_dict(self):
+        return {f: int(getattr(self, f)) for f, _ in self._fields_}
+
+
+_LIB = None
+
+
+class AbyssError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"abyss error {code}: {msg}")
+        self.code = code
+
+
+def lib():
+    """Load libabyss_reg.so; raises if it has not been built."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -c 'import __graft_entry__ as g; "
+                           "g.build()'` or `make -C abyss_b200/csrc`")
+    L = C.CDLL(LIB_PATH)
+    L.abyss_create.argtypes = [C.c_int, C.POINTER(_vp)]
+    L.abyss_destroy.argtypes = [_vp]
+    L.abyss_last_error.argtypes = [_vp]
+    L.abyss_last_error.restype = C.c_char_p
+    L.abyss_stream.argtypes = [_vp]
+    L.abyss_stream.restype = _vp
+    L.abyss_synchronize.argtypes = [_vp]
+    L.abyss_reserve.argtypes = [_vp, C.c_int, C.c_int, C.c_int]
+    L.abyss_upload_state.argtypes = [_vp, C.c_int] + [_dp] * 7
+    L.abyss_predict.argtypes = [_vp, C.c_double, C.c_double]
+    L.abyss_upload_predicted.argtypes = [_vp, C.c_int] + [_dp] * 4
+    L.abyss_read_predicted.argtypes = [_vp, _dp, _dp, _fp]
+    L.abyss_set_targets.argtypes = [_vp, C.c_int, _ip]
+    L.abyss_launch.argtypes = [_vp, C.c_double, C.c_int, C.POINTER(Tuning)]
+    L.abyss_fetch.argtypes = [_vp, _dp, _dp, _dp, _dp, _ip, _ip, _ip]
+    L.abyss_regular_force.argtypes = [_vp, C.c_int, _ip, C.c_double, C.c_int, C.POINTER(Tuning),
+                                      _dp, _dp, _dp, _dp, _ip, _ip, _ip]
+    L.abyss_last_plan.argtypes = [_vp, C.POINTER(Tuning), _ip]
+    L.abyss_set_profiling.argtypes = [_vp, C.c_int]
+    L.abyss_last_timing.argtypes = [_vp, _fp]
+    L.abyss_set_tuning_table.argtypes = [_vp, C.c_int, _ip, C.POINTER(Tuning)]
+    L.abyss_energy.argtypes = [_vp, C.c_int, _dp, _dp, _dp, C.c_double, _dp]
+    # reference-compatible drop-in
+    L.InitializeDevice.argtypes = [_ip]
+    L.OpenDevice.argtypes = [_ip]
+    L.CloseDevice.argtypes = []
+    L.ProfileDevice.argtypes = [_ip]
+    L.SendToDevice.argtypes = [_ip, _fp, _fp, _fp, _fp, _fp]
+    L.CalculateAccelerationOnDevice.argtypes = [_ip, _ip, _fp, _fp, _ip, _ip]
+    L.SendToDevice_f64.argtypes = [_ip, _dp, _dp, _dp, _dp, _dp]
+    L.CalculateAccelerationOnDevice_f64.argtypes = [_ip, _ip, _dp, _dp, _ip, _ip]
+    L.abyss_compat_set_list_stride.argtypes = [C.c_int]
+    L.abyss_compat_status.argtypes = []
+    _LIB = L
+    return L
+
+
+def ptr(a, t=_dp):
+    if a is None:
+        return C.cast(None, t)
+    return a.ctypes.data_as(t)

@@ -1,0 +1,560 @@
+// Context, buffers, launch planning and the status-returning C ABI
+// (include/abyss_reg.h).
+//
+// The reference keeps its device state in file-static globals sized by
+// new_size(N) and reallocated on growth (src_mpi/cuda/cuda_my_acceleration.cu:
+// 603-778) and launches compute_forces -> reduce_forces_kernel ->
+// gather_neighbor -> gather_numneighbor (:158-218).  Here a context owns
+// growable device buffers and one stream; a launch is
+//   [target ordering] -> force kernel (tile or j-major) -> finalize
+// all enqueued on the context stream.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/abyss_reg.h"
+#include "abyss_internal.cuh"
+#include "kernels.cuh"
+
+using namespace abyss;
+
+namespace {
+
+template <class T>
+struct DevBuf {
+  T *p = nullptr;
+  size_t cap = 0;  // elements
+  cudaError_t ensure(size_t n) {
+    if (n <= cap && p) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    size_t want = std::max<size_t>(n, 1);
+    want = (want + kPad - 1) / kPad * kPad;
+    cudaError_t e = cudaMalloc((void **)&p, want * sizeof(T));
+    if (e != cudaSuccess) {
+      p = nullptr;
+      return e;
+    }
+    cap = want;
+    return cudaSuccess;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+};
+
+struct Table {
+  std::vector<int> m_max;
+  std::vector<abyss_tuning> entries;
+};
+
+}  // namespace
+
+struct abyss_ctx {
+  int device = 0;
+  int sm_count = 148;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  // j-set
+  int n = 0;
+  bool have_state = false, have_jset = false;
+  DevBuf<double> x, v, a0, a1, t0, mass, r2nb;           // state (AoS for vectors)
+  DevBuf<double> px, py, pz, pvx, pvy, pvz;              // predicted SoA
+  DevBuf<float4> vm;
+  // targets and ordering
+  int m = 0;
+  DevBuf<int> targets, order_t, order_o, iota, rows, rows_alt, bbox;
+  DevBuf<uint32_t> keys, keys_alt;
+  DevBuf<char> cub_tmp;
+  size_t cub_bytes = 0;
+  // per-launch work and outputs
+  DevBuf<int> cnt, lst, status, ovf;
+  DevBuf<double> part;
+  DevBuf<double> acc_reg, jerk_reg, acc_irr, jerk_irr;
+  DevBuf<int> nnb, list;
+  int launched_m = 0, launched_cap = 0;
+  bool launched = false;
+  abyss_tuning plan{};
+  int plan_chunks = 0;
+  Table table;
+  // profiling
+  bool profiling = false;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  // scratch for energies
+  DevBuf<double> e_x, e_v, e_m, e_row;
+};
+
+static int fail(abyss_ctx *c, int code, const std::string &msg) {
+  if (c) c->err = msg;
+  return code;
+}
+
+static int cuda_fail(abyss_ctx *c, cudaError_t e, const char *what) {
+  return fail(c, e == cudaErrorMemoryAllocation ? ABYSS_ERR_OOM : ABYSS_ERR_CUDA,
+              std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(expr, what)                                  \
+  do {                                                  \
+    cudaError_t _e = (expr);                            \
+    if (_e != cudaSuccess) return cuda_fail(c, _e, what); \
+  } while (0)
+
+static JSet jset_of(abyss_ctx *c) {
+  JSet js;
+  js.px = c->px.p;
+  js.py = c->py.p;
+  js.pz = c->pz.p;
+  js.vm = c->vm.p;
+  js.pvx = c->pvx.p;
+  js.pvy = c->pvy.p;
+  js.pvz = c->pvz.p;
+  js.mass = c->mass.p;
+  js.r2nb = c->r2nb.p;
+  js.n = c->n;
+  return js;
+}
+
+static int ensure_jset(abyss_ctx *c, int n) {
+  const size_t n1 = (size_t)n + 2;  // slack for the even-count bulk copies
+  CK(c->px.ensure(n1), "alloc px");
+  CK(c->py.ensure(n1), "alloc py");
+  CK(c->pz.ensure(n1), "alloc pz");
+  CK(c->pvx.ensure(n1), "alloc pvx");
+  CK(c->pvy.ensure(n1), "alloc pvy");
+  CK(c->pvz.ensure(n1), "alloc pvz");
+  CK(c->vm.ensure(n1), "alloc vm");
+  CK(c->mass.ensure(n1), "alloc mass");
+  CK(c->r2nb.ensure(n1), "alloc r2nb");
+  return ABYSS_OK;
+}
+
+static int ensure_targets(abyss_ctx *c, int m) {
+  CK(c->targets.ensure(m), "alloc targets");
+  CK(c->order_t.ensure(m), "alloc order_t");
+  CK(c->order_o.ensure(m), "alloc order_o");
+  if (c->iota.cap < (size_t)m) {
+    CK(c->iota.ensure(m), "alloc iota");
+    launch_iota(c->stream, (int)c->iota.cap, c->iota.p, c->sm_count);
+  }
+  return ABYSS_OK;
+}
+
+static int ensure_outputs(abyss_ctx *c, int m, int cap) {
+  CK(c->acc_reg.ensure((size_t)3 * m), "alloc acc_reg");
+  CK(c->jerk_reg.ensure((size_t)3 * m), "alloc jerk_reg");
+  CK(c->acc_irr.ensure((size_t)3 * m), "alloc acc_irr");
+  CK(c->jerk_irr.ensure((size_t)3 * m), "alloc jerk_irr");
+  CK(c->nnb.ensure(m), "alloc nnb");
+  CK(c->list.ensure((size_t)m * cap), "alloc list");
+  CK(c->status.ensure(1), "alloc status");
+  CK(c->ovf.ensure(1), "alloc ovf");
+  return ABYSS_OK;
+}
+
+extern "C" {
+
+int abyss_create(int device, abyss_ctx **out) {
+  if (!out) return ABYSS_ERR_ARG;
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count <= 0) return ABYSS_ERR_NODEVICE;
+  if (device < 0 || device >= count) return ABYSS_ERR_ARG;
+  abyss_ctx *c = new abyss_ctx;
+  c->device = device;
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  for (int i = 0; i < 4 && e == cudaSuccess; ++i) e = cudaEventCreate(&c->ev[i]);
+  if (e != cudaSuccess) {
+    delete c;
+    return ABYSS_ERR_CUDA;
+  }
+  *out = c;
+  return ABYSS_OK;
+}
+
+int abyss_destroy(abyss_ctx *c) {
+  if (!c) return ABYSS_ERR_ARG;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  DevBuf<double> *dbl[] = {&c->x, &c->v, &c->a0, &c->a1, &c->t0, &c->mass, &c->r2nb, &c->px, &c->py,
+                           &c->pz, &c->pvx, &c->pvy, &c->pvz, &c->part, &c->acc_reg, &c->jerk_reg,
+                           &c->acc_irr, &c->jerk_irr, &c->e_x, &c->e_v, &c->e_m, &c->e_row};
+  for (auto *b : dbl) b->release();
+  DevBuf<int> *ints[] = {&c->targets, &c->order_t, &c->order_o, &c->iota, &c->rows, &c->rows_alt,
+                         &c->bbox, &c->cnt, &c->lst, &c->status, &c->ovf, &c->nnb, &c->list};
+  for (auto *b : ints) b->release();
+  c->vm.release();
+  c->keys.release();
+  c->keys_alt.release();
+  c->cub_tmp.release();
+  for (auto &e : c->ev)
+    if (e) cudaEventDestroy(e);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return ABYSS_OK;
+}
+
+const char *abyss_last_error(const abyss_ctx *c) { return c ? c->err.c_str() : "null context"; }
+
+void *abyss_stream(abyss_ctx *c) { return c ? (void *)c->stream : nullptr; }
+
+int abyss_synchronize(abyss_ctx *c) {
+  if (!c) return ABYSS_ERR_ARG;
+  cudaSetDevice(c->device);
+  CK(cudaStreamSynchronize(c->stream), "synchronize");
+  return ABYSS_OK;
+}
+
+int abyss_reserve(abyss_ctx *c, int n, int m, int list_cap) {
+  if (!c || n < 0 || m < 0 || list_cap < 0) return fail(c, ABYSS_ERR_ARG, "reserve: negative size");
+  cudaSetDevice(c->device);
+  int rc;
+  if ((rc = ensure_jset(c, n)) != ABYSS_OK) return rc;
+  if ((rc = ensure_targets(c, std::max(m, 1))) != ABYSS_OK) return rc;
+  if ((rc = ensure_outputs(c, std::max(m, 1), std::max(list_cap, 1))) != ABYSS_OK) return rc;
+  return ABYSS_OK;
+}
+
+int abyss_upload_state(abyss_ctx *c, int n, const double *x, const double *v, const double *a0,
+                       const double *a1, const double *t0, const double *mass, const double *r2nb) {
+  if (!c) return ABYSS_ERR_ARG;
+  if (n <= 0 || !x || !v || !a0 || !a1 || !t0 || !mass || !r2nb)
+    return fail(c, ABYSS_ERR_ARG, "upload_state: n <= 0 or null array");
+  cudaSetDevice(c->device);
+  int rc = ensure_jset(c, n);
+  if (rc != ABYSS_OK) return rc;
+  const size_t v3 = (size_t)3 * n;
+  CK(c->x.ensure(v3), "alloc x");
+  CK(c->v.ensure(v3), "alloc v");
+  CK(c->a0.ensure(v3), "alloc a0");
+  CK(c->a1.ensure(v3), "alloc a1");
+  CK(c->t0.ensure(n), "alloc t0");
+  CK(cudaMemcpyAsync(c->x.p, x, v3 * 8, cudaMemcpyHostToDevice, c->stream), "H2D x");
+  CK(cudaMemcpyAsync(c->v.p, v, v3 * 8, cudaMemcpyHostToDevice, c->stream), "H2D v");
+  CK(cudaMemcpyAsync(c->a0.p, a0, v3 * 8, cudaMemcpyHostToDevice, c->stream), "H2D a0");
+  CK(cudaMemcpyAsync(c->a1.p, a1, v3 * 8, cudaMemcpyHostToDevice, c->stream), "H2D a1");
+  CK(cudaMemcpyAsync(c->t0.p, t0, (size_t)n * 8, cudaMemcpyHostToDevice, c->stream), "H2D t0");
+  CK(cudaMemcpyAsync(c->mass.p, mass, (size_t)n * 8, cudaMemcpyHostToDevice, c->stream), "H2D mass");
+  CK(cudaMemcpyAsync(c->r2nb.p, r2nb, (size_t)n * 8, cudaMemcpyHostToDevice, c->stream), "H2D r2nb");
+  c->n = n;
+  c->have_state = true;
+  c->have_jset = false;
+  return ABYSS_OK;
+}
+
+int abyss_predict(abyss_ctx *c, double new_time, double time_scale) {
+  if (!c) return ABYSS_ERR_ARG;
+  if (!c->have_state) return fail(c, ABYSS_ERR_STATE, "predict: no state uploaded");
+  cudaSetDevice(c->device);
+  launch_predict(c->stream, c->n, c->x.p, c->v.p, c->a0.p, c->a1.p, c->t0.p, c->mass.p, new_time,
+                 time_scale, c->px.p, c->py.p, c->pz.p, c->pvx.p, c->pvy.p, c->pvz.p, c->vm.p,
+                 c->sm_count);
+  CK(cudaGetLastError(), "predict launch");
+  c->have_jset = true;
+  return ABYSS_OK;
+}
+
+int abyss_upload_predicted(abyss_ctx *c, int n, const double *px, const double *pv,
+                           const double *mass, const double *r2nb) {
+  if (!c) return ABYSS_ERR_ARG;
+  if (n <= 0 || !px || !pv || !mass || !r2nb)
+    return fail(c, ABYSS_ERR_ARG, "upload_predicted: n <= 0 or null array");
+  cudaSetDevice(c->device);
+  int rc = ensure_jset(c, n);
+  if (rc != ABYSS_OK) return rc;
+  const size_t v3 = (size_t)3 * n;
+  CK(c->x.ensure(v3), "alloc x");
+  CK(c->v.ensure(v3), "alloc v");
+  CK(cudaMemcpyAsync(c->x.p, px, v3 * 8, cudaMemcpyHostToDevice, c->stream), "H2D px");
+  CK(cudaMemcpyAsync(c->v.p, pv, v3 * 8, cudaMemcpyHostToDevice, c->stream), "H2D pv");
+  CK(cudaMemcpyAsync(c->mass.p, mass, (size_t)n * 8, cudaMemcpyHostToDevice, c->stream), "H2D mass");
+  CK(cudaMemcpyAsync(c->r2nb.p, r2nb, (size_t)n * 8, cudaMemcpyHostToDevice, c->stream), "H2D r2nb");
+  launch_unpack_predicted(c->stream, n, c->x.p, c->v.p, c->mass.p, c->px.p, c->py.p, c->pz.p,
+                          c->pvx.p, c->pvy.p, c->pvz.p, c->vm.p, c->sm_count);
+  CK(cudaGetLastError(), "unpack launch");
+  c->n = n;
+  c->have_state = false;
+  c->have_jset = true;
+  return ABYSS_OK;
+}
+
+int abyss_read_predicted(abyss_ctx *c, double *px, double *pv, float *vm4) {
+  if (!c) return ABYSS_ERR_ARG;
+  if (!c->have_jset) return fail(c, ABYSS_ERR_STATE, "read_predicted: no predicted j-set");
+  cudaSetDevice(c->device);
+  const size_t n = c->n;
+  std::vector<double> tmp(6 * n);
+  double *dst[6] = {tmp.data(), tmp.data() + n, tmp.data() + 2 * n,
+                    tmp.data() + 3 * n, tmp.data() + 4 * n, tmp.data() + 5 * n};
+  const double *src[6] = {c->px.p, c->py.p, c->pz.p, c->pvx.p, c->pvy.p, c->pvz.p};
+  for (int k = 0; k < 6; ++k)
+    CK(cudaMemcpyAsync(dst[k], src[k], n * 8, cudaMemcpyDeviceToHost, c->stream), "D2H predicted");
+  if (vm4) CK(cudaMemcpyAsync(vm4, c->vm.p, n * 16, cudaMemcpyDeviceToHost, c->stream), "D2H vm");
+  CK(cudaStreamSynchronize(c->stream), "synchronize");
+  for (size_t j = 0; j < n; ++j)
+    for (int d = 0; d < 3; ++d) {
+      if (px) px[3 * j + d] = dst[d][j];
+      if (pv) pv[3 * j + d] = dst[3 + d][j];
+    }
+  return ABYSS_OK;
+}
+
+int abyss_set_targets(abyss_ctx *c, int m, const int *targets) {
+  if (!c) return ABYSS_ERR_ARG;
+  if (m <= 0 || !targets) return fail(c, ABYSS_ERR_ARG, "set_targets: m <= 0 or null targets");
+  if (c->n <= 0) return fail(c, ABYSS_ERR_STATE, "set_targets: no j-set uploaded");
+  if (m > c->n) return fail(c, ABYSS_ERR_ARG, "set_targets: m > n");
+  for (int k = 0; k < m; ++k)
+    if (targets[k] < 0 || targets[k] >= c->n)
+      return fail(c, ABYSS_ERR_ARG, "set_targets: target index out of range");
+  cudaSetDevice(c->device);
+  int rc = ensure_targets(c, m);
+  if (rc != ABYSS_OK) return rc;
+  CK(cudaMemcpyAsync(c->targets.p, targets, (size_t)m * 4, cudaMemcpyHostToDevice, c->stream),
+     "H2D targets");
+  c->m = m;
+  return ABYSS_OK;
+}
+
+// ------------------------------------------------------------------ planning
+static abyss_tuning plan_for(abyss_ctx *c, int m, const abyss_tuning *user) {
+  abyss_tuning t{};
+  if (user) t = *user;
+  if (t.kernel == 0) {
+    for (size_t k = 0; k < c->table.m_max.size(); ++k)
+      if (m <= c->table.m_max[k]) {
+        const abyss_tuning &e = c->table.entries[k];
+        if (t.kernel == 0) t.kernel = e.kernel;
+        if (t.mode == 0) t.mode = e.mode;
+        if (t.threads == 0) t.threads = e.threads;
+        if (t.ipt == 0) t.ipt = e.ipt;
+        if (t.j_split == 0) t.j_split = e.j_split;
+        if (t.grid == 0) t.grid = e.grid;
+        break;
+      }
+  }
+  if (t.kernel == 0) t.kernel = (m <= 64) ? 2 : 1;
+  if (t.kernel == 2) {
+    if (t.ipt == 0) t.ipt = m <= 1 ? 1 : m <= 2 ? 2 : m <= 4 ? 4 : 8;
+  } else {
+    if (t.mode == 0) t.mode = (m >= 4096) ? 1 : 2;
+    if (t.threads == 0) t.threads = 128;
+    if (t.ipt == 0) t.ipt = (m >= 65536) ? 2 : 1;
+  }
+  return t;
+}
+
+int abyss_launch(abyss_ctx *c, double eps2, int list_cap, const abyss_tuning *tuning) {
+  if (!c) return ABYSS_ERR_ARG;
+  if (!c->have_jset) return fail(c, ABYSS_ERR_STATE, "launch: no predicted j-set");
+  if (c->m <= 0) return fail(c, ABYSS_ERR_STATE, "launch: no targets");
+  if (list_cap <= 0) return fail(c, ABYSS_ERR_ARG, "launch: list_cap must be positive");
+  if (!(eps2 >= 0.0)) return fail(c, ABYSS_ERR_ARG, "launch: eps2 must be >= 0");
+  cudaSetDevice(c->device);
+  const int n = c->n, m = c->m;
+  abyss_tuning t = plan_for(c, m, tuning);
+  constexpr int TJ = 128;
+  int S = 1, L = 0, grid = 0, n_iblocks = 0;
+  if (t.kernel == 2) {
+    if (t.ipt != 1 && t.ipt != 2 && t.ipt != 4 && t.ipt != 8)
+      return fail(c, ABYSS_ERR_ARG, "launch: j-major ipt must be 1, 2, 4 or 8");
+    int want = t.j_split > 0 ? t.j_split : c->sm_count * 16;
+    L = (n + want - 1) / want;
+    L = std::max(32, (L + 31) / 32 * 32);
+    S = (n + L - 1) / L;
+  } else if (t.kernel == 1) {
+    const int per_block = t.threads * t.ipt;
+    n_iblocks = (m + per_block - 1) / per_block;
+    const int occ = tile_occupancy(t.threads, t.ipt, t.mode == 1);
+    if (occ <= 0) return fail(c, ABYSS_ERR_ARG, "launch: unsupported tile shape");
+    const int resident = occ * c->sm_count;
+    int s_want = t.j_split;
+    if (s_want <= 0) s_want = std::max(1, (2 * resident + n_iblocks - 1) / n_iblocks);
+    const int max_chunks = std::max(1, (n + 2 * TJ - 1) / (2 * TJ));
+    s_want = std::min(s_want, max_chunks);
+    int chunk = (n + s_want - 1) / s_want;
+    chunk = (chunk + TJ - 1) / TJ * TJ;
+    L = chunk;
+    S = (n + chunk - 1) / chunk;
+    const int items = n_iblocks * S;
+    if (t.grid > 0) {
+      grid = std::min(t.grid, items);
+    } else {
+      const int waves = (items + resident - 1) / resident;
+      grid = (items + waves - 1) / waves;
+    }
+  } else {
+    return fail(c, ABYSS_ERR_ARG, "launch: unknown kernel");
+  }
+  int rc = ensure_outputs(c, m, list_cap);
+  if (rc != ABYSS_OK) return rc;
+  CK(c->cnt.ensure((size_t)S * m), "alloc cnt");
+  CK(c->lst.ensure((size_t)S * m * list_cap), "alloc lst");
+  CK(c->part.ensure((size_t)S * m * 6), "alloc part");
+  CK(cudaMemsetAsync(c->status.p, 0, sizeof(int), c->stream), "clear status");
+  CK(cudaMemsetAsync(c->ovf.p, 0, sizeof(int), c->stream), "clear ovf");
+
+  JSet js = jset_of(c);
+  Work w;
+  w.m = m;
+  w.n_chunks = S;
+  w.chunk_len = L;
+  w.cap = list_cap;
+  w.eps2 = eps2;
+  w.eps2f = (float)eps2;
+  w.cnt = c->cnt.p;
+  w.lst = c->lst.p;
+  w.part = c->part.p;
+  w.status = c->status.p;
+
+  if (c->profiling) CK(cudaEventRecord(c->ev[0], c->stream), "event");
+  if (t.kernel == 1 && t.mode == 1) {
+    if (c->cub_bytes == 0 || c->keys.cap < (size_t)m) {
+      CK(c->keys.ensure(m), "alloc keys");
+      CK(c->keys_alt.ensure(m), "alloc keys");
+      CK(c->rows.ensure(m), "alloc rows");
+      CK(c->rows_alt.ensure(m), "alloc rows");
+      CK(c->bbox.ensure(6), "alloc bbox");
+      c->cub_bytes = morton_temp_bytes((int)c->keys.cap);
+      CK(c->cub_tmp.ensure(c->cub_bytes), "alloc sort scratch");
+    }
+    launch_morton_order(c->stream, m, c->targets.p, js, c->bbox.p, c->keys.p, c->keys_alt.p,
+                        c->rows.p, c->rows_alt.p, c->cub_tmp.p, c->cub_bytes, c->order_t.p,
+                        c->order_o.p, c->sm_count);
+    w.order_t = c->order_t.p;
+    w.order_o = c->order_o.p;
+  } else {
+    w.order_t = c->targets.p;
+    w.order_o = c->iota.p;
+  }
+  if (c->profiling) CK(cudaEventRecord(c->ev[1], c->stream), "event");
+  if (t.kernel == 1) {
+    if (launch_tile(c->stream, t.threads, t.ipt, t.mode == 1, grid, js, w, n_iblocks) != 0)
+      return fail(c, ABYSS_ERR_ARG, "launch: unsupported tile shape");
+    t.grid = grid;
+  } else {
+    if (launch_jmajor(c->stream, t.ipt, js, w, L) != 0)
+      return fail(c, ABYSS_ERR_ARG, "launch: unsupported j-major shape");
+  }
+  CK(cudaGetLastError(), "force kernel launch");
+  if (c->profiling) CK(cudaEventRecord(c->ev[2], c->stream), "event");
+  Outputs o;
+  o.targets = c->targets.p;
+  o.acc_reg = c->acc_reg.p;
+  o.jerk_reg = c->jerk_reg.p;
+  o.acc_irr = c->acc_irr.p;
+  o.jerk_irr = c->jerk_irr.p;
+  o.nnb = c->nnb.p;
+  o.list = c->list.p;
+  o.overflow_rows = c->ovf.p;
+  launch_finalize(c->stream, js, w, o, c->sm_count);
+  CK(cudaGetLastError(), "finalize launch");
+  if (c->profiling) CK(cudaEventRecord(c->ev[3], c->stream), "event");
+  t.j_split = S;
+  c->plan = t;
+  c->plan_chunks = S;
+  c->launched = true;
+  c->launched_m = m;
+  c->launched_cap = list_cap;
+  return ABYSS_OK;
+}
+
+int abyss_fetch(abyss_ctx *c, double *acc_reg, double *jerk_reg, double *acc_irr, double *jerk_irr,
+                int *nnb, int *list, int *overflow_rows) {
+  if (!c) return ABYSS_ERR_ARG;
+  if (!c->launched) return fail(c, ABYSS_ERR_STATE, "fetch: nothing launched");
+  cudaSetDevice(c->device);
+  const size_t m = c->launched_m;
+  int st = 0, ovf = 0;
+  CK(cudaMemcpyAsync(&st, c->status.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "D2H status");
+  CK(cudaMemcpyAsync(&ovf, c->ovf.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "D2H ovf");
+  if (acc_reg) CK(cudaMemcpyAsync(acc_reg, c->acc_reg.p, m * 24, cudaMemcpyDeviceToHost, c->stream), "D2H");
+  if (jerk_reg) CK(cudaMemcpyAsync(jerk_reg, c->jerk_reg.p, m * 24, cudaMemcpyDeviceToHost, c->stream), "D2H");
+  if (acc_irr) CK(cudaMemcpyAsync(acc_irr, c->acc_irr.p, m * 24, cudaMemcpyDeviceToHost, c->stream), "D2H");
+  if (jerk_irr) CK(cudaMemcpyAsync(jerk_irr, c->jerk_irr.p, m * 24, cudaMemcpyDeviceToHost, c->stream), "D2H");
+  if (nnb) CK(cudaMemcpyAsync(nnb, c->nnb.p, m * 4, cudaMemcpyDeviceToHost, c->stream), "D2H");
+  if (list)
+    CK(cudaMemcpyAsync(list, c->list.p, m * (size_t)c->launched_cap * 4, cudaMemcpyDeviceToHost,
+                       c->stream),
+       "D2H list");
+  CK(cudaStreamSynchronize(c->stream), "synchronize");
+  if (overflow_rows) *overflow_rows = ovf;
+  if (st & kErrTimeout) return fail(c, ABYSS_ERR_TIMEOUT, "device wait timed out");
+  if (ovf > 0) {
+    c->err = "neighbour list overflow in " + std::to_string(ovf) + " rows";
+    return ABYSS_WARN_OVERFLOW;
+  }
+  return ABYSS_OK;
+}
+
+int abyss_regular_force(abyss_ctx *c, int m, const int *targets, double eps2, int list_cap,
+                        const abyss_tuning *tuning, double *acc_reg, double *jerk_reg,
+                        double *acc_irr, double *jerk_irr, int *nnb, int *list,
+                        int *overflow_rows) {
+  int rc = abyss_set_targets(c, m, targets);
+  if (rc != ABYSS_OK) return rc;
+  rc = abyss_launch(c, eps2, list_cap, tuning);
+  if (rc != ABYSS_OK) return rc;
+  return abyss_fetch(c, acc_reg, jerk_reg, acc_irr, jerk_irr, nnb, list, overflow_rows);
+}
+
+int abyss_last_plan(const abyss_ctx *c, abyss_tuning *plan, int *n_chunks) {
+  if (!c) return ABYSS_ERR_ARG;
+  if (plan) *plan = c->plan;
+  if (n_chunks) *n_chunks = c->plan_chunks;
+  return ABYSS_OK;
+}
+
+int abyss_set_profiling(abyss_ctx *c, int on) {
+  if (!c) return ABYSS_ERR_ARG;
+  c->profiling = on != 0;
+  return ABYSS_OK;
+}
+
+int abyss_last_timing(abyss_ctx *c, float *ms3) {
+  if (!c || !ms3) return ABYSS_ERR_ARG;
+  if (!c->profiling) return fail(c, ABYSS_ERR_STATE, "last_timing: profiling is off");
+  cudaSetDevice(c->device);
+  CK(cudaStreamSynchronize(c->stream), "synchronize");
+  for (int i = 0; i < 3; ++i) CK(cudaEventElapsedTime(&ms3[i], c->ev[i], c->ev[i + 1]), "event time");
+  return ABYSS_OK;
+}
+
+int abyss_set_tuning_table(abyss_ctx *c, int k, const int *m_max, const abyss_tuning *entries) {
+  if (!c || k < 0 || (k > 0 && (!m_max || !entries))) return ABYSS_ERR_ARG;
+  c->table.m_max.assign(m_max, m_max + k);
+  c->table.entries.assign(entries, entries + k);
+  return ABYSS_OK;
+}
+
+int abyss_energy(abyss_ctx *c, int n, const double *x, const double *v, const double *mass,
+                 double eps2, double *energy) {
+  if (!c || n <= 0 || !x || !v || !mass || !energy) return fail(c, ABYSS_ERR_ARG, "energy: bad args");
+  cudaSetDevice(c->device);
+  CK(c->e_x.ensure((size_t)3 * n), "alloc");
+  CK(c->e_v.ensure((size_t)3 * n), "alloc");
+  CK(c->e_m.ensure(n), "alloc");
+  CK(c->e_row.ensure(n), "alloc");
+  CK(cudaMemcpyAsync(c->e_x.p, x, (size_t)24 * n, cudaMemcpyHostToDevice, c->stream), "H2D");
+  CK(cudaMemcpyAsync(c->e_v.p, v, (size_t)24 * n, cudaMemcpyHostToDevice, c->stream), "H2D");
+  CK(cudaMemcpyAsync(c->e_m.p, mass, (size_t)8 * n, cudaMemcpyHostToDevice, c->stream), "H2D");
+  launch_energy(c->stream, n, c->e_x.p, c->e_v.p, c->e_m.p, eps2, c->e_row.p);
+  CK(cudaGetLastError(), "energy launch");
+  std::vector<double> rows(n);
+  CK(cudaMemcpyAsync(rows.data(), c->e_row.p, (size_t)8 * n, cudaMemcpyDeviceToHost, c->stream), "D2H");
+  CK(cudaStreamSynchronize(c->stream), "synchronize");
+  double e = 0.0;
+  for (int i = 0; i < n; ++i) e += rows[i];
+  *energy = e;
+  return ABYSS_OK;
+}
+
+}  // extern "C"

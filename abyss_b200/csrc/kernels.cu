@@ -1,0 +1,830 @@
+// sm_100a kernels of the Ahmad-Cohen regular-force path.
+//
+//   predict_jset      device-side j prediction (UpdateParticle.cpp:37-59), FP64
+//   target_bbox/morton  spatial ordering of targets for the anchor mode
+//   reg_force_tile    i in registers, j-tiles through shared memory by TMA bulk
+//                     copies, FP32 pair arithmetic with Kahan-folded tile sums,
+//                     guarded FP32 neighbour test re-decided in FP64
+//   reg_force_jmajor  lanes over j for very small active sets; exact FP64
+//                     neighbour test, ballot + popc ordered list compaction
+//   finalize_rows     FP64 cross-chunk sum, ordered list concatenation,
+//                     FP64 irregular part over the final list
+//
+// Semantics follow the reference's CPU regular force
+// (src_mpi/Particle/ComputeAcceleration.cpp:235-299): j ranges over all
+// particles except the target; r2 < R_nb^2 (FP64, unsoftened) makes j a
+// neighbour (irregular part, list in ascending j); every other j adds
+// m r^-3 dx to the regular acceleration and m r^-3 (dv - 3 (dx.dv) dx / r^2)
+// to the regular jerk, with r^2 softened by eps^2 in the force terms.
+#include <cfloat>
+#include <cstdint>
+#include <cub/cub.cuh>
+
+#include "abyss_internal.cuh"
+#include "kernels.cuh"
+
+namespace abyss {
+
+// ============================================================ prediction
+// One thread per particle.  Intrinsics keep the reference's operation order
+// with no fused multiply-add, so predicted values equal the host predictor's.
+__global__ void predict_jset(int n, const double *__restrict__ x, const double *__restrict__ v,
+                             const double *__restrict__ a0, const double *__restrict__ a1,
+                             const double *__restrict__ t0, const double *__restrict__ mass,
+                             double new_time, double time_scale, double *__restrict__ px,
+                             double *__restrict__ py, double *__restrict__ pz,
+                             double *__restrict__ pvx, double *__restrict__ pvy,
+                             double *__restrict__ pvz, float4 *__restrict__ vm) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    const double dt = __dmul_rn(__dsub_rn(new_time, t0[j]), time_scale);
+    double p[3], q[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double xd = x[3 * j + d], vd = v[3 * j + d];
+      if (dt == 0.0) {
+        p[d] = xd;
+        q[d] = vd;
+      } else {
+        const double a0d = a0[3 * j + d], a1d = a1[3 * j + d];
+        double t = __dmul_rn(a1d, dt);
+        t = __ddiv_rn(t, 3.0);
+        t = __dadd_rn(t, a0d);
+        t = __dmul_rn(t, dt);
+        t = __ddiv_rn(t, 2.0);
+        t = __dadd_rn(t, vd);
+        t = __dmul_rn(t, dt);
+        p[d] = __dadd_rn(t, xd);
+        double u = __dmul_rn(a1d, dt);
+        u = __ddiv_rn(u, 2.0);
+        u = __dadd_rn(u, a0d);
+        u = __dmul_rn(u, dt);
+        q[d] = __dadd_rn(u, vd);
+      }
+    }
+    px[j] = p[0];
+    py[j] = p[1];
+    pz[j] = p[2];
+    pvx[j] = q[0];
+    pvy[j] = q[1];
+    pvz[j] = q[2];
+    vm[j] = make_float4((float)q[0], (float)q[1], (float)q[2], (float)mass[j]);
+  }
+}
+
+// j-set already predicted by the caller (reference-compatible SendToDevice):
+// fill the FP32 (v, m) records from the FP64 arrays.
+__global__ void pack_vm(int n, const double *__restrict__ pvx, const double *__restrict__ pvy,
+                        const double *__restrict__ pvz, const double *__restrict__ mass,
+                        float4 *__restrict__ vm) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+    vm[j] = make_float4((float)pvx[j], (float)pvy[j], (float)pvz[j], (float)mass[j]);
+}
+
+// j-set given as predicted AoS [n][3] positions and velocities: split into the
+// SoA FP64 arrays and the FP32 (v, m) records.
+__global__ void unpack_predicted(int n, const double *__restrict__ pos, const double *__restrict__ vel,
+                                 const double *__restrict__ mass, double *__restrict__ px,
+                                 double *__restrict__ py, double *__restrict__ pz,
+                                 double *__restrict__ pvx, double *__restrict__ pvy,
+                                 double *__restrict__ pvz, float4 *__restrict__ vm) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    px[j] = pos[3 * j];
+    py[j] = pos[3 * j + 1];
+    pz[j] = pos[3 * j + 2];
+    pvx[j] = vel[3 * j];
+    pvy[j] = vel[3 * j + 1];
+    pvz[j] = vel[3 * j + 2];
+    vm[j] = make_float4((float)vel[3 * j], (float)vel[3 * j + 1], (float)vel[3 * j + 2], (float)mass[j]);
+  }
+}
+
+// ============================================================ target ordering
+__device__ __forceinline__ int ordered_int(float f) {
+  const int i = __float_as_int(f);
+  return i >= 0 ? i : i ^ 0x7fffffff;
+}
+__device__ __forceinline__ float from_ordered(int i) {
+  return __int_as_float(i >= 0 ? i : i ^ 0x7fffffff);
+}
+
+__global__ void target_bbox(int m, const int *__restrict__ targets, const double *__restrict__ px,
+                            const double *__restrict__ py, const double *__restrict__ pz,
+                            int *__restrict__ bbox /* [6]: min xyz, max xyz */) {
+  int mn[3] = {INT_MAX, INT_MAX, INT_MAX}, mx[3] = {INT_MIN, INT_MIN, INT_MIN};
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < m; s += gridDim.x * blockDim.x) {
+    const int t = targets[s];
+    const int c[3] = {ordered_int((float)px[t]), ordered_int((float)py[t]), ordered_int((float)pz[t])};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      mn[d] = min(mn[d], c[d]);
+      mx[d] = max(mx[d], c[d]);
+    }
+  }
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    for (int o = 16; o > 0; o >>= 1) {
+      mn[d] = min(mn[d], __shfl_xor_sync(0xffffffffu, mn[d], o));
+      mx[d] = max(mx[d], __shfl_xor_sync(0xffffffffu, mx[d], o));
+    }
+  }
+  if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      atomicMin(&bbox[d], mn[d]);
+      atomicMax(&bbox[3 + d], mx[d]);
+    }
+  }
+}
+
+__device__ __forceinline__ uint32_t spread10(uint32_t v) {
+  v &= 0x3ffu;
+  v = (v | (v << 16)) & 0x030000ffu;
+  v = (v | (v << 8)) & 0x0300f00fu;
+  v = (v | (v << 4)) & 0x030c30c3u;
+  v = (v | (v << 2)) & 0x09249249u;
+  return v;
+}
+
+__global__ void target_morton(int m, const int *__restrict__ targets, const double *__restrict__ px,
+                              const double *__restrict__ py, const double *__restrict__ pz,
+                              const int *__restrict__ bbox, uint32_t *__restrict__ keys,
+                              int *__restrict__ rows) {
+  const float lo[3] = {from_ordered(bbox[0]), from_ordered(bbox[1]), from_ordered(bbox[2])};
+  const float hi[3] = {from_ordered(bbox[3]), from_ordered(bbox[4]), from_ordered(bbox[5])};
+  float sc[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) sc[d] = hi[d] > lo[d] ? 1023.0f / (hi[d] - lo[d]) : 0.0f;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < m; s += gridDim.x * blockDim.x) {
+    const int t = targets[s];
+    const float c[3] = {(float)px[t], (float)py[t], (float)pz[t]};
+    uint32_t q[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      float f = (c[d] - lo[d]) * sc[d];
+      f = fminf(fmaxf(f, 0.0f), 1023.0f);
+      q[d] = (uint32_t)f;
+    }
+    keys[s] = (spread10(q[0]) << 2) | (spread10(q[1]) << 1) | spread10(q[2]);
+    rows[s] = s;
+  }
+}
+
+__global__ void gather_order(int m, const int *__restrict__ targets, const int *__restrict__ rows_sorted,
+                             int *__restrict__ order_t, int *__restrict__ order_o) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < m; s += gridDim.x * blockDim.x) {
+    const int r = rows_sorted[s];
+    order_o[s] = r;
+    order_t[s] = targets[r];
+  }
+}
+
+__global__ void iota_kernel(int m, int *__restrict__ out) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < m; s += gridDim.x * blockDim.x) out[s] = s;
+}
+
+// ============================================================ pair arithmetic
+// Shared by the fast path and the slow (candidate) path so that both see the
+// very same FP32 r^2: explicit round-to-nearest intrinsics forbid the compiler
+// from contracting or reordering either copy.
+struct PairGeom {
+  float dx, dy, dz, dvx, dvy, dvz, r2, rv;
+};
+
+__device__ __forceinline__ PairGeom pair_geom(float xj, float yj, float zj, float vxj, float vyj,
+                                              float vzj, float xi, float yi, float zi, float vxi,
+                                              float vyi, float vzi, float eps2) {
+  PairGeom g;
+  g.dx = __fsub_rn(xj, xi);
+  g.dy = __fsub_rn(yj, yi);
+  g.dz = __fsub_rn(zj, zi);
+  g.dvx = __fsub_rn(vxj, vxi);
+  g.dvy = __fsub_rn(vyj, vyi);
+  g.dvz = __fsub_rn(vzj, vzi);
+  g.r2 = __fmaf_rn(g.dx, g.dx, __fmaf_rn(g.dy, g.dy, __fmaf_rn(g.dz, g.dz, eps2)));
+  g.rv = __fmaf_rn(g.dx, g.dvx, __fmaf_rn(g.dy, g.dvy, __fmul_rn(g.dz, g.dvz)));
+  return g;
+}
+
+// Double-single differencing: d = (hj - hi) + (lj - li).
+__device__ __forceinline__ PairGeom pair_geom_ds(float xj, float yj, float zj, float xjl, float yjl,
+                                                 float zjl, float vxj, float vyj, float vzj,
+                                                 float xi, float yi, float zi, float xil, float yil,
+                                                 float zil, float vxi, float vyi, float vzi,
+                                                 float eps2) {
+  PairGeom g;
+  g.dx = __fadd_rn(__fsub_rn(xj, xi), __fsub_rn(xjl, xil));
+  g.dy = __fadd_rn(__fsub_rn(yj, yi), __fsub_rn(yjl, yil));
+  g.dz = __fadd_rn(__fsub_rn(zj, zi), __fsub_rn(zjl, zil));
+  g.dvx = __fsub_rn(vxj, vxi);
+  g.dvy = __fsub_rn(vyj, vyi);
+  g.dvz = __fsub_rn(vzj, vzi);
+  g.r2 = __fmaf_rn(g.dx, g.dx, __fmaf_rn(g.dy, g.dy, __fmaf_rn(g.dz, g.dz, eps2)));
+  g.rv = __fmaf_rn(g.dx, g.dvx, __fmaf_rn(g.dy, g.dvy, __fmul_rn(g.dz, g.dvz)));
+  return g;
+}
+
+// acc += m r^-3 d;  jerk += m r^-3 (dv - 3 (d.dv)/r^2 d)  with rinv possibly masked to 0.
+__device__ __forceinline__ void pair_accum(const PairGeom &g, float mj, float rinv, float *p) {
+  const float q = rinv * rinv;
+  const float mr3 = mj * rinv * q;
+  const float al = -3.0f * g.rv * q;
+  p[0] = fmaf(mr3, g.dx, p[0]);
+  p[1] = fmaf(mr3, g.dy, p[1]);
+  p[2] = fmaf(mr3, g.dz, p[2]);
+  p[3] = fmaf(mr3, fmaf(al, g.dx, g.dvx), p[3]);
+  p[4] = fmaf(mr3, fmaf(al, g.dy, g.dvy), p[4]);
+  p[5] = fmaf(mr3, fmaf(al, g.dz, g.dvz), p[5]);
+}
+
+// ============================================================ tile kernel
+template <int TJ>
+struct __align__(16) JStage {
+  double x[TJ];
+  double y[TJ];
+  double z[TJ];
+  float4 vm[TJ];
+};
+
+template <int TJ>
+__device__ __forceinline__ void issue_tile(JStage<TJ> *st, uint64_t *bar, const JSet &js, int jt0,
+                                           int j1) {
+  const int cnt = min(TJ, j1 - jt0);
+  const uint32_t cc = (uint32_t)((cnt + 1) & ~1);  // even count: 16-byte multiples
+  const uint32_t b8 = cc * 8u, b16 = cc * 16u;
+  mbar_arrive_expect_tx(bar, 3u * b8 + b16);
+  bulk_g2s(st->x, js.px + jt0, b8, bar);
+  bulk_g2s(st->y, js.py + jt0, b8, bar);
+  bulk_g2s(st->z, js.pz + jt0, b8, bar);
+  bulk_g2s(st->vm, js.vm + jt0, b16, bar);
+}
+
+template <int NT, int IPT, int TJ, int NST, bool ANCHOR>
+__global__ void __launch_bounds__(NT) reg_force_tile(JSet js, Work w, int n_iblocks) {
+  constexpr int UNR = 2;                 // j per vote
+  constexpr int TJP = TJ + UNR;          // compute buffer with pad entries
+  constexpr int CW = ANCHOR ? 2 : 3;     // float4 records per j in the compute buffer
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  JStage<TJ> *st = reinterpret_cast<JStage<TJ> *>(smem_raw);
+  float4 *cbuf = reinterpret_cast<float4 *>(smem_raw + NST * sizeof(JStage<TJ>));
+  uint64_t *bar = reinterpret_cast<uint64_t *>(cbuf + 2 * CW * TJP);
+  const int tid = threadIdx.x;
+  const unsigned FULL = 0xffffffffu;
+
+  if (tid == 0) {
+    for (int s = 0; s < NST; ++s) mbar_init(&bar[s], 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+
+  uint32_t g_cons = 0, g_issue = 0;
+  const int n_items = n_iblocks * w.n_chunks;
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const int ch = item % w.n_chunks;
+    const int ib = item / w.n_chunks;
+    const int j0 = ch * w.chunk_len;
+    const int j1 = min(js.n, j0 + w.chunk_len);
+    const int ntile = (j1 - j0 + TJ - 1) / TJ;
+
+    if (tid == 0) {
+      const int pro = min(NST, ntile);
+      for (int p = 0; p < pro; ++p, ++g_issue)
+        issue_tile<TJ>(&st[g_issue % NST], &bar[g_issue % NST], js, j0 + p * TJ, j1);
+    }
+
+    // ---- i-particles of this block into registers
+    const int base = ib * NT * IPT;
+    double ax = 0.0, ay = 0.0, az = 0.0;
+    if (ANCHOR) {
+      const int t0 = w.order_t[base];
+      ax = js.px[t0];
+      ay = js.py[t0];
+      az = js.pz[t0];
+    }
+    float xi[IPT], yi[IPT], zi[IPT], xl[IPT], yl[IPT], zl[IPT], vxi[IPT], vyi[IPT], vzi[IPT];
+    float r2g[IPT];
+    int ti[IPT], row[IPT], nbc[IPT];
+    float ks[IPT][6], kc[IPT][6];
+#pragma unroll
+    for (int k = 0; k < IPT; ++k) {
+      const int s = base + k * NT + tid;
+      const bool valid = s < w.m;
+      const int si = valid ? s : base;
+      ti[k] = w.order_t[si];
+      row[k] = valid ? w.order_o[si] : -1;
+      const double X = js.px[ti[k]], Y = js.py[ti[k]], Z = js.pz[ti[k]];
+      double spread = 0.0;
+      if (ANCHOR) {
+        xi[k] = (float)(X - ax);
+        yi[k] = (float)(Y - ay);
+        zi[k] = (float)(Z - az);
+        xl[k] = yl[k] = zl[k] = 0.0f;
+        spread = fmax(fabs(X - ax), fmax(fabs(Y - ay), fabs(Z - az)));
+      } else {
+        xi[k] = (float)X;
+        yi[k] = (float)Y;
+        zi[k] = (float)Z;
+        xl[k] = (float)(X - (double)xi[k]);
+        yl[k] = (float)(Y - (double)yi[k]);
+        zl[k] = (float)(Z - (double)zi[k]);
+      }
+      const float4 vmi = js.vm[ti[k]];
+      vxi[k] = vmi.x;
+      vyi[k] = vmi.y;
+      vzi[k] = vmi.z;
+      // Candidate threshold: every FP64 neighbour (r2 < R2) passes the FP32
+      // test r2f < r2g.  FP32 offsets err by at most ~2^-23 (|d| + 2 spread)
+      // per component; the margin below covers that many times over.
+      const double R2 = js.r2nb[ti[k]];
+      const double R = sqrt(fmax(R2, 0.0));
+      const double Rg = R * (1.0 + 0x1p-17) + 0x1p-19 * spread + 1e-30;
+      float g = __double2float_ru(Rg * Rg + w.eps2);
+      g = fmaxf(g, nextafterf(w.eps2f, FLT_MAX));  // the self pair (r2 = eps2) is always a candidate
+      r2g[k] = valid ? g : -1.0f;
+      nbc[k] = 0;
+#pragma unroll
+      for (int c = 0; c < 6; ++c) ks[k][c] = kc[k][c] = 0.0f;
+    }
+
+    // ---- stream the chunk's j-tiles
+    for (int t = 0; t < ntile; ++t, ++g_cons) {
+      const int stg = g_cons % NST;
+      const bool ok = mbar_wait(&bar[stg], (g_cons / NST) & 1u);
+      const int jt0 = j0 + t * TJ;
+      const int cnt = min(TJ, j1 - jt0);
+      float4 *cb = cbuf + (g_cons & 1u) * CW * TJP;
+      for (int jj = tid; jj < TJP; jj += NT) {
+        if (jj < cnt && ok) {
+          const double X = st[stg].x[jj], Y = st[stg].y[jj], Z = st[stg].z[jj];
+          const float4 vmj = st[stg].vm[jj];
+          if (ANCHOR) {
+            cb[jj] = make_float4((float)(X - ax), (float)(Y - ay), (float)(Z - az), vmj.w);
+            cb[TJP + jj] = make_float4(vmj.x, vmj.y, vmj.z, 0.0f);
+          } else {
+            const float hx = (float)X, hy = (float)Y, hz = (float)Z;
+            cb[jj] = make_float4(hx, hy, hz, vmj.w);
+            cb[TJP + jj] = make_float4((float)(X - (double)hx), (float)(Y - (double)hy),
+                                       (float)(Z - (double)hz), 0.0f);
+            cb[2 * TJP + jj] = make_float4(vmj.x, vmj.y, vmj.z, 0.0f);
+          }
+        } else {
+          // pad entry: massless and far away (never a candidate, contributes 0)
+          cb[jj] = make_float4(1e30f, 1e30f, 1e30f, 0.0f);
+          cb[TJP + jj] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+          if (!ANCHOR) cb[2 * TJP + jj] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
+      }
+      if (!__syncthreads_and(ok)) {
+        if (tid == 0) {
+          atomicOr(w.status, kErrTimeout);
+          // let the copies already in flight land before the CTA leaves
+          for (uint32_t g = g_cons; g < g_issue; ++g) (void)mbar_wait(&bar[g % NST], (g / NST) & 1u);
+        }
+        __syncthreads();
+        return;
+      }
+      if (tid == 0 && t + NST < ntile) {
+        issue_tile<TJ>(&st[g_issue % NST], &bar[g_issue % NST], js, j0 + (t + NST) * TJ, j1);
+        ++g_issue;
+      }
+
+      float p[IPT][6];
+#pragma unroll
+      for (int k = 0; k < IPT; ++k)
+#pragma unroll
+        for (int c = 0; c < 6; ++c) p[k][c] = 0.0f;
+
+      for (int jj = 0; jj < cnt; jj += UNR) {
+        bool any = false;
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+          const float4 P = cb[jj + u];
+          const float4 L = ANCHOR ? make_float4(0.f, 0.f, 0.f, 0.f) : cb[TJP + jj + u];
+          const float4 V = cb[(ANCHOR ? 1 : 2) * TJP + jj + u];
+#pragma unroll
+          for (int k = 0; k < IPT; ++k) {
+            const PairGeom g =
+                ANCHOR ? pair_geom(P.x, P.y, P.z, V.x, V.y, V.z, xi[k], yi[k], zi[k], vxi[k], vyi[k],
+                                   vzi[k], w.eps2f)
+                       : pair_geom_ds(P.x, P.y, P.z, L.x, L.y, L.z, V.x, V.y, V.z, xi[k], yi[k],
+                                      zi[k], xl[k], yl[k], zl[k], vxi[k], vyi[k], vzi[k], w.eps2f);
+            const bool cand = g.r2 < r2g[k];
+            float rinv = rsqrtf(g.r2);
+            rinv = cand ? 0.0f : rinv;
+            any |= cand;
+            pair_accum(g, P.w, rinv, p[k]);
+          }
+        }
+        if (__any_sync(FULL, any)) {
+          // Slow path: candidates are re-decided with the FP64 test.
+#pragma unroll
+          for (int u = 0; u < UNR; ++u) {
+            const int jl = jj + u;
+            if (jl >= cnt) continue;
+            const int jg = jt0 + jl;
+            const float4 P = cb[jl];
+            const float4 L = ANCHOR ? make_float4(0.f, 0.f, 0.f, 0.f) : cb[TJP + jl];
+            const float4 V = cb[(ANCHOR ? 1 : 2) * TJP + jl];
+#pragma unroll
+            for (int k = 0; k < IPT; ++k) {
+              const PairGeom g =
+                  ANCHOR ? pair_geom(P.x, P.y, P.z, V.x, V.y, V.z, xi[k], yi[k], zi[k], vxi[k],
+                                     vyi[k], vzi[k], w.eps2f)
+                         : pair_geom_ds(P.x, P.y, P.z, L.x, L.y, L.z, V.x, V.y, V.z, xi[k], yi[k],
+                                        zi[k], xl[k], yl[k], zl[k], vxi[k], vyi[k], vzi[k],
+                                        w.eps2f);
+              if (!(g.r2 < r2g[k]) || jg == ti[k]) continue;
+              const double r2e = exact_r2(js.px[ti[k]], js.py[ti[k]], js.pz[ti[k]], js.px[jg],
+                                          js.py[jg], js.pz[jg]);
+              if (r2e < js.r2nb[ti[k]]) {
+                if (nbc[k] < w.cap)
+                  w.lst[((size_t)ch * w.m + row[k]) * w.cap + nbc[k]] = jg;
+                ++nbc[k];
+              } else {
+                pair_accum(g, P.w, rsqrtf(g.r2), p[k]);
+              }
+            }
+          }
+        }
+      }
+      // Kahan fold of the tile partials
+#pragma unroll
+      for (int k = 0; k < IPT; ++k)
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+          const float y = __fsub_rn(p[k][c], kc[k][c]);
+          const float tt = __fadd_rn(ks[k][c], y);
+          kc[k][c] = __fsub_rn(__fsub_rn(tt, ks[k][c]), y);
+          ks[k][c] = tt;
+        }
+    }
+
+#pragma unroll
+    for (int k = 0; k < IPT; ++k) {
+      if (row[k] < 0) continue;
+      double *dst = w.part + ((size_t)ch * w.m + row[k]) * 6;
+      float4 unused;
+      (void)unused;
+#pragma unroll
+      for (int c = 0; c < 6; ++c) dst[c] = (double)ks[k][c] - (double)kc[k][c];
+      w.cnt[(size_t)ch * w.m + row[k]] = nbc[k];
+    }
+  }
+}
+
+// ============================================================ j-major kernel
+// One warp per j-chunk of L consecutive particles; lanes take j = j0 + lane +
+// 32 k; the MI targets of a group are held by every lane.  The neighbour test is
+// the exact FP64 one; __ballot_sync + __popc give each neighbour its slot in
+// ascending-j order.
+template <int MI>
+__global__ void __launch_bounds__(128) reg_force_jmajor(JSet js, Work w, int L) {
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (c >= w.n_chunks) return;
+  const int j0 = c * L;
+  const int j1 = min(js.n, j0 + L);
+  const unsigned lt_mask = (1u << lane) - 1u;
+  for (int ig = 0; ig < w.m; ig += MI) {
+    double xi[MI], yi[MI], zi[MI], R2[MI];
+    float vxi[MI], vyi[MI], vzi[MI];
+    int ti[MI], row[MI], nbc[MI];
+    float p[MI][6];
+#pragma unroll
+    for (int k = 0; k < MI; ++k) {
+      const bool valid = ig + k < w.m;
+      const int s = valid ? ig + k : ig;
+      ti[k] = w.order_t[s];
+      row[k] = valid ? w.order_o[s] : -1;
+      xi[k] = js.px[ti[k]];
+      yi[k] = js.py[ti[k]];
+      zi[k] = js.pz[ti[k]];
+      R2[k] = js.r2nb[ti[k]];
+      const float4 vmi = js.vm[ti[k]];
+      vxi[k] = vmi.x;
+      vyi[k] = vmi.y;
+      vzi[k] = vmi.z;
+      nbc[k] = 0;
+#pragma unroll
+      for (int q = 0; q < 6; ++q) p[k][q] = 0.0f;
+    }
+    for (int jb = j0; jb < j1; jb += 32) {
+      const int j = jb + lane;
+      const bool inr = j < j1;
+      double X = 0.0, Y = 0.0, Z = 0.0;
+      float4 V = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (inr) {
+        X = js.px[j];
+        Y = js.py[j];
+        Z = js.pz[j];
+        V = js.vm[j];
+      }
+#pragma unroll
+      for (int k = 0; k < MI; ++k) {
+        if (row[k] < 0) continue;  // uniform across the warp
+        const double dxd = __dsub_rn(X, xi[k]), dyd = __dsub_rn(Y, yi[k]), dzd = __dsub_rn(Z, zi[k]);
+        double r2e = __dmul_rn(dxd, dxd);
+        r2e = __dadd_rn(r2e, __dmul_rn(dyd, dyd));
+        r2e = __dadd_rn(r2e, __dmul_rn(dzd, dzd));
+        const bool self = (j == ti[k]);
+        const bool isnb = inr && !self && (r2e < R2[k]);
+        const bool isreg = inr && !self && !isnb;
+        PairGeom g;
+        g.dx = (float)dxd;
+        g.dy = (float)dyd;
+        g.dz = (float)dzd;
+        g.dvx = V.x - vxi[k];
+        g.dvy = V.y - vyi[k];
+        g.dvz = V.z - vzi[k];
+        g.r2 = (float)__dadd_rn(r2e, w.eps2);
+        g.rv = fmaf(g.dx, g.dvx, fmaf(g.dy, g.dvy, g.dz * g.dvz));
+        const float rinv = isreg ? rsqrtf(g.r2) : 0.0f;
+        pair_accum(g, V.w, rinv, p[k]);
+        const unsigned mask = __ballot_sync(FULL, isnb);
+        if (mask) {
+          if (isnb) {
+            const int idx = nbc[k] + __popc(mask & lt_mask);
+            if (idx < w.cap) w.lst[((size_t)c * w.m + row[k]) * w.cap + idx] = j;
+          }
+          nbc[k] += __popc(mask);
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < MI; ++k) {
+      if (row[k] < 0) continue;
+      double s[6];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) {
+        s[q] = (double)p[k][q];
+        for (int o = 16; o > 0; o >>= 1) s[q] += __shfl_xor_sync(FULL, s[q], o);
+      }
+      if (lane == 0) {
+        double *dst = w.part + ((size_t)c * w.m + row[k]) * 6;
+#pragma unroll
+        for (int q = 0; q < 6; ++q) dst[q] = s[q];
+        w.cnt[(size_t)c * w.m + row[k]] = nbc[k];
+      }
+    }
+  }
+}
+
+// ============================================================ finalize
+// One warp per output row.  Regular part: FP64 sum of the chunk partials in a
+// fixed lane/tree order.  List: chunk counts prefix-summed in chunk order, so
+// the concatenation is in ascending j.  Irregular part: the reference's FP64
+// formula (ComputeAcceleration.cpp:285-292, softened as for the regular part)
+// over the final list, lane-strided with a fixed reduction tree.
+__global__ void finalize_rows(JSet js, Work w, Outputs o) {
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < w.m; r += nwarps) {
+    double s[6] = {0, 0, 0, 0, 0, 0};
+    for (int c = lane; c < w.n_chunks; c += 32) {
+      const double *src = w.part + ((size_t)c * w.m + r) * 6;
+#pragma unroll
+      for (int q = 0; q < 6; ++q) s[q] += src[q];
+    }
+#pragma unroll
+    for (int q = 0; q < 6; ++q)
+      for (int off = 16; off > 0; off >>= 1) s[q] += __shfl_xor_sync(FULL, s[q], off);
+
+    int total = 0;
+    int *out = o.list + (size_t)r * w.cap;
+    for (int cb = 0; cb < w.n_chunks; cb += 32) {
+      const int c = cb + lane;
+      const int cc = c < w.n_chunks ? w.cnt[(size_t)c * w.m + r] : 0;
+      int incl = cc;
+      for (int off = 1; off < 32; off <<= 1) {
+        const int v = __shfl_up_sync(FULL, incl, off);
+        if (lane >= off) incl += v;
+      }
+      const int start = total + incl - cc;
+      const int stored = min(cc, w.cap);
+      const int *src = w.lst + ((size_t)c * w.m + r) * w.cap;
+      for (int k = 0; k < stored && start + k < w.cap; ++k) out[start + k] = src[k];
+      total += __shfl_sync(FULL, incl, 31);
+    }
+    __syncwarp();
+
+    const int t = o.targets[r];
+    const double xi = js.px[t], yi = js.py[t], zi = js.pz[t];
+    const double vxi = js.pvx[t], vyi = js.pvy[t], vzi = js.pvz[t];
+    double a[6] = {0, 0, 0, 0, 0, 0};
+    const int nl = min(total, w.cap);
+    for (int k = lane; k < nl; k += 32) {
+      const int j = out[k];
+      const double x[3] = {__dsub_rn(js.px[j], xi), __dsub_rn(js.py[j], yi), __dsub_rn(js.pz[j], zi)};
+      const double v[3] = {__dsub_rn(js.pvx[j], vxi), __dsub_rn(js.pvy[j], vyi),
+                           __dsub_rn(js.pvz[j], vzi)};
+      double r2 = 0.0, vx = 0.0;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        r2 = __dadd_rn(r2, __dmul_rn(x[d], x[d]));
+        vx = __dadd_rn(vx, __dmul_rn(v[d], x[d]));
+      }
+      const double r2s = __dadd_rn(r2, w.eps2);
+      const double m_r3 = __ddiv_rn(__ddiv_rn(js.mass[j], r2s), __dsqrt_rn(r2s));
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        a[d] = __dadd_rn(a[d], __dmul_rn(m_r3, x[d]));
+        const double corr = __ddiv_rn(__dmul_rn(__dmul_rn(3.0, x[d]), vx), r2s);
+        a[3 + d] = __dadd_rn(a[3 + d], __dmul_rn(m_r3, __dsub_rn(v[d], corr)));
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 6; ++q)
+      for (int off = 16; off > 0; off >>= 1) a[q] += __shfl_xor_sync(FULL, a[q], off);
+
+    if (lane == 0) {
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        o.acc_reg[3 * r + d] = s[d];
+        o.jerk_reg[3 * r + d] = s[3 + d];
+        o.acc_irr[3 * r + d] = a[d];
+        o.jerk_irr[3 * r + d] = a[3 + d];
+      }
+      o.nnb[r] = total;
+      if (total > w.cap) {
+        atomicAdd(o.overflow_rows, 1);
+        atomicOr(w.status, kErrOverflow);
+      }
+    }
+  }
+}
+
+// ============================================================ energy
+// FP64 kinetic + softened potential energy; one block of 256 threads per i-tile
+// of 256, j looped; per-i potentials written for a deterministic host sum.
+__global__ void energy_rows(int n, const double *__restrict__ x, const double *__restrict__ v,
+                            const double *__restrict__ mass, double eps2,
+                            double *__restrict__ e_row) {
+  __shared__ double sx[256], sy[256], sz[256], sm[256];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double xi = 0, yi = 0, zi = 0;
+  if (i < n) {
+    xi = x[3 * i];
+    yi = x[3 * i + 1];
+    zi = x[3 * i + 2];
+  }
+  double w = 0.0;
+  for (int jt = 0; jt < n; jt += 256) {
+    const int j = jt + threadIdx.x;
+    __syncthreads();
+    if (j < n) {
+      sx[threadIdx.x] = x[3 * j];
+      sy[threadIdx.x] = x[3 * j + 1];
+      sz[threadIdx.x] = x[3 * j + 2];
+      sm[threadIdx.x] = mass[j];
+    } else {
+      sx[threadIdx.x] = sy[threadIdx.x] = sz[threadIdx.x] = 0.0;
+      sm[threadIdx.x] = 0.0;
+    }
+    __syncthreads();
+    const int lim = min(256, n - jt);
+    for (int jj = 0; jj < lim; ++jj) {
+      if (jt + jj == i) continue;
+      const double dx = sx[jj] - xi, dy = sy[jj] - yi, dz = sz[jj] - zi;
+      const double r2 = dx * dx + dy * dy + dz * dz + eps2;
+      w += sm[jj] * rsqrt(r2);
+    }
+  }
+  if (i < n) {
+    const double v2 = v[3 * i] * v[3 * i] + v[3 * i + 1] * v[3 * i + 1] + v[3 * i + 2] * v[3 * i + 2];
+    e_row[i] = 0.5 * mass[i] * v2 - 0.5 * mass[i] * w;
+  }
+}
+
+// ============================================================ launch wrappers
+void launch_predict(cudaStream_t s, int n, const double *x, const double *v, const double *a0,
+                    const double *a1, const double *t0, const double *mass, double new_time,
+                    double time_scale, double *px, double *py, double *pz, double *pvx,
+                    double *pvy, double *pvz, float4 *vm, int sm_count) {
+  const int blocks = min((n + 255) / 256, sm_count * 8);
+  predict_jset<<<max(blocks, 1), 256, 0, s>>>(n, x, v, a0, a1, t0, mass, new_time, time_scale, px, py,
+                                               pz, pvx, pvy, pvz, vm);
+}
+
+void launch_pack_vm(cudaStream_t s, int n, const double *pvx, const double *pvy, const double *pvz,
+                    const double *mass, float4 *vm, int sm_count) {
+  const int blocks = min((n + 255) / 256, sm_count * 8);
+  pack_vm<<<max(blocks, 1), 256, 0, s>>>(n, pvx, pvy, pvz, mass, vm);
+}
+
+void launch_unpack_predicted(cudaStream_t s, int n, const double *pos, const double *vel,
+                             const double *mass, double *px, double *py, double *pz, double *pvx,
+                             double *pvy, double *pvz, float4 *vm, int sm_count) {
+  const int blocks = min((n + 255) / 256, sm_count * 8);
+  unpack_predicted<<<max(blocks, 1), 256, 0, s>>>(n, pos, vel, mass, px, py, pz, pvx, pvy, pvz, vm);
+}
+
+void launch_iota(cudaStream_t s, int m, int *out, int sm_count) {
+  iota_kernel<<<max(1, min((m + 255) / 256, sm_count * 8)), 256, 0, s>>>(m, out);
+}
+
+size_t morton_temp_bytes(int m_cap) {
+  size_t bytes = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const uint32_t *)nullptr, (uint32_t *)nullptr,
+                                  (const int *)nullptr, (int *)nullptr, m_cap, 0, 30);
+  return bytes;
+}
+
+void launch_morton_order(cudaStream_t s, int m, const int *targets, const JSet &js, int *bbox,
+                         uint32_t *keys, uint32_t *keys_alt, int *rows, int *rows_alt,
+                         void *cub_tmp, size_t cub_bytes, int *order_t, int *order_o,
+                         int sm_count) {
+  const int init[6] = {INT_MAX, INT_MAX, INT_MAX, INT_MIN, INT_MIN, INT_MIN};
+  cudaMemcpyAsync(bbox, init, sizeof(init), cudaMemcpyHostToDevice, s);
+  const int blocks = max(1, min((m + 255) / 256, sm_count * 4));
+  target_bbox<<<blocks, 256, 0, s>>>(m, targets, js.px, js.py, js.pz, bbox);
+  target_morton<<<blocks, 256, 0, s>>>(m, targets, js.px, js.py, js.pz, bbox, keys, rows);
+  size_t bytes = cub_bytes;
+  cub::DeviceRadixSort::SortPairs(cub_tmp, bytes, keys, keys_alt, rows, rows_alt, m, 0, 30, s);
+  gather_order<<<blocks, 256, 0, s>>>(m, targets, rows_alt, order_t, order_o);
+}
+
+template <int NT, int IPT, int TJ, int NST, bool ANCHOR>
+static size_t tile_smem() {
+  constexpr int CW = ANCHOR ? 2 : 3;
+  return NST * sizeof(JStage<TJ>) + 2 * CW * (TJ + 2) * sizeof(float4) + NST * sizeof(uint64_t);
+}
+
+template <int NT, int IPT, bool ANCHOR>
+static int tile_occupancy_impl() {
+  constexpr int TJ = 128, NST = 3;
+  auto k = reg_force_tile<NT, IPT, TJ, NST, ANCHOR>;
+  const size_t sm = tile_smem<NT, IPT, TJ, NST, ANCHOR>();
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  int blocks = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k, NT, sm);
+  return blocks;
+}
+
+template <int NT, int IPT, bool ANCHOR>
+static void tile_launch_impl(cudaStream_t s, int grid, const JSet &js, const Work &w, int n_iblocks) {
+  constexpr int TJ = 128, NST = 3;
+  auto k = reg_force_tile<NT, IPT, TJ, NST, ANCHOR>;
+  const size_t sm = tile_smem<NT, IPT, TJ, NST, ANCHOR>();
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  k<<<grid, NT, sm, s>>>(js, w, n_iblocks);
+}
+
+#define ABYSS_TILE_SWITCH(NT_, IPT_, ANCHOR_, CALL)                        \
+  do {                                                                     \
+    if (ANCHOR_) {                                                         \
+      if (NT_ == 128 && IPT_ == 1) CALL(128, 1, true);                     \
+      else if (NT_ == 128 && IPT_ == 2) CALL(128, 2, true);                \
+      else if (NT_ == 128 && IPT_ == 4) CALL(128, 4, true);                \
+      else if (NT_ == 256 && IPT_ == 2) CALL(256, 2, true);                \
+      else return -1;                                                      \
+    } else {                                                               \
+      if (NT_ == 128 && IPT_ == 1) CALL(128, 1, false);                    \
+      else if (NT_ == 128 && IPT_ == 2) CALL(128, 2, false);               \
+      else if (NT_ == 128 && IPT_ == 4) CALL(128, 4, false);               \
+      else if (NT_ == 256 && IPT_ == 2) CALL(256, 2, false);               \
+      else return -1;                                                      \
+    }                                                                      \
+  } while (0)
+
+int tile_occupancy(int nt, int ipt, bool anchor) {
+  int r = 0;
+#define OCC_CALL(a, b, c) r = tile_occupancy_impl<a, b, c>()
+  ABYSS_TILE_SWITCH(nt, ipt, anchor, OCC_CALL);
+#undef OCC_CALL
+  return r;
+}
+
+int launch_tile(cudaStream_t s, int nt, int ipt, bool anchor, int grid, const JSet &js,
+                const Work &w, int n_iblocks) {
+#define LAUNCH_CALL(a, b, c) tile_launch_impl<a, b, c>(s, grid, js, w, n_iblocks)
+  ABYSS_TILE_SWITCH(nt, ipt, anchor, LAUNCH_CALL);
+#undef LAUNCH_CALL
+  return 0;
+}
+
+int launch_jmajor(cudaStream_t s, int mi, const JSet &js, const Work &w, int L) {
+  const int warps = w.n_chunks;
+  const int blocks = (warps * 32 + 127) / 128;
+  switch (mi) {
+    case 1: reg_force_jmajor<1><<<blocks, 128, 0, s>>>(js, w, L); break;
+    case 2: reg_force_jmajor<2><<<blocks, 128, 0, s>>>(js, w, L); break;
+    case 4: reg_force_jmajor<4><<<blocks, 128, 0, s>>>(js, w, L); break;
+    case 8: reg_force_jmajor<8><<<blocks, 128, 0, s>>>(js, w, L); break;
+    default: return -1;
+  }
+  return 0;
+}
+
+void launch_finalize(cudaStream_t s, const JSet &js, const Work &w, const Outputs &o, int sm_count) {
+  const int warps = w.m;
+  const int blocks = max(1, min((warps * 32 + 255) / 256, sm_count * 16));
+  finalize_rows<<<blocks, 256, 0, s>>>(js, w, o);
+}
+
+void launch_energy(cudaStream_t s, int n, const double *x, const double *v, const double *mass,
+                   double eps2, double *e_row) {
+  energy_rows<<<(n + 255) / 256, 256, 0, s>>>(n, x, v, mass, eps2, e_row);
+}
+
+}  // namespace abyss

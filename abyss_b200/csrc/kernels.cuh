@@ -1,0 +1,33 @@
+// Host-side launch wrappers of the kernels in kernels.cu.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "abyss_internal.cuh"
+
+namespace abyss {
+
+void launch_predict(cudaStream_t s, int n, const double *x, const double *v, const double *a0,
+                    const double *a1, const double *t0, const double *mass, double new_time,
+                    double time_scale, double *px, double *py, double *pz, double *pvx,
+                    double *pvy, double *pvz, float4 *vm, int sm_count);
+void launch_pack_vm(cudaStream_t s, int n, const double *pvx, const double *pvy, const double *pvz,
+                    const double *mass, float4 *vm, int sm_count);
+void launch_unpack_predicted(cudaStream_t s, int n, const double *pos, const double *vel,
+                             const double *mass, double *px, double *py, double *pz, double *pvx,
+                             double *pvy, double *pvz, float4 *vm, int sm_count);
+void launch_iota(cudaStream_t s, int m, int *out, int sm_count);
+size_t morton_temp_bytes(int m_cap);
+void launch_morton_order(cudaStream_t s, int m, const int *targets, const JSet &js, int *bbox,
+                         uint32_t *keys, uint32_t *keys_alt, int *rows, int *rows_alt,
+                         void *cub_tmp, size_t cub_bytes, int *order_t, int *order_o, int sm_count);
+int tile_occupancy(int nt, int ipt, bool anchor);
+int launch_tile(cudaStream_t s, int nt, int ipt, bool anchor, int grid, const JSet &js,
+                const Work &w, int n_iblocks);
+int launch_jmajor(cudaStream_t s, int mi, const JSet &js, const Work &w, int L);
+void launch_finalize(cudaStream_t s, const JSet &js, const Work &w, const Outputs &o, int sm_count);
+void launch_energy(cudaStream_t s, int n, const double *x, const double *v, const double *mass,
+                   double eps2, double *e_row);
+
+}  // namespace abyss

@@ -1,0 +1,123 @@
+/* abyss_reg.h -- C ABI of the B200 Ahmad-Cohen regular-force library
+ * (libabyss_reg.so).  Plain pointers and sizes only.
+ *
+ * Two layers:
+ *   1. The reference-compatible drop-in (abyss_reg_compat.h): the six
+ *      entry points of src_mpi/cuda/cuda_functions.h:3-10.
+ *   2. This status-returning context API, used by the drop-in, the host
+ *      integrator, the batched ensemble and the serving loop.
+ *
+ * Conventions
+ *   - Every function returns ABYSS_OK (0) or a negative ABYSS_ERR_* code;
+ *     abyss_last_error() gives a message.  Nothing traps the GPU: a list
+ *     longer than its capacity is reported (ABYSS_WARN_OVERFLOW, exact
+ *     counts, truncated lists), never asserted.
+ *   - Vectors are row-major double [k][3]; lists are int [m][list_cap],
+ *     ascending particle index, row r holding target r's neighbours.
+ *   - A "j-set" is the n particles of one cluster; "targets" are the m
+ *     active particle indices of a regular block (0 <= target < n).
+ *   - Neighbour rule (src_mpi/Particle/ComputeAcceleration.cpp:285): j != i is
+ *     a neighbour of target i when |x_j - x_i|^2 < r2nb[i] in FP64; its force
+ *     goes to the irregular part, every other j's to the regular part.
+ *     Softening eps2 enters the force terms only.
+ *   - One context per host thread at a time; calls on one context are
+ *     ordered on the context's CUDA stream.
+ */
+#ifndef ABYSS_REG_H
+#define ABYSS_REG_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ABYSS_OK 0
+#define ABYSS_WARN_OVERFLOW 1   /* some target had more neighbours than list_cap */
+#define ABYSS_ERR_ARG (-1)      /* bad argument (size, index, pointer) */
+#define ABYSS_ERR_CUDA (-2)     /* CUDA runtime error */
+#define ABYSS_ERR_OOM (-3)      /* device or pinned allocation failed */
+#define ABYSS_ERR_TIMEOUT (-4)  /* a bounded device wait ran out */
+#define ABYSS_ERR_STATE (-5)    /* call out of order (e.g. no j-set uploaded) */
+#define ABYSS_ERR_NODEVICE (-6) /* no usable CUDA device */
+
+typedef struct abyss_ctx abyss_ctx;
+
+/* Launch shape.  Zero fields are chosen by the library (or by a tuning table
+ * installed with abyss_set_tuning_table). */
+typedef struct abyss_tuning {
+  int kernel;  /* 1 = tile kernel (i in registers, j-tiles by TMA), 2 = j-major kernel */
+  int mode;    /* tile kernel: 1 = anchor offsets on spatially ordered targets, 2 = double-single */
+  int threads; /* tile kernel: 128 or 256 */
+  int ipt;     /* tile: targets per thread 1, 2, 4;  j-major: targets per pass 1, 2, 4, 8 */
+  int j_split; /* j-chunks per target (0 = auto) */
+  int grid;    /* tile kernel persistent grid size (0 = auto) */
+} abyss_tuning;
+
+/* Replaces the reference's _InitializeDevice/_OpenDevice state
+ * (src_mpi/cuda/cuda_my_acceleration.cu:782-882, 886-903) with an explicit
+ * context on `device`. */
+int abyss_create(int device, abyss_ctx **out);
+/* Frees every device and pinned buffer (the reference's CloseDevice frees
+ * nothing, cuda_my_acceleration.cu:905-947). */
+int abyss_destroy(abyss_ctx *ctx);
+const char *abyss_last_error(const abyss_ctx *ctx);
+/* Opaque cudaStream_t of the context (all work of the context runs on it). */
+void *abyss_stream(abyss_ctx *ctx);
+int abyss_synchronize(abyss_ctx *ctx);
+
+/* Pre-size buffers for n particles, m targets, list capacity list_cap
+ * (replaces the grow-on-demand reallocation at cuda_my_acceleration.cu:635-727). */
+int abyss_reserve(abyss_ctx *ctx, int n, int m, int list_cap);
+
+/* Upload un-predicted FP64 state (host arrays); prediction then runs on the
+ * device.  x, v, a0 (= a_tot[.][0]), a1 (= a_tot[.][1]) are [n][3]; t0 is the
+ * time each particle was last advanced to (CurrentTimeReg when it has no
+ * neighbours, else CurrentTimeIrr: CalculateRegularAcceleration.cpp:371-374). */
+int abyss_upload_state(abyss_ctx *ctx, int n, const double *x, const double *v,
+                       const double *a0, const double *a1, const double *t0,
+                       const double *mass, const double *r2nb);
+/* Second-order prediction of the whole j-set to new_time on the device
+ * (UpdateParticle.cpp:37-59): dt = (new_time - t0) * time_scale. */
+int abyss_predict(abyss_ctx *ctx, double new_time, double time_scale);
+/* Upload an already predicted j-set (positions/velocities [n][3]). */
+int abyss_upload_predicted(abyss_ctx *ctx, int n, const double *px, const double *pv,
+                           const double *mass, const double *r2nb);
+
+/* Copy the predicted j-set back: px, pv [n][3] FP64, vm [n][4] FP32
+ * (vx, vy, vz, m) as the force kernels read it; any pointer may be NULL. */
+int abyss_read_predicted(abyss_ctx *ctx, double *px, double *pv, float *vm);
+
+/* Copy the m target indices to the device. */
+int abyss_set_targets(abyss_ctx *ctx, int m, const int *targets);
+/* Enqueue the regular force of the current targets on the context stream
+ * (asynchronous).  tuning may be NULL. */
+int abyss_launch(abyss_ctx *ctx, double eps2, int list_cap, const abyss_tuning *tuning);
+/* Wait for the last launch and copy its results to host memory; any output
+ * pointer may be NULL.  acc/jerk are [m][3]; nnb [m] holds exact counts; list is
+ * [m][list_cap].  Returns ABYSS_WARN_OVERFLOW (with *overflow_rows set) when a
+ * list was truncated. */
+int abyss_fetch(abyss_ctx *ctx, double *acc_reg, double *jerk_reg, double *acc_irr,
+                double *jerk_irr, int *nnb, int *list, int *overflow_rows);
+/* set_targets + launch + fetch. */
+int abyss_regular_force(abyss_ctx *ctx, int m, const int *targets, double eps2, int list_cap,
+                        const abyss_tuning *tuning, double *acc_reg, double *jerk_reg,
+                        double *acc_irr, double *jerk_irr, int *nnb, int *list,
+                        int *overflow_rows);
+
+/* The shape the last abyss_launch used (after auto selection) and its j-chunk count. */
+int abyss_last_plan(const abyss_ctx *ctx, abyss_tuning *plan, int *n_chunks);
+/* Time each phase of subsequent launches with CUDA events on the context stream. */
+int abyss_set_profiling(abyss_ctx *ctx, int on);
+/* Milliseconds of the last profiled launch: [0] target ordering, [1] force
+ * kernel, [2] finalize.  Synchronizes the stream. */
+int abyss_last_timing(abyss_ctx *ctx, float *ms3);
+/* Auto-selection table from the autotuner: k entries, each (m_max, tuning);
+ * the first entry with m <= m_max wins.  k = 0 restores the built-in rule. */
+int abyss_set_tuning_table(abyss_ctx *ctx, int k, const int *m_max, const abyss_tuning *entries);
+
+/* FP64 total energy (kinetic + softened potential) of n particles. */
+int abyss_energy(abyss_ctx *ctx, int n, const double *x, const double *v, const double *mass,
+                 double eps2, double *energy);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,57 @@
+"""The C-ABI library loads and exports every function that include/*.h declares
+(no compute calls: this runs without a GPU)."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+from abyss_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+INC = os.path.join(ROOT, "include")
+
+
+def declared_functions():
+    names = set()
+    for fn in sorted(os.listdir(INC)):
+        if not fn.endswith(".h"):
+            continue
+        text = open(os.path.join(INC, fn)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        text = re.sub(r"//[^\n]*", "", text)
+        for m in re.finditer(r"^[A-Za-z_][\w \*]*?\b([A-Za-z_]\w*)\s*\([^;{]*\)\s*;", text, flags=re.M):
+            name = m.group(1)
+            if name not in ("if", "while", "for", "return", "sizeof"):
+                names.add(name)
+    return sorted(names)
+
+
+def test_headers_declare_the_reference_abi():
+    names = declared_functions()
+    for ref in ("InitializeDevice", "OpenDevice", "CloseDevice", "ProfileDevice", "SendToDevice",
+                "CalculateAccelerationOnDevice"):
+        assert ref in names
+
+
+@pytest.mark.parametrize("name", declared_functions())
+def test_library_exports_declared_symbol(name):
+    L = C.CDLL(_lib.LIB_PATH)
+    assert hasattr(L, name), f"{name} declared in include/ but not exported"
+
+
+def test_loader_binds_everything():
+    L = _lib.lib()
+    for name in declared_functions():
+        getattr(L, name)
+
+
+def test_context_creation_without_gpu_reports_error():
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    L = _lib.lib()
+    h = C.c_void_p()
+    rc = L.abyss_create(0, C.byref(h))
+    assert rc == _lib.ABYSS_ERR_NODEVICE

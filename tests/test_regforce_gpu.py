@@ -1,0 +1,180 @@
+"""GPU parity of the regular-force path against the CPU oracle, through the C ABI.
+
+Bar (written here, checked below):
+  * neighbour lists and counts: bit-exact against the FP64 oracle
+    (rule r2 < R_nb^2, self excluded, ascending index);
+  * regular acceleration: per-target relative error <= ACC_TOL;
+  * regular jerk: per-target relative error <= JERK_TOL;
+  * irregular part (FP64 on the device): <= 1e-12 relative.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from abyss_b200 import ic
+from abyss_b200.regforce import RegularForce
+from tests.helpers import first_list_mismatch, golden, lists_equal, row_rel_err
+
+pytestmark = pytest.mark.gpu
+
+ACC_TOL = 1e-6
+JERK_TOL = 1e-5
+IRR_TOL = 1e-12
+
+TILE_DS = dict(kernel=1, mode=2)
+TILE_ANCHOR = dict(kernel=1, mode=1)
+JMAJOR = dict(kernel=2)
+SHAPES = [
+    ("tile-ds-128x1", dict(kernel=1, mode=2, threads=128, ipt=1)),
+    ("tile-ds-128x2", dict(kernel=1, mode=2, threads=128, ipt=2)),
+    ("tile-ds-256x2", dict(kernel=1, mode=2, threads=256, ipt=2)),
+    ("tile-anchor-128x1", dict(kernel=1, mode=1, threads=128, ipt=1)),
+    ("tile-anchor-128x4", dict(kernel=1, mode=1, threads=128, ipt=4)),
+    ("jmajor-1", dict(kernel=2, ipt=1)),
+    ("jmajor-8", dict(kernel=2, ipt=8)),
+]
+
+
+@pytest.fixture(scope="module")
+def rf():
+    r = RegularForce(0)
+    yield r
+    r.close()
+
+
+def check(res, ref, tag, acc_tol=ACC_TOL, jerk_tol=JERK_TOL):
+    mm = first_list_mismatch(res.nnb, res.list, ref["nnb"], ref["list"])
+    assert mm is None, f"{tag}: list mismatch at row {mm}"
+    ea = row_rel_err(res.acc_reg, ref["acc_reg"])
+    ej = row_rel_err(res.jerk_reg, ref["jerk_reg"])
+    print(f"{tag}: acc max {ea.max():.2e} med {np.median(ea):.2e}  jerk max {ej.max():.2e} "
+          f"med {np.median(ej):.2e}  plan {res.plan}")
+    assert ea.max() <= acc_tol, f"{tag}: acc error {ea.max():.3e}"
+    assert ej.max() <= jerk_tol, f"{tag}: jerk error {ej.max():.3e}"
+    has = ref["nnb"] > 0
+    if has.any():
+        ei = row_rel_err(res.acc_irr[has], ref["acc_irr"][has])
+        eij = row_rel_err(res.jerk_irr[has], ref["jerk_irr"][has])
+        assert ei.max() <= IRR_TOL and eij.max() <= IRR_TOL, f"{tag}: irregular {ei.max()} {eij.max()}"
+
+
+@pytest.mark.parametrize("name", ["ref_plummer1024_s1.npz", "ref_king2048_s3.npz"])
+@pytest.mark.parametrize("tag,tuning", SHAPES)
+def test_golden_reference_outputs(rf, name, tag, tuning):
+    """The reference's own CPU outputs (golden vectors, eps = 0)."""
+    g = golden(name)
+    rf.send_to_device(g["m"], g["px"], g["pv"], g["r2nb"])
+    res = rf.calculate_acceleration(g["targets"], eps2=0.0, list_cap=512, tuning=tuning)
+    ref = dict(nnb=g["out_nnb"], list=g["out_list"], acc_reg=g["out_a_reg"][:, :, 0],
+               jerk_reg=g["out_a_reg"][:, :, 1], acc_irr=g["out_a_irr"][:, :, 0],
+               jerk_irr=g["out_a_irr"][:, :, 1])
+    check(res, ref, f"{name}/{tag}")
+
+
+@pytest.mark.parametrize("name", ["ref_plummer1024_s1.npz", "ref_king2048_s3.npz"])
+def test_device_predictor_bit_exact(rf, name):
+    g = golden(name)
+    rf.upload_state(g["x"], g["v"], g["a_tot"][:, :, 0], g["a_tot"][:, :, 1], g["t0"], g["m"], g["r2nb"])
+    rf.predict(float(g["new_time"]), float(g["time_scale"]))
+    px, pv, vm = rf.read_predicted()
+    assert np.array_equal(px, g["px"])
+    assert np.array_equal(pv, g["pv"])
+    assert np.array_equal(vm[:, 3], g["m"].astype(np.float32))
+    # and the force through the device-predicted j-set equals the golden output lists
+    res = rf.calculate_acceleration(g["targets"], eps2=0.0, list_cap=512)
+    assert lists_equal(res.nnb, res.list, g["out_nnb"], g["out_list"])
+
+
+@pytest.mark.parametrize("tag,tuning", SHAPES)
+def test_softened_plummer_vs_oracle(rf, tag, tuning):
+    c = ic.plummer(3000, 21, k_nb=40)
+    t = np.sort(np.random.default_rng(1).choice(c.n, 1111, replace=False)).astype(np.int32)
+    rf.send_to_device(c.m, c.x, c.v, c.r2nb)
+    res = rf.calculate_acceleration(t, eps2=1e-8, list_cap=256, tuning=tuning)
+    ref = oracle.reg_force(c.x, c.v, c.m, c.r2nb, 1e-8, t, 256)
+    check(res, ref, f"plummer3000-eps/{tag}")
+
+
+@pytest.mark.parametrize("m", [1, 2, 3, 31, 33, 64, 65, 257, 4095, 4096, 10000])
+def test_active_block_sizes_auto(rf, m):
+    c = ic.king(12000, 3, 6.0, k_nb=60)
+    t = np.sort(np.random.default_rng(m).choice(c.n, m, replace=False)).astype(np.int32)
+    rf.send_to_device(c.m, c.x, c.v, c.r2nb)
+    res = rf.calculate_acceleration(t, eps2=1e-8, list_cap=256)
+    ref = oracle.reg_force(c.x, c.v, c.m, c.r2nb, 1e-8, t, 256)
+    check(res, ref, f"king12000/m={m}")
+
+
+@pytest.mark.parametrize("split", [1, 2, 3, 7, 40])
+def test_forced_j_splits(rf, split):
+    c = ic.plummer(5001, 5, k_nb=50)
+    t = np.arange(0, c.n, 3, dtype=np.int32)
+    rf.send_to_device(c.m, c.x, c.v, c.r2nb)
+    ref = oracle.reg_force(c.x, c.v, c.m, c.r2nb, 0.0, t, 256)
+    for tu in (dict(kernel=1, mode=2, j_split=split), dict(kernel=1, mode=1, j_split=split),
+               dict(kernel=2, ipt=8, j_split=split)):
+        res = rf.calculate_acceleration(t, eps2=0.0, list_cap=256, tuning=tu)
+        check(res, ref, f"split{split}/{tu}")
+
+
+def test_unsorted_and_repeated_targets(rf):
+    c = ic.plummer(2000, 8, k_nb=30)
+    rng = np.random.default_rng(3)
+    t = rng.integers(0, c.n, 900).astype(np.int32)  # unsorted, with repeats
+    rf.send_to_device(c.m, c.x, c.v, c.r2nb)
+    ref = oracle.reg_force(c.x, c.v, c.m, c.r2nb, 0.0, t, 256)
+    for tu in (TILE_DS, TILE_ANCHOR, JMAJOR):
+        res = rf.calculate_acceleration(t, 0.0, 256, tu)
+        check(res, ref, f"unsorted/{tu}")
+
+
+def test_no_neighbours_and_all_neighbours(rf):
+    c = ic.plummer(700, 4, k_nb=10)
+    t = np.arange(c.n, dtype=np.int32)
+    # R_nb = 0: every j is regular
+    r0 = np.zeros(c.n)
+    rf.send_to_device(c.m, c.x, c.v, r0)
+    ref = oracle.reg_force(c.x, c.v, c.m, r0, 1e-8, t, 64)
+    for tu in (TILE_DS, TILE_ANCHOR, JMAJOR):
+        res = rf.calculate_acceleration(t, 1e-8, 64, tu)
+        assert res.nnb.sum() == 0
+        check(res, ref, f"R=0/{tu}")
+    # R_nb huge: every j is a neighbour, lists overflow a small cap with exact counts
+    big = np.full(c.n, 1e6)
+    rf.send_to_device(c.m, c.x, c.v, big)
+    ref = oracle.reg_force(c.x, c.v, c.m, big, 1e-8, t, 100)
+    for tu in (TILE_DS, TILE_ANCHOR, JMAJOR):
+        res = rf.calculate_acceleration(t, 1e-8, 100, tu)
+        assert res.overflow_rows == c.n
+        assert np.all(res.nnb == c.n - 1)
+        assert np.array_equal(res.list, ref["list"])
+        assert np.abs(res.acc_reg).max() == 0.0 and np.abs(res.jerk_reg).max() == 0.0
+
+
+@pytest.mark.parametrize("n", [2, 3, 5, 127, 129, 255, 257])
+def test_tiny_and_ragged_jsets(rf, n):
+    c = ic.plummer(n, 100 + n, k_nb=min(4, n - 1) + 0.5)
+    t = np.arange(n, dtype=np.int32)
+    rf.send_to_device(c.m, c.x, c.v, c.r2nb)
+    ref = oracle.reg_force(c.x, c.v, c.m, c.r2nb, 0.0, t, 32)
+    for tu in (TILE_DS, TILE_ANCHOR, JMAJOR):
+        res = rf.calculate_acceleration(t, 0.0, 32, tu)
+        check(res, ref, f"n={n}/{tu}")
+
+
+def test_bad_arguments_are_reported_not_trapped(rf):
+    from abyss_b200._lib import AbyssError
+
+    c = ic.plummer(100, 1, k_nb=5)
+    rf.send_to_device(c.m, c.x, c.v, c.r2nb)
+    with pytest.raises(AbyssError):
+        rf.calculate_acceleration(np.array([0, 100], np.int32))  # index out of range
+    with pytest.raises(AbyssError):
+        rf.calculate_acceleration(np.array([], np.int32))
+    with pytest.raises(AbyssError):
+        rf.calculate_acceleration(np.array([1], np.int32), eps2=-1.0)
+    with pytest.raises(AbyssError):
+        rf.calculate_acceleration(np.array([1], np.int32), tuning=dict(kernel=1, threads=96))
+    # the context is still usable
+    res = rf.calculate_acceleration(np.array([1, 2], np.int32), list_cap=16)
+    assert res.acc_reg.shape == (2, 3)
