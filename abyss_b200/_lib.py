@@ -37,6 +37,25 @@ class Tuning(C.Structure):
         return {f: int(getattr(self, f)) for f, _ in self._fields_}
 
 
+class ACParams(C.Structure):
+    """abyss_ac_params (include/abyss_ac.h)."""
+
+    _fields_ = [("eps2", C.c_double), ("eta_reg", C.c_double), ("eta_irr", C.c_double),
+                ("fix_nb", C.c_int), ("nb_max", C.c_int), ("t_end", C.c_double), ("threads", C.c_int)]
+
+
+class ACStats(C.Structure):
+    """abyss_ac_stats (include/abyss_ac.h)."""
+
+    _fields_ = [("blocks", C.c_longlong), ("reg_steps", C.c_longlong), ("irr_steps", C.c_longlong),
+                ("irr_levels", C.c_longlong), ("radius_retries", C.c_longlong), ("pairs", C.c_double),
+                ("sec_reg_gpu", C.c_double), ("sec_reg_host", C.c_double), ("sec_irr", C.c_double),
+                ("sec_init", C.c_double)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 _LIB = None
 
 
@@ -88,6 +107,30 @@ def lib():
     L.CalculateAccelerationOnDevice_f64.argtypes = [_ip, _ip, _dp, _dp, _ip, _ip]
     L.abyss_compat_set_list_stride.argtypes = [C.c_int]
     L.abyss_compat_status.argtypes = []
+    # host integrator rules (include/abyss_host.h)
+    L.abyss_host_predict.argtypes = [_dp] * 4 + [C.c_double, C.c_double, _dp, _dp]
+    L.abyss_host_time_step_reg.argtypes = [_dp, C.c_double]
+    L.abyss_host_time_step_reg.restype = C.c_double
+    L.abyss_host_time_step_irr.argtypes = [_dp, _dp, C.c_double]
+    L.abyss_host_time_step_irr.restype = C.c_double
+    L.abyss_host_block_time_step.argtypes = [C.c_double, C.c_double, C.c_int, _ip,
+                                             C.POINTER(C.c_ulonglong), _dp]
+    L.abyss_host_regular_correct.argtypes = ([C.c_int, _dp, _dp, _dp, _dp, _dp, C.c_double, C.c_double,
+                                              C.c_double, C.c_int, C.c_double, _dp, C.c_int, _ip, C.c_int,
+                                              _ip] + [_dp] * 8)
+    # host integrator (include/abyss_ac.h)
+    L.abyss_ac_create.argtypes = [_vp, C.POINTER(ACParams), C.c_int, _dp, _dp, _dp, _dp, C.POINTER(_vp)]
+    L.abyss_ac_destroy.argtypes = [_vp]
+    L.abyss_ac_advance_block.argtypes = [_vp, _ip]
+    L.abyss_ac_run.argtypes = [_vp, C.c_double]
+    L.abyss_ac_time.argtypes = [_vp]
+    L.abyss_ac_time.restype = C.c_double
+    L.abyss_ac_get_state.argtypes = [_vp, _dp, _dp, _ip, _dp]
+    L.abyss_ac_energy.argtypes = [_vp, _dp]
+    L.abyss_ac_get_stats.argtypes = [_vp, C.POINTER(ACStats)]
+    L.abyss_ac_last_regular.argtypes = [_vp, _ip, _ip, _dp, _dp, _dp, _dp, _dp, _ip, _ip, C.c_int]
+    L.abyss_ac_last_error.argtypes = [_vp]
+    L.abyss_ac_last_error.restype = C.c_char_p
     _LIB = L
     return L
 

@@ -1,0 +1,996 @@
+// Host Ahmad-Cohen integrator (include/abyss_ac.h).
+//
+// Single-process restatement of the reference's block-timestep loop with the
+// GPU regular force behind the C ABI:
+//   initialisation  RootRoutines.cpp:104-330 (InitAcc1, InitAcc2, InitTime,
+//                   time-step correction, time_block)
+//   main loop       RootRoutines.cpp:448-1075: next regular block
+//                   (updateNextRegTime, :1310-1338), irregular levels in
+//                   increasing NextBlockIrr (skip list, :488-1005), then the
+//                   regular step (calculateRegAccelerationOnGPU + RegCudaUpdate)
+//   per particle    ComputeAcceleration.cpp:14-190 (irregular),
+//                   :405-661 (regular corrector after the GPU force),
+//                   UpdateParticle.cpp:13-407 (predictor, radius, time steps),
+//                   TimeStepRoutines.cpp:10-115, Initialize.cpp:16-230.
+// Deliberate differences, each for a reason stated at the site:
+//   * softening eps2 in all force terms (the configurations ask for it);
+//   * separate eta for regular and irregular steps;
+//   * the irregular corrector's dt^5 is dt^4 * dt (the reference reads an
+//     uninitialised dt5 at ComputeAcceleration.cpp:162, line 120 commented out);
+//   * two-phase blocks: every particle of a block is computed from the
+//     pre-block state before any is committed (the reference's workers
+//     overwrite a_tot while others still predict from it);
+//   * a target whose list overflows nb_max has its radius shrunk and the
+//     regular call re-run, instead of a device assert.
+#include <algorithm>
+#include <array>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <stdexcept>
+#include <string>
+#include <unordered_set>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "../../../include/abyss_ac.h"
+#include "../../../include/abyss_reg.h"
+
+namespace {
+
+typedef unsigned long long ULL;
+
+double now_s() {
+  using namespace std::chrono;
+  return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+struct Star {
+  double x[3], v[3], m;
+  double a_tot[3][4], a_reg[3][4], a_irr[3][4];
+  std::vector<int> nb;
+  double r2nb;
+  double t_reg = 0, t_irr = 0, dt_reg = 0, dt_irr = 0;
+  ULL cur_reg = 0, cur_irr = 0, new_cur_irr = 0, next_irr = 0, tb_reg = 0, tb_irr = 0;
+  int lv_reg = 0, lv_irr = 0;
+};
+
+// Result of one particle's block computation, committed in phase two.
+struct Pending {
+  double new_x[3], new_v[3];
+  double a_tot[3][4], a_reg[3][4], a_irr[3][4];
+  std::vector<int> new_nb;
+  bool move = false;
+  // irregular step bookkeeping (calculateTimeStepIrr results)
+  int lv_irr = 0;
+  double dt_irr = 0;
+  ULL tb_irr = 0, new_cur_irr = 0;
+};
+
+}  // namespace
+
+struct abyss_ac {
+  abyss_ctx *ctx = nullptr;
+  abyss_ac_params p{};
+  std::vector<Star> s;
+  int n = 0;
+  double scale = 1.0;  // EnzoTimeStep
+  int time_block = -30;
+  ULL block_max = 1ull << 30;
+  double time_step = std::ldexp(1.0, -30);
+  ULL next_reg_block = 0;
+  bool done = false;
+  std::string err;
+  abyss_ac_stats st{};
+  // last regular call
+  std::vector<int> last_targets, last_nnb, last_list;
+  std::vector<double> last_px, last_pv, last_r2, last_acc, last_jerk;
+  int last_cap = 0;
+};
+
+namespace {
+
+// UpdateParticle.cpp:37-59.
+inline void predict(const Star &p, double dt_code, double scale, double pos[3], double vel[3]) {
+  const double dt = dt_code * scale;
+  for (int d = 0; d < 3; ++d) {
+    if (dt == 0) {
+      pos[d] = p.x[d];
+      vel[d] = p.v[d];
+    } else {
+      pos[d] = ((p.a_tot[d][1] * dt / 3 + p.a_tot[d][0]) * dt / 2 + p.v[d]) * dt + p.x[d];
+      vel[d] = (p.a_tot[d][1] * dt / 2 + p.a_tot[d][0]) * dt + p.v[d];
+    }
+  }
+}
+
+// TimeStepRoutines.cpp:10-25 (eta passed in).
+double new_step_reg(const double df[3][4], double eta) {
+  const double F2 = df[0][0] * df[0][0] + df[1][0] * df[1][0] + df[2][0] * df[2][0];
+  const double Fdot2 = df[0][1] * df[0][1] + df[1][1] * df[1][1] + df[2][1] * df[2][1];
+  const double F2dot2 = df[0][2] * df[0][2] + df[1][2] * df[1][2] + df[2][2] * df[2][2];
+  const double F3dot2 = df[0][3] * df[0][3] + df[1][3] * df[1][3] + df[2][3] * df[2][3];
+  double dta = (std::sqrt(F2 * F2dot2) + Fdot2) / (std::sqrt(Fdot2 * F3dot2) + F2dot2);
+  return std::sqrt(eta * dta);
+}
+
+// TimeStepRoutines.cpp:28-63 and :65-100 (same formula).
+double new_step_irr(const double f[3][4], const double df[3][4], double eta) {
+  const double F2 = f[0][0] * f[0][0] + f[1][0] * f[1][0] + f[2][0] * f[2][0];
+  const double Fdot2 = df[0][1] * df[0][1] + df[1][1] * df[1][1] + df[2][1] * df[2][1];
+  const double F2dot2 = df[0][2] * df[0][2] + df[1][2] * df[1][2] + df[2][2] * df[2][2];
+  const double F3dot2 = df[0][3] * df[0][3] + df[1][3] * df[1][3] + df[2][3] * df[2][3];
+  double ts = (std::sqrt(F2 * F2dot2) + Fdot2) / (std::sqrt(Fdot2 * F3dot2) + F2dot2);
+  return std::sqrt(eta * ts);
+}
+
+// TimeStepRoutines.cpp:102-115.
+void block_step(const abyss_ac *ac, double dt, int &level, ULL &block, double &step) {
+  level = static_cast<int>(std::floor(std::log(dt / ac->scale) / std::log(2.0)));
+  if (level < ac->time_block) level = ac->time_block;
+  step = static_cast<double>(std::pow(2, level));
+  block = static_cast<ULL>(std::pow(2, level - ac->time_block));
+}
+
+// UpdateParticle.cpp:151-241 (calculateTimeStepIrr).
+void time_step_irr(const abyss_ac *ac, Star &p) {
+  if (p.nb.empty()) {
+    p.lv_irr = p.lv_reg;
+    p.dt_irr = static_cast<double>(std::pow(2, p.lv_reg));
+    p.tb_irr = static_cast<ULL>(std::pow(2, p.lv_reg - ac->time_block));
+    return;
+  }
+  int lv;
+  ULL tb;
+  double stp;
+  block_step(ac, new_step_irr(p.a_tot, p.a_irr, ac->p.eta_irr), lv, tb, stp);
+  if (lv > p.lv_irr) {
+    if (std::fmod((double)p.new_cur_irr, 2.0 * (double)p.tb_irr) == 0) {
+      lv = p.lv_irr + 1;
+      tb = 2 * p.tb_irr;
+    } else {
+      lv = p.lv_irr;
+      tb = p.tb_irr;
+    }
+  } else if (lv < p.lv_irr) {
+    if (lv < p.lv_irr - 1) {
+      lv = p.lv_irr - 2;
+      tb = p.tb_irr / 4;
+    } else {
+      lv = p.lv_irr - 1;
+      tb = p.tb_irr / 2;
+    }
+  } else {
+    lv = p.lv_irr;
+    tb = p.tb_irr;
+  }
+  const ULL reg_end = p.cur_reg + p.tb_reg;
+  while (((p.new_cur_irr < reg_end) && (p.new_cur_irr + tb > reg_end)) || (lv >= p.lv_reg)) {
+    lv--;
+    tb = (ULL)(tb * 0.5);
+  }
+  p.lv_irr = std::max(ac->time_block, lv);
+  p.dt_irr = static_cast<double>(std::pow(2, p.lv_irr));
+  p.tb_irr = static_cast<ULL>(std::pow(2, p.lv_irr - ac->time_block));
+  if (p.dt_irr > 1) throw std::runtime_error("irregular time step exceeds the run");
+}
+
+// UpdateParticle.cpp:314-407 (calculateTimeStepReg).
+void time_step_reg(const abyss_ac *ac, Star &p) {
+  int lv;
+  ULL tb;
+  double stp;
+  block_step(ac, new_step_reg(p.a_reg, ac->p.eta_reg), lv, tb, stp);
+  const int lv0 = lv;
+  if (lv >= p.lv_reg + 1) {
+    if (std::fmod((double)p.cur_reg, 2.0 * (double)p.tb_reg) == 0 && p.t_reg != 0) {
+      lv = p.lv_reg + 1;
+      tb = p.tb_reg * 2;
+      while ((lv0 > lv) && (std::fmod((double)p.cur_reg, 2.0 * (double)tb) == 0)) {
+        tb = 2 * tb;
+        lv = lv + 1;
+      }
+    } else {
+      lv = p.lv_reg;
+    }
+  } else if (lv < p.lv_reg) {
+    lv = p.lv_reg - 1;
+    if (lv0 < lv) lv--;
+  } else {
+    lv = p.lv_reg;
+  }
+  p.lv_reg = std::max(ac->time_block, lv);
+  if (p.nb.empty()) p.lv_irr = p.lv_reg;
+  p.dt_reg = static_cast<double>(std::pow(2, p.lv_reg));
+  p.tb_reg = static_cast<ULL>(std::pow(2, p.lv_reg - ac->time_block));
+  if (p.t_reg + p.dt_reg > 1 && p.t_reg != 1.0) {
+    p.dt_reg = 1 - p.t_reg;
+    p.tb_reg = ac->block_max - p.cur_reg;
+  }
+  if (p.dt_reg * ac->scale < 1e-13) throw std::runtime_error("regular time step is too small");
+  if (p.dt_reg > 1) throw std::runtime_error("regular time step exceeds the run");
+}
+
+// UpdateParticle.cpp:108-139 (updateRadius), FixNumNeighbor/NumNeighborMax as parameters.
+void update_radius(const abyss_ac *ac, Star &p) {
+  const int nnb = (int)p.nb.size();
+  const int fix = ac->p.fix_nb, nbmax = ac->p.nb_max;
+  if (nnb > fix) {
+    const int n = 2;
+    const double c = (nbmax - fix);
+    const double b = 0.9 / std::pow(c, n);
+    const double x = nnb - fix;
+    const double a = n % 2 == 0 ? b * std::abs(x) * std::pow(x, n - 1) : b * std::pow(x, n);
+    p.r2nb *= (1. - a);
+  } else if (nnb < fix) {
+    const int n = 3;
+    const double c = (nbmax - fix);
+    const double b = 0.5 / std::pow(c, n);
+    const double x = nnb - fix;
+    const double a = n % 2 == 0 ? b * std::abs(x) * std::pow(x, n - 1) : b * std::pow(x, n);
+    p.r2nb *= (1. - a);
+  }
+}
+
+// Force of j on i (predicted pos/vel of both), softened.
+inline void pair_force(const double pi[3], const double vi[3], const double pj[3], const double vj[3],
+                       double mj, double eps2, double a[3], double ad[3], double sign) {
+  double x[3], v[3], r2 = 0.0, vx = 0.0;
+  for (int d = 0; d < 3; ++d) {
+    x[d] = pj[d] - pi[d];
+    v[d] = vj[d] - vi[d];
+    r2 += x[d] * x[d];
+    vx += x[d] * v[d];
+  }
+  const double r2s = r2 + eps2;
+  const double m_r3 = mj / r2s / std::sqrt(r2s);
+  for (int d = 0; d < 3; ++d) {
+    a[d] += sign * m_r3 * x[d];
+    ad[d] += sign * m_r3 * (v[d] - 3 * x[d] * vx / r2s);
+  }
+}
+
+int set_threads(const abyss_ac *ac) {
+#ifdef _OPENMP
+  if (ac->p.threads > 0) omp_set_num_threads(ac->p.threads);
+  return omp_get_max_threads();
+#else
+  (void)ac;
+  return 1;
+#endif
+}
+
+// One GPU regular-force call over `targets` with the j-set already predicted on
+// the device.  Overflowing targets get r2nb *= 0.8 and the call is repeated.
+int regular_gpu(abyss_ac *ac, const std::vector<int> &targets, bool upload_r2,
+                std::vector<double> &acc, std::vector<double> &jerk, std::vector<double> &airr,
+                std::vector<double> &jirr, std::vector<int> &nnb, std::vector<int> &lst) {
+  const int m = (int)targets.size();
+  const int cap = ac->p.nb_max;
+  acc.assign(3 * (size_t)m, 0);
+  jerk.assign(3 * (size_t)m, 0);
+  airr.assign(3 * (size_t)m, 0);
+  jirr.assign(3 * (size_t)m, 0);
+  nnb.assign(m, 0);
+  lst.assign((size_t)m * cap, 0);
+  (void)upload_r2;
+  for (int attempt = 0; attempt < 40; ++attempt) {
+    int ovf = 0;
+    const double t0 = now_s();
+    int rc = abyss_regular_force(ac->ctx, m, targets.data(), ac->p.eps2, cap, nullptr, acc.data(),
+                                 jerk.data(), airr.data(), jirr.data(), nnb.data(), lst.data(), &ovf);
+    ac->st.sec_reg_gpu += now_s() - t0;
+    if (rc < 0) {
+      ac->err = std::string("regular force: ") + abyss_last_error(ac->ctx);
+      return rc;
+    }
+    if (rc != ABYSS_WARN_OVERFLOW) return ABYSS_OK;
+    // shrink the radius of every overflowing target and re-upload the j-set radii
+    ac->st.radius_retries++;
+    for (int k = 0; k < m; ++k)
+      if (nnb[k] > cap) ac->s[targets[k]].r2nb *= 0.8;
+    return 2;  // caller re-predicts and retries
+  }
+  ac->err = "regular force: neighbour lists kept overflowing";
+  return ABYSS_ERR_STATE;
+}
+
+int upload_and_predict(abyss_ac *ac, double new_time) {
+  const int n = ac->n;
+  std::vector<double> x(3 * (size_t)n), v(3 * (size_t)n), a0(3 * (size_t)n), a1(3 * (size_t)n), t0(n),
+      m(n), r2(n);
+  for (int j = 0; j < n; ++j) {
+    const Star &p = ac->s[j];
+    for (int d = 0; d < 3; ++d) {
+      x[3 * (size_t)j + d] = p.x[d];
+      v[3 * (size_t)j + d] = p.v[d];
+      a0[3 * (size_t)j + d] = p.a_tot[d][0];
+      a1[3 * (size_t)j + d] = p.a_tot[d][1];
+    }
+    // CalculateRegularAcceleration.cpp:371-374
+    t0[j] = p.nb.empty() ? p.t_reg : p.t_irr;
+    m[j] = p.m;
+    r2[j] = p.r2nb;
+  }
+  int rc = abyss_upload_state(ac->ctx, n, x.data(), v.data(), a0.data(), a1.data(), t0.data(), m.data(),
+                              r2.data());
+  ac->last_r2 = r2;
+  if (rc == ABYSS_OK) rc = abyss_predict(ac->ctx, new_time, ac->scale);
+  if (rc == ABYSS_OK) rc = abyss_synchronize(ac->ctx);
+  if (rc != ABYSS_OK) ac->err = std::string("upload/predict: ") + abyss_last_error(ac->ctx);
+  return rc;
+}
+
+// Initialize.cpp:102-185 (CalculateAcceleration23) with softened r^2, for all i.
+void init_acc23(abyss_ac *ac) {
+  const int n = ac->n;
+  const double eps2 = ac->p.eps2;
+  std::vector<std::array<double, 24>> out(n);
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int i = 0; i < n; ++i) {
+    const Star &p1 = ac->s[i];
+    double reg2[3] = {0, 0, 0}, reg3[3] = {0, 0, 0}, irr2[3] = {0, 0, 0}, irr3[3] = {0, 0, 0};
+    double a1[3], a1dot[3];
+    for (int d = 0; d < 3; ++d) {
+      a1[d] = p1.a_tot[d][0];
+      a1dot[d] = p1.a_tot[d][1];
+    }
+    for (int j = 0; j < n; ++j) {
+      if (j == i) continue;
+      const Star &p2 = ac->s[j];
+      double x[3], v[3], a21[3], a21dot[3];
+      double r2u = 0, vr = 0, v2 = 0, rdf_r2 = 0, vdf_r2 = 0, rdfdot_r2 = 0;
+      for (int d = 0; d < 3; ++d) {
+        x[d] = p2.x[d] - p1.x[d];
+        v[d] = p2.v[d] - p1.v[d];
+        r2u += x[d] * x[d];
+        vr += v[d] * x[d];
+        v2 += v[d] * v[d];
+      }
+      const double r2 = r2u + eps2;
+      const double r3 = r2 * std::sqrt(r2);
+      const double m_r3 = p2.m / r3;
+      for (int d = 0; d < 3; ++d) {
+        a21[d] = m_r3 * x[d];
+        a21dot[d] = m_r3 * (v[d] - 3 * x[d] * vr / r2);
+        rdf_r2 += x[d] * (a1[d] - p2.a_tot[d][0]) / r2;
+        vdf_r2 += v[d] * (a1[d] - p2.a_tot[d][0]) / r2;
+        rdfdot_r2 += x[d] * (a1dot[d] - p2.a_tot[d][1]) / r2;
+      }
+      const double a = vr / r2;
+      const double b = v2 / r2 + rdf_r2 + a * a;
+      const double c = 3 * vdf_r2 + rdfdot_r2 + a * (3 * b - 4 * a * a);
+      const bool reg = !(r2u < p1.r2nb);  // the regular-step neighbour rule
+      for (int d = 0; d < 3; ++d) {
+        const double adot2 = -p2.m * (a1[d] - p2.a_tot[d][0]) / r3 - 6 * a * a21dot[d] - 3 * b * a21[d];
+        const double adot3 =
+            -p2.m * (a1dot[d] - p2.a_tot[d][1]) / r3 - 9 * a * adot2 - 9 * b * a21dot[d] - 3 * c * a21[d];
+        if (reg) {
+          reg2[d] += adot2;
+          reg3[d] += adot3;
+        } else {
+          irr2[d] += adot2;
+          irr3[d] += adot3;
+        }
+      }
+    }
+    for (int d = 0; d < 3; ++d) {
+      out[i][d] = reg2[d];
+      out[i][3 + d] = reg3[d];
+      out[i][6 + d] = irr2[d];
+      out[i][9 + d] = irr3[d];
+    }
+  }
+  for (int i = 0; i < n; ++i) {
+    Star &p = ac->s[i];
+    for (int d = 0; d < 3; ++d) {
+      p.a_reg[d][2] = out[i][d];
+      p.a_reg[d][3] = out[i][3 + d];
+      p.a_irr[d][2] = out[i][6 + d];
+      p.a_irr[d][3] = out[i][9 + d];
+      p.a_tot[d][2] = p.a_reg[d][2] + p.a_irr[d][2];
+      p.a_tot[d][3] = p.a_reg[d][3] + p.a_irr[d][3];
+    }
+  }
+}
+
+// Initialize.cpp:199-230 (initializeTimeStep).
+void init_time_step(abyss_ac *ac, Star &p) {
+  double stp;
+  block_step(ac, new_step_irr(p.a_reg, p.a_reg, ac->p.eta_reg), p.lv_reg, p.tb_reg, stp);
+  p.dt_reg = std::min(1.0, stp);
+  p.tb_reg = std::min(ac->block_max, p.tb_reg);
+  p.lv_reg = std::min(0, p.lv_reg);
+  if (!p.nb.empty()) {
+    block_step(ac, new_step_irr(p.a_tot, p.a_irr, ac->p.eta_irr), p.lv_irr, p.tb_irr, p.dt_irr);
+  } else {
+    p.tb_irr = p.tb_reg;
+    p.lv_irr = p.lv_reg;
+    p.dt_irr = p.dt_reg;
+  }
+  p.t_irr = p.t_reg = 0;
+  p.cur_irr = p.cur_reg = 0;
+}
+
+int initialise(abyss_ac *ac, const double *r2nb) {
+  const double t0 = now_s();
+  const int n = ac->n;
+  set_threads(ac);
+  // InitAcc1: FP64-split acc and jerk at t = 0 on the GPU (CalculateAcceleration01,
+  // Initialize.cpp:16-92, uses r2 > R2 for the regular part; the regular-step rule
+  // r2 < R2 is used here so that lists agree with every later regular step).
+  std::vector<int> all(n);
+  for (int i = 0; i < n; ++i) {
+    all[i] = i;
+    ac->s[i].r2nb = r2nb[i];
+  }
+  std::vector<double> acc, jerk, airr, jirr;
+  std::vector<int> nnb, lst;
+  for (int attempt = 0;; ++attempt) {
+    int rc = upload_and_predict(ac, 0.0);
+    if (rc != ABYSS_OK) return rc;
+    rc = regular_gpu(ac, all, true, acc, jerk, airr, jirr, nnb, lst);
+    if (rc == ABYSS_OK) break;
+    if (rc != 2 || attempt > 40) return rc < 0 ? rc : ABYSS_ERR_STATE;
+  }
+  const int cap = ac->p.nb_max;
+  for (int i = 0; i < n; ++i) {
+    Star &p = ac->s[i];
+    for (int d = 0; d < 3; ++d) {
+      for (int o = 0; o < 4; ++o) p.a_reg[d][o] = p.a_irr[d][o] = p.a_tot[d][o] = 0.0;
+      p.a_reg[d][0] = acc[3 * (size_t)i + d];
+      p.a_reg[d][1] = jerk[3 * (size_t)i + d];
+      p.a_irr[d][0] = airr[3 * (size_t)i + d];
+      p.a_irr[d][1] = jirr[3 * (size_t)i + d];
+      p.a_tot[d][0] = p.a_reg[d][0] + p.a_irr[d][0];
+      p.a_tot[d][1] = p.a_reg[d][1] + p.a_irr[d][1];
+    }
+    p.nb.assign(lst.begin() + (size_t)i * cap, lst.begin() + (size_t)i * cap + nnb[i]);
+  }
+  init_acc23(ac);  // InitAcc2
+  for (int i = 0; i < n; ++i) init_time_step(ac, ac->s[i]);  // InitTime
+  // time-step correction and time_block (RootRoutines.cpp:240-270)
+  int min_level = 0;
+  for (int i = 0; i < n; ++i) {
+    Star &p = ac->s[i];
+    if (!p.nb.empty())
+      while (p.lv_irr >= p.lv_reg) {
+        p.dt_irr *= 0.5;
+        p.tb_irr = (ULL)(p.tb_irr * 0.5);
+        p.lv_irr--;
+      }
+    min_level = std::min(min_level, p.lv_irr);
+  }
+  ac->time_block = std::max(-60, min_level - 30);  // MIN_LEVEL_BUFFER, def.h:33
+  ac->block_max = static_cast<ULL>(std::pow(2, -ac->time_block));
+  ac->time_step = std::pow(2, ac->time_block);
+  for (int i = 0; i < n; ++i) {
+    Star &p = ac->s[i];
+    p.tb_irr = static_cast<ULL>(std::pow(2, p.lv_irr - ac->time_block));
+    p.tb_reg = static_cast<ULL>(std::pow(2, p.lv_reg - ac->time_block));
+    p.next_irr = p.cur_irr + p.tb_irr;
+  }
+  ac->next_reg_block = 0;
+  ac->st.sec_init += now_s() - t0;
+  return ABYSS_OK;
+}
+
+// ComputeAcceleration.cpp:14-190 for one particle, into `out` (phase one).
+void irregular_one(const abyss_ac *ac, int i, Pending &out) {
+  const Star &p = ac->s[i];
+  std::memcpy(out.a_tot, p.a_tot, sizeof(out.a_tot));
+  std::memcpy(out.a_reg, p.a_reg, sizeof(out.a_reg));
+  std::memcpy(out.a_irr, p.a_irr, sizeof(out.a_irr));
+  if (p.nb.empty()) {
+    out.move = false;
+    return;
+  }
+  out.move = true;
+  const double new_time = p.t_irr + p.dt_irr;
+  const double dt = p.dt_irr * ac->scale;
+  double pos[3], vel[3], a_tmp[3] = {0, 0, 0}, adot_tmp[3] = {0, 0, 0};
+  predict(p, p.dt_irr, ac->scale, pos, vel);
+  for (int j : p.nb) {
+    const Star &q = ac->s[j];
+    double pj[3], vj[3];
+    predict(q, new_time - q.t_irr, ac->scale, pj, vj);
+    double x[3], v[3], r2 = 0.0, vx = 0.0;
+    for (int d = 0; d < 3; ++d) {
+      x[d] = pj[d] - pos[d];
+      v[d] = vj[d] - vel[d];
+      r2 += x[d] * x[d];
+      vx += v[d] * x[d];
+    }
+    const double r2s = r2 + ac->p.eps2;
+    const double m_r3 = q.m / (r2s * std::sqrt(r2s));
+    for (int d = 0; d < 3; ++d) {
+      a_tmp[d] += m_r3 * x[d];
+      adot_tmp[d] += m_r3 * (v[d] - 3 * x[d] * vx / r2s);
+    }
+  }
+  const double dt_ex = (new_time - p.t_reg) * ac->scale;
+  const double dt2 = dt * dt, dt3 = dt2 * dt, dt4 = dt3 * dt, dt5 = dt4 * dt;
+  for (int d = 0; d < 3; ++d) {
+    const double da_dt2 = (p.a_irr[d][0] - a_tmp[d]) / dt2;
+    const double adot_dt = (p.a_irr[d][1] + adot_tmp[d]) / dt;
+    const double a2 = -6 * da_dt2 - 2 * adot_dt - 2 * p.a_irr[d][1] / dt;
+    const double a3 = (12 * da_dt2 + 6 * adot_dt) / dt;
+    out.new_x[d] = pos[d] + a2 * dt4 / 24 + a3 * dt5 / 120;
+    out.new_v[d] = vel[d] + a2 * dt3 / 6 + a3 * dt4 / 24;
+    out.a_irr[d][0] = a_tmp[d];
+    out.a_irr[d][1] = adot_tmp[d];
+    out.a_irr[d][2] = a2;
+    out.a_irr[d][3] = a3;
+  }
+  for (int d = 0; d < 3; ++d) {
+    out.a_tot[d][0] = p.a_reg[d][0] + out.a_irr[d][0] + p.a_reg[d][1] * dt_ex;
+    out.a_tot[d][1] = p.a_reg[d][1] + out.a_irr[d][1];
+    out.a_tot[d][2] = p.a_reg[d][2] + out.a_irr[d][2];
+    out.a_tot[d][3] = p.a_reg[d][3] + out.a_irr[d][3];
+  }
+}
+
+int irregular_levels(abyss_ac *ac) {
+  const double t0 = now_s();
+  std::map<ULL, std::vector<int>> levels;
+  for (int i = 0; i < ac->n; ++i)
+    if (ac->s[i].next_irr <= ac->next_reg_block) levels[ac->s[i].next_irr].push_back(i);
+  std::vector<Pending> pend;
+  while (!levels.empty()) {
+    auto it = levels.begin();
+    std::vector<int> P = std::move(it->second);
+    levels.erase(it);
+    std::sort(P.begin(), P.end());
+    pend.resize(P.size());
+    int bad = 0;
+#pragma omp parallel for schedule(dynamic, 8) reduction(+ : bad)
+    for (int k = 0; k < (int)P.size(); ++k) {
+      irregular_one(ac, P[k], pend[k]);
+      // NewCurrentBlockIrr and the new irregular step use this particle's new
+      // derivatives (WorkerRoutines.cpp:46-64); computed here on a copy.
+      Star tmp = ac->s[P[k]];
+      std::memcpy(tmp.a_tot, pend[k].a_tot, sizeof(tmp.a_tot));
+      std::memcpy(tmp.a_irr, pend[k].a_irr, sizeof(tmp.a_irr));
+      tmp.new_cur_irr = tmp.cur_irr + tmp.tb_irr;
+      try {
+        time_step_irr(ac, tmp);
+      } catch (const std::exception &) {
+        bad++;
+      }
+      pend[k].lv_irr = tmp.lv_irr;
+      pend[k].dt_irr = tmp.dt_irr;
+      pend[k].tb_irr = tmp.tb_irr;
+      pend[k].new_cur_irr = tmp.new_cur_irr;
+    }
+    if (bad) {
+      ac->err = "irregular time step out of range";
+      return ABYSS_ERR_STATE;
+    }
+    // phase two: commit (IrrForce results + IrrUpdate, WorkerRoutines.cpp:76-87)
+    for (size_t k = 0; k < P.size(); ++k) {
+      Star &p = ac->s[P[k]];
+      const Pending &q = pend[k];
+      p.lv_irr = q.lv_irr;
+      p.dt_irr = q.dt_irr;
+      p.tb_irr = q.tb_irr;
+      p.new_cur_irr = q.new_cur_irr;
+      std::memcpy(p.a_tot, q.a_tot, sizeof(p.a_tot));
+      std::memcpy(p.a_irr, q.a_irr, sizeof(p.a_irr));
+      p.next_irr = p.new_cur_irr + p.tb_irr;
+      if (!p.nb.empty() && q.move) {
+        for (int d = 0; d < 3; ++d) {
+          p.x[d] = q.new_x[d];
+          p.v[d] = q.new_v[d];
+        }
+      }
+      p.cur_irr = p.new_cur_irr;
+      p.t_irr = p.cur_irr * ac->time_step;
+      if (p.next_irr <= ac->next_reg_block) levels[p.next_irr].push_back(P[k]);
+    }
+    ac->st.irr_levels++;
+    ac->st.irr_steps += (long long)P.size();
+  }
+  ac->st.sec_irr += now_s() - t0;
+  return ABYSS_OK;
+}
+
+// Neighbour-change correction of updateRegularParticleCuda
+// (ComputeAcceleration.cpp:457-577): walking both lists in step, the force of a
+// lost neighbour (old, not new) is subtracted and that of a gained one (new,
+// not old) added, in that interleaved order.  pred(j, pos, vel) gives j's
+// predicted state.
+template <class Pred, class Mass>
+void neighbour_change(const int *old_nb, int n_old, const int *new_nb, int n_new, Pred pred,
+                      Mass mass, double eps2, const double pos[3], const double vel[3],
+                      double a_tmp[3], double adot_tmp[3]) {
+  std::unordered_set<int> old_set(old_nb, old_nb + n_old);
+  std::unordered_set<int> new_set(new_nb, new_nb + n_new);
+  const int size = std::max(n_old, n_new);
+  for (int k = 0; k < size; ++k) {
+    if (k < n_old && !new_set.count(old_nb[k])) {
+      double pj[3], vj[3];
+      pred(old_nb[k], pj, vj);
+      pair_force(pos, vel, pj, vj, mass(old_nb[k]), eps2, a_tmp, adot_tmp, -1.0);
+    }
+    if (k < n_new && !old_set.count(new_nb[k])) {
+      double pj[3], vj[3];
+      pred(new_nb[k], pj, vj);
+      pair_force(pos, vel, pj, vj, mass(new_nb[k]), eps2, a_tmp, adot_tmp, +1.0);
+    }
+  }
+}
+
+// Fourth-order Hermite corrector of a regular step (ComputeAcceleration.cpp:592-632).
+void hermite_regular(const double pos[3], const double vel[3], const double a_reg[3][4],
+                     const double acc[3], const double jerk[3], const double a_tmp[3],
+                     const double adot_tmp[3], double dt, double new_x[3], double new_v[3],
+                     double a2o[3], double a3o[3]) {
+  const double dt2 = dt * dt, dt3 = dt2 * dt, dt4 = dt3 * dt, dt5 = dt4 * dt;
+  for (int d = 0; d < 3; ++d) {
+    const double da_dt2 = (a_reg[d][0] - acc[d] - a_tmp[d]) / dt2;
+    const double adot_dt = (a_reg[d][1] + jerk[d] + adot_tmp[d]) / dt;
+    const double a2 = -6 * da_dt2 - 2 * adot_dt - 2 * a_reg[d][1] / dt;
+    const double a3 = (12 * da_dt2 + 6 * adot_dt) / dt;
+    new_x[d] = pos[d] + a2 * dt4 / 24 + a3 * dt5 / 120;
+    new_v[d] = vel[d] + a2 * dt3 / 6 + a3 * dt4 / 24;
+    a2o[d] = a2;
+    a3o[d] = a3;
+  }
+}
+
+// Assemble the new regular/irregular/total derivatives (ComputeAcceleration.cpp:647-660).
+void commit_derivatives(const double acc[3], const double jerk[3], const double airr[3],
+                        const double jirr[3], const double a2[3], const double a3[3], int nnb,
+                        double a_reg[3][4], double a_irr[3][4], double a_tot[3][4]) {
+  for (int d = 0; d < 3; ++d) {
+    a_reg[d][2] = a2[d];
+    a_reg[d][3] = a3[d];
+    a_reg[d][0] = acc[d];
+    a_reg[d][1] = jerk[d];
+    a_irr[d][0] = airr[d];
+    a_irr[d][1] = jirr[d];
+    a_tot[d][0] = a_reg[d][0] + a_irr[d][0];
+    a_tot[d][1] = a_reg[d][1] + a_irr[d][1];
+    if (nnb == 0) {
+      a_tot[d][2] = a_reg[d][2];
+      a_tot[d][3] = a_reg[d][3];
+    }
+  }
+}
+
+// updateRegularParticleCuda (ComputeAcceleration.cpp:405-661) for one target
+// of a regular call, with the irregular part taken from the device (FP64 over
+// the new list, same predicted positions).
+void regular_correct_one(const abyss_ac *ac, int i, const double *acc, const double *jerk,
+                         const double *airr, const double *jirr, const int *lst, int nnb,
+                         Pending &out) {
+  const Star &p = ac->s[i];
+  const double new_time = p.t_reg + p.dt_reg;
+  double pos[3], vel[3];
+  predict(p, p.nb.empty() ? p.dt_reg : 0.0, ac->scale, pos, vel);
+  double a_tmp[3] = {0, 0, 0}, adot_tmp[3] = {0, 0, 0};
+  auto pred = [&](int j, double pj[3], double vj[3]) {
+    const Star &q = ac->s[j];
+    predict(q, new_time - (q.nb.empty() ? q.t_reg : q.t_irr), ac->scale, pj, vj);
+  };
+  auto mass = [&](int j) { return ac->s[j].m; };
+  neighbour_change(p.nb.data(), (int)p.nb.size(), lst, nnb, pred, mass, ac->p.eps2, pos, vel, a_tmp,
+                   adot_tmp);
+  const double dt = p.dt_reg * ac->scale;
+  double a2[3], a3[3];
+  hermite_regular(pos, vel, p.a_reg, acc, jerk, a_tmp, adot_tmp, dt, out.new_x, out.new_v, a2, a3);
+  std::memcpy(out.a_reg, p.a_reg, sizeof(out.a_reg));
+  std::memcpy(out.a_irr, p.a_irr, sizeof(out.a_irr));
+  std::memcpy(out.a_tot, p.a_tot, sizeof(out.a_tot));
+  commit_derivatives(acc, jerk, airr, jirr, a2, a3, nnb, out.a_reg, out.a_irr, out.a_tot);
+  out.new_nb.assign(lst, lst + nnb);
+  out.move = true;
+}
+
+int regular_block(abyss_ac *ac, const std::vector<int> &targets) {
+  const double new_time = ac->next_reg_block * ac->time_step;
+  std::vector<double> acc, jerk, airr, jirr;
+  std::vector<int> nnb, lst;
+  for (int attempt = 0;; ++attempt) {
+    int rc = upload_and_predict(ac, new_time);
+    if (rc != ABYSS_OK) return rc;
+    rc = regular_gpu(ac, targets, true, acc, jerk, airr, jirr, nnb, lst);
+    if (rc == ABYSS_OK) break;
+    if (rc != 2 || attempt > 40) return rc < 0 ? rc : ABYSS_ERR_STATE;
+  }
+  const int m = (int)targets.size();
+  const int cap = ac->p.nb_max;
+  ac->st.pairs += (double)m * ac->n;
+  // keep the last call for parity checks
+  ac->last_targets = targets;
+  ac->last_acc = acc;
+  ac->last_jerk = jerk;
+  ac->last_nnb = nnb;
+  ac->last_list = lst;
+  ac->last_cap = cap;
+  const double t0 = now_s();
+  std::vector<Pending> pend(m);
+#pragma omp parallel for schedule(dynamic, 8)
+  for (int k = 0; k < m; ++k)
+    regular_correct_one(ac, targets[k], &acc[3 * (size_t)k], &jerk[3 * (size_t)k], &airr[3 * (size_t)k],
+                        &jirr[3 * (size_t)k], &lst[(size_t)k * cap], nnb[k], pend[k]);
+  // RegCudaUpdate (WorkerRoutines.cpp:124-143), committed after every corrector ran
+  int bad = 0;
+  for (int k = 0; k < m; ++k) {
+    Star &p = ac->s[targets[k]];
+    Pending &q = pend[k];
+    p.nb = std::move(q.new_nb);
+    std::memcpy(p.a_reg, q.a_reg, sizeof(p.a_reg));
+    std::memcpy(p.a_irr, q.a_irr, sizeof(p.a_irr));
+    std::memcpy(p.a_tot, q.a_tot, sizeof(p.a_tot));
+    for (int d = 0; d < 3; ++d) {
+      p.x[d] = q.new_x[d];
+      p.v[d] = q.new_v[d];
+    }
+  }
+#pragma omp parallel for schedule(static) reduction(+ : bad)
+  for (int k = 0; k < m; ++k) {
+    Star &p = ac->s[targets[k]];
+    p.cur_reg = p.cur_reg + p.tb_reg;
+    p.t_reg = p.cur_reg * ac->time_step;
+    try {
+      time_step_reg(ac, p);
+      time_step_irr(ac, p);
+    } catch (const std::exception &) {
+      bad++;
+    }
+    if (p.nb.empty()) {
+      p.cur_irr = p.cur_reg;
+      p.t_irr = p.cur_reg * ac->time_step;
+    }
+    update_radius(ac, p);
+    p.next_irr = p.cur_irr + p.tb_irr;
+  }
+  ac->st.sec_reg_host += now_s() - t0;
+  if (bad) {
+    ac->err = "regular time step out of range";
+    return ABYSS_ERR_STATE;
+  }
+  ac->st.reg_steps += m;
+  ac->st.blocks++;
+  return ABYSS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int abyss_ac_create(abyss_ctx *ctx, const abyss_ac_params *p, int n, const double *x, const double *v,
+                    const double *mass, const double *r2nb, abyss_ac **out) {
+  if (!ctx || !p || n < 2 || !x || !v || !mass || !r2nb || !out) return ABYSS_ERR_ARG;
+  if (p->nb_max <= 0 || p->fix_nb <= 0 || p->fix_nb >= p->nb_max || !(p->t_end > 0) ||
+      !(p->eta_reg > 0) || !(p->eta_irr > 0) || !(p->eps2 >= 0))
+    return ABYSS_ERR_ARG;
+  abyss_ac *ac = new abyss_ac;
+  ac->ctx = ctx;
+  ac->p = *p;
+  ac->n = n;
+  ac->scale = p->t_end;
+  ac->s.resize(n);
+  for (int i = 0; i < n; ++i) {
+    Star &s = ac->s[i];
+    for (int d = 0; d < 3; ++d) {
+      s.x[d] = x[3 * (size_t)i + d];
+      s.v[d] = v[3 * (size_t)i + d];
+    }
+    s.m = mass[i];
+  }
+  int rc;
+  try {
+    rc = initialise(ac, r2nb);
+  } catch (const std::exception &e) {
+    ac->err = e.what();
+    rc = ABYSS_ERR_STATE;
+  }
+  if (rc != ABYSS_OK) {
+    delete ac;
+    return rc;
+  }
+  *out = ac;
+  return ABYSS_OK;
+}
+
+int abyss_ac_destroy(abyss_ac *ac) {
+  delete ac;
+  return ABYSS_OK;
+}
+
+int abyss_ac_advance_block(abyss_ac *ac, int *done) {
+  if (!ac) return ABYSS_ERR_ARG;
+  set_threads(ac);
+  if (ac->done || ac->next_reg_block * ac->time_step >= 1) {
+    ac->done = true;
+    if (done) *done = 1;
+    return ABYSS_OK;
+  }
+  // updateNextRegTime (RootRoutines.cpp:1310-1338)
+  ULL tmin = ac->block_max;
+  std::vector<int> targets;
+  for (int i = 0; i < ac->n; ++i) {
+    const ULL t = ac->s[i].cur_reg + ac->s[i].tb_reg;
+    if (t <= tmin) {
+      if (t < tmin) {
+        targets.clear();
+        tmin = t;
+      }
+      targets.push_back(i);
+    }
+  }
+  ac->next_reg_block = tmin;
+  int rc = irregular_levels(ac);
+  if (rc != ABYSS_OK) return rc;
+  try {
+    rc = regular_block(ac, targets);
+  } catch (const std::exception &e) {
+    ac->err = e.what();
+    rc = ABYSS_ERR_STATE;
+  }
+  if (rc != ABYSS_OK) return rc;
+  if (ac->next_reg_block * ac->time_step >= 1) ac->done = true;
+  if (done) *done = ac->done ? 1 : 0;
+  return ABYSS_OK;
+}
+
+int abyss_ac_run(abyss_ac *ac, double t_code) {
+  if (!ac) return ABYSS_ERR_ARG;
+  int done = 0;
+  while (!done && ac->next_reg_block * ac->time_step < t_code) {
+    int rc = abyss_ac_advance_block(ac, &done);
+    if (rc != ABYSS_OK) return rc;
+  }
+  return ABYSS_OK;
+}
+
+double abyss_ac_time(const abyss_ac *ac) { return ac ? ac->next_reg_block * ac->time_step : 0.0; }
+
+int abyss_ac_get_state(const abyss_ac *ac, double *x, double *v, int *nnb, double *r2nb) {
+  if (!ac) return ABYSS_ERR_ARG;
+  for (int i = 0; i < ac->n; ++i) {
+    const Star &s = ac->s[i];
+    for (int d = 0; d < 3; ++d) {
+      if (x) x[3 * (size_t)i + d] = s.x[d];
+      if (v) v[3 * (size_t)i + d] = s.v[d];
+    }
+    if (nnb) nnb[i] = (int)s.nb.size();
+    if (r2nb) r2nb[i] = s.r2nb;
+  }
+  return ABYSS_OK;
+}
+
+int abyss_ac_energy(abyss_ac *ac, double *energy) {
+  if (!ac || !energy) return ABYSS_ERR_ARG;
+  std::vector<double> x(3 * (size_t)ac->n), v(3 * (size_t)ac->n), m(ac->n);
+  abyss_ac_get_state(ac, x.data(), v.data(), nullptr, nullptr);
+  for (int i = 0; i < ac->n; ++i) m[i] = ac->s[i].m;
+  int rc = abyss_energy(ac->ctx, ac->n, x.data(), v.data(), m.data(), ac->p.eps2, energy);
+  if (rc != ABYSS_OK) ac->err = abyss_last_error(ac->ctx);
+  return rc;
+}
+
+int abyss_ac_get_stats(const abyss_ac *ac, abyss_ac_stats *st) {
+  if (!ac || !st) return ABYSS_ERR_ARG;
+  *st = ac->st;
+  return ABYSS_OK;
+}
+
+int abyss_ac_last_regular(const abyss_ac *ac, int *m, int *targets, double *px, double *pv,
+                          double *r2nb, double *acc_reg, double *jerk_reg, int *nnb, int *list,
+                          int list_cap) {
+  if (!ac || !m) return ABYSS_ERR_ARG;
+  const int mm = (int)ac->last_targets.size();
+  *m = mm;
+  if (px || pv) {
+    int rc = abyss_read_predicted(ac->ctx, px, pv, nullptr);
+    if (rc != ABYSS_OK) return rc;
+  }
+  for (int k = 0; k < mm; ++k) {
+    if (targets) targets[k] = ac->last_targets[k];
+    for (int d = 0; d < 3; ++d) {
+      if (acc_reg) acc_reg[3 * (size_t)k + d] = ac->last_acc[3 * (size_t)k + d];
+      if (jerk_reg) jerk_reg[3 * (size_t)k + d] = ac->last_jerk[3 * (size_t)k + d];
+    }
+    if (nnb) nnb[k] = ac->last_nnb[k];
+    if (list)
+      for (int q = 0; q < std::min(list_cap, ac->last_cap); ++q)
+        list[(size_t)k * list_cap + q] = ac->last_list[(size_t)k * ac->last_cap + q];
+  }
+  if (r2nb)
+    for (size_t j = 0; j < ac->last_r2.size(); ++j) r2nb[j] = ac->last_r2[j];
+  return ABYSS_OK;
+}
+
+const char *abyss_ac_last_error(const abyss_ac *ac) { return ac ? ac->err.c_str() : "null integrator"; }
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ host rules
+// The integrator's per-particle rules, exported so they can be checked against
+// the reference's outputs without a GPU (include/abyss_host.h).
+extern "C" {
+
+void abyss_host_predict(const double *x, const double *v, const double *a0, const double *a1,
+                        double dt_code, double scale, double *pos, double *vel) {
+  Star p{};
+  for (int d = 0; d < 3; ++d) {
+    p.x[d] = x[d];
+    p.v[d] = v[d];
+    p.a_tot[d][0] = a0[d];
+    p.a_tot[d][1] = a1[d];
+  }
+  predict(p, dt_code, scale, pos, vel);
+}
+
+double abyss_host_time_step_reg(const double *df12, double eta) {
+  double df[3][4];
+  std::memcpy(df, df12, sizeof(df));
+  return new_step_reg(df, eta);
+}
+
+double abyss_host_time_step_irr(const double *f12, const double *df12, double eta) {
+  double f[3][4], df[3][4];
+  std::memcpy(f, f12, sizeof(f));
+  std::memcpy(df, df12, sizeof(df));
+  return new_step_irr(f, df, eta);
+}
+
+void abyss_host_block_time_step(double dt, double scale, int time_block, int *level,
+                                unsigned long long *block, double *step) {
+  abyss_ac tmp;
+  tmp.scale = scale;
+  tmp.time_block = time_block;
+  int lv;
+  ULL bl;
+  double st;
+  block_step(&tmp, dt, lv, bl, st);
+  *level = lv;
+  *block = bl;
+  *step = st;
+}
+
+int abyss_host_regular_correct(int n, const double *x, const double *v, const double *a_tot,
+                               const double *t0, const double *mass, double eps2, double new_time,
+                               double scale, int i, double dt_reg, const double *a_reg_i, int n_old,
+                               const int *old_nb, int n_new, const int *new_nb, const double *acc,
+                               const double *jerk, const double *acc_irr, const double *jerk_irr,
+                               double *new_pos, double *new_vel, double *a_reg_out,
+                               double *a_tot_out) {
+  if (n <= 0 || i < 0 || i >= n || n_old < 0 || n_new < 0) return ABYSS_ERR_ARG;
+  auto star = [&](int j) {
+    Star q{};
+    for (int d = 0; d < 3; ++d) {
+      q.x[d] = x[3 * (size_t)j + d];
+      q.v[d] = v[3 * (size_t)j + d];
+      for (int o = 0; o < 4; ++o) q.a_tot[d][o] = a_tot[12 * (size_t)j + 4 * d + o];
+    }
+    return q;
+  };
+  const Star self = star(i);
+  double pos[3], vel[3];
+  predict(self, n_old == 0 ? dt_reg : 0.0, scale, pos, vel);
+  auto pred = [&](int j, double pj[3], double vj[3]) {
+    const Star q = star(j);
+    predict(q, new_time - t0[j], scale, pj, vj);
+  };
+  auto mfun = [&](int j) { return mass[j]; };
+  double a_tmp[3] = {0, 0, 0}, adot_tmp[3] = {0, 0, 0};
+  neighbour_change(old_nb, n_old, new_nb, n_new, pred, mfun, eps2, pos, vel, a_tmp, adot_tmp);
+  double a_reg[3][4], a_irr[3][4], at[3][4], a2[3], a3[3];
+  std::memcpy(a_reg, a_reg_i, sizeof(a_reg));
+  std::memcpy(at, a_tot + 12 * (size_t)i, sizeof(at));
+  std::memset(a_irr, 0, sizeof(a_irr));
+  hermite_regular(pos, vel, a_reg, acc, jerk, a_tmp, adot_tmp, dt_reg * scale, new_pos, new_vel, a2, a3);
+  commit_derivatives(acc, jerk, acc_irr, jerk_irr, a2, a3, n_new, a_reg, a_irr, at);
+  std::memcpy(a_reg_out, a_reg, sizeof(a_reg));
+  std::memcpy(a_tot_out, at, sizeof(at));
+  return ABYSS_OK;
+}
+
+}  // extern "C"

@@ -14,10 +14,11 @@ published methods, seeded:
 * Kroupa (2001, MNRAS 322, 231) IMF: dN/dm ~ m^-1.3 on [0.08, 0.5) and m^-2.3 on
   [0.5, 100] Msun, sampled segment-wise by inverse CDF and rescaled to sum 1.
 
-Each generator also returns a per-particle squared neighbour radius R_nb^2 aimed
-at a target neighbour count from the model's local number density
-(N n(r) 4/3 pi R^3 = k), or from the exact k-th neighbour distance when
-``exact_k`` is set (scipy cKDTree; small N only).
+Each generator also returns a per-particle squared neighbour radius R_nb^2 for a
+target neighbour count k: by default the midpoint of the squared k-th and
+(k+1)-th neighbour distances (scipy cKDTree), so every particle starts with
+exactly k neighbours; with ``exact_k=False`` it comes from the model's local
+number density (N n(r) 4/3 pi R^3 = k), which is only right on average.
 """
 from __future__ import annotations
 
@@ -85,7 +86,8 @@ def _r2_exact_k(x: np.ndarray, k: int) -> np.ndarray:
     from scipy.spatial import cKDTree
 
     tree = cKDTree(x)
-    d, _ = tree.query(x, k=k + 2)
+    k = min(k, x.shape[0] - 2)
+    d, _ = tree.query(x, k=k + 2, workers=-1)
     # self is d[:, 0]; place R between the k-th and (k+1)-th neighbour
     lo = d[:, k] ** 2
     hi = d[:, k + 1] ** 2
@@ -93,7 +95,7 @@ def _r2_exact_k(x: np.ndarray, k: int) -> np.ndarray:
 
 
 def plummer(n: int, seed: int, rmax_a: float = 10.0, masses: str = "equal",
-            k_nb: float = 32.0, exact_k: bool = False) -> Cluster:
+            k_nb: float = 32.0, exact_k: bool = True) -> Cluster:
     """Plummer sphere, Aarseth-Henon-Wielen sampling, radii truncated at rmax_a * a."""
     rng = np.random.default_rng(seed)
     r = np.empty(n)
@@ -195,7 +197,7 @@ def _king_profile(w0: float, npts: int = 4000):
 
 
 def king(n: int, seed: int, w0: float = 6.0, masses: str = "equal",
-         k_nb: float = 100.0, exact_k: bool = False) -> Cluster:
+         k_nb: float = 100.0, exact_k: bool = True) -> Cluster:
     """King (1966) model with central dimensionless potential w0."""
     rng = np.random.default_rng(seed)
     rs, ws, mcum, rho, rt = _king_profile(w0)

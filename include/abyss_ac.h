@@ -1,0 +1,75 @@
+/* abyss_ac.h -- C ABI of the host Ahmad-Cohen integrator (libabyss_reg.so).
+ *
+ * The host keeps the reference's 4th-order Hermite predictor/corrector, block
+ * timesteps and regular/irregular scheduling (src_mpi/RootRoutines.cpp:240-330,
+ * 448-1075, 1310-1338; src_mpi/WorkerRoutines.cpp:46-143;
+ * src_mpi/Particle/*.cpp) and calls the GPU regular force through abyss_reg.h
+ * at every regular block, in place of calculateRegAccelerationOnGPU
+ * (src_mpi/cuda/CalculateRegularAcceleration.cpp:27-324).
+ *
+ * Units: N-body (G = 1).  Code time runs over [0, 1] and one code-time unit is
+ * t_end N-body time units (the reference's EnzoTimeStep, DefaultGlobal.cpp:92).
+ * Irregular steps and the corrector run on host threads; every phase computes
+ * all of a block's new values before committing any of them, so results do not
+ * depend on thread scheduling.
+ */
+#ifndef ABYSS_AC_H
+#define ABYSS_AC_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct abyss_ac abyss_ac;
+struct abyss_ctx;
+
+typedef struct abyss_ac_params {
+  double eps2;     /* softening^2, force terms only */
+  double eta_reg;  /* Aarseth accuracy parameter, regular steps (reference: eta, def.h:36) */
+  double eta_irr;  /* Aarseth accuracy parameter, irregular steps */
+  int fix_nb;      /* target neighbour count (FixNumNeighbor, def.h:18) */
+  int nb_max;      /* radius-adaptation scale and list capacity (NumNeighborMax, def.h:20) */
+  double t_end;    /* N-body time of code time 1 */
+  int threads;     /* host threads (0 = all) */
+} abyss_ac_params;
+
+typedef struct abyss_ac_stats {
+  long long blocks;        /* regular blocks advanced */
+  long long reg_steps;     /* particle regular steps */
+  long long irr_steps;     /* particle irregular steps */
+  long long irr_levels;    /* irregular block levels processed */
+  long long radius_retries;/* regular calls re-run after a list overflow */
+  double pairs;            /* regular-force pairs (m * N summed) */
+  double sec_reg_gpu;      /* wall seconds in the regular-force ABI calls */
+  double sec_reg_host;     /* wall seconds in the host regular corrector/update */
+  double sec_irr;          /* wall seconds in irregular steps */
+  double sec_init;         /* wall seconds in initialisation */
+} abyss_ac_stats;
+
+/* ctx must outlive the integrator.  r2nb = initial squared neighbour radii. */
+int abyss_ac_create(struct abyss_ctx *ctx, const abyss_ac_params *p, int n, const double *x,
+                    const double *v, const double *mass, const double *r2nb, abyss_ac **out);
+int abyss_ac_destroy(abyss_ac *ac);
+/* Advance through the next regular block (its irregular levels first, then the
+ * regular step).  *done = 1 once code time 1 is reached. */
+int abyss_ac_advance_block(abyss_ac *ac, int *done);
+/* Advance until code time >= t_code (<= 1). */
+int abyss_ac_run(abyss_ac *ac, double t_code);
+/* Current code time (the last regular block time reached). */
+double abyss_ac_time(const abyss_ac *ac);
+/* Positions/velocities [n][3], neighbour counts, squared radii (any may be NULL). */
+int abyss_ac_get_state(const abyss_ac *ac, double *x, double *v, int *nnb, double *r2nb);
+/* Total energy (FP64, softened) of the current state; valid when all particles
+ * share one time (start, end). */
+int abyss_ac_energy(abyss_ac *ac, double *energy);
+int abyss_ac_get_stats(const abyss_ac *ac, abyss_ac_stats *st);
+/* The last regular call: m targets, the predicted j-set (n x 3 FP64), the
+ * squared radii used and the GPU results, for parity checks. */
+int abyss_ac_last_regular(const abyss_ac *ac, int *m, int *targets, double *px, double *pv,
+                          double *r2nb, double *acc_reg, double *jerk_reg, int *nnb, int *list,
+                          int list_cap);
+const char *abyss_ac_last_error(const abyss_ac *ac);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

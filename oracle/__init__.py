@@ -88,6 +88,7 @@ def ref():
         L.ref_compute_irr.argtypes = [C.c_int, _ip, C.c_int]
         L.ref_compute_reg_isolated.argtypes = [C.c_int, _ip, _dp, _dp, _dp, _dp, _dp, _ip, _ip, C.c_int]
         L.ref_update_reg_cuda.argtypes = [C.c_int, _ip, C.c_int, _dp, _dp]
+        L.ref_update_reg_cuda_isolated.argtypes = [C.c_int, _ip, C.c_int, _dp, _dp, _dp, _dp, _dp, _dp, _dp]
         L.ref_predict.argtypes = [C.c_int, C.c_double, _dp, _dp]
         L.ref_predict_f32.argtypes = [C.c_int, C.c_double, _fp, _fp]
         for name in ("ref_update_particle", "ref_update_radius", "ref_time_step_reg",

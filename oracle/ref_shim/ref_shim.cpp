@@ -221,6 +221,30 @@ void ref_update_reg_cuda(int i, const int *list, int nnb, const double *new_a, c
     particles[i].updateRegularParticleCuda(tmp.data(), nnb, a, ad);
 }
 
+// updateRegularParticleCuda for target i with the same predict-first semantics
+// as ref_compute_reg_isolated: outputs are copied out, then the target's
+// derivative state is restored so later targets see the pre-step state.
+void ref_update_reg_cuda_isolated(int i, const int *list, int nnb, const double *new_a,
+                                  const double *new_adot, double *a_reg, double *a_irr,
+                                  double *a_tot, double *newpos, double *newvel) {
+    Particle &p = particles[i];
+    double s_tot[3][4], s_reg[3][4], s_irr[3][4];
+    std::memcpy(s_tot, p.a_tot, sizeof(s_tot));
+    std::memcpy(s_reg, p.a_reg, sizeof(s_reg));
+    std::memcpy(s_irr, p.a_irr, sizeof(s_irr));
+    ref_update_reg_cuda(i, list, nnb, new_a, new_adot);
+    std::memcpy(a_reg, p.a_reg, sizeof(s_reg));
+    std::memcpy(a_irr, p.a_irr, sizeof(s_irr));
+    std::memcpy(a_tot, p.a_tot, sizeof(s_tot));
+    for (int d = 0; d < 3; ++d) {
+        newpos[d] = p.NewPosition[d];
+        newvel[d] = p.NewVelocity[d];
+    }
+    std::memcpy(p.a_tot, s_tot, sizeof(s_tot));
+    std::memcpy(p.a_reg, s_reg, sizeof(s_reg));
+    std::memcpy(p.a_irr, s_irr, sizeof(s_irr));
+}
+
 // Particle::predictParticleSecondOrder, double overload (UpdateParticle.cpp:37-59).
 void ref_predict(int i, double dt, double *pos, double *vel) {
     particles[i].predictParticleSecondOrder(dt, pos, vel);

