@@ -344,6 +344,10 @@ static abyss_tuning plan_for(abyss_ctx *c, int m, const abyss_tuning *user) {
   if (t.kernel == 0) t.kernel = (m <= 64) ? 2 : 1;
   if (t.kernel == 2) {
     if (t.ipt == 0) t.ipt = m <= 1 ? 1 : m <= 2 ? 2 : m <= 4 ? 4 : 8;
+  } else if (t.kernel == 3) {
+    if (t.mode == 0) t.mode = (m >= 16384) ? 1 : 2;
+    if (t.threads == 0) t.threads = 128;
+    if (t.ipt == 0) t.ipt = 2;
   } else {
     if (t.mode == 0) t.mode = (m >= 4096) ? 1 : 2;
     if (t.threads == 0) t.threads = 128;
@@ -370,10 +374,11 @@ int abyss_launch(abyss_ctx *c, double eps2, int list_cap, const abyss_tuning *tu
     L = (n + want - 1) / want;
     L = std::max(32, (L + 31) / 32 * 32);
     S = (n + L - 1) / L;
-  } else if (t.kernel == 1) {
+  } else if (t.kernel == 1 || t.kernel == 3) {
     const int per_block = t.threads * t.ipt;
     n_iblocks = (m + per_block - 1) / per_block;
-    const int occ = tile_occupancy(t.threads, t.ipt, t.mode == 1);
+    const int occ = t.kernel == 1 ? tile_occupancy(t.threads, t.ipt, t.mode == 1)
+                                  : tile2_occupancy(t.threads, t.ipt, t.mode == 1);
     if (occ <= 0) return fail(c, ABYSS_ERR_ARG, "launch: unsupported tile shape");
     const int resident = occ * c->sm_count;
     int s_want = t.j_split;
@@ -416,7 +421,7 @@ int abyss_launch(abyss_ctx *c, double eps2, int list_cap, const abyss_tuning *tu
   w.status = c->status.p;
 
   if (c->profiling) CK(cudaEventRecord(c->ev[0], c->stream), "event");
-  if (t.kernel == 1 && t.mode == 1) {
+  if ((t.kernel == 1 || t.kernel == 3) && t.mode == 1) {
     if (c->cub_bytes == 0 || c->keys.cap < (size_t)m) {
       CK(c->keys.ensure(m), "alloc keys");
       CK(c->keys_alt.ensure(m), "alloc keys");
@@ -439,6 +444,10 @@ int abyss_launch(abyss_ctx *c, double eps2, int list_cap, const abyss_tuning *tu
   if (t.kernel == 1) {
     if (launch_tile(c->stream, t.threads, t.ipt, t.mode == 1, grid, js, w, n_iblocks) != 0)
       return fail(c, ABYSS_ERR_ARG, "launch: unsupported tile shape");
+    t.grid = grid;
+  } else if (t.kernel == 3) {
+    if (launch_tile2(c->stream, t.threads, t.ipt, t.mode == 1, grid, js, w, n_iblocks) != 0)
+      return fail(c, ABYSS_ERR_ARG, "launch: unsupported packed tile shape");
     t.grid = grid;
   } else {
     if (launch_jmajor(c->stream, t.ipt, js, w, L) != 0)

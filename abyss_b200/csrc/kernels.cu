@@ -471,6 +471,290 @@ __global__ void __launch_bounds__(NT) reg_force_tile(JSet js, Work w, int n_iblo
   }
 }
 
+// ============================================================ packed tile kernel
+// The tile kernel with two targets per instruction: sm_100's packed FP32x2
+// add/mul/fma (__fadd2_rn, __fmul2_rn, __ffma2_rn) carry the pair arithmetic
+// of targets (i0, i1) in one instruction, which halves the issue slots per
+// pair; only rsqrt and the candidate select stay scalar.  Target coordinates
+// are held negated so that every difference is an addition.
+struct PairGeom2 {
+  float2 dx, dy, dz, dvx, dvy, dvz, r2, rv;
+};
+
+__device__ __forceinline__ float2 dup2(float a) { return make_float2(a, a); }
+
+__device__ __forceinline__ PairGeom2 pair_geom2(float2 xj, float2 yj, float2 zj, float2 vxj, float2 vyj,
+                                                float2 vzj, float2 nxi, float2 nyi, float2 nzi,
+                                                float2 nvxi, float2 nvyi, float2 nvzi, float2 eps2) {
+  PairGeom2 g;
+  g.dx = __fadd2_rn(xj, nxi);
+  g.dy = __fadd2_rn(yj, nyi);
+  g.dz = __fadd2_rn(zj, nzi);
+  g.dvx = __fadd2_rn(vxj, nvxi);
+  g.dvy = __fadd2_rn(vyj, nvyi);
+  g.dvz = __fadd2_rn(vzj, nvzi);
+  g.r2 = __ffma2_rn(g.dx, g.dx, __ffma2_rn(g.dy, g.dy, __ffma2_rn(g.dz, g.dz, eps2)));
+  g.rv = __ffma2_rn(g.dx, g.dvx, __ffma2_rn(g.dy, g.dvy, __fmul2_rn(g.dz, g.dvz)));
+  return g;
+}
+
+// double-single differencing: d = (hj - hi) + (lj - li), with hi, li held negated
+__device__ __forceinline__ PairGeom2 pair_geom2_ds(float2 xj, float2 yj, float2 zj, float2 xjl, float2 yjl,
+                                                   float2 zjl, float2 vxj, float2 vyj, float2 vzj,
+                                                   float2 nxi, float2 nyi, float2 nzi, float2 nxil,
+                                                   float2 nyil, float2 nzil, float2 nvxi, float2 nvyi,
+                                                   float2 nvzi, float2 eps2) {
+  PairGeom2 g;
+  g.dx = __fadd2_rn(__fadd2_rn(xj, nxi), __fadd2_rn(xjl, nxil));
+  g.dy = __fadd2_rn(__fadd2_rn(yj, nyi), __fadd2_rn(yjl, nyil));
+  g.dz = __fadd2_rn(__fadd2_rn(zj, nzi), __fadd2_rn(zjl, nzil));
+  g.dvx = __fadd2_rn(vxj, nvxi);
+  g.dvy = __fadd2_rn(vyj, nvyi);
+  g.dvz = __fadd2_rn(vzj, nvzi);
+  g.r2 = __ffma2_rn(g.dx, g.dx, __ffma2_rn(g.dy, g.dy, __ffma2_rn(g.dz, g.dz, eps2)));
+  g.rv = __ffma2_rn(g.dx, g.dvx, __ffma2_rn(g.dy, g.dvy, __fmul2_rn(g.dz, g.dvz)));
+  return g;
+}
+
+__device__ __forceinline__ void pair_accum2(const PairGeom2 &g, float2 mj, float2 rinv, float2 *p) {
+  const float2 q = __fmul2_rn(rinv, rinv);
+  const float2 mr3 = __fmul2_rn(__fmul2_rn(mj, rinv), q);
+  const float2 al = __fmul2_rn(__fmul2_rn(dup2(-3.0f), g.rv), q);
+  p[0] = __ffma2_rn(mr3, g.dx, p[0]);
+  p[1] = __ffma2_rn(mr3, g.dy, p[1]);
+  p[2] = __ffma2_rn(mr3, g.dz, p[2]);
+  p[3] = __ffma2_rn(mr3, __ffma2_rn(al, g.dx, g.dvx), p[3]);
+  p[4] = __ffma2_rn(mr3, __ffma2_rn(al, g.dy, g.dvy), p[4]);
+  p[5] = __ffma2_rn(mr3, __ffma2_rn(al, g.dz, g.dvz), p[5]);
+}
+
+template <int NT, int IPT, int TJ, int NST, bool ANCHOR>
+__global__ void __launch_bounds__(NT) reg_force_tile2(JSet js, Work w, int n_iblocks) {
+  static_assert(IPT % 2 == 0, "packed kernel holds targets in pairs");
+  constexpr int PP = IPT / 2;
+  constexpr int UNR = 2;
+  constexpr int TJP = TJ + UNR;
+  constexpr int CW = ANCHOR ? 2 : 3;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  JStage<TJ> *st = reinterpret_cast<JStage<TJ> *>(smem_raw);
+  float4 *cbuf = reinterpret_cast<float4 *>(smem_raw + NST * sizeof(JStage<TJ>));
+  uint64_t *bar = reinterpret_cast<uint64_t *>(cbuf + 2 * CW * TJP);
+  const int tid = threadIdx.x;
+  const unsigned FULL = 0xffffffffu;
+
+  if (tid == 0) {
+    for (int s = 0; s < NST; ++s) mbar_init(&bar[s], 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+
+  uint32_t g_cons = 0, g_issue = 0;
+  const int n_items = n_iblocks * w.n_chunks;
+  const float2 eps2v = dup2(w.eps2f);
+  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const int ch = item % w.n_chunks;
+    const int ib = item / w.n_chunks;
+    const int j0 = ch * w.chunk_len;
+    const int j1 = min(js.n, j0 + w.chunk_len);
+    const int ntile = (j1 - j0 + TJ - 1) / TJ;
+
+    if (tid == 0) {
+      const int pro = min(NST, ntile);
+      for (int p = 0; p < pro; ++p, ++g_issue)
+        issue_tile<TJ>(&st[g_issue % NST], &bar[g_issue % NST], js, j0 + p * TJ, j1);
+    }
+
+    const int base = ib * NT * IPT;
+    double ax = 0.0, ay = 0.0, az = 0.0;
+    if (ANCHOR) {
+      const int t0 = w.order_t[base];
+      ax = js.px[t0];
+      ay = js.py[t0];
+      az = js.pz[t0];
+    }
+    float2 nx[PP], ny[PP], nz[PP], nxl[PP], nyl[PP], nzl[PP], nvx[PP], nvy[PP], nvz[PP], r2g[PP];
+    int ti[IPT], row[IPT], nbc[IPT];
+    float ks[IPT][6], kc[IPT][6];
+#pragma unroll
+    for (int k = 0; k < IPT; ++k) {
+      const int s = base + k * NT + tid;
+      const bool valid = s < w.m;
+      const int si = valid ? s : base;
+      ti[k] = w.order_t[si];
+      row[k] = valid ? w.order_o[si] : -1;
+      const double X = js.px[ti[k]], Y = js.py[ti[k]], Z = js.pz[ti[k]];
+      double spread = 0.0;
+      float hx, hy, hz, lx = 0.0f, ly = 0.0f, lz = 0.0f;
+      if (ANCHOR) {
+        hx = (float)(X - ax);
+        hy = (float)(Y - ay);
+        hz = (float)(Z - az);
+        spread = fmax(fabs(X - ax), fmax(fabs(Y - ay), fabs(Z - az)));
+      } else {
+        hx = (float)X;
+        hy = (float)Y;
+        hz = (float)Z;
+        lx = (float)(X - (double)hx);
+        ly = (float)(Y - (double)hy);
+        lz = (float)(Z - (double)hz);
+      }
+      const float4 vmi = js.vm[ti[k]];
+      const double R2 = js.r2nb[ti[k]];
+      const double R = sqrt(fmax(R2, 0.0));
+      const double Rg = R * (1.0 + 0x1p-17) + 0x1p-19 * spread + 1e-30;
+      float g = __double2float_ru(Rg * Rg + w.eps2);
+      g = fmaxf(g, nextafterf(w.eps2f, FLT_MAX));
+      g = valid ? g : -1.0f;
+      const int p = k >> 1;
+      if (k & 1) {
+        nx[p].y = -hx; ny[p].y = -hy; nz[p].y = -hz;
+        nxl[p].y = -lx; nyl[p].y = -ly; nzl[p].y = -lz;
+        nvx[p].y = -vmi.x; nvy[p].y = -vmi.y; nvz[p].y = -vmi.z;
+        r2g[p].y = g;
+      } else {
+        nx[p].x = -hx; ny[p].x = -hy; nz[p].x = -hz;
+        nxl[p].x = -lx; nyl[p].x = -ly; nzl[p].x = -lz;
+        nvx[p].x = -vmi.x; nvy[p].x = -vmi.y; nvz[p].x = -vmi.z;
+        r2g[p].x = g;
+      }
+      nbc[k] = 0;
+#pragma unroll
+      for (int c = 0; c < 6; ++c) ks[k][c] = kc[k][c] = 0.0f;
+    }
+
+    for (int t = 0; t < ntile; ++t, ++g_cons) {
+      const int stg = g_cons % NST;
+      const bool ok = mbar_wait(&bar[stg], (g_cons / NST) & 1u);
+      const int jt0 = j0 + t * TJ;
+      const int cnt = min(TJ, j1 - jt0);
+      float4 *cb = cbuf + (g_cons & 1u) * CW * TJP;
+      for (int jj = tid; jj < TJP; jj += NT) {
+        if (jj < cnt && ok) {
+          const double X = st[stg].x[jj], Y = st[stg].y[jj], Z = st[stg].z[jj];
+          const float4 vmj = st[stg].vm[jj];
+          if (ANCHOR) {
+            cb[jj] = make_float4((float)(X - ax), (float)(Y - ay), (float)(Z - az), vmj.w);
+            cb[TJP + jj] = make_float4(vmj.x, vmj.y, vmj.z, 0.0f);
+          } else {
+            const float hx = (float)X, hy = (float)Y, hz = (float)Z;
+            cb[jj] = make_float4(hx, hy, hz, vmj.w);
+            cb[TJP + jj] = make_float4((float)(X - (double)hx), (float)(Y - (double)hy),
+                                       (float)(Z - (double)hz), 0.0f);
+            cb[2 * TJP + jj] = make_float4(vmj.x, vmj.y, vmj.z, 0.0f);
+          }
+        } else {
+          cb[jj] = make_float4(1e30f, 1e30f, 1e30f, 0.0f);
+          cb[TJP + jj] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+          if (!ANCHOR) cb[2 * TJP + jj] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
+      }
+      if (!__syncthreads_and(ok)) {
+        if (tid == 0) {
+          atomicOr(w.status, kErrTimeout);
+          for (uint32_t g = g_cons; g < g_issue; ++g) (void)mbar_wait(&bar[g % NST], (g / NST) & 1u);
+        }
+        __syncthreads();
+        return;
+      }
+      if (tid == 0 && t + NST < ntile) {
+        issue_tile<TJ>(&st[g_issue % NST], &bar[g_issue % NST], js, j0 + (t + NST) * TJ, j1);
+        ++g_issue;
+      }
+
+      float2 p[PP][6];
+#pragma unroll
+      for (int q = 0; q < PP; ++q)
+#pragma unroll
+        for (int c = 0; c < 6; ++c) p[q][c] = make_float2(0.0f, 0.0f);
+
+      for (int jj = 0; jj < cnt; jj += UNR) {
+        bool any = false;
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+          const float4 P = cb[jj + u];
+          const float4 L = ANCHOR ? make_float4(0.f, 0.f, 0.f, 0.f) : cb[TJP + jj + u];
+          const float4 V = cb[(ANCHOR ? 1 : 2) * TJP + jj + u];
+#pragma unroll
+          for (int q = 0; q < PP; ++q) {
+            const PairGeom2 g =
+                ANCHOR ? pair_geom2(dup2(P.x), dup2(P.y), dup2(P.z), dup2(V.x), dup2(V.y), dup2(V.z),
+                                    nx[q], ny[q], nz[q], nvx[q], nvy[q], nvz[q], eps2v)
+                       : pair_geom2_ds(dup2(P.x), dup2(P.y), dup2(P.z), dup2(L.x), dup2(L.y), dup2(L.z),
+                                       dup2(V.x), dup2(V.y), dup2(V.z), nx[q], ny[q], nz[q], nxl[q],
+                                       nyl[q], nzl[q], nvx[q], nvy[q], nvz[q], eps2v);
+            const bool c0 = g.r2.x < r2g[q].x;
+            const bool c1 = g.r2.y < r2g[q].y;
+            float2 ri;
+            ri.x = c0 ? 0.0f : rsqrtf(g.r2.x);
+            ri.y = c1 ? 0.0f : rsqrtf(g.r2.y);
+            any |= (c0 | c1);
+            pair_accum2(g, dup2(P.w), ri, p[q]);
+          }
+        }
+        if (__any_sync(FULL, any)) {
+#pragma unroll
+          for (int u = 0; u < UNR; ++u) {
+            const int jl = jj + u;
+            if (jl >= cnt) continue;
+            const int jg = jt0 + jl;
+            const float4 P = cb[jl];
+            const float4 L = ANCHOR ? make_float4(0.f, 0.f, 0.f, 0.f) : cb[TJP + jl];
+            const float4 V = cb[(ANCHOR ? 1 : 2) * TJP + jl];
+#pragma unroll
+            for (int q = 0; q < PP; ++q) {
+              const PairGeom2 g =
+                  ANCHOR ? pair_geom2(dup2(P.x), dup2(P.y), dup2(P.z), dup2(V.x), dup2(V.y), dup2(V.z),
+                                      nx[q], ny[q], nz[q], nvx[q], nvy[q], nvz[q], eps2v)
+                         : pair_geom2_ds(dup2(P.x), dup2(P.y), dup2(P.z), dup2(L.x), dup2(L.y),
+                                         dup2(L.z), dup2(V.x), dup2(V.y), dup2(V.z), nx[q], ny[q],
+                                         nz[q], nxl[q], nyl[q], nzl[q], nvx[q], nvy[q], nvz[q], eps2v);
+#pragma unroll
+              for (int h = 0; h < 2; ++h) {
+                const int k = 2 * q + h;
+                const float r2h = h ? g.r2.y : g.r2.x;
+                const float gh = h ? r2g[q].y : r2g[q].x;
+                if (!(r2h < gh) || jg == ti[k]) continue;
+                const double r2e = exact_r2(js.px[ti[k]], js.py[ti[k]], js.pz[ti[k]], js.px[jg],
+                                            js.py[jg], js.pz[jg]);
+                if (r2e < js.r2nb[ti[k]]) {
+                  if (nbc[k] < w.cap)
+                    w.lst[((size_t)ch * w.m + row[k]) * w.cap + nbc[k]] = jg;
+                  ++nbc[k];
+                } else {
+                  const float rr = rsqrtf(r2h);
+                  pair_accum2(g, dup2(P.w), h ? make_float2(0.0f, rr) : make_float2(rr, 0.0f), p[q]);
+                }
+              }
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < PP; ++q)
+#pragma unroll
+        for (int c = 0; c < 6; ++c)
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int k = 2 * q + h;
+            const float pv = h ? p[q][c].y : p[q][c].x;
+            const float y = __fsub_rn(pv, kc[k][c]);
+            const float tt = __fadd_rn(ks[k][c], y);
+            kc[k][c] = __fsub_rn(__fsub_rn(tt, ks[k][c]), y);
+            ks[k][c] = tt;
+          }
+    }
+
+#pragma unroll
+    for (int k = 0; k < IPT; ++k) {
+      if (row[k] < 0) continue;
+      double *dst = w.part + ((size_t)ch * w.m + row[k]) * 6;
+#pragma unroll
+      for (int c = 0; c < 6; ++c) dst[c] = (double)ks[k][c] - (double)kc[k][c];
+      w.cnt[(size_t)ch * w.m + row[k]] = nbc[k];
+    }
+  }
+}
+
 // ============================================================ j-major kernel
 // One warp per j-chunk of L consecutive particles; lanes take j = j0 + lane +
 // 32 k; the MI targets of a group are held by every lane.  The neighbour test is
@@ -751,6 +1035,26 @@ static size_t tile_smem() {
 }
 
 template <int NT, int IPT, bool ANCHOR>
+static int tile2_occupancy_impl() {
+  constexpr int TJ = 128, NST = 3;
+  auto k = reg_force_tile2<NT, IPT, TJ, NST, ANCHOR>;
+  const size_t sm = tile_smem<NT, IPT, TJ, NST, ANCHOR>();
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  int blocks = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k, NT, sm);
+  return blocks;
+}
+
+template <int NT, int IPT, bool ANCHOR>
+static void tile2_launch_impl(cudaStream_t s, int grid, const JSet &js, const Work &w, int n_iblocks) {
+  constexpr int TJ = 128, NST = 3;
+  auto k = reg_force_tile2<NT, IPT, TJ, NST, ANCHOR>;
+  const size_t sm = tile_smem<NT, IPT, TJ, NST, ANCHOR>();
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  k<<<grid, NT, sm, s>>>(js, w, n_iblocks);
+}
+
+template <int NT, int IPT, bool ANCHOR>
 static int tile_occupancy_impl() {
   constexpr int TJ = 128, NST = 3;
   auto k = reg_force_tile<NT, IPT, TJ, NST, ANCHOR>;
@@ -786,6 +1090,39 @@ static void tile_launch_impl(cudaStream_t s, int grid, const JSet &js, const Wor
       else return -1;                                                      \
     }                                                                      \
   } while (0)
+
+#define ABYSS_TILE2_SWITCH(NT_, IPT_, ANCHOR_, CALL)                       \
+  do {                                                                     \
+    if (ANCHOR_) {                                                         \
+      if (NT_ == 128 && IPT_ == 2) CALL(128, 2, true);                     \
+      else if (NT_ == 128 && IPT_ == 4) CALL(128, 4, true);                \
+      else if (NT_ == 256 && IPT_ == 2) CALL(256, 2, true);                \
+      else if (NT_ == 256 && IPT_ == 4) CALL(256, 4, true);                \
+      else return -1;                                                      \
+    } else {                                                               \
+      if (NT_ == 128 && IPT_ == 2) CALL(128, 2, false);                    \
+      else if (NT_ == 128 && IPT_ == 4) CALL(128, 4, false);               \
+      else if (NT_ == 256 && IPT_ == 2) CALL(256, 2, false);               \
+      else if (NT_ == 256 && IPT_ == 4) CALL(256, 4, false);               \
+      else return -1;                                                      \
+    }                                                                      \
+  } while (0)
+
+int tile2_occupancy(int nt, int ipt, bool anchor) {
+  int r = 0;
+#define OCC2_CALL(a, b, c) r = tile2_occupancy_impl<a, b, c>()
+  ABYSS_TILE2_SWITCH(nt, ipt, anchor, OCC2_CALL);
+#undef OCC2_CALL
+  return r;
+}
+
+int launch_tile2(cudaStream_t s, int nt, int ipt, bool anchor, int grid, const JSet &js,
+                 const Work &w, int n_iblocks) {
+#define LAUNCH2_CALL(a, b, c) tile2_launch_impl<a, b, c>(s, grid, js, w, n_iblocks)
+  ABYSS_TILE2_SWITCH(nt, ipt, anchor, LAUNCH2_CALL);
+#undef LAUNCH2_CALL
+  return 0;
+}
 
 int tile_occupancy(int nt, int ipt, bool anchor) {
   int r = 0;

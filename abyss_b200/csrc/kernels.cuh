@@ -25,6 +25,9 @@ void launch_morton_order(cudaStream_t s, int m, const int *targets, const JSet &
 int tile_occupancy(int nt, int ipt, bool anchor);
 int launch_tile(cudaStream_t s, int nt, int ipt, bool anchor, int grid, const JSet &js,
                 const Work &w, int n_iblocks);
+int tile2_occupancy(int nt, int ipt, bool anchor);
+int launch_tile2(cudaStream_t s, int nt, int ipt, bool anchor, int grid, const JSet &js,
+                 const Work &w, int n_iblocks);
 int launch_jmajor(cudaStream_t s, int mi, const JSet &js, const Work &w, int L);
 void launch_finalize(cudaStream_t s, const JSet &js, const Work &w, const Outputs &o, int sm_count);
 void launch_energy(cudaStream_t s, int n, const double *x, const double *v, const double *mass,

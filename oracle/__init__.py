@@ -60,6 +60,8 @@ def lib():
         L.oracle_block_time_step.argtypes = [C.c_double, C.c_double, C.c_int, _ip,
                                              C.POINTER(C.c_ulonglong), _dp]
         L.oracle_energy.argtypes = [C.c_int, _dp, _dp, _dp, C.c_double, C.c_int]
+        L.oracle_reg_scale.argtypes = [C.c_int, _dp, _dp, _dp, _dp, C.c_double, C.c_int, _ip, _dp, _dp,
+                                       C.c_int]
         L.oracle_energy.restype = C.c_double
         _LIB = L
     return _LIB
@@ -147,6 +149,17 @@ def reg_force_range(px, pv, m, r2nb, eps2, targets, j0, j1, nthreads=0):
     lib().oracle_reg_force_range(px.shape[0], _p(px), _p(pv), _p(m), _p(r2nb), eps2, nt, _p(t, _ip),
                                  j0, j1, _p(acc), _p(jerk), _p(nnb, _ip), nthreads)
     return acc, jerk, nnb
+
+
+def reg_scale(px, pv, m, r2nb, eps2, targets, nthreads=0):
+    """Per-target sums of |regular acc term| and |regular jerk term|."""
+    t = np.ascontiguousarray(targets, np.int32)
+    a = np.zeros(t.shape[0])
+    j = np.zeros(t.shape[0])
+    lib().oracle_reg_scale(px.shape[0], _p(np.ascontiguousarray(px)), _p(np.ascontiguousarray(pv)),
+                           _p(np.ascontiguousarray(m)), _p(np.ascontiguousarray(r2nb)), eps2, t.shape[0],
+                           _p(t, _ip), _p(a), _p(j), nthreads)
+    return a, j
 
 
 def hermite_correct(pos, vel, a_reg_old, a_new, adot_new, a_tmp, adot_tmp, dt):

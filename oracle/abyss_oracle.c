@@ -196,3 +196,43 @@ double oracle_energy(int n, const double *x, const double *v, const double *mass
     free(pot);
     return e;
 }
+
+/* Error scale of the regular sums: for each target, sum over the regular j of
+ * |m r^-3 dx| and |m r^-3 (dv - 3 (dx.dv) dx / r^2)| (vector norms).  A sum
+ * computed with FP32 pair terms carries an absolute error proportional to
+ * these, whatever the cancellation between terms; tests use them as the scale
+ * for degenerate inputs (tiny N, R_nb = 0). */
+void oracle_reg_scale(int n, const double *px, const double *pv, const double *mass,
+                      const double *r2nb, double eps2, int nt, const int *targets,
+                      double *acc_abs, double *jerk_abs, int nthreads) {
+    set_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int k = 0; k < nt; ++k) {
+        const int i = targets[k];
+        double sa = 0.0, sj = 0.0;
+        for (int j = 0; j < n; ++j) {
+            if (j == i) continue;
+            double x[3], v[3], r2 = 0.0, vx = 0.0;
+            for (int d = 0; d < 3; ++d) {
+                x[d] = px[3 * j + d] - px[3 * i + d];
+                v[d] = pv[3 * j + d] - pv[3 * i + d];
+                r2 += x[d] * x[d];
+                vx += v[d] * x[d];
+            }
+            if (r2 < r2nb[i]) continue;
+            const double r2s = r2 + eps2;
+            const double m_r3 = mass[j] / r2s / sqrt(r2s);
+            double a2 = 0.0, j2 = 0.0;
+            for (int d = 0; d < 3; ++d) {
+                const double a = m_r3 * x[d];
+                const double jj = m_r3 * (v[d] - 3 * x[d] * vx / r2s);
+                a2 += a * a;
+                j2 += jj * jj;
+            }
+            sa += sqrt(a2);
+            sj += sqrt(j2);
+        }
+        acc_abs[k] = sa;
+        jerk_abs[k] = sj;
+    }
+}

@@ -67,6 +67,12 @@ double oracle_time_step_irr(const double *f, const double *df, double eta);
 void oracle_block_time_step(double dt, double time_scale, int time_block, int *level,
                             unsigned long long *block, double *step);
 
+/* Per-target sums of the magnitudes of the regular acc and jerk terms (the
+ * natural error scale of an FP32 pair sum). */
+void oracle_reg_scale(int n, const double *px, const double *pv, const double *mass,
+                      const double *r2nb, double eps2, int nt, const int *targets,
+                      double *acc_abs, double *jerk_abs, int nthreads);
+
 /* Total energy T + W (FP64, softened potential) of n particles. */
 double oracle_energy(int n, const double *x, const double *v, const double *mass,
                      double eps2, int nthreads);
