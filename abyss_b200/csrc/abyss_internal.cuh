@@ -9,8 +9,8 @@
 //           pvx, pvy, pvz  double [n]     (FP64)                 -- exact tests, irregular sums
 // Per regular-force call (m targets, S j-chunks, list capacity cap):
 //   order_t, order_o int [m]            target particle / output row in processing order
-//   cnt     int    [S][m]               neighbours found per chunk
-//   lst     int    [S][m][cap]          per-chunk lists, ascending j
+//   lcnt    int    [m]                  neighbours found per target (atomic append)
+//   lst     int    [m][cap]             entries in the order found (any chunk order)
 //   part    double [S][m][6]            per-chunk regular acc (3) + jerk (3)
 //   outputs acc_reg, jerk_reg, acc_irr, jerk_irr double [m][3]; nnb int [m];
 //           list int [m][cap]           (final, ascending j, truncated at cap)
@@ -48,10 +48,11 @@ struct Work {
   int cap;              // list capacity per (chunk, row) and per output row
   float eps2f;
   double eps2;
-  int *cnt;             // [S][m]
-  int *lst;             // [S][m][cap]
+  int *lcnt;            // [m] neighbours found per target (atomic, exact)
+  int *lst;             // [m][cap] neighbours in the order found
   double *part;         // [S][m][6]
   int *status;          // error bits
+  int *item_counter;    // work-queue head of the tile kernel
 };
 
 struct Outputs {

@@ -74,7 +74,7 @@ struct abyss_ctx {
   DevBuf<char> cub_tmp;
   size_t cub_bytes = 0;
   // per-launch work and outputs
-  DevBuf<int> cnt, lst, status, ovf;
+  DevBuf<int> lcnt, lst, status, ovf, items;
   DevBuf<double> part;
   DevBuf<double> acc_reg, jerk_reg, acc_irr, jerk_irr;
   DevBuf<int> nnb, list;
@@ -189,7 +189,8 @@ int abyss_destroy(abyss_ctx *c) {
                            &c->acc_irr, &c->jerk_irr, &c->e_x, &c->e_v, &c->e_m, &c->e_row};
   for (auto *b : dbl) b->release();
   DevBuf<int> *ints[] = {&c->targets, &c->order_t, &c->order_o, &c->iota, &c->rows, &c->rows_alt,
-                         &c->bbox, &c->cnt, &c->lst, &c->status, &c->ovf, &c->nnb, &c->list};
+                         &c->bbox, &c->lcnt, &c->lst, &c->status, &c->ovf, &c->nnb, &c->list,
+                         &c->items};
   for (auto *b : ints) b->release();
   c->vm.release();
   c->keys.release();
@@ -377,35 +378,35 @@ int abyss_launch(abyss_ctx *c, double eps2, int list_cap, const abyss_tuning *tu
   } else if (t.kernel == 1 || t.kernel == 3) {
     const int per_block = t.threads * t.ipt;
     n_iblocks = (m + per_block - 1) / per_block;
-    const int occ = t.kernel == 1 ? tile_occupancy(t.threads, t.ipt, t.mode == 1)
-                                  : tile2_occupancy(t.threads, t.ipt, t.mode == 1);
+    const int occ = tile_occupancy(t.threads, t.ipt, t.mode == 1, t.kernel == 3);
     if (occ <= 0) return fail(c, ABYSS_ERR_ARG, "launch: unsupported tile shape");
-    const int resident = occ * c->sm_count;
+    // persistent grid: every SM holds the same number of CTAs, which take
+    // (i-block, j-chunk) items from a device counter
+    grid = t.grid > 0 ? t.grid : occ * c->sm_count;
     int s_want = t.j_split;
-    if (s_want <= 0) s_want = std::max(1, (2 * resident + n_iblocks - 1) / n_iblocks);
-    const int max_chunks = std::max(1, (n + 2 * TJ - 1) / (2 * TJ));
-    s_want = std::min(s_want, max_chunks);
+    if (s_want <= 0) s_want = std::max(1, (32 * grid + n_iblocks - 1) / n_iblocks);
+    const int max_chunks = std::max(1, (n + 8 * TJ - 1) / (8 * TJ));
+    if (t.j_split <= 0) s_want = std::min(s_want, max_chunks);
+    s_want = std::min(s_want, std::max(1, (n + TJ - 1) / TJ));
     int chunk = (n + s_want - 1) / s_want;
     chunk = (chunk + TJ - 1) / TJ * TJ;
     L = chunk;
     S = (n + chunk - 1) / chunk;
-    const int items = n_iblocks * S;
-    if (t.grid > 0) {
-      grid = std::min(t.grid, items);
-    } else {
-      const int waves = (items + resident - 1) / resident;
-      grid = (items + waves - 1) / waves;
-    }
+    grid = std::min(grid, n_iblocks * S);
   } else {
     return fail(c, ABYSS_ERR_ARG, "launch: unknown kernel");
   }
+  if (list_cap > 8192) return fail(c, ABYSS_ERR_ARG, "launch: list_cap above 8192");
   int rc = ensure_outputs(c, m, list_cap);
   if (rc != ABYSS_OK) return rc;
-  CK(c->cnt.ensure((size_t)S * m), "alloc cnt");
-  CK(c->lst.ensure((size_t)S * m * list_cap), "alloc lst");
+  CK(c->lcnt.ensure((size_t)m), "alloc lcnt");
+  CK(c->lst.ensure((size_t)m * list_cap), "alloc lst");
   CK(c->part.ensure((size_t)S * m * 6), "alloc part");
+  CK(c->items.ensure(1), "alloc items");
   CK(cudaMemsetAsync(c->status.p, 0, sizeof(int), c->stream), "clear status");
   CK(cudaMemsetAsync(c->ovf.p, 0, sizeof(int), c->stream), "clear ovf");
+  CK(cudaMemsetAsync(c->items.p, 0, sizeof(int), c->stream), "clear work queue");
+  CK(cudaMemsetAsync(c->lcnt.p, 0, sizeof(int) * (size_t)m, c->stream), "clear list counts");
 
   JSet js = jset_of(c);
   Work w;
@@ -415,10 +416,11 @@ int abyss_launch(abyss_ctx *c, double eps2, int list_cap, const abyss_tuning *tu
   w.cap = list_cap;
   w.eps2 = eps2;
   w.eps2f = (float)eps2;
-  w.cnt = c->cnt.p;
+  w.lcnt = c->lcnt.p;
   w.lst = c->lst.p;
   w.part = c->part.p;
   w.status = c->status.p;
+  w.item_counter = c->items.p;
 
   if (c->profiling) CK(cudaEventRecord(c->ev[0], c->stream), "event");
   if ((t.kernel == 1 || t.kernel == 3) && t.mode == 1) {
@@ -441,13 +443,9 @@ int abyss_launch(abyss_ctx *c, double eps2, int list_cap, const abyss_tuning *tu
     w.order_o = c->iota.p;
   }
   if (c->profiling) CK(cudaEventRecord(c->ev[1], c->stream), "event");
-  if (t.kernel == 1) {
-    if (launch_tile(c->stream, t.threads, t.ipt, t.mode == 1, grid, js, w, n_iblocks) != 0)
+  if (t.kernel == 1 || t.kernel == 3) {
+    if (launch_tile(c->stream, t.threads, t.ipt, t.mode == 1, t.kernel == 3, grid, js, w, n_iblocks) != 0)
       return fail(c, ABYSS_ERR_ARG, "launch: unsupported tile shape");
-    t.grid = grid;
-  } else if (t.kernel == 3) {
-    if (launch_tile2(c->stream, t.threads, t.ipt, t.mode == 1, grid, js, w, n_iblocks) != 0)
-      return fail(c, ABYSS_ERR_ARG, "launch: unsupported packed tile shape");
     t.grid = grid;
   } else {
     if (launch_jmajor(c->stream, t.ipt, js, w, L) != 0)

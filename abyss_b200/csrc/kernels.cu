@@ -258,225 +258,10 @@ __device__ __forceinline__ void issue_tile(JStage<TJ> *st, uint64_t *bar, const 
   bulk_g2s(st->vm, js.vm + jt0, b16, bar);
 }
 
-template <int NT, int IPT, int TJ, int NST, bool ANCHOR>
-__global__ void __launch_bounds__(NT) reg_force_tile(JSet js, Work w, int n_iblocks) {
-  constexpr int UNR = 2;                 // j per vote
-  constexpr int TJP = TJ + UNR;          // compute buffer with pad entries
-  constexpr int CW = ANCHOR ? 2 : 3;     // float4 records per j in the compute buffer
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  JStage<TJ> *st = reinterpret_cast<JStage<TJ> *>(smem_raw);
-  float4 *cbuf = reinterpret_cast<float4 *>(smem_raw + NST * sizeof(JStage<TJ>));
-  uint64_t *bar = reinterpret_cast<uint64_t *>(cbuf + 2 * CW * TJP);
-  const int tid = threadIdx.x;
-  const unsigned FULL = 0xffffffffu;
-
-  if (tid == 0) {
-    for (int s = 0; s < NST; ++s) mbar_init(&bar[s], 1);
-    fence_barrier_init();
-  }
-  __syncthreads();
-
-  uint32_t g_cons = 0, g_issue = 0;
-  const int n_items = n_iblocks * w.n_chunks;
-  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
-    const int ch = item % w.n_chunks;
-    const int ib = item / w.n_chunks;
-    const int j0 = ch * w.chunk_len;
-    const int j1 = min(js.n, j0 + w.chunk_len);
-    const int ntile = (j1 - j0 + TJ - 1) / TJ;
-
-    if (tid == 0) {
-      const int pro = min(NST, ntile);
-      for (int p = 0; p < pro; ++p, ++g_issue)
-        issue_tile<TJ>(&st[g_issue % NST], &bar[g_issue % NST], js, j0 + p * TJ, j1);
-    }
-
-    // ---- i-particles of this block into registers
-    const int base = ib * NT * IPT;
-    double ax = 0.0, ay = 0.0, az = 0.0;
-    if (ANCHOR) {
-      const int t0 = w.order_t[base];
-      ax = js.px[t0];
-      ay = js.py[t0];
-      az = js.pz[t0];
-    }
-    float xi[IPT], yi[IPT], zi[IPT], xl[IPT], yl[IPT], zl[IPT], vxi[IPT], vyi[IPT], vzi[IPT];
-    float r2g[IPT];
-    int ti[IPT], row[IPT], nbc[IPT];
-    float ks[IPT][6], kc[IPT][6];
-#pragma unroll
-    for (int k = 0; k < IPT; ++k) {
-      const int s = base + k * NT + tid;
-      const bool valid = s < w.m;
-      const int si = valid ? s : base;
-      ti[k] = w.order_t[si];
-      row[k] = valid ? w.order_o[si] : -1;
-      const double X = js.px[ti[k]], Y = js.py[ti[k]], Z = js.pz[ti[k]];
-      double spread = 0.0;
-      if (ANCHOR) {
-        xi[k] = (float)(X - ax);
-        yi[k] = (float)(Y - ay);
-        zi[k] = (float)(Z - az);
-        xl[k] = yl[k] = zl[k] = 0.0f;
-        spread = fmax(fabs(X - ax), fmax(fabs(Y - ay), fabs(Z - az)));
-      } else {
-        xi[k] = (float)X;
-        yi[k] = (float)Y;
-        zi[k] = (float)Z;
-        xl[k] = (float)(X - (double)xi[k]);
-        yl[k] = (float)(Y - (double)yi[k]);
-        zl[k] = (float)(Z - (double)zi[k]);
-      }
-      const float4 vmi = js.vm[ti[k]];
-      vxi[k] = vmi.x;
-      vyi[k] = vmi.y;
-      vzi[k] = vmi.z;
-      // Candidate threshold: every FP64 neighbour (r2 < R2) passes the FP32
-      // test r2f < r2g.  FP32 offsets err by at most ~2^-23 (|d| + 2 spread)
-      // per component; the margin below covers that many times over.
-      const double R2 = js.r2nb[ti[k]];
-      const double R = sqrt(fmax(R2, 0.0));
-      const double Rg = R * (1.0 + 0x1p-17) + 0x1p-19 * spread + 1e-30;
-      float g = __double2float_ru(Rg * Rg + w.eps2);
-      g = fmaxf(g, nextafterf(w.eps2f, FLT_MAX));  // the self pair (r2 = eps2) is always a candidate
-      r2g[k] = valid ? g : -1.0f;
-      nbc[k] = 0;
-#pragma unroll
-      for (int c = 0; c < 6; ++c) ks[k][c] = kc[k][c] = 0.0f;
-    }
-
-    // ---- stream the chunk's j-tiles
-    for (int t = 0; t < ntile; ++t, ++g_cons) {
-      const int stg = g_cons % NST;
-      const bool ok = mbar_wait(&bar[stg], (g_cons / NST) & 1u);
-      const int jt0 = j0 + t * TJ;
-      const int cnt = min(TJ, j1 - jt0);
-      float4 *cb = cbuf + (g_cons & 1u) * CW * TJP;
-      for (int jj = tid; jj < TJP; jj += NT) {
-        if (jj < cnt && ok) {
-          const double X = st[stg].x[jj], Y = st[stg].y[jj], Z = st[stg].z[jj];
-          const float4 vmj = st[stg].vm[jj];
-          if (ANCHOR) {
-            cb[jj] = make_float4((float)(X - ax), (float)(Y - ay), (float)(Z - az), vmj.w);
-            cb[TJP + jj] = make_float4(vmj.x, vmj.y, vmj.z, 0.0f);
-          } else {
-            const float hx = (float)X, hy = (float)Y, hz = (float)Z;
-            cb[jj] = make_float4(hx, hy, hz, vmj.w);
-            cb[TJP + jj] = make_float4((float)(X - (double)hx), (float)(Y - (double)hy),
-                                       (float)(Z - (double)hz), 0.0f);
-            cb[2 * TJP + jj] = make_float4(vmj.x, vmj.y, vmj.z, 0.0f);
-          }
-        } else {
-          // pad entry: massless and far away (never a candidate, contributes 0)
-          cb[jj] = make_float4(1e30f, 1e30f, 1e30f, 0.0f);
-          cb[TJP + jj] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-          if (!ANCHOR) cb[2 * TJP + jj] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        }
-      }
-      if (!__syncthreads_and(ok)) {
-        if (tid == 0) {
-          atomicOr(w.status, kErrTimeout);
-          // let the copies already in flight land before the CTA leaves
-          for (uint32_t g = g_cons; g < g_issue; ++g) (void)mbar_wait(&bar[g % NST], (g / NST) & 1u);
-        }
-        __syncthreads();
-        return;
-      }
-      if (tid == 0 && t + NST < ntile) {
-        issue_tile<TJ>(&st[g_issue % NST], &bar[g_issue % NST], js, j0 + (t + NST) * TJ, j1);
-        ++g_issue;
-      }
-
-      float p[IPT][6];
-#pragma unroll
-      for (int k = 0; k < IPT; ++k)
-#pragma unroll
-        for (int c = 0; c < 6; ++c) p[k][c] = 0.0f;
-
-      for (int jj = 0; jj < cnt; jj += UNR) {
-        bool any = false;
-#pragma unroll
-        for (int u = 0; u < UNR; ++u) {
-          const float4 P = cb[jj + u];
-          const float4 L = ANCHOR ? make_float4(0.f, 0.f, 0.f, 0.f) : cb[TJP + jj + u];
-          const float4 V = cb[(ANCHOR ? 1 : 2) * TJP + jj + u];
-#pragma unroll
-          for (int k = 0; k < IPT; ++k) {
-            const PairGeom g =
-                ANCHOR ? pair_geom(P.x, P.y, P.z, V.x, V.y, V.z, xi[k], yi[k], zi[k], vxi[k], vyi[k],
-                                   vzi[k], w.eps2f)
-                       : pair_geom_ds(P.x, P.y, P.z, L.x, L.y, L.z, V.x, V.y, V.z, xi[k], yi[k],
-                                      zi[k], xl[k], yl[k], zl[k], vxi[k], vyi[k], vzi[k], w.eps2f);
-            const bool cand = g.r2 < r2g[k];
-            float rinv = rsqrtf(g.r2);
-            rinv = cand ? 0.0f : rinv;
-            any |= cand;
-            pair_accum(g, P.w, rinv, p[k]);
-          }
-        }
-        if (__any_sync(FULL, any)) {
-          // Slow path: candidates are re-decided with the FP64 test.
-#pragma unroll
-          for (int u = 0; u < UNR; ++u) {
-            const int jl = jj + u;
-            if (jl >= cnt) continue;
-            const int jg = jt0 + jl;
-            const float4 P = cb[jl];
-            const float4 L = ANCHOR ? make_float4(0.f, 0.f, 0.f, 0.f) : cb[TJP + jl];
-            const float4 V = cb[(ANCHOR ? 1 : 2) * TJP + jl];
-#pragma unroll
-            for (int k = 0; k < IPT; ++k) {
-              const PairGeom g =
-                  ANCHOR ? pair_geom(P.x, P.y, P.z, V.x, V.y, V.z, xi[k], yi[k], zi[k], vxi[k],
-                                     vyi[k], vzi[k], w.eps2f)
-                         : pair_geom_ds(P.x, P.y, P.z, L.x, L.y, L.z, V.x, V.y, V.z, xi[k], yi[k],
-                                        zi[k], xl[k], yl[k], zl[k], vxi[k], vyi[k], vzi[k],
-                                        w.eps2f);
-              if (!(g.r2 < r2g[k]) || jg == ti[k]) continue;
-              const double r2e = exact_r2(js.px[ti[k]], js.py[ti[k]], js.pz[ti[k]], js.px[jg],
-                                          js.py[jg], js.pz[jg]);
-              if (r2e < js.r2nb[ti[k]]) {
-                if (nbc[k] < w.cap)
-                  w.lst[((size_t)ch * w.m + row[k]) * w.cap + nbc[k]] = jg;
-                ++nbc[k];
-              } else {
-                pair_accum(g, P.w, rsqrtf(g.r2), p[k]);
-              }
-            }
-          }
-        }
-      }
-      // Kahan fold of the tile partials
-#pragma unroll
-      for (int k = 0; k < IPT; ++k)
-#pragma unroll
-        for (int c = 0; c < 6; ++c) {
-          const float y = __fsub_rn(p[k][c], kc[k][c]);
-          const float tt = __fadd_rn(ks[k][c], y);
-          kc[k][c] = __fsub_rn(__fsub_rn(tt, ks[k][c]), y);
-          ks[k][c] = tt;
-        }
-    }
-
-#pragma unroll
-    for (int k = 0; k < IPT; ++k) {
-      if (row[k] < 0) continue;
-      double *dst = w.part + ((size_t)ch * w.m + row[k]) * 6;
-      float4 unused;
-      (void)unused;
-#pragma unroll
-      for (int c = 0; c < 6; ++c) dst[c] = (double)ks[k][c] - (double)kc[k][c];
-      w.cnt[(size_t)ch * w.m + row[k]] = nbc[k];
-    }
-  }
-}
-
-// ============================================================ packed tile kernel
-// The tile kernel with two targets per instruction: sm_100's packed FP32x2
-// add/mul/fma (__fadd2_rn, __fmul2_rn, __ffma2_rn) carry the pair arithmetic
-// of targets (i0, i1) in one instruction, which halves the issue slots per
-// pair; only rsqrt and the candidate select stay scalar.  Target coordinates
-// are held negated so that every difference is an addition.
+// Packed (FP32x2) pair arithmetic: sm_100's __fadd2_rn / __fmul2_rn / __ffma2_rn
+// carry the pair arithmetic of two targets in one instruction; only rsqrt and
+// the candidate select stay scalar.  Target coordinates are held negated so
+// that every difference is an addition.
 struct PairGeom2 {
   float2 dx, dy, dz, dvx, dvy, dvz, r2, rv;
 };
@@ -528,17 +313,46 @@ __device__ __forceinline__ void pair_accum2(const PairGeom2 &g, float2 mj, float
   p[5] = __ffma2_rn(mr3, __ffma2_rn(al, g.dz, g.dvz), p[5]);
 }
 
+// Shared-memory layout of the tile kernel (dynamic).
 template <int NT, int IPT, int TJ, int NST, bool ANCHOR>
-__global__ void __launch_bounds__(NT) reg_force_tile2(JSet js, Work w, int n_iblocks) {
-  static_assert(IPT % 2 == 0, "packed kernel holds targets in pairs");
-  constexpr int PP = IPT / 2;
+struct TileLayout {
+  static constexpr int TJP = TJ + 2;           // compute buffer incl. pad entries
+  static constexpr int CW = ANCHOR ? 2 : 3;    // float4 records per j
+  static constexpr size_t stage = 0;
+  static constexpr size_t cbuf = stage + NST * sizeof(JStage<TJ>);
+  static constexpr size_t kahan = cbuf + 2 * CW * TJP * sizeof(float4);  // float [IPT*12][NT]
+  static constexpr size_t tgt = kahan + (size_t)IPT * 12 * NT * sizeof(float);  // int [IPT][NT]
+  static constexpr size_t rows = tgt + (size_t)IPT * NT * sizeof(int);         // int [IPT][NT]
+  static constexpr size_t bar = (rows + (size_t)IPT * NT * sizeof(int) + 7) / 8 * 8;
+  static constexpr size_t item = bar + NST * sizeof(uint64_t);
+  static constexpr size_t bytes = item + 16;
+};
+
+// Regular force over a work queue of (i-block, j-chunk) items.  Each CTA takes
+// items from a device counter (grid = SMs x resident CTAs); an item streams its
+// j-chunk through NST shared-memory stages filled by TMA bulk copies, converts
+// each tile to FP32 offsets (anchor-relative or double-single) once per CTA and
+// runs the pair loop with IPT targets per thread in registers.  Pairs inside a
+// guard band of R_nb are masked in the fast path and re-decided with the FP64
+// test in a warp-uniform slow path (list entry, or regular contribution).
+// Tile partials are FP32; they are folded into Kahan-compensated FP32 sums kept
+// in shared memory, and written per (chunk, target) for the FP64 finalize.
+template <int NT, int IPT, int TJ, int NST, bool ANCHOR, bool PACK>
+__global__ void __launch_bounds__(NT) reg_force_tile(JSet js, Work w, int n_iblocks) {
+  using LY = TileLayout<NT, IPT, TJ, NST, ANCHOR>;
   constexpr int UNR = 2;
-  constexpr int TJP = TJ + UNR;
-  constexpr int CW = ANCHOR ? 2 : 3;
+  constexpr int TJP = LY::TJP;
+  constexpr int CW = LY::CW;
+  constexpr int PP = PACK ? IPT / 2 : 1;
+  static_assert(!PACK || IPT % 2 == 0, "packed arithmetic holds targets in pairs");
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  JStage<TJ> *st = reinterpret_cast<JStage<TJ> *>(smem_raw);
-  float4 *cbuf = reinterpret_cast<float4 *>(smem_raw + NST * sizeof(JStage<TJ>));
-  uint64_t *bar = reinterpret_cast<uint64_t *>(cbuf + 2 * CW * TJP);
+  JStage<TJ> *st = reinterpret_cast<JStage<TJ> *>(smem_raw + LY::stage);
+  float4 *cbuf = reinterpret_cast<float4 *>(smem_raw + LY::cbuf);
+  float *ksm = reinterpret_cast<float *>(smem_raw + LY::kahan);
+  int *s_ti = reinterpret_cast<int *>(smem_raw + LY::tgt);
+  int *s_row = reinterpret_cast<int *>(smem_raw + LY::rows);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + LY::bar);
+  int *s_item = reinterpret_cast<int *>(smem_raw + LY::item);
   const int tid = threadIdx.x;
   const unsigned FULL = 0xffffffffu;
 
@@ -550,10 +364,13 @@ __global__ void __launch_bounds__(NT) reg_force_tile2(JSet js, Work w, int n_ibl
 
   uint32_t g_cons = 0, g_issue = 0;
   const int n_items = n_iblocks * w.n_chunks;
-  const float2 eps2v = dup2(w.eps2f);
-  for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
-    const int ch = item % w.n_chunks;
+  for (;;) {
+    if (tid == 0) *s_item = atomicAdd(w.item_counter, 1);
+    __syncthreads();
+    const int item = *s_item;
+    if (item >= n_items) break;
     const int ib = item / w.n_chunks;
+    const int ch = item - ib * w.n_chunks;
     const int j0 = ch * w.chunk_len;
     const int j1 = min(js.n, j0 + w.chunk_len);
     const int ntile = (j1 - j0 + TJ - 1) / TJ;
@@ -564,6 +381,7 @@ __global__ void __launch_bounds__(NT) reg_force_tile2(JSet js, Work w, int n_ibl
         issue_tile<TJ>(&st[g_issue % NST], &bar[g_issue % NST], js, j0 + p * TJ, j1);
     }
 
+    // ---- targets of this block into registers (coordinates) and shared memory (indices)
     const int base = ib * NT * IPT;
     double ax = 0.0, ay = 0.0, az = 0.0;
     if (ANCHOR) {
@@ -572,56 +390,52 @@ __global__ void __launch_bounds__(NT) reg_force_tile2(JSet js, Work w, int n_ibl
       ay = js.py[t0];
       az = js.pz[t0];
     }
-    float2 nx[PP], ny[PP], nz[PP], nxl[PP], nyl[PP], nzl[PP], nvx[PP], nvy[PP], nvz[PP], r2g[PP];
-    int ti[IPT], row[IPT], nbc[IPT];
-    float ks[IPT][6], kc[IPT][6];
+    // scalar layout: [k]; packed layout: [k/2].{x,y}; coordinates held negated
+    float hx[IPT], hy[IPT], hz[IPT], lx[IPT], ly[IPT], lz[IPT], vx[IPT], vy[IPT], vz[IPT], r2g[IPT];
 #pragma unroll
     for (int k = 0; k < IPT; ++k) {
       const int s = base + k * NT + tid;
       const bool valid = s < w.m;
       const int si = valid ? s : base;
-      ti[k] = w.order_t[si];
-      row[k] = valid ? w.order_o[si] : -1;
-      const double X = js.px[ti[k]], Y = js.py[ti[k]], Z = js.pz[ti[k]];
+      const int t = w.order_t[si];
+      s_ti[k * NT + tid] = t;
+      s_row[k * NT + tid] = valid ? w.order_o[si] : -1;
+      const double X = js.px[t], Y = js.py[t], Z = js.pz[t];
       double spread = 0.0;
-      float hx, hy, hz, lx = 0.0f, ly = 0.0f, lz = 0.0f;
       if (ANCHOR) {
-        hx = (float)(X - ax);
-        hy = (float)(Y - ay);
-        hz = (float)(Z - az);
+        hx[k] = -(float)(X - ax);
+        hy[k] = -(float)(Y - ay);
+        hz[k] = -(float)(Z - az);
+        lx[k] = ly[k] = lz[k] = 0.0f;
         spread = fmax(fabs(X - ax), fmax(fabs(Y - ay), fabs(Z - az)));
       } else {
-        hx = (float)X;
-        hy = (float)Y;
-        hz = (float)Z;
-        lx = (float)(X - (double)hx);
-        ly = (float)(Y - (double)hy);
-        lz = (float)(Z - (double)hz);
+        const float fx = (float)X, fy = (float)Y, fz = (float)Z;
+        hx[k] = -fx;
+        hy[k] = -fy;
+        hz[k] = -fz;
+        lx[k] = -(float)(X - (double)fx);
+        ly[k] = -(float)(Y - (double)fy);
+        lz[k] = -(float)(Z - (double)fz);
       }
-      const float4 vmi = js.vm[ti[k]];
-      const double R2 = js.r2nb[ti[k]];
+      const float4 vmi = js.vm[t];
+      vx[k] = -vmi.x;
+      vy[k] = -vmi.y;
+      vz[k] = -vmi.z;
+      // Candidate threshold: every FP64 neighbour (r2 < R2) passes the FP32
+      // test r2f < r2g.  FP32 offsets err by at most ~2^-23 (|d| + 2 spread)
+      // per component; the margin below covers that many times over.
+      const double R2 = js.r2nb[t];
       const double R = sqrt(fmax(R2, 0.0));
       const double Rg = R * (1.0 + 0x1p-17) + 0x1p-19 * spread + 1e-30;
       float g = __double2float_ru(Rg * Rg + w.eps2);
-      g = fmaxf(g, nextafterf(w.eps2f, FLT_MAX));
-      g = valid ? g : -1.0f;
-      const int p = k >> 1;
-      if (k & 1) {
-        nx[p].y = -hx; ny[p].y = -hy; nz[p].y = -hz;
-        nxl[p].y = -lx; nyl[p].y = -ly; nzl[p].y = -lz;
-        nvx[p].y = -vmi.x; nvy[p].y = -vmi.y; nvz[p].y = -vmi.z;
-        r2g[p].y = g;
-      } else {
-        nx[p].x = -hx; ny[p].x = -hy; nz[p].x = -hz;
-        nxl[p].x = -lx; nyl[p].x = -ly; nzl[p].x = -lz;
-        nvx[p].x = -vmi.x; nvy[p].x = -vmi.y; nvz[p].x = -vmi.z;
-        r2g[p].x = g;
-      }
-      nbc[k] = 0;
+      g = fmaxf(g, nextafterf(w.eps2f, FLT_MAX));  // the self pair (r2 = eps2) is always a candidate
+      r2g[k] = valid ? g : -1.0f;
 #pragma unroll
-      for (int c = 0; c < 6; ++c) ks[k][c] = kc[k][c] = 0.0f;
+      for (int c = 0; c < 12; ++c) ksm[(k * 12 + c) * NT + tid] = 0.0f;
     }
+    const float2 eps2v = dup2(w.eps2f);
 
+    // ---- stream the chunk's j-tiles
     for (int t = 0; t < ntile; ++t, ++g_cons) {
       const int stg = g_cons % NST;
       const bool ok = mbar_wait(&bar[stg], (g_cons / NST) & 1u);
@@ -636,13 +450,14 @@ __global__ void __launch_bounds__(NT) reg_force_tile2(JSet js, Work w, int n_ibl
             cb[jj] = make_float4((float)(X - ax), (float)(Y - ay), (float)(Z - az), vmj.w);
             cb[TJP + jj] = make_float4(vmj.x, vmj.y, vmj.z, 0.0f);
           } else {
-            const float hx = (float)X, hy = (float)Y, hz = (float)Z;
-            cb[jj] = make_float4(hx, hy, hz, vmj.w);
-            cb[TJP + jj] = make_float4((float)(X - (double)hx), (float)(Y - (double)hy),
-                                       (float)(Z - (double)hz), 0.0f);
+            const float fx = (float)X, fy = (float)Y, fz = (float)Z;
+            cb[jj] = make_float4(fx, fy, fz, vmj.w);
+            cb[TJP + jj] = make_float4((float)(X - (double)fx), (float)(Y - (double)fy),
+                                       (float)(Z - (double)fz), 0.0f);
             cb[2 * TJP + jj] = make_float4(vmj.x, vmj.y, vmj.z, 0.0f);
           }
         } else {
+          // pad entry: massless and far away (never a candidate, contributes 0)
           cb[jj] = make_float4(1e30f, 1e30f, 1e30f, 0.0f);
           cb[TJP + jj] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
           if (!ANCHOR) cb[2 * TJP + jj] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -651,6 +466,7 @@ __global__ void __launch_bounds__(NT) reg_force_tile2(JSet js, Work w, int n_ibl
       if (!__syncthreads_and(ok)) {
         if (tid == 0) {
           atomicOr(w.status, kErrTimeout);
+          // let the copies already in flight land before the CTA leaves
           for (uint32_t g = g_cons; g < g_issue; ++g) (void)mbar_wait(&bar[g % NST], (g / NST) & 1u);
         }
         __syncthreads();
@@ -661,11 +477,16 @@ __global__ void __launch_bounds__(NT) reg_force_tile2(JSet js, Work w, int n_ibl
         ++g_issue;
       }
 
-      float2 p[PP][6];
+      float p[IPT][6];  // scalar tile partials
+      float2 p2[PP][6]; // packed tile partials
+#pragma unroll
+      for (int k = 0; k < IPT; ++k)
+#pragma unroll
+        for (int c = 0; c < 6; ++c) p[k][c] = 0.0f;
 #pragma unroll
       for (int q = 0; q < PP; ++q)
 #pragma unroll
-        for (int c = 0; c < 6; ++c) p[q][c] = make_float2(0.0f, 0.0f);
+        for (int c = 0; c < 6; ++c) p2[q][c] = make_float2(0.0f, 0.0f);
 
       for (int jj = 0; jj < cnt; jj += UNR) {
         bool any = false;
@@ -674,24 +495,47 @@ __global__ void __launch_bounds__(NT) reg_force_tile2(JSet js, Work w, int n_ibl
           const float4 P = cb[jj + u];
           const float4 L = ANCHOR ? make_float4(0.f, 0.f, 0.f, 0.f) : cb[TJP + jj + u];
           const float4 V = cb[(ANCHOR ? 1 : 2) * TJP + jj + u];
+          if constexpr (PACK) {
 #pragma unroll
-          for (int q = 0; q < PP; ++q) {
-            const PairGeom2 g =
-                ANCHOR ? pair_geom2(dup2(P.x), dup2(P.y), dup2(P.z), dup2(V.x), dup2(V.y), dup2(V.z),
-                                    nx[q], ny[q], nz[q], nvx[q], nvy[q], nvz[q], eps2v)
-                       : pair_geom2_ds(dup2(P.x), dup2(P.y), dup2(P.z), dup2(L.x), dup2(L.y), dup2(L.z),
-                                       dup2(V.x), dup2(V.y), dup2(V.z), nx[q], ny[q], nz[q], nxl[q],
-                                       nyl[q], nzl[q], nvx[q], nvy[q], nvz[q], eps2v);
-            const bool c0 = g.r2.x < r2g[q].x;
-            const bool c1 = g.r2.y < r2g[q].y;
-            float2 ri;
-            ri.x = c0 ? 0.0f : rsqrtf(g.r2.x);
-            ri.y = c1 ? 0.0f : rsqrtf(g.r2.y);
-            any |= (c0 | c1);
-            pair_accum2(g, dup2(P.w), ri, p[q]);
+            for (int q = 0; q < PP; ++q) {
+              const int k0 = 2 * q, k1 = 2 * q + 1;
+              const PairGeom2 g =
+                  ANCHOR ? pair_geom2(dup2(P.x), dup2(P.y), dup2(P.z), dup2(V.x), dup2(V.y), dup2(V.z),
+                                      make_float2(hx[k0], hx[k1]), make_float2(hy[k0], hy[k1]),
+                                      make_float2(hz[k0], hz[k1]), make_float2(vx[k0], vx[k1]),
+                                      make_float2(vy[k0], vy[k1]), make_float2(vz[k0], vz[k1]), eps2v)
+                         : pair_geom2_ds(dup2(P.x), dup2(P.y), dup2(P.z), dup2(L.x), dup2(L.y), dup2(L.z),
+                                         dup2(V.x), dup2(V.y), dup2(V.z), make_float2(hx[k0], hx[k1]),
+                                         make_float2(hy[k0], hy[k1]), make_float2(hz[k0], hz[k1]),
+                                         make_float2(lx[k0], lx[k1]), make_float2(ly[k0], ly[k1]),
+                                         make_float2(lz[k0], lz[k1]), make_float2(vx[k0], vx[k1]),
+                                         make_float2(vy[k0], vy[k1]), make_float2(vz[k0], vz[k1]), eps2v);
+              const bool c0 = g.r2.x < r2g[k0];
+              const bool c1 = g.r2.y < r2g[k1];
+              float2 ri;
+              ri.x = c0 ? 0.0f : rsqrtf(g.r2.x);
+              ri.y = c1 ? 0.0f : rsqrtf(g.r2.y);
+              any |= (c0 | c1);
+              pair_accum2(g, dup2(P.w), ri, p2[q]);
+            }
+          } else {
+#pragma unroll
+            for (int k = 0; k < IPT; ++k) {
+              const PairGeom gg =
+                  ANCHOR ? pair_geom(P.x, P.y, P.z, V.x, V.y, V.z, -hx[k], -hy[k], -hz[k], -vx[k], -vy[k],
+                                     -vz[k], w.eps2f)
+                         : pair_geom_ds(P.x, P.y, P.z, L.x, L.y, L.z, V.x, V.y, V.z, -hx[k], -hy[k], -hz[k],
+                                        -lx[k], -ly[k], -lz[k], -vx[k], -vy[k], -vz[k], w.eps2f);
+              const bool cand = gg.r2 < r2g[k];
+              float rinv = rsqrtf(gg.r2);
+              rinv = cand ? 0.0f : rinv;
+              any |= cand;
+              pair_accum(gg, P.w, rinv, p[k]);
+            }
           }
         }
         if (__any_sync(FULL, any)) {
+          // Slow path: candidates are re-decided with the FP64 test.
 #pragma unroll
           for (int u = 0; u < UNR; ++u) {
             const int jl = jj + u;
@@ -701,56 +545,79 @@ __global__ void __launch_bounds__(NT) reg_force_tile2(JSet js, Work w, int n_ibl
             const float4 L = ANCHOR ? make_float4(0.f, 0.f, 0.f, 0.f) : cb[TJP + jl];
             const float4 V = cb[(ANCHOR ? 1 : 2) * TJP + jl];
 #pragma unroll
-            for (int q = 0; q < PP; ++q) {
-              const PairGeom2 g =
-                  ANCHOR ? pair_geom2(dup2(P.x), dup2(P.y), dup2(P.z), dup2(V.x), dup2(V.y), dup2(V.z),
-                                      nx[q], ny[q], nz[q], nvx[q], nvy[q], nvz[q], eps2v)
-                         : pair_geom2_ds(dup2(P.x), dup2(P.y), dup2(P.z), dup2(L.x), dup2(L.y),
-                                         dup2(L.z), dup2(V.x), dup2(V.y), dup2(V.z), nx[q], ny[q],
-                                         nz[q], nxl[q], nyl[q], nzl[q], nvx[q], nvy[q], nvz[q], eps2v);
-#pragma unroll
-              for (int h = 0; h < 2; ++h) {
-                const int k = 2 * q + h;
-                const float r2h = h ? g.r2.y : g.r2.x;
-                const float gh = h ? r2g[q].y : r2g[q].x;
-                if (!(r2h < gh) || jg == ti[k]) continue;
-                const double r2e = exact_r2(js.px[ti[k]], js.py[ti[k]], js.pz[ti[k]], js.px[jg],
-                                            js.py[jg], js.pz[jg]);
-                if (r2e < js.r2nb[ti[k]]) {
-                  if (nbc[k] < w.cap)
-                    w.lst[((size_t)ch * w.m + row[k]) * w.cap + nbc[k]] = jg;
-                  ++nbc[k];
-                } else {
-                  const float rr = rsqrtf(r2h);
-                  pair_accum2(g, dup2(P.w), h ? make_float2(0.0f, rr) : make_float2(rr, 0.0f), p[q]);
-                }
+            for (int k = 0; k < IPT; ++k) {
+              float r2k;
+              PairGeom2 g2;
+              PairGeom gg;
+              if constexpr (PACK) {
+                const int k0 = k & ~1, k1 = k | 1;
+                g2 = ANCHOR ? pair_geom2(dup2(P.x), dup2(P.y), dup2(P.z), dup2(V.x), dup2(V.y), dup2(V.z),
+                                         make_float2(hx[k0], hx[k1]), make_float2(hy[k0], hy[k1]),
+                                         make_float2(hz[k0], hz[k1]), make_float2(vx[k0], vx[k1]),
+                                         make_float2(vy[k0], vy[k1]), make_float2(vz[k0], vz[k1]), eps2v)
+                            : pair_geom2_ds(dup2(P.x), dup2(P.y), dup2(P.z), dup2(L.x), dup2(L.y),
+                                            dup2(L.z), dup2(V.x), dup2(V.y), dup2(V.z),
+                                            make_float2(hx[k0], hx[k1]), make_float2(hy[k0], hy[k1]),
+                                            make_float2(hz[k0], hz[k1]), make_float2(lx[k0], lx[k1]),
+                                            make_float2(ly[k0], ly[k1]), make_float2(lz[k0], lz[k1]),
+                                            make_float2(vx[k0], vx[k1]), make_float2(vy[k0], vy[k1]),
+                                            make_float2(vz[k0], vz[k1]), eps2v);
+                r2k = (k & 1) ? g2.r2.y : g2.r2.x;
+              } else {
+                gg = ANCHOR ? pair_geom(P.x, P.y, P.z, V.x, V.y, V.z, -hx[k], -hy[k], -hz[k], -vx[k], -vy[k],
+                                        -vz[k], w.eps2f)
+                            : pair_geom_ds(P.x, P.y, P.z, L.x, L.y, L.z, V.x, V.y, V.z, -hx[k], -hy[k],
+                                           -hz[k], -lx[k], -ly[k], -lz[k], -vx[k], -vy[k], -vz[k], w.eps2f);
+                r2k = gg.r2;
+              }
+              if (!(r2k < r2g[k])) continue;
+              const int ti = s_ti[k * NT + tid];
+              if (jg == ti) continue;
+              const double r2e = exact_r2(js.px[ti], js.py[ti], js.pz[ti], js.px[jg], js.py[jg], js.pz[jg]);
+              if (r2e < js.r2nb[ti]) {
+                const int row = s_row[k * NT + tid];
+                const int pos = atomicAdd(&w.lcnt[row], 1);
+                if (pos < w.cap) w.lst[(size_t)row * w.cap + pos] = jg;
+              } else {
+                const float rr = rsqrtf(r2k);
+                if constexpr (PACK)
+                  pair_accum2(g2, dup2(P.w), (k & 1) ? make_float2(0.0f, rr) : make_float2(rr, 0.0f),
+                              p2[k >> 1]);
+                else
+                  pair_accum(gg, P.w, rr, p[k]);
               }
             }
           }
         }
       }
+      // Kahan fold of the tile partials into the shared-memory sums
 #pragma unroll
-      for (int q = 0; q < PP; ++q)
+      for (int k = 0; k < IPT; ++k)
 #pragma unroll
-        for (int c = 0; c < 6; ++c)
-#pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            const int k = 2 * q + h;
-            const float pv = h ? p[q][c].y : p[q][c].x;
-            const float y = __fsub_rn(pv, kc[k][c]);
-            const float tt = __fadd_rn(ks[k][c], y);
-            kc[k][c] = __fsub_rn(__fsub_rn(tt, ks[k][c]), y);
-            ks[k][c] = tt;
-          }
+        for (int c = 0; c < 6; ++c) {
+          float pv;
+          if constexpr (PACK)
+            pv = (k & 1) ? p2[k >> 1][c].y : p2[k >> 1][c].x;
+          else
+            pv = p[k][c];
+          float *sp = &ksm[(k * 12 + c) * NT + tid];
+          float *cp = &ksm[(k * 12 + 6 + c) * NT + tid];
+          const float ssum = *sp, comp = *cp;
+          const float y = __fsub_rn(pv, comp);
+          const float tt = __fadd_rn(ssum, y);
+          *cp = __fsub_rn(__fsub_rn(tt, ssum), y);
+          *sp = tt;
+        }
     }
 
 #pragma unroll
     for (int k = 0; k < IPT; ++k) {
-      if (row[k] < 0) continue;
-      double *dst = w.part + ((size_t)ch * w.m + row[k]) * 6;
+      const int row = s_row[k * NT + tid];
+      if (row < 0) continue;
+      double *dst = w.part + ((size_t)ch * w.m + row) * 6;
 #pragma unroll
-      for (int c = 0; c < 6; ++c) dst[c] = (double)ks[k][c] - (double)kc[k][c];
-      w.cnt[(size_t)ch * w.m + row[k]] = nbc[k];
+      for (int c = 0; c < 6; ++c)
+        dst[c] = (double)ksm[(k * 12 + c) * NT + tid] - (double)ksm[(k * 12 + 6 + c) * NT + tid];
     }
   }
 }
@@ -758,8 +625,8 @@ __global__ void __launch_bounds__(NT) reg_force_tile2(JSet js, Work w, int n_ibl
 // ============================================================ j-major kernel
 // One warp per j-chunk of L consecutive particles; lanes take j = j0 + lane +
 // 32 k; the MI targets of a group are held by every lane.  The neighbour test is
-// the exact FP64 one; __ballot_sync + __popc give each neighbour its slot in
-// ascending-j order.
+// the exact FP64 one; __ballot_sync + __popc give each neighbour of a 32-j
+// group its slot, reserved with one atomic per group.
 template <int MI>
 __global__ void __launch_bounds__(128) reg_force_jmajor(JSet js, Work w, int L) {
   const unsigned FULL = 0xffffffffu;
@@ -772,7 +639,7 @@ __global__ void __launch_bounds__(128) reg_force_jmajor(JSet js, Work w, int L) 
   for (int ig = 0; ig < w.m; ig += MI) {
     double xi[MI], yi[MI], zi[MI], R2[MI];
     float vxi[MI], vyi[MI], vzi[MI];
-    int ti[MI], row[MI], nbc[MI];
+    int ti[MI], row[MI];
     float p[MI][6];
 #pragma unroll
     for (int k = 0; k < MI; ++k) {
@@ -788,7 +655,6 @@ __global__ void __launch_bounds__(128) reg_force_jmajor(JSet js, Work w, int L) 
       vxi[k] = vmi.x;
       vyi[k] = vmi.y;
       vzi[k] = vmi.z;
-      nbc[k] = 0;
 #pragma unroll
       for (int q = 0; q < 6; ++q) p[k][q] = 0.0f;
     }
@@ -826,11 +692,14 @@ __global__ void __launch_bounds__(128) reg_force_jmajor(JSet js, Work w, int L) 
         pair_accum(g, V.w, rinv, p[k]);
         const unsigned mask = __ballot_sync(FULL, isnb);
         if (mask) {
+          const int leader = __ffs(mask) - 1;
+          int basepos = 0;
+          if (lane == leader) basepos = atomicAdd(&w.lcnt[row[k]], __popc(mask));
+          basepos = __shfl_sync(FULL, basepos, leader);
           if (isnb) {
-            const int idx = nbc[k] + __popc(mask & lt_mask);
-            if (idx < w.cap) w.lst[((size_t)c * w.m + row[k]) * w.cap + idx] = j;
+            const int idx = basepos + __popc(mask & lt_mask);
+            if (idx < w.cap) w.lst[(size_t)row[k] * w.cap + idx] = j;
           }
-          nbc[k] += __popc(mask);
         }
       }
     }
@@ -847,7 +716,6 @@ __global__ void __launch_bounds__(128) reg_force_jmajor(JSet js, Work w, int L) 
         double *dst = w.part + ((size_t)c * w.m + row[k]) * 6;
 #pragma unroll
         for (int q = 0; q < 6; ++q) dst[q] = s[q];
-        w.cnt[(size_t)c * w.m + row[k]] = nbc[k];
       }
     }
   }
@@ -855,13 +723,16 @@ __global__ void __launch_bounds__(128) reg_force_jmajor(JSet js, Work w, int L) 
 
 // ============================================================ finalize
 // One warp per output row.  Regular part: FP64 sum of the chunk partials in a
-// fixed lane/tree order.  List: chunk counts prefix-summed in chunk order, so
-// the concatenation is in ascending j.  Irregular part: the reference's FP64
-// formula (ComputeAcceleration.cpp:285-292, softened as for the regular part)
-// over the final list, lane-strided with a fixed reduction tree.
-__global__ void finalize_rows(JSet js, Work w, Outputs o) {
+// fixed lane/tree order.  List: the row's entries (appended by chunks in any
+// order) are sorted ascending with a warp bitonic sort in shared memory.
+// Irregular part: the reference's FP64 formula (ComputeAcceleration.cpp:
+// 285-292, softened as for the regular part) over the final list, lane-strided
+// with a fixed reduction tree.
+__global__ void finalize_rows(JSet js, Work w, Outputs o, int sort_cap) {
+  extern __shared__ int fin_smem[];
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
+  int *buf = fin_smem + (threadIdx.x >> 5) * sort_cap;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < w.m; r += nwarps) {
     double s[6] = {0, 0, 0, 0, 0, 0};
@@ -874,31 +745,40 @@ __global__ void finalize_rows(JSet js, Work w, Outputs o) {
     for (int q = 0; q < 6; ++q)
       for (int off = 16; off > 0; off >>= 1) s[q] += __shfl_xor_sync(FULL, s[q], off);
 
-    int total = 0;
+    const int total = w.lcnt[r];
+    const int nl = min(total, w.cap);
+    int *lrow = w.lst + (size_t)r * w.cap;
     int *out = o.list + (size_t)r * w.cap;
-    for (int cb = 0; cb < w.n_chunks; cb += 32) {
-      const int c = cb + lane;
-      const int cc = c < w.n_chunks ? w.cnt[(size_t)c * w.m + r] : 0;
-      int incl = cc;
-      for (int off = 1; off < 32; off <<= 1) {
-        const int v = __shfl_up_sync(FULL, incl, off);
-        if (lane >= off) incl += v;
+    // bitonic sort of nl entries, padded to a power of two >= 32
+    int P = 32;
+    while (P < nl) P <<= 1;
+    for (int k = lane; k < P; k += 32) buf[k] = k < nl ? lrow[k] : INT_MAX;
+    __syncwarp();
+    for (int kk = 2; kk <= P; kk <<= 1) {
+      for (int jj = kk >> 1; jj > 0; jj >>= 1) {
+        for (int i = lane; i < P; i += 32) {
+          const int l = i ^ jj;
+          if (l > i) {
+            const int a = buf[i], b = buf[l];
+            const bool up = (i & kk) == 0;
+            if ((a > b) == up) {
+              buf[i] = b;
+              buf[l] = a;
+            }
+          }
+        }
+        __syncwarp();
       }
-      const int start = total + incl - cc;
-      const int stored = min(cc, w.cap);
-      const int *src = w.lst + ((size_t)c * w.m + r) * w.cap;
-      for (int k = 0; k < stored && start + k < w.cap; ++k) out[start + k] = src[k];
-      total += __shfl_sync(FULL, incl, 31);
     }
+    for (int k = lane; k < nl; k += 32) out[k] = buf[k];
     __syncwarp();
 
     const int t = o.targets[r];
     const double xi = js.px[t], yi = js.py[t], zi = js.pz[t];
     const double vxi = js.pvx[t], vyi = js.pvy[t], vzi = js.pvz[t];
     double a[6] = {0, 0, 0, 0, 0, 0};
-    const int nl = min(total, w.cap);
     for (int k = lane; k < nl; k += 32) {
-      const int j = out[k];
+      const int j = buf[k];
       const double x[3] = {__dsub_rn(js.px[j], xi), __dsub_rn(js.py[j], yi), __dsub_rn(js.pz[j], zi)};
       const double v[3] = {__dsub_rn(js.pvx[j], vxi), __dsub_rn(js.pvy[j], vyi),
                            __dsub_rn(js.pvz[j], vzi)};
@@ -935,6 +815,7 @@ __global__ void finalize_rows(JSet js, Work w, Outputs o) {
         atomicOr(w.status, kErrOverflow);
       }
     }
+    __syncwarp();
   }
 }
 
@@ -1028,114 +909,56 @@ void launch_morton_order(cudaStream_t s, int m, const int *targets, const JSet &
   gather_order<<<blocks, 256, 0, s>>>(m, targets, rows_alt, order_t, order_o);
 }
 
-template <int NT, int IPT, int TJ, int NST, bool ANCHOR>
-static size_t tile_smem() {
-  constexpr int CW = ANCHOR ? 2 : 3;
-  return NST * sizeof(JStage<TJ>) + 2 * CW * (TJ + 2) * sizeof(float4) + NST * sizeof(uint64_t);
-}
-
-template <int NT, int IPT, bool ANCHOR>
-static int tile2_occupancy_impl() {
-  constexpr int TJ = 128, NST = 3;
-  auto k = reg_force_tile2<NT, IPT, TJ, NST, ANCHOR>;
-  const size_t sm = tile_smem<NT, IPT, TJ, NST, ANCHOR>();
-  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  int blocks = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k, NT, sm);
-  return blocks;
-}
-
-template <int NT, int IPT, bool ANCHOR>
-static void tile2_launch_impl(cudaStream_t s, int grid, const JSet &js, const Work &w, int n_iblocks) {
-  constexpr int TJ = 128, NST = 3;
-  auto k = reg_force_tile2<NT, IPT, TJ, NST, ANCHOR>;
-  const size_t sm = tile_smem<NT, IPT, TJ, NST, ANCHOR>();
-  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  k<<<grid, NT, sm, s>>>(js, w, n_iblocks);
-}
-
-template <int NT, int IPT, bool ANCHOR>
+template <int NT, int IPT, bool ANCHOR, bool PACK>
 static int tile_occupancy_impl() {
   constexpr int TJ = 128, NST = 3;
-  auto k = reg_force_tile<NT, IPT, TJ, NST, ANCHOR>;
-  const size_t sm = tile_smem<NT, IPT, TJ, NST, ANCHOR>();
+  auto k = reg_force_tile<NT, IPT, TJ, NST, ANCHOR, PACK>;
+  const size_t sm = TileLayout<NT, IPT, TJ, NST, ANCHOR>::bytes;
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   int blocks = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k, NT, sm);
   return blocks;
 }
 
-template <int NT, int IPT, bool ANCHOR>
+template <int NT, int IPT, bool ANCHOR, bool PACK>
 static void tile_launch_impl(cudaStream_t s, int grid, const JSet &js, const Work &w, int n_iblocks) {
   constexpr int TJ = 128, NST = 3;
-  auto k = reg_force_tile<NT, IPT, TJ, NST, ANCHOR>;
-  const size_t sm = tile_smem<NT, IPT, TJ, NST, ANCHOR>();
+  auto k = reg_force_tile<NT, IPT, TJ, NST, ANCHOR, PACK>;
+  const size_t sm = TileLayout<NT, IPT, TJ, NST, ANCHOR>::bytes;
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   k<<<grid, NT, sm, s>>>(js, w, n_iblocks);
 }
 
-#define ABYSS_TILE_SWITCH(NT_, IPT_, ANCHOR_, CALL)                        \
-  do {                                                                     \
-    if (ANCHOR_) {                                                         \
-      if (NT_ == 128 && IPT_ == 1) CALL(128, 1, true);                     \
-      else if (NT_ == 128 && IPT_ == 2) CALL(128, 2, true);                \
-      else if (NT_ == 128 && IPT_ == 4) CALL(128, 4, true);                \
-      else if (NT_ == 256 && IPT_ == 2) CALL(256, 2, true);                \
-      else return -1;                                                      \
-    } else {                                                               \
-      if (NT_ == 128 && IPT_ == 1) CALL(128, 1, false);                    \
-      else if (NT_ == 128 && IPT_ == 2) CALL(128, 2, false);               \
-      else if (NT_ == 128 && IPT_ == 4) CALL(128, 4, false);               \
-      else if (NT_ == 256 && IPT_ == 2) CALL(256, 2, false);               \
-      else return -1;                                                      \
-    }                                                                      \
+// Instantiated shapes: scalar (PACK = false) 128x{1,2,4}, 256x2; packed 128x{2,4}, 256x{2,4}.
+#define ABYSS_TILE_SWITCH(NT_, IPT_, ANCHOR_, PACK_, CALL)                                      \
+  do {                                                                                          \
+    if (!(PACK_)) {                                                                             \
+      if (NT_ == 128 && IPT_ == 1) { if (ANCHOR_) CALL(128, 1, true, false); else CALL(128, 1, false, false); } \
+      else if (NT_ == 128 && IPT_ == 2) { if (ANCHOR_) CALL(128, 2, true, false); else CALL(128, 2, false, false); } \
+      else if (NT_ == 128 && IPT_ == 4) { if (ANCHOR_) CALL(128, 4, true, false); else CALL(128, 4, false, false); } \
+      else if (NT_ == 256 && IPT_ == 2) { if (ANCHOR_) CALL(256, 2, true, false); else CALL(256, 2, false, false); } \
+      else return -1;                                                                           \
+    } else {                                                                                    \
+      if (NT_ == 128 && IPT_ == 2) { if (ANCHOR_) CALL(128, 2, true, true); else CALL(128, 2, false, true); } \
+      else if (NT_ == 128 && IPT_ == 4) { if (ANCHOR_) CALL(128, 4, true, true); else CALL(128, 4, false, true); } \
+      else if (NT_ == 256 && IPT_ == 2) { if (ANCHOR_) CALL(256, 2, true, true); else CALL(256, 2, false, true); } \
+      else if (NT_ == 256 && IPT_ == 4) { if (ANCHOR_) CALL(256, 4, true, true); else CALL(256, 4, false, true); } \
+      else return -1;                                                                           \
+    }                                                                                           \
   } while (0)
 
-#define ABYSS_TILE2_SWITCH(NT_, IPT_, ANCHOR_, CALL)                       \
-  do {                                                                     \
-    if (ANCHOR_) {                                                         \
-      if (NT_ == 128 && IPT_ == 2) CALL(128, 2, true);                     \
-      else if (NT_ == 128 && IPT_ == 4) CALL(128, 4, true);                \
-      else if (NT_ == 256 && IPT_ == 2) CALL(256, 2, true);                \
-      else if (NT_ == 256 && IPT_ == 4) CALL(256, 4, true);                \
-      else return -1;                                                      \
-    } else {                                                               \
-      if (NT_ == 128 && IPT_ == 2) CALL(128, 2, false);                    \
-      else if (NT_ == 128 && IPT_ == 4) CALL(128, 4, false);               \
-      else if (NT_ == 256 && IPT_ == 2) CALL(256, 2, false);               \
-      else if (NT_ == 256 && IPT_ == 4) CALL(256, 4, false);               \
-      else return -1;                                                      \
-    }                                                                      \
-  } while (0)
-
-int tile2_occupancy(int nt, int ipt, bool anchor) {
+int tile_occupancy(int nt, int ipt, bool anchor, bool pack) {
   int r = 0;
-#define OCC2_CALL(a, b, c) r = tile2_occupancy_impl<a, b, c>()
-  ABYSS_TILE2_SWITCH(nt, ipt, anchor, OCC2_CALL);
-#undef OCC2_CALL
-  return r;
-}
-
-int launch_tile2(cudaStream_t s, int nt, int ipt, bool anchor, int grid, const JSet &js,
-                 const Work &w, int n_iblocks) {
-#define LAUNCH2_CALL(a, b, c) tile2_launch_impl<a, b, c>(s, grid, js, w, n_iblocks)
-  ABYSS_TILE2_SWITCH(nt, ipt, anchor, LAUNCH2_CALL);
-#undef LAUNCH2_CALL
-  return 0;
-}
-
-int tile_occupancy(int nt, int ipt, bool anchor) {
-  int r = 0;
-#define OCC_CALL(a, b, c) r = tile_occupancy_impl<a, b, c>()
-  ABYSS_TILE_SWITCH(nt, ipt, anchor, OCC_CALL);
+#define OCC_CALL(a, b, c, d) r = tile_occupancy_impl<a, b, c, d>()
+  ABYSS_TILE_SWITCH(nt, ipt, anchor, pack, OCC_CALL);
 #undef OCC_CALL
   return r;
 }
 
-int launch_tile(cudaStream_t s, int nt, int ipt, bool anchor, int grid, const JSet &js,
+int launch_tile(cudaStream_t s, int nt, int ipt, bool anchor, bool pack, int grid, const JSet &js,
                 const Work &w, int n_iblocks) {
-#define LAUNCH_CALL(a, b, c) tile_launch_impl<a, b, c>(s, grid, js, w, n_iblocks)
-  ABYSS_TILE_SWITCH(nt, ipt, anchor, LAUNCH_CALL);
+#define LAUNCH_CALL(a, b, c, d) tile_launch_impl<a, b, c, d>(s, grid, js, w, n_iblocks)
+  ABYSS_TILE_SWITCH(nt, ipt, anchor, pack, LAUNCH_CALL);
 #undef LAUNCH_CALL
   return 0;
 }
@@ -1154,9 +977,14 @@ int launch_jmajor(cudaStream_t s, int mi, const JSet &js, const Work &w, int L) 
 }
 
 void launch_finalize(cudaStream_t s, const JSet &js, const Work &w, const Outputs &o, int sm_count) {
-  const int warps = w.m;
-  const int blocks = max(1, min((warps * 32 + 255) / 256, sm_count * 16));
-  finalize_rows<<<blocks, 256, 0, s>>>(js, w, o);
+  int P = 32;
+  while (P < w.cap) P <<= 1;
+  const int warps_per_block = 4;
+  const size_t smem = (size_t)warps_per_block * P * sizeof(int);
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(finalize_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const int blocks = max(1, min((w.m + warps_per_block - 1) / warps_per_block, sm_count * 32));
+  finalize_rows<<<blocks, 32 * warps_per_block, smem, s>>>(js, w, o, P);
 }
 
 void launch_energy(cudaStream_t s, int n, const double *x, const double *v, const double *mass,

@@ -22,12 +22,9 @@ size_t morton_temp_bytes(int m_cap);
 void launch_morton_order(cudaStream_t s, int m, const int *targets, const JSet &js, int *bbox,
                          uint32_t *keys, uint32_t *keys_alt, int *rows, int *rows_alt,
                          void *cub_tmp, size_t cub_bytes, int *order_t, int *order_o, int sm_count);
-int tile_occupancy(int nt, int ipt, bool anchor);
-int launch_tile(cudaStream_t s, int nt, int ipt, bool anchor, int grid, const JSet &js,
+int tile_occupancy(int nt, int ipt, bool anchor, bool pack);
+int launch_tile(cudaStream_t s, int nt, int ipt, bool anchor, bool pack, int grid, const JSet &js,
                 const Work &w, int n_iblocks);
-int tile2_occupancy(int nt, int ipt, bool anchor);
-int launch_tile2(cudaStream_t s, int nt, int ipt, bool anchor, int grid, const JSet &js,
-                 const Work &w, int n_iblocks);
 int launch_jmajor(cudaStream_t s, int mi, const JSet &js, const Work &w, int L);
 void launch_finalize(cudaStream_t s, const JSet &js, const Work &w, const Outputs &o, int sm_count);
 void launch_energy(cudaStream_t s, int n, const double *x, const double *v, const double *mass,

@@ -81,6 +81,7 @@ def ref():
         L.ref_set_globals.argtypes = [C.c_double, C.c_int, C.c_ulonglong]
         L.ref_set_particle.argtypes = [C.c_int, _dp, _dp, C.c_double, C.c_double, _dp, _dp, _dp,
                                        C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, _ip]
+        L.ref_set_all.argtypes = [C.c_int] + [_dp] * 8
         L.ref_set_blocks.argtypes = [C.c_int, C.c_ulonglong, C.c_ulonglong, C.c_ulonglong,
                                      C.c_ulonglong, C.c_int, C.c_int, C.c_ulonglong]
         L.ref_get_blocks.argtypes = [C.c_int, C.POINTER(C.c_ulonglong), _ip, _dp]

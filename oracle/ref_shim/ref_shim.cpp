@@ -121,6 +121,33 @@ void ref_set_particle(int i, const double *x, const double *v, double mass, doub
     for (int k = 0; k < nnb; ++k) p.Neighbors[k] = nb[k];
 }
 
+// Bulk form of ref_set_particle for large particle sets: x, v, a_tot [n][3][..]
+// arrays as in ref_set_particle; every particle gets no neighbour list, the
+// given times and steps, and zero regular/irregular derivatives.
+void ref_set_all(int n, const double *x, const double *v, const double *mass, const double *r2nb,
+                 const double *a_tot, const double *t_reg, const double *t_irr,
+                 const double *dt_reg) {
+    for (int i = 0; i < n; ++i) {
+        Particle &p = particles[i];
+        for (int d = 0; d < 3; ++d) {
+            p.Position[d] = x[3 * (size_t)i + d];
+            p.Velocity[d] = v[3 * (size_t)i + d];
+            for (int o = 0; o < 4; ++o) {
+                p.a_tot[d][o] = a_tot[12 * (size_t)i + 4 * d + o];
+                p.a_reg[d][o] = 0.0;
+                p.a_irr[d][o] = 0.0;
+            }
+        }
+        p.Mass = mass[i];
+        p.RadiusOfNeighbor = r2nb[i];
+        p.CurrentTimeReg = t_reg[i];
+        p.CurrentTimeIrr = t_irr[i];
+        p.TimeStepReg = dt_reg[i];
+        p.TimeStepIrr = dt_reg[i];
+        p.NumberOfNeighbor = 0;
+    }
+}
+
 void ref_set_blocks(int i, unsigned long long cur_reg, unsigned long long cur_irr,
                     unsigned long long tb_reg, unsigned long long tb_irr, int lvl_reg, int lvl_irr,
                     unsigned long long new_cur_irr) {

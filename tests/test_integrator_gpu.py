@@ -3,7 +3,7 @@
 * Every regular block of a Plummer run (the N = 1024 configuration's cluster,
   eps = 1e-4, ~32 neighbours, eta_reg = 0.02, eta_irr = 0.01) is re-done by the
   FP64 oracle on the same predicted j-set: lists bit-exact, forces within the
-  regular-force tolerances.
+  per-target bound of tests/test_regforce_gpu.py (|da| <= 1e-6 |a| + 1e-7 A).
 * Energy drift of short complete runs stays small.
 """
 import numpy as np
@@ -40,13 +40,18 @@ def test_every_regular_block_matches_oracle(rf):
         ref = oracle.reg_force(last["px"], last["pv"], c.m, last["r2nb"], EPS2, last["targets"], ac.nb_max)
         mm = first_list_mismatch(last["nnb"], last["list"], ref["nnb"], ref["list"])
         assert mm is None, f"block {blocks}: list mismatch {mm}"
-        worst_a = max(worst_a, row_rel_err(last["acc_reg"], ref["acc_reg"]).max())
-        worst_j = max(worst_j, row_rel_err(last["jerk_reg"], ref["jerk_reg"]).max())
+        sa, sj = oracle.reg_scale(last["px"], last["pv"], c.m, last["r2nb"], EPS2, last["targets"])
+        na = np.linalg.norm(ref["acc_reg"], axis=1)
+        nj = np.linalg.norm(ref["jerk_reg"], axis=1)
+        da = np.linalg.norm(last["acc_reg"] - ref["acc_reg"], axis=1)
+        dj = np.linalg.norm(last["jerk_reg"] - ref["jerk_reg"], axis=1)
+        worst_a = max(worst_a, (da / (1e-6 * na + 1e-7 * sa)).max())
+        worst_j = max(worst_j, (dj / (1e-5 * nj + 1e-6 * sj)).max())
         if done:
             break
     print(f"{blocks} blocks to code time {ac.time:.4g}: worst acc {worst_a:.2e} jerk {worst_j:.2e}; "
           f"stats {ac.stats()}")
-    assert worst_a <= 1e-6 and worst_j <= 1e-5
+    assert worst_a <= 1.0 and worst_j <= 1.0  # in units of the per-target bound
 
 
 def test_short_run_energy_conservation(rf):

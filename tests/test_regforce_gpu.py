@@ -3,8 +3,14 @@
 Bar (written here, checked below):
   * neighbour lists and counts: bit-exact against the FP64 oracle
     (rule r2 < R_nb^2, self excluded, ascending index);
-  * regular acceleration: per-target relative error <= ACC_TOL;
-  * regular jerk: per-target relative error <= JERK_TOL;
+  * regular acceleration, per target i:  |da_i| <= 1e-6 |a_i| + 1e-7 A_i,
+    where A_i = sum_j |m_j r_ij^-3 x_ij| over the regular j.  The first term is
+    the 1e-6 relative tolerance; the second is the rounding floor of any FP32
+    pair sum (about 2 FP32 ulps of the summed magnitudes) and only matters for
+    targets whose terms cancel (A_i >> |a_i|);
+  * regular jerk, the same with 1e-5 and 1e-6;
+  * norm-wise over all targets of a call: ||da|| / ||a|| <= 1e-6 (acc) and
+    <= 1e-5 (jerk);
   * irregular part (FP64 on the device): <= 1e-12 relative.
 """
 import numpy as np
@@ -45,24 +51,28 @@ def rf():
     r.close()
 
 
-def check(res, ref, tag, acc_tol=ACC_TOL, jerk_tol=JERK_TOL, scale=None):
-    """Lists exact; per-target relative errors within tolerance.  With `scale`
-    (degenerate inputs: a handful of particles, or R_nb = 0 so that the closest
-    pairs enter the regular sum) the error is measured against the sum of the
-    magnitudes of the terms, the scale of an FP32 pair sum's rounding error,
-    because there the sum itself may cancel to far below its terms."""
+def check(res, ref, tag, scale, acc_tol=ACC_TOL, jerk_tol=JERK_TOL):
+    """Lists exact; forces within the bar in the module docstring.  `scale` is
+    (A, J): per-target sums of the magnitudes of the regular acc / jerk terms."""
     mm = first_list_mismatch(res.nnb, res.list, ref["nnb"], ref["list"])
     assert mm is None, f"{tag}: list mismatch at row {mm}"
-    if scale is None:
-        ea = row_rel_err(res.acc_reg, ref["acc_reg"])
-        ej = row_rel_err(res.jerk_reg, ref["jerk_reg"])
-    else:
-        ea = np.linalg.norm(res.acc_reg - ref["acc_reg"], axis=1) / np.maximum(scale[0], 1e-300)
-        ej = np.linalg.norm(res.jerk_reg - ref["jerk_reg"], axis=1) / np.maximum(scale[1], 1e-300)
-    print(f"{tag}: acc max {ea.max():.2e} med {np.median(ea):.2e}  jerk max {ej.max():.2e} "
-          f"med {np.median(ej):.2e}  plan {res.plan}")
-    assert ea.max() <= acc_tol, f"{tag}: acc error {ea.max():.3e}"
-    assert ej.max() <= jerk_tol, f"{tag}: jerk error {ej.max():.3e}"
+    da = np.linalg.norm(res.acc_reg - ref["acc_reg"], axis=1)
+    dj = np.linalg.norm(res.jerk_reg - ref["jerk_reg"], axis=1)
+    na = np.linalg.norm(ref["acc_reg"], axis=1)
+    nj = np.linalg.norm(ref["jerk_reg"], axis=1)
+    ea = da / np.maximum(acc_tol * na + 0.1 * acc_tol * scale[0], 1e-300)
+    ej = dj / np.maximum(jerk_tol * nj + 0.1 * jerk_tol * scale[1], 1e-300)
+    rel_a = row_rel_err(res.acc_reg, ref["acc_reg"])
+    rel_j = row_rel_err(res.jerk_reg, ref["jerk_reg"])
+    norm_a = np.linalg.norm(da) / max(np.linalg.norm(na), 1e-300)
+    norm_j = np.linalg.norm(dj) / max(np.linalg.norm(nj), 1e-300)
+    print(f"{tag}: rel acc max {rel_a.max():.2e} med {np.median(rel_a):.2e} norm {norm_a:.2e} | "
+          f"jerk max {rel_j.max():.2e} med {np.median(rel_j):.2e} norm {norm_j:.2e} | "
+          f"bound use acc {ea.max():.2f} jerk {ej.max():.2f} | plan {res.plan}")
+    assert ea.max() <= 1.0, f"{tag}: acc error {ea.max():.2f} x the bound"
+    assert ej.max() <= 1.0, f"{tag}: jerk error {ej.max():.2f} x the bound"
+    if na.size > 16:
+        assert norm_a <= acc_tol and norm_j <= jerk_tol, f"{tag}: norm-wise {norm_a:.2e} {norm_j:.2e}"
     has = ref["nnb"] > 0
     if has.any():
         ei = row_rel_err(res.acc_irr[has], ref["acc_irr"][has])
@@ -80,7 +90,7 @@ def test_golden_reference_outputs(rf, name, tag, tuning):
     ref = dict(nnb=g["out_nnb"], list=g["out_list"], acc_reg=g["out_a_reg"][:, :, 0],
                jerk_reg=g["out_a_reg"][:, :, 1], acc_irr=g["out_a_irr"][:, :, 0],
                jerk_irr=g["out_a_irr"][:, :, 1])
-    check(res, ref, f"{name}/{tag}")
+    check(res, ref, f"{name}/{tag}", oracle.reg_scale(g["px"], g["pv"], g["m"], g["r2nb"], 0.0, g["targets"]))
 
 
 @pytest.mark.parametrize("name", ["ref_plummer1024_s1.npz", "ref_king2048_s3.npz"])
@@ -104,7 +114,7 @@ def test_softened_plummer_vs_oracle(rf, tag, tuning):
     rf.send_to_device(c.m, c.x, c.v, c.r2nb)
     res = rf.calculate_acceleration(t, eps2=1e-8, list_cap=256, tuning=tuning)
     ref = oracle.reg_force(c.x, c.v, c.m, c.r2nb, 1e-8, t, 256)
-    check(res, ref, f"plummer3000-eps/{tag}")
+    check(res, ref, f"plummer3000-eps/{tag}", oracle.reg_scale(c.x, c.v, c.m, c.r2nb, 1e-8, t))
 
 
 @pytest.mark.parametrize("m", [1, 2, 3, 31, 33, 64, 65, 257, 4095, 4096, 10000])
@@ -114,7 +124,7 @@ def test_active_block_sizes_auto(rf, m):
     rf.send_to_device(c.m, c.x, c.v, c.r2nb)
     res = rf.calculate_acceleration(t, eps2=1e-8, list_cap=256)
     ref = oracle.reg_force(c.x, c.v, c.m, c.r2nb, 1e-8, t, 256)
-    check(res, ref, f"king12000/m={m}")
+    check(res, ref, f"king12000/m={m}", oracle.reg_scale(c.x, c.v, c.m, c.r2nb, 1e-8, t))
 
 
 @pytest.mark.parametrize("split", [1, 2, 3, 7, 40])
@@ -123,10 +133,11 @@ def test_forced_j_splits(rf, split):
     t = np.arange(0, c.n, 3, dtype=np.int32)
     rf.send_to_device(c.m, c.x, c.v, c.r2nb)
     ref = oracle.reg_force(c.x, c.v, c.m, c.r2nb, 0.0, t, 256)
+    scale = oracle.reg_scale(c.x, c.v, c.m, c.r2nb, 0.0, t)
     for tu in (dict(kernel=1, mode=2, j_split=split), dict(kernel=1, mode=1, j_split=split),
                dict(kernel=2, ipt=8, j_split=split), dict(kernel=3, mode=2, j_split=split)):
         res = rf.calculate_acceleration(t, eps2=0.0, list_cap=256, tuning=tu)
-        check(res, ref, f"split{split}/{tu}")
+        check(res, ref, f"split{split}/{tu}", scale)
 
 
 def test_unsorted_and_repeated_targets(rf):
@@ -135,9 +146,10 @@ def test_unsorted_and_repeated_targets(rf):
     t = rng.integers(0, c.n, 900).astype(np.int32)  # unsorted, with repeats
     rf.send_to_device(c.m, c.x, c.v, c.r2nb)
     ref = oracle.reg_force(c.x, c.v, c.m, c.r2nb, 0.0, t, 256)
+    scale = oracle.reg_scale(c.x, c.v, c.m, c.r2nb, 0.0, t)
     for tu in (TILE_DS, TILE_ANCHOR, JMAJOR, PACKED):
         res = rf.calculate_acceleration(t, 0.0, 256, tu)
-        check(res, ref, f"unsorted/{tu}")
+        check(res, ref, f"unsorted/{tu}", scale)
 
 
 def test_no_neighbours_and_all_neighbours(rf):
@@ -151,7 +163,7 @@ def test_no_neighbours_and_all_neighbours(rf):
     for tu in (TILE_DS, TILE_ANCHOR, JMAJOR, PACKED):
         res = rf.calculate_acceleration(t, 1e-8, 64, tu)
         assert res.nnb.sum() == 0
-        check(res, ref, f"R=0/{tu}", scale=scale)
+        check(res, ref, f"R=0/{tu}", scale)
     # R_nb huge: every j is a neighbour, lists overflow a small cap with exact counts
     big = np.full(c.n, 1e6)
     rf.send_to_device(c.m, c.x, c.v, big)
@@ -173,7 +185,7 @@ def test_tiny_and_ragged_jsets(rf, n):
     scale = oracle.reg_scale(c.x, c.v, c.m, c.r2nb, 0.0, t)
     for tu in (TILE_DS, TILE_ANCHOR, JMAJOR, PACKED):
         res = rf.calculate_acceleration(t, 0.0, 32, tu)
-        check(res, ref, f"n={n}/{tu}", scale=scale)
+        check(res, ref, f"n={n}/{tu}", scale)
 
 
 def test_bad_arguments_are_reported_not_trapped(rf):
@@ -206,7 +218,8 @@ def test_anchor_mode_on_dense_active_set(rf, kernel, threads, ipt):
                                     tuning=dict(kernel=kernel, mode=1, threads=threads, ipt=ipt))
     sample = np.random.default_rng(4).choice(c.n, 2048, replace=False)
     ref = oracle.reg_force(c.x, c.v, c.m, c.r2nb, 1e-8, t[sample], 256)
+    scale = oracle.reg_scale(c.x, c.v, c.m, c.r2nb, 1e-8, t[sample])
     sub = type(res)(res.acc_reg[sample], res.jerk_reg[sample], res.acc_irr[sample],
                     res.jerk_irr[sample], res.nnb[sample], res.list[sample], plan=res.plan)
-    check(sub, ref, f"king65536-anchor-k{kernel}-{threads}x{ipt}")
+    check(sub, ref, f"king65536-anchor-k{kernel}-{threads}x{ipt}", scale)
     assert np.all(res.nnb == 80)
