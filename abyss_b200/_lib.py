@@ -31,7 +31,7 @@ class Tuning(C.Structure):
     """abyss_tuning: launch shape (zero = automatic)."""
 
     _fields_ = [("kernel", C.c_int), ("mode", C.c_int), ("threads", C.c_int), ("ipt", C.c_int),
-                ("j_split", C.c_int), ("grid", C.c_int)]
+                ("j_split", C.c_int), ("grid", C.c_int), ("unroll", C.c_int), ("min_blocks", C.c_int)]
 
     def as_dict(self):
         return {f: int(getattr(self, f)) for f, _ in self._fields_}
@@ -96,6 +96,7 @@ def lib():
     L.abyss_last_timing.argtypes = [_vp, _fp]
     L.abyss_set_tuning_table.argtypes = [_vp, C.c_int, _ip, C.POINTER(Tuning)]
     L.abyss_energy.argtypes = [_vp, C.c_int, _dp, _dp, _dp, C.c_double, _dp]
+    L.abyss_tile_variant.argtypes = [C.c_int, _ip]
     # reference-compatible drop-in
     L.InitializeDevice.argtypes = [_ip]
     L.OpenDevice.argtypes = [_ip]

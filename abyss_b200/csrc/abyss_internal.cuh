@@ -11,7 +11,7 @@
 //   order_t, order_o int [m]            target particle / output row in processing order
 //   lcnt    int    [m]                  neighbours found per target (atomic append)
 //   lst     int    [m][cap]             entries in the order found (any chunk order)
-//   part    double [S][m][6]            per-chunk regular acc (3) + jerk (3)
+//   part    double [m][S][6]            per-chunk regular acc (3) + jerk (3)
 //   outputs acc_reg, jerk_reg, acc_irr, jerk_irr double [m][3]; nnb int [m];
 //           list int [m][cap]           (final, ascending j, truncated at cap)
 #pragma once
@@ -39,6 +39,15 @@ struct JSet {
   int n;
 };
 
+// One (target slice, j-range) unit of a batched launch over many clusters.
+struct WorkItem {
+  int t_begin;  // first entry in the order arrays
+  int t_count;  // targets in the slice (<= threads x targets per thread)
+  int j0, j1;   // j-range (the cluster's particles, or a chunk of them)
+  int ch;       // chunk index of this j-range within the cluster
+  int pad[3];
+};
+
 struct Work {
   const int *order_t;   // [m] target particle index, processing order
   const int *order_o;   // [m] output row, processing order
@@ -50,9 +59,16 @@ struct Work {
   double eps2;
   int *lcnt;            // [m] neighbours found per target (atomic, exact)
   int *lst;             // [m][cap] neighbours in the order found
-  double *part;         // [S][m][6]
+  double *part;         // [m][s_stride][6]
   int *status;          // error bits
   int *item_counter;    // work-queue head of the tile kernel
+  int s_stride;         // partial-sum slots per row: part[(row * s_stride + ch) * 6]
+  // batched launches (null/zero for a single cluster):
+  const WorkItem *items;     // explicit work list
+  const int *n_items_dev;    // its length, read on the device
+  const int *m_dev;          // number of rows, read on the device
+  const int *row_nchunks;    // chunks per row (else n_chunks)
+  const int *row_joff;       // first particle of the row's cluster (lists are cluster-local)
 };
 
 struct Outputs {

@@ -158,6 +158,13 @@ static int ensure_outputs(abyss_ctx *c, int m, int cap) {
   return ABYSS_OK;
 }
 
+namespace abyss {
+// accessors used by the batched-ensemble layer (ensemble.cu)
+cudaStream_t ctx_stream(abyss_ctx *c) { return c->stream; }
+int ctx_device(abyss_ctx *c) { return c->device; }
+int ctx_sm_count(abyss_ctx *c) { return c->sm_count; }
+}  // namespace abyss
+
 extern "C" {
 
 int abyss_create(int device, abyss_ctx **out) {
@@ -339,6 +346,8 @@ static abyss_tuning plan_for(abyss_ctx *c, int m, const abyss_tuning *user) {
         if (t.ipt == 0) t.ipt = e.ipt;
         if (t.j_split == 0) t.j_split = e.j_split;
         if (t.grid == 0) t.grid = e.grid;
+        if (t.unroll == 0) t.unroll = e.unroll;
+        if (t.min_blocks == 0) t.min_blocks = e.min_blocks;
         break;
       }
   }
@@ -378,7 +387,7 @@ int abyss_launch(abyss_ctx *c, double eps2, int list_cap, const abyss_tuning *tu
   } else if (t.kernel == 1 || t.kernel == 3) {
     const int per_block = t.threads * t.ipt;
     n_iblocks = (m + per_block - 1) / per_block;
-    const int occ = tile_occupancy(t.threads, t.ipt, t.mode == 1, t.kernel == 3);
+    const int occ = tile_occupancy(t.threads, t.ipt, t.mode == 1, t.kernel == 3, t.unroll, t.min_blocks);
     if (occ <= 0) return fail(c, ABYSS_ERR_ARG, "launch: unsupported tile shape");
     // persistent grid: every SM holds the same number of CTAs, which take
     // (i-block, j-chunk) items from a device counter
@@ -421,6 +430,12 @@ int abyss_launch(abyss_ctx *c, double eps2, int list_cap, const abyss_tuning *tu
   w.part = c->part.p;
   w.status = c->status.p;
   w.item_counter = c->items.p;
+  w.s_stride = S;
+  w.items = nullptr;
+  w.n_items_dev = nullptr;
+  w.m_dev = nullptr;
+  w.row_nchunks = nullptr;
+  w.row_joff = nullptr;
 
   if (c->profiling) CK(cudaEventRecord(c->ev[0], c->stream), "event");
   if ((t.kernel == 1 || t.kernel == 3) && t.mode == 1) {
@@ -444,7 +459,8 @@ int abyss_launch(abyss_ctx *c, double eps2, int list_cap, const abyss_tuning *tu
   }
   if (c->profiling) CK(cudaEventRecord(c->ev[1], c->stream), "event");
   if (t.kernel == 1 || t.kernel == 3) {
-    if (launch_tile(c->stream, t.threads, t.ipt, t.mode == 1, t.kernel == 3, grid, js, w, n_iblocks) != 0)
+    if (launch_tile(c->stream, t.threads, t.ipt, t.mode == 1, t.kernel == 3, t.unroll, t.min_blocks, grid, js,
+                    w, n_iblocks) != 0)
       return fail(c, ABYSS_ERR_ARG, "launch: unsupported tile shape");
     t.grid = grid;
   } else {
@@ -511,6 +527,13 @@ int abyss_regular_force(abyss_ctx *c, int m, const int *targets, double eps2, in
   rc = abyss_launch(c, eps2, list_cap, tuning);
   if (rc != ABYSS_OK) return rc;
   return abyss_fetch(c, acc_reg, jerk_reg, acc_irr, jerk_irr, nnb, list, overflow_rows);
+}
+
+int abyss_tile_variants(void) { return tile_variant_count(); }
+
+int abyss_tile_variant(int i, int *shape6) {
+  if (!shape6) return ABYSS_ERR_ARG;
+  return tile_variant_shape(i, shape6) == 0 ? ABYSS_OK : ABYSS_ERR_ARG;
 }
 
 int abyss_last_plan(const abyss_ctx *c, abyss_tuning *plan, int *n_chunks) {

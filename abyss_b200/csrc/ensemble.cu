@@ -1,0 +1,510 @@
+// Batched regular force over an ensemble of independent clusters
+// (include/abyss_ens.h).
+//
+// All clusters live in one set of device arrays (cluster k owns particles
+// [off_k, off_k + n_k)).  A wave lists (cluster, targets) blocks; the host turns
+// it into a work list of (target slice, j-chunk) items sorted longest first,
+// and the device runs
+//     predict_multi   every active cluster to its own time
+//     reg_force_tile  one persistent launch draining the work list
+//     finalize_rows   FP64 sums, sorted cluster-local lists, irregular part
+// Counts (rows, items) are read on the device, so the same three kernels can
+// be captured once into a CUDA graph and replayed for every wave.
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/abyss_ens.h"
+#include "../../include/abyss_reg.h"
+#include "abyss_internal.cuh"
+#include "kernels.cuh"
+
+using namespace abyss;
+
+namespace {
+constexpr int kSMax = 16;   // j-chunks per cluster at most
+constexpr int kTJ = 128;
+
+template <class T>
+struct Buf {
+  T *p = nullptr;
+  size_t n = 0;
+  cudaError_t alloc(size_t count) {
+    n = std::max<size_t>(count, 1) + kPad;
+    return cudaMalloc((void **)&p, n * sizeof(T));
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+  }
+};
+}  // namespace
+
+struct abyss_ens {
+  abyss_ctx *ctx = nullptr;
+  cudaStream_t stream = nullptr;
+  int device = 0, sm_count = 148;
+  int nc = 0, n_total = 0, cap = 0;
+  std::vector<int> n_k, off_k;
+  long long bytes = 0;
+  // state and predicted j-set
+  Buf<double> x, v, a0, a1, t0, mass, r2nb, px, py, pz, pvx, pvy, pvz;
+  Buf<float4> vm;
+  Buf<int> cid, active;
+  Buf<double> new_time, scale;
+  // wave
+  Buf<int> order_t, order_o, row_nch, row_joff, counts;  // counts: [0] rows, [1] items
+  Buf<WorkItem> items;
+  size_t items_cap = 0;
+  // work and outputs
+  Buf<int> lcnt, lst, status, ovf, qhead, list, nnb;
+  Buf<double> part, acc_reg, jerk_reg, acc_irr, jerk_irr;
+  // host wave description
+  int rows = 0, n_items = 0, launches = 0;
+  std::vector<int> h_order, h_nch, h_joff, h_active;
+  std::vector<double> h_time, h_scale;
+  std::vector<WorkItem> h_items;
+  std::vector<int> wave_clusters, wave_rows_begin, wave_m;
+  std::vector<std::vector<WorkItem>> cluster_items;  // plain mode, slices relative to the cluster's rows
+  // launch shape
+  abyss_tuning shape{};
+  int grid = 0;
+  // graph
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  abyss_tuning graph_shape{};
+  double graph_eps2 = -1.0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::string err;
+};
+
+namespace {
+
+int efail(abyss_ens *e, int code, const std::string &m) {
+  if (e) e->err = m;
+  return code;
+}
+
+#define ECK(expr, what)                                                                          \
+  do {                                                                                           \
+    cudaError_t _e = (expr);                                                                     \
+    if (_e != cudaSuccess)                                                                       \
+      return efail(e, _e == cudaErrorMemoryAllocation ? ABYSS_ERR_OOM : ABYSS_ERR_CUDA,          \
+                   std::string(what) + ": " + cudaGetErrorString(_e));                           \
+  } while (0)
+
+JSet jset_of(abyss_ens *e) {
+  JSet js;
+  js.px = e->px.p;
+  js.py = e->py.p;
+  js.pz = e->pz.p;
+  js.vm = e->vm.p;
+  js.pvx = e->pvx.p;
+  js.pvy = e->pvy.p;
+  js.pvz = e->pvz.p;
+  js.mass = e->mass.p;
+  js.r2nb = e->r2nb.p;
+  js.n = e->n_total;
+  return js;
+}
+
+// Work and outputs of the batched wave (device counts) or of one cluster
+// (plain mode: row and item pointers offset to the cluster's slice).
+void make_work(abyss_ens *e, double eps2, int row_begin, const WorkItem *items, const int *n_items_dev,
+               const int *m_dev, int m_host, Work &w, Outputs &o) {
+  w.order_t = e->order_t.p + row_begin;
+  w.order_o = e->order_o.p;  // identity rows; slices index from 0
+  w.m = m_host;
+  w.n_chunks = kSMax;
+  w.chunk_len = 0;
+  w.cap = e->cap;
+  w.eps2 = eps2;
+  w.eps2f = (float)eps2;
+  w.lcnt = e->lcnt.p + row_begin;
+  w.lst = e->lst.p + (size_t)row_begin * e->cap;
+  w.part = e->part.p + (size_t)row_begin * kSMax * 6;
+  w.status = e->status.p;
+  w.item_counter = e->qhead.p;
+  w.s_stride = kSMax;
+  w.items = items;
+  w.n_items_dev = n_items_dev;
+  w.m_dev = m_dev;
+  w.row_nchunks = e->row_nch.p + row_begin;
+  w.row_joff = e->row_joff.p + row_begin;
+  o.targets = e->order_t.p + row_begin;
+  o.acc_reg = e->acc_reg.p + 3 * (size_t)row_begin;
+  o.jerk_reg = e->jerk_reg.p + 3 * (size_t)row_begin;
+  o.acc_irr = e->acc_irr.p + 3 * (size_t)row_begin;
+  o.jerk_irr = e->jerk_irr.p + 3 * (size_t)row_begin;
+  o.nnb = e->nnb.p + row_begin;
+  o.list = e->list.p + (size_t)row_begin * e->cap;
+  o.overflow_rows = e->ovf.p;
+}
+
+// The batched wave: reset, predict, one tile launch, finalize.  Everything
+// depends only on device memory and fixed pointers, so it can be captured.
+int enqueue_batched(abyss_ens *e, double eps2) {
+  cudaStream_t s = e->stream;
+  ECK(cudaMemsetAsync(e->qhead.p, 0, sizeof(int), s), "reset queue");
+  ECK(cudaMemsetAsync(e->status.p, 0, sizeof(int), s), "reset status");
+  ECK(cudaMemsetAsync(e->ovf.p, 0, sizeof(int), s), "reset overflow");
+  ECK(cudaMemsetAsync(e->lcnt.p, 0, sizeof(int) * (size_t)e->n_total, s), "reset list counts");
+  launch_predict_multi(s, e->n_total, e->cid.p, e->active.p, e->new_time.p, e->scale.p, e->x.p, e->v.p,
+                       e->a0.p, e->a1.p, e->t0.p, e->mass.p, e->px.p, e->py.p, e->pz.p, e->pvx.p,
+                       e->pvy.p, e->pvz.p, e->vm.p, e->sm_count);
+  JSet js = jset_of(e);
+  Work w;
+  Outputs o;
+  make_work(e, eps2, 0, e->items.p, e->counts.p + 1, e->counts.p, e->n_total, w, o);
+  if (launch_tile(s, e->shape.threads, e->shape.ipt, e->shape.mode == 1, e->shape.kernel == 3, e->shape.unroll,
+                  e->shape.min_blocks, e->grid, js, w, 0) != 0)
+    return efail(e, ABYSS_ERR_ARG, "unsupported tile shape");
+  launch_finalize_grid(s, js, w, o, e->sm_count * 32);
+  ECK(cudaGetLastError(), "batched wave launch");
+  return ABYSS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int abyss_ens_create(abyss_ctx *ctx, int n_clusters, const int *n_per_cluster, int list_cap,
+                     abyss_ens **out) {
+  if (!ctx || n_clusters <= 0 || !n_per_cluster || list_cap <= 0 || list_cap > 8192 || !out)
+    return ABYSS_ERR_ARG;
+  for (int k = 0; k < n_clusters; ++k)
+    if (n_per_cluster[k] < 2) return ABYSS_ERR_ARG;
+  abyss_ens *e = new abyss_ens;
+  e->ctx = ctx;
+  e->stream = ctx_stream(ctx);
+  e->device = ctx_device(ctx);
+  e->sm_count = ctx_sm_count(ctx);
+  cudaSetDevice(e->device);
+  e->nc = n_clusters;
+  e->cap = list_cap;
+  e->n_k.assign(n_per_cluster, n_per_cluster + n_clusters);
+  e->off_k.resize(n_clusters);
+  long long tot = 0;
+  for (int k = 0; k < n_clusters; ++k) {
+    e->off_k[k] = (int)tot;
+    tot += n_per_cluster[k];
+  }
+  if (tot > (1ll << 30)) {
+    delete e;
+    return ABYSS_ERR_ARG;
+  }
+  e->n_total = (int)tot;
+  const size_t n = e->n_total;
+  e->shape.kernel = 3;
+  e->shape.mode = 2;
+  e->shape.threads = 128;
+  e->shape.ipt = 2;
+  size_t items_cap = 0;
+  for (int k = 0; k < n_clusters; ++k) items_cap += (size_t)((n_per_cluster[k] + 127) / 128) * kSMax;
+  e->items_cap = items_cap;
+  cudaError_t err = cudaSuccess;
+  auto A = [&](auto &b, size_t count) {
+    if (err == cudaSuccess) {
+      err = b.alloc(count);
+      e->bytes += (long long)b.n * (long long)sizeof(*b.p);
+    }
+  };
+  A(e->x, 3 * n); A(e->v, 3 * n); A(e->a0, 3 * n); A(e->a1, 3 * n);
+  A(e->t0, n); A(e->mass, n + 2); A(e->r2nb, n + 2);
+  A(e->px, n + 2); A(e->py, n + 2); A(e->pz, n + 2); A(e->pvx, n + 2); A(e->pvy, n + 2); A(e->pvz, n + 2);
+  A(e->vm, n + 2); A(e->cid, n); A(e->active, n_clusters); A(e->new_time, n_clusters); A(e->scale, n_clusters);
+  A(e->order_t, n); A(e->order_o, n); A(e->row_nch, n); A(e->row_joff, n); A(e->counts, 2);
+  A(e->items, 2 * items_cap);  // the batched list, then per-cluster lists of the plain mode
+  A(e->lcnt, n); A(e->lst, n * (size_t)list_cap); A(e->status, 1); A(e->ovf, 1); A(e->qhead, 1);
+  A(e->list, n * (size_t)list_cap); A(e->nnb, n);
+  A(e->part, n * (size_t)kSMax * 6);
+  A(e->acc_reg, 3 * n); A(e->jerk_reg, 3 * n); A(e->acc_irr, 3 * n); A(e->jerk_irr, 3 * n);
+  if (err == cudaSuccess) err = cudaEventCreate(&e->ev0);
+  if (err == cudaSuccess) err = cudaEventCreate(&e->ev1);
+  if (err != cudaSuccess) {
+    abyss_ens_destroy(e);
+    return err == cudaErrorMemoryAllocation ? ABYSS_ERR_OOM : ABYSS_ERR_CUDA;
+  }
+  // cluster id per particle, identity rows
+  std::vector<int> cid(n), iota(n);
+  for (int k = 0; k < n_clusters; ++k)
+    std::fill(cid.begin() + e->off_k[k], cid.begin() + e->off_k[k] + n_per_cluster[k], k);
+  std::iota(iota.begin(), iota.end(), 0);
+  cudaMemcpy(e->cid.p, cid.data(), n * 4, cudaMemcpyHostToDevice);
+  cudaMemcpy(e->order_o.p, iota.data(), n * 4, cudaMemcpyHostToDevice);
+  cudaMemset(e->active.p, 0, sizeof(int) * n_clusters);
+  e->h_active.assign(n_clusters, 0);
+  e->h_time.assign(n_clusters, 0.0);
+  e->h_scale.assign(n_clusters, 1.0);
+  const int occ = tile_occupancy(e->shape.threads, e->shape.ipt, e->shape.mode == 1, e->shape.kernel == 3,
+                                 e->shape.unroll, e->shape.min_blocks);
+  e->grid = std::max(1, occ) * e->sm_count;
+  if (cudaDeviceSynchronize() != cudaSuccess) {
+    abyss_ens_destroy(e);
+    return ABYSS_ERR_CUDA;
+  }
+  *out = e;
+  return ABYSS_OK;
+}
+
+int abyss_ens_destroy(abyss_ens *e) {
+  if (!e) return ABYSS_ERR_ARG;
+  cudaSetDevice(e->device);
+  if (e->stream) cudaStreamSynchronize(e->stream);
+  if (e->graph_exec) cudaGraphExecDestroy(e->graph_exec);
+  if (e->graph) cudaGraphDestroy(e->graph);
+  Buf<double> *d[] = {&e->x, &e->v, &e->a0, &e->a1, &e->t0, &e->mass, &e->r2nb, &e->px, &e->py, &e->pz,
+                      &e->pvx, &e->pvy, &e->pvz, &e->new_time, &e->scale, &e->part, &e->acc_reg,
+                      &e->jerk_reg, &e->acc_irr, &e->jerk_irr};
+  for (auto *b : d) b->release();
+  Buf<int> *i[] = {&e->cid, &e->active, &e->order_t, &e->order_o, &e->row_nch, &e->row_joff, &e->counts,
+                   &e->lcnt, &e->lst, &e->status, &e->ovf, &e->qhead, &e->list, &e->nnb};
+  for (auto *b : i) b->release();
+  e->vm.release();
+  e->items.release();
+  if (e->ev0) cudaEventDestroy(e->ev0);
+  if (e->ev1) cudaEventDestroy(e->ev1);
+  delete e;
+  return ABYSS_OK;
+}
+
+long long abyss_ens_device_bytes(const abyss_ens *e) { return e ? e->bytes : 0; }
+
+int abyss_ens_upload_state(abyss_ens *e, int k, const double *x, const double *v, const double *a0,
+                           const double *a1, const double *t0, const double *mass, const double *r2nb) {
+  if (!e || k < 0 || k >= e->nc || !x || !v || !a0 || !a1 || !t0 || !mass || !r2nb) return ABYSS_ERR_ARG;
+  cudaSetDevice(e->device);
+  const size_t off = e->off_k[k], n = e->n_k[k];
+  cudaStream_t s = e->stream;
+  ECK(cudaMemcpyAsync(e->x.p + 3 * off, x, 24 * n, cudaMemcpyHostToDevice, s), "H2D x");
+  ECK(cudaMemcpyAsync(e->v.p + 3 * off, v, 24 * n, cudaMemcpyHostToDevice, s), "H2D v");
+  ECK(cudaMemcpyAsync(e->a0.p + 3 * off, a0, 24 * n, cudaMemcpyHostToDevice, s), "H2D a0");
+  ECK(cudaMemcpyAsync(e->a1.p + 3 * off, a1, 24 * n, cudaMemcpyHostToDevice, s), "H2D a1");
+  ECK(cudaMemcpyAsync(e->t0.p + off, t0, 8 * n, cudaMemcpyHostToDevice, s), "H2D t0");
+  ECK(cudaMemcpyAsync(e->mass.p + off, mass, 8 * n, cudaMemcpyHostToDevice, s), "H2D mass");
+  ECK(cudaMemcpyAsync(e->r2nb.p + off, r2nb, 8 * n, cudaMemcpyHostToDevice, s), "H2D r2nb");
+  ECK(cudaStreamSynchronize(s), "upload");
+  return ABYSS_OK;
+}
+
+int abyss_ens_set_wave(abyss_ens *e, int nk, const int *clusters, const double *new_time,
+                       const double *time_scale, const int *m_per, const int *targets_local) {
+  if (!e || nk <= 0 || !clusters || !new_time || !time_scale || !m_per || !targets_local)
+    return efail(e, ABYSS_ERR_ARG, "set_wave: bad arguments");
+  cudaSetDevice(e->device);
+  std::vector<char> seen(e->nc, 0);
+  const int per_block = e->shape.threads * e->shape.ipt;
+  e->h_order.clear();
+  e->h_nch.clear();
+  e->h_joff.clear();
+  e->h_items.clear();
+  e->wave_clusters.assign(clusters, clusters + nk);
+  e->wave_rows_begin.assign(nk, 0);
+  e->wave_m.assign(m_per, m_per + nk);
+  e->cluster_items.assign(nk, {});
+  std::fill(e->h_active.begin(), e->h_active.end(), 0);
+  // spread the work over at least ~8 items per CTA in total
+  long long tot_blocks = 0;
+  for (int i = 0; i < nk; ++i) tot_blocks += (m_per[i] + per_block - 1) / per_block;
+  const long long want_items = 8ll * e->grid;
+  int split = (int)std::min<long long>(kSMax, std::max<long long>(1, (want_items + tot_blocks - 1) / std::max(1ll, tot_blocks)));
+  const int *tp = targets_local;
+  int row = 0;
+  for (int i = 0; i < nk; ++i) {
+    const int k = clusters[i];
+    if (k < 0 || k >= e->nc || seen[k]) return efail(e, ABYSS_ERR_ARG, "set_wave: bad or repeated cluster");
+    seen[k] = 1;
+    const int m = m_per[i], nkp = e->n_k[k], off = e->off_k[k];
+    if (m <= 0 || m > nkp) return efail(e, ABYSS_ERR_ARG, "set_wave: bad target count");
+    e->h_active[k] = 1;
+    e->h_time[k] = new_time[i];
+    e->h_scale[k] = time_scale[i];
+    // j-chunks: split (rounded to tiles) but never shorter than two tiles
+    int S = std::max(1, std::min(split, (nkp + 2 * kTJ - 1) / (2 * kTJ)));
+    int chunk = ((nkp + S - 1) / S + kTJ - 1) / kTJ * kTJ;
+    S = (nkp + chunk - 1) / chunk;
+    e->wave_rows_begin[i] = row;
+    for (int q = 0; q < m; ++q) {
+      const int t = tp[q];
+      if (t < 0 || t >= nkp) return efail(e, ABYSS_ERR_ARG, "set_wave: target index out of range");
+      e->h_order.push_back(off + t);
+      e->h_nch.push_back(S);
+      e->h_joff.push_back(off);
+    }
+    for (int b = 0; b < m; b += per_block)
+      for (int c = 0; c < S; ++c) {
+        WorkItem it{};
+        it.t_begin = row + b;
+        it.t_count = std::min(per_block, m - b);
+        it.j0 = off + c * chunk;
+        it.j1 = off + std::min(nkp, (c + 1) * chunk);
+        it.ch = c;
+        e->h_items.push_back(it);
+        WorkItem local = it;
+        local.t_begin = b;
+        e->cluster_items[i].push_back(local);
+      }
+    row += m;
+    tp += m;
+  }
+  // longest items first: the work queue then drains evenly
+  std::stable_sort(e->h_items.begin(), e->h_items.end(), [](const WorkItem &a, const WorkItem &b) {
+    return (long long)a.t_count * (a.j1 - a.j0) > (long long)b.t_count * (b.j1 - b.j0);
+  });
+  if (e->h_items.size() > e->items_cap) return efail(e, ABYSS_ERR_ARG, "set_wave: too many work items");
+  e->rows = row;
+  e->n_items = (int)e->h_items.size();
+  cudaStream_t s = e->stream;
+  const int counts[2] = {e->rows, e->n_items};
+  ECK(cudaMemcpyAsync(e->order_t.p, e->h_order.data(), 4 * (size_t)row, cudaMemcpyHostToDevice, s), "H2D order");
+  ECK(cudaMemcpyAsync(e->row_nch.p, e->h_nch.data(), 4 * (size_t)row, cudaMemcpyHostToDevice, s), "H2D nch");
+  ECK(cudaMemcpyAsync(e->row_joff.p, e->h_joff.data(), 4 * (size_t)row, cudaMemcpyHostToDevice, s), "H2D joff");
+  ECK(cudaMemcpyAsync(e->items.p, e->h_items.data(), sizeof(WorkItem) * e->h_items.size(),
+                      cudaMemcpyHostToDevice, s), "H2D items");
+  ECK(cudaMemcpyAsync(e->counts.p, counts, sizeof(counts), cudaMemcpyHostToDevice, s), "H2D counts");
+  ECK(cudaMemcpyAsync(e->active.p, e->h_active.data(), 4 * (size_t)e->nc, cudaMemcpyHostToDevice, s), "H2D active");
+  ECK(cudaMemcpyAsync(e->new_time.p, e->h_time.data(), 8 * (size_t)e->nc, cudaMemcpyHostToDevice, s), "H2D times");
+  ECK(cudaMemcpyAsync(e->scale.p, e->h_scale.data(), 8 * (size_t)e->nc, cudaMemcpyHostToDevice, s), "H2D scales");
+  ECK(cudaStreamSynchronize(s), "set_wave");  // host vectors may change after return
+  return ABYSS_OK;
+}
+
+int abyss_ens_launch(abyss_ens *e, double eps2, int mode, const abyss_tuning *tuning) {
+  if (!e || !(eps2 >= 0.0)) return efail(e, ABYSS_ERR_ARG, "launch: bad arguments");
+  if (e->rows <= 0) return efail(e, ABYSS_ERR_STATE, "launch: no wave set");
+  cudaSetDevice(e->device);
+  cudaStream_t s = e->stream;
+  if (tuning && tuning->kernel != 0) {
+    abyss_tuning t = *tuning;
+    if (t.kernel != 1 && t.kernel != 3) return efail(e, ABYSS_ERR_ARG, "launch: ensemble needs a tile kernel");
+    if (t.mode == 0) t.mode = 2;
+    if (t.threads == 0) t.threads = 128;
+    if (t.ipt == 0) t.ipt = t.kernel == 3 ? 2 : 1;
+    if (t.threads * t.ipt != e->shape.threads * e->shape.ipt)
+      return efail(e, ABYSS_ERR_ARG, "launch: targets per block must match the wave's work list");
+    const int occ = tile_occupancy(t.threads, t.ipt, t.mode == 1, t.kernel == 3, t.unroll, t.min_blocks);
+    if (occ <= 0) return efail(e, ABYSS_ERR_ARG, "launch: unsupported tile shape");
+    e->shape = t;
+    e->grid = occ * e->sm_count;
+  }
+  ECK(cudaEventRecord(e->ev0, s), "event");
+  if (mode == ABYSS_ENS_BATCHED) {
+    int rc = enqueue_batched(e, eps2);
+    if (rc != ABYSS_OK) return rc;
+    e->launches = 3;
+  } else if (mode == ABYSS_ENS_GRAPH) {
+    const bool same = e->graph_exec && e->graph_eps2 == eps2 &&
+                      std::memcmp(&e->graph_shape, &e->shape, sizeof(abyss_tuning)) == 0;
+    if (!same) {
+      if (e->graph_exec) cudaGraphExecDestroy(e->graph_exec);
+      if (e->graph) cudaGraphDestroy(e->graph);
+      e->graph_exec = nullptr;
+      e->graph = nullptr;
+      // attributes are set outside capture
+      (void)tile_occupancy(e->shape.threads, e->shape.ipt, e->shape.mode == 1, e->shape.kernel == 3,
+                           e->shape.unroll, e->shape.min_blocks);
+      ECK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
+      int rc = enqueue_batched(e, eps2);
+      cudaGraph_t g = nullptr;
+      cudaError_t ce = cudaStreamEndCapture(s, &g);
+      if (rc != ABYSS_OK) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+      }
+      ECK(ce, "end capture");
+      e->graph = g;
+      ECK(cudaGraphInstantiate(&e->graph_exec, g, 0), "instantiate graph");
+      e->graph_shape = e->shape;
+      e->graph_eps2 = eps2;
+    }
+    ECK(cudaGraphLaunch(e->graph_exec, s), "graph launch");
+    e->launches = 3;
+  } else if (mode == ABYSS_ENS_PLAIN) {
+    // one cluster per launch: predict the cluster, its own work list, its finalize
+    ECK(cudaMemsetAsync(e->status.p, 0, sizeof(int), s), "reset status");
+    ECK(cudaMemsetAsync(e->ovf.p, 0, sizeof(int), s), "reset overflow");
+    ECK(cudaMemsetAsync(e->lcnt.p, 0, sizeof(int) * (size_t)e->rows, s), "reset list counts");
+    JSet js = jset_of(e);
+    e->launches = 0;
+    for (size_t i = 0; i < e->wave_clusters.size(); ++i) {
+      const int k = e->wave_clusters[i];
+      const int rb = e->wave_rows_begin[i], m = e->wave_m[i];
+      const int off = e->off_k[k], nkp = e->n_k[k];
+      // the cluster's slice of the ensemble arrays
+      launch_predict(s, nkp, e->x.p + 3 * (size_t)off, e->v.p + 3 * (size_t)off, e->a0.p + 3 * (size_t)off,
+                     e->a1.p + 3 * (size_t)off, e->t0.p + off, e->mass.p + off, e->h_time[k], e->h_scale[k],
+                     e->px.p + off, e->py.p + off, e->pz.p + off, e->pvx.p + off, e->pvy.p + off,
+                     e->pvz.p + off, e->vm.p + off, e->sm_count);
+      const std::vector<WorkItem> &ci = e->cluster_items[i];
+      // per-cluster item list and count after the batched list in device memory
+      WorkItem *d_items = e->items.p + e->n_items;
+      int *d_cnt = e->counts.p;  // reused per cluster; ordered on the stream
+      const int cnts[2] = {m, (int)ci.size()};
+      if ((size_t)e->n_items + ci.size() > 2 * e->items_cap)
+        return efail(e, ABYSS_ERR_ARG, "launch: work list does not fit");
+      ECK(cudaMemcpyAsync(d_items, ci.data(), sizeof(WorkItem) * ci.size(), cudaMemcpyHostToDevice, s),
+          "H2D items");
+      ECK(cudaMemcpyAsync(d_cnt, cnts, sizeof(cnts), cudaMemcpyHostToDevice, s), "H2D counts");
+      ECK(cudaMemsetAsync(e->qhead.p, 0, sizeof(int), s), "reset queue");
+      Work w;
+      Outputs o;
+      make_work(e, eps2, rb, d_items, d_cnt + 1, d_cnt, m, w, o);
+      const int g = std::min(e->grid, (int)ci.size());
+      if (launch_tile(s, e->shape.threads, e->shape.ipt, e->shape.mode == 1, e->shape.kernel == 3,
+                      e->shape.unroll, e->shape.min_blocks, g, js, w, 0) != 0)
+        return efail(e, ABYSS_ERR_ARG, "unsupported tile shape");
+      launch_finalize_grid(s, js, w, o, std::max(1, std::min(e->sm_count * 32, (m + 3) / 4)));
+      e->launches += 3;
+      // the counts buffer is restored for later batched waves
+      const int all[2] = {e->rows, e->n_items};
+      ECK(cudaMemcpyAsync(d_cnt, all, sizeof(all), cudaMemcpyHostToDevice, s), "H2D counts");
+      ECK(cudaStreamSynchronize(s), "plain cluster");  // host arrays reused per cluster
+    }
+    ECK(cudaGetLastError(), "plain launches");
+  } else {
+    return efail(e, ABYSS_ERR_ARG, "launch: unknown mode");
+  }
+  ECK(cudaEventRecord(e->ev1, s), "event");
+  return ABYSS_OK;
+}
+
+int abyss_ens_fetch(abyss_ens *e, double *acc_reg, double *jerk_reg, double *acc_irr, double *jerk_irr,
+                    int *nnb, int *list, int *overflow_rows) {
+  if (!e) return ABYSS_ERR_ARG;
+  cudaSetDevice(e->device);
+  cudaStream_t s = e->stream;
+  const size_t m = e->rows;
+  int st = 0, ov = 0;
+  ECK(cudaMemcpyAsync(&st, e->status.p, 4, cudaMemcpyDeviceToHost, s), "D2H");
+  ECK(cudaMemcpyAsync(&ov, e->ovf.p, 4, cudaMemcpyDeviceToHost, s), "D2H");
+  if (acc_reg) ECK(cudaMemcpyAsync(acc_reg, e->acc_reg.p, 24 * m, cudaMemcpyDeviceToHost, s), "D2H");
+  if (jerk_reg) ECK(cudaMemcpyAsync(jerk_reg, e->jerk_reg.p, 24 * m, cudaMemcpyDeviceToHost, s), "D2H");
+  if (acc_irr) ECK(cudaMemcpyAsync(acc_irr, e->acc_irr.p, 24 * m, cudaMemcpyDeviceToHost, s), "D2H");
+  if (jerk_irr) ECK(cudaMemcpyAsync(jerk_irr, e->jerk_irr.p, 24 * m, cudaMemcpyDeviceToHost, s), "D2H");
+  if (nnb) ECK(cudaMemcpyAsync(nnb, e->nnb.p, 4 * m, cudaMemcpyDeviceToHost, s), "D2H");
+  if (list) ECK(cudaMemcpyAsync(list, e->list.p, 4 * m * e->cap, cudaMemcpyDeviceToHost, s), "D2H");
+  ECK(cudaStreamSynchronize(s), "fetch");
+  if (overflow_rows) *overflow_rows = ov;
+  if (st & kErrTimeout) return efail(e, ABYSS_ERR_TIMEOUT, "device wait timed out");
+  return ov > 0 ? ABYSS_WARN_OVERFLOW : ABYSS_OK;
+}
+
+int abyss_ens_last_ms(abyss_ens *e, float *ms) {
+  if (!e || !ms) return ABYSS_ERR_ARG;
+  cudaSetDevice(e->device);
+  ECK(cudaEventSynchronize(e->ev1), "event sync");
+  ECK(cudaEventElapsedTime(ms, e->ev0, e->ev1), "event time");
+  return ABYSS_OK;
+}
+
+int abyss_ens_last_stats(const abyss_ens *e, int *rows, int *items, int *launches) {
+  if (!e) return ABYSS_ERR_ARG;
+  if (rows) *rows = e->rows;
+  if (items) *items = e->n_items;
+  if (launches) *launches = e->launches;
+  return ABYSS_OK;
+}
+
+}  // extern "C"

@@ -71,6 +71,54 @@ __global__ void predict_jset(int n, const double *__restrict__ x, const double *
   }
 }
 
+// Prediction for a batched ensemble: particle j belongs to cluster cid[j]; only
+// clusters flagged active this wave are predicted, each to its own time.
+__global__ void predict_multi(int n, const int *__restrict__ cid, const int *__restrict__ active,
+                              const double *__restrict__ new_time, const double *__restrict__ time_scale,
+                              const double *__restrict__ x, const double *__restrict__ v,
+                              const double *__restrict__ a0, const double *__restrict__ a1,
+                              const double *__restrict__ t0, const double *__restrict__ mass,
+                              double *__restrict__ px, double *__restrict__ py, double *__restrict__ pz,
+                              double *__restrict__ pvx, double *__restrict__ pvy,
+                              double *__restrict__ pvz, float4 *__restrict__ vm) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    const int k = cid[j];
+    if (!active[k]) continue;
+    const double dt = __dmul_rn(__dsub_rn(new_time[k], t0[j]), time_scale[k]);
+    double p[3], q[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double xd = x[3 * j + d], vd = v[3 * j + d];
+      if (dt == 0.0) {
+        p[d] = xd;
+        q[d] = vd;
+      } else {
+        const double a0d = a0[3 * j + d], a1d = a1[3 * j + d];
+        double t = __dmul_rn(a1d, dt);
+        t = __ddiv_rn(t, 3.0);
+        t = __dadd_rn(t, a0d);
+        t = __dmul_rn(t, dt);
+        t = __ddiv_rn(t, 2.0);
+        t = __dadd_rn(t, vd);
+        t = __dmul_rn(t, dt);
+        p[d] = __dadd_rn(t, xd);
+        double u = __dmul_rn(a1d, dt);
+        u = __ddiv_rn(u, 2.0);
+        u = __dadd_rn(u, a0d);
+        u = __dmul_rn(u, dt);
+        q[d] = __dadd_rn(u, vd);
+      }
+    }
+    px[j] = p[0];
+    py[j] = p[1];
+    pz[j] = p[2];
+    pvx[j] = q[0];
+    pvy[j] = q[1];
+    pvz[j] = q[2];
+    vm[j] = make_float4((float)q[0], (float)q[1], (float)q[2], (float)mass[j]);
+  }
+}
+
 // j-set already predicted by the caller (reference-compatible SendToDevice):
 // fill the FP32 (v, m) records from the FP64 arrays.
 __global__ void pack_vm(int n, const double *__restrict__ pvx, const double *__restrict__ pvy,
@@ -313,11 +361,60 @@ __device__ __forceinline__ void pair_accum2(const PairGeom2 &g, float2 mj, float
   p[5] = __ffma2_rn(mr3, __ffma2_rn(al, g.dz, g.dvz), p[5]);
 }
 
+// A j-particle in the packed compute buffer: every value duplicated, so each
+// half of a float4 record is a ready float2 operand.
+struct JPair2 {
+  float2 x, y, z, m, vx, vy, vz, lx, ly, lz;
+};
+
+template <bool ANCHOR>
+__device__ __forceinline__ JPair2 load_jpair2(const float4 *cb, int TJP, int jl) {
+  JPair2 J;
+  const float4 A = cb[jl], B = cb[TJP + jl], C = cb[2 * TJP + jl], D = cb[3 * TJP + jl];
+  J.x = make_float2(A.x, A.y);
+  J.y = make_float2(A.z, A.w);
+  J.z = make_float2(B.x, B.y);
+  J.m = make_float2(B.z, B.w);
+  J.vx = make_float2(C.x, C.y);
+  J.vy = make_float2(C.z, C.w);
+  J.vz = make_float2(D.x, D.y);
+  if (!ANCHOR) {
+    const float4 E = cb[4 * TJP + jl], F = cb[5 * TJP + jl];
+    J.lx = make_float2(E.x, E.y);
+    J.ly = make_float2(E.z, E.w);
+    J.lz = make_float2(F.x, F.y);
+  } else {
+    J.lx = J.ly = J.lz = make_float2(0.f, 0.f);
+  }
+  return J;
+}
+
+// Geometry of j against the target pair q (targets 2q, 2q+1) held negated.
+template <bool ANCHOR, int IPT>
+__device__ __forceinline__ PairGeom2 geom2_of(const JPair2 &J, int q, const float (&hx)[IPT],
+                                              const float (&hy)[IPT], const float (&hz)[IPT],
+                                              const float (&lx)[IPT], const float (&ly)[IPT],
+                                              const float (&lz)[IPT], const float (&vx)[IPT],
+                                              const float (&vy)[IPT], const float (&vz)[IPT], float2 eps2) {
+  const int k0 = 2 * q, k1 = 2 * q + 1;
+  if (ANCHOR)
+    return pair_geom2(J.x, J.y, J.z, J.vx, J.vy, J.vz, make_float2(hx[k0], hx[k1]), make_float2(hy[k0], hy[k1]),
+                      make_float2(hz[k0], hz[k1]), make_float2(vx[k0], vx[k1]), make_float2(vy[k0], vy[k1]),
+                      make_float2(vz[k0], vz[k1]), eps2);
+  return pair_geom2_ds(J.x, J.y, J.z, J.lx, J.ly, J.lz, J.vx, J.vy, J.vz, make_float2(hx[k0], hx[k1]),
+                       make_float2(hy[k0], hy[k1]), make_float2(hz[k0], hz[k1]), make_float2(lx[k0], lx[k1]),
+                       make_float2(ly[k0], ly[k1]), make_float2(lz[k0], lz[k1]), make_float2(vx[k0], vx[k1]),
+                       make_float2(vy[k0], vy[k1]), make_float2(vz[k0], vz[k1]), eps2);
+}
+
 // Shared-memory layout of the tile kernel (dynamic).
-template <int NT, int IPT, int TJ, int NST, bool ANCHOR>
+template <int NT, int IPT, int TJ, int NST, bool ANCHOR, bool PACK>
 struct TileLayout {
-  static constexpr int TJP = TJ + 2;           // compute buffer incl. pad entries
-  static constexpr int CW = ANCHOR ? 2 : 3;    // float4 records per j
+  static constexpr int TJP = TJ + 4;           // compute buffer incl. pad entries
+  // float4 records per j.  Scalar: (x,y,z,m) (vx,vy,vz,-) [+ (xl,yl,zl,-)].
+  // Packed: every value duplicated so that each half of a float4 is a ready
+  // float2 operand: (x,x,y,y) (z,z,m,m) (vx,vx,vy,vy) (vz,vz,-,-) [+ (xl,xl,yl,yl) (zl,zl,-,-)].
+  static constexpr int CW = PACK ? (ANCHOR ? 4 : 6) : (ANCHOR ? 2 : 3);
   static constexpr size_t stage = 0;
   static constexpr size_t cbuf = stage + NST * sizeof(JStage<TJ>);
   static constexpr size_t kahan = cbuf + 2 * CW * TJP * sizeof(float4);  // float [IPT*12][NT]
@@ -337,10 +434,9 @@ struct TileLayout {
 // test in a warp-uniform slow path (list entry, or regular contribution).
 // Tile partials are FP32; they are folded into Kahan-compensated FP32 sums kept
 // in shared memory, and written per (chunk, target) for the FP64 finalize.
-template <int NT, int IPT, int TJ, int NST, bool ANCHOR, bool PACK>
-__global__ void __launch_bounds__(NT) reg_force_tile(JSet js, Work w, int n_iblocks) {
-  using LY = TileLayout<NT, IPT, TJ, NST, ANCHOR>;
-  constexpr int UNR = 2;
+template <int NT, int IPT, int TJ, int NST, bool ANCHOR, bool PACK, int UNR, int MINB>
+__global__ void __launch_bounds__(NT, MINB) reg_force_tile(JSet js, Work w, int n_iblocks) {
+  using LY = TileLayout<NT, IPT, TJ, NST, ANCHOR, PACK>;
   constexpr int TJP = LY::TJP;
   constexpr int CW = LY::CW;
   constexpr int PP = PACK ? IPT / 2 : 1;
@@ -363,16 +459,29 @@ __global__ void __launch_bounds__(NT) reg_force_tile(JSet js, Work w, int n_iblo
   __syncthreads();
 
   uint32_t g_cons = 0, g_issue = 0;
-  const int n_items = n_iblocks * w.n_chunks;
+  const int n_items = w.items ? *w.n_items_dev : n_iblocks * w.n_chunks;
+  const int m_rows = w.m_dev ? *w.m_dev : w.m;
   for (;;) {
     if (tid == 0) *s_item = atomicAdd(w.item_counter, 1);
     __syncthreads();
     const int item = *s_item;
     if (item >= n_items) break;
-    const int ib = item / w.n_chunks;
-    const int ch = item - ib * w.n_chunks;
-    const int j0 = ch * w.chunk_len;
-    const int j1 = min(js.n, j0 + w.chunk_len);
+    int base, count, ch, j0, j1;
+    if (w.items) {
+      const WorkItem it = w.items[item];
+      base = it.t_begin;
+      count = it.t_count;
+      ch = it.ch;
+      j0 = it.j0;
+      j1 = it.j1;
+    } else {
+      const int ib = item / w.n_chunks;
+      ch = item - ib * w.n_chunks;
+      base = ib * NT * IPT;
+      count = min(NT * IPT, m_rows - base);
+      j0 = ch * w.chunk_len;
+      j1 = min(js.n, j0 + w.chunk_len);
+    }
     const int ntile = (j1 - j0 + TJ - 1) / TJ;
 
     if (tid == 0) {
@@ -382,7 +491,6 @@ __global__ void __launch_bounds__(NT) reg_force_tile(JSet js, Work w, int n_iblo
     }
 
     // ---- targets of this block into registers (coordinates) and shared memory (indices)
-    const int base = ib * NT * IPT;
     double ax = 0.0, ay = 0.0, az = 0.0;
     if (ANCHOR) {
       const int t0 = w.order_t[base];
@@ -395,7 +503,7 @@ __global__ void __launch_bounds__(NT) reg_force_tile(JSet js, Work w, int n_iblo
 #pragma unroll
     for (int k = 0; k < IPT; ++k) {
       const int s = base + k * NT + tid;
-      const bool valid = s < w.m;
+      const bool valid = k * NT + tid < count;
       const int si = valid ? s : base;
       const int t = w.order_t[si];
       s_ti[k * NT + tid] = t;
@@ -443,24 +551,44 @@ __global__ void __launch_bounds__(NT) reg_force_tile(JSet js, Work w, int n_iblo
       const int cnt = min(TJ, j1 - jt0);
       float4 *cb = cbuf + (g_cons & 1u) * CW * TJP;
       for (int jj = tid; jj < TJP; jj += NT) {
-        if (jj < cnt && ok) {
-          const double X = st[stg].x[jj], Y = st[stg].y[jj], Z = st[stg].z[jj];
-          const float4 vmj = st[stg].vm[jj];
-          if (ANCHOR) {
-            cb[jj] = make_float4((float)(X - ax), (float)(Y - ay), (float)(Z - az), vmj.w);
-            cb[TJP + jj] = make_float4(vmj.x, vmj.y, vmj.z, 0.0f);
-          } else {
-            const float fx = (float)X, fy = (float)Y, fz = (float)Z;
-            cb[jj] = make_float4(fx, fy, fz, vmj.w);
-            cb[TJP + jj] = make_float4((float)(X - (double)fx), (float)(Y - (double)fy),
-                                       (float)(Z - (double)fz), 0.0f);
-            cb[2 * TJP + jj] = make_float4(vmj.x, vmj.y, vmj.z, 0.0f);
+        const bool real = jj < cnt && ok;
+        double X = 0.0, Y = 0.0, Z = 0.0;
+        float4 vmj = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (real) {
+          X = st[stg].x[jj];
+          Y = st[stg].y[jj];
+          Z = st[stg].z[jj];
+          vmj = st[stg].vm[jj];
+        }
+        // pad entries are massless and far away: never a candidate, contribute 0
+        float fx, fy, fz, lxj = 0.0f, lyj = 0.0f, lzj = 0.0f;
+        if (!real) {
+          fx = fy = fz = 1e30f;
+        } else if (ANCHOR) {
+          fx = (float)(X - ax);
+          fy = (float)(Y - ay);
+          fz = (float)(Z - az);
+        } else {
+          fx = (float)X;
+          fy = (float)Y;
+          fz = (float)Z;
+          lxj = (float)(X - (double)fx);
+          lyj = (float)(Y - (double)fy);
+          lzj = (float)(Z - (double)fz);
+        }
+        if constexpr (PACK) {
+          cb[jj] = make_float4(fx, fx, fy, fy);
+          cb[TJP + jj] = make_float4(fz, fz, vmj.w, vmj.w);
+          cb[2 * TJP + jj] = make_float4(vmj.x, vmj.x, vmj.y, vmj.y);
+          cb[3 * TJP + jj] = make_float4(vmj.z, vmj.z, 0.0f, 0.0f);
+          if (!ANCHOR) {
+            cb[4 * TJP + jj] = make_float4(lxj, lxj, lyj, lyj);
+            cb[5 * TJP + jj] = make_float4(lzj, lzj, 0.0f, 0.0f);
           }
         } else {
-          // pad entry: massless and far away (never a candidate, contributes 0)
-          cb[jj] = make_float4(1e30f, 1e30f, 1e30f, 0.0f);
-          cb[TJP + jj] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-          if (!ANCHOR) cb[2 * TJP + jj] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+          cb[jj] = make_float4(fx, fy, fz, vmj.w);
+          cb[TJP + jj] = make_float4(vmj.x, vmj.y, vmj.z, 0.0f);
+          if (!ANCHOR) cb[2 * TJP + jj] = make_float4(lxj, lyj, lzj, 0.0f);
         }
       }
       if (!__syncthreads_and(ok)) {
@@ -492,33 +620,23 @@ __global__ void __launch_bounds__(NT) reg_force_tile(JSet js, Work w, int n_iblo
         bool any = false;
 #pragma unroll
         for (int u = 0; u < UNR; ++u) {
-          const float4 P = cb[jj + u];
-          const float4 L = ANCHOR ? make_float4(0.f, 0.f, 0.f, 0.f) : cb[TJP + jj + u];
-          const float4 V = cb[(ANCHOR ? 1 : 2) * TJP + jj + u];
           if constexpr (PACK) {
+            const JPair2 J = load_jpair2<ANCHOR>(cb, TJP, jj + u);
 #pragma unroll
             for (int q = 0; q < PP; ++q) {
-              const int k0 = 2 * q, k1 = 2 * q + 1;
-              const PairGeom2 g =
-                  ANCHOR ? pair_geom2(dup2(P.x), dup2(P.y), dup2(P.z), dup2(V.x), dup2(V.y), dup2(V.z),
-                                      make_float2(hx[k0], hx[k1]), make_float2(hy[k0], hy[k1]),
-                                      make_float2(hz[k0], hz[k1]), make_float2(vx[k0], vx[k1]),
-                                      make_float2(vy[k0], vy[k1]), make_float2(vz[k0], vz[k1]), eps2v)
-                         : pair_geom2_ds(dup2(P.x), dup2(P.y), dup2(P.z), dup2(L.x), dup2(L.y), dup2(L.z),
-                                         dup2(V.x), dup2(V.y), dup2(V.z), make_float2(hx[k0], hx[k1]),
-                                         make_float2(hy[k0], hy[k1]), make_float2(hz[k0], hz[k1]),
-                                         make_float2(lx[k0], lx[k1]), make_float2(ly[k0], ly[k1]),
-                                         make_float2(lz[k0], lz[k1]), make_float2(vx[k0], vx[k1]),
-                                         make_float2(vy[k0], vy[k1]), make_float2(vz[k0], vz[k1]), eps2v);
-              const bool c0 = g.r2.x < r2g[k0];
-              const bool c1 = g.r2.y < r2g[k1];
+              const PairGeom2 g = geom2_of<ANCHOR>(J, q, hx, hy, hz, lx, ly, lz, vx, vy, vz, eps2v);
+              const bool c0 = g.r2.x < r2g[2 * q];
+              const bool c1 = g.r2.y < r2g[2 * q + 1];
               float2 ri;
               ri.x = c0 ? 0.0f : rsqrtf(g.r2.x);
               ri.y = c1 ? 0.0f : rsqrtf(g.r2.y);
               any |= (c0 | c1);
-              pair_accum2(g, dup2(P.w), ri, p2[q]);
+              pair_accum2(g, J.m, ri, p2[q]);
             }
           } else {
+            const float4 P = cb[jj + u];
+            const float4 V = cb[TJP + jj + u];
+            const float4 L = ANCHOR ? make_float4(0.f, 0.f, 0.f, 0.f) : cb[2 * TJP + jj + u];
 #pragma unroll
             for (int k = 0; k < IPT; ++k) {
               const PairGeom gg =
@@ -541,34 +659,27 @@ __global__ void __launch_bounds__(NT) reg_force_tile(JSet js, Work w, int n_iblo
             const int jl = jj + u;
             if (jl >= cnt) continue;
             const int jg = jt0 + jl;
-            const float4 P = cb[jl];
-            const float4 L = ANCHOR ? make_float4(0.f, 0.f, 0.f, 0.f) : cb[TJP + jl];
-            const float4 V = cb[(ANCHOR ? 1 : 2) * TJP + jl];
 #pragma unroll
             for (int k = 0; k < IPT; ++k) {
               float r2k;
               PairGeom2 g2;
               PairGeom gg;
+              float mj;
               if constexpr (PACK) {
-                const int k0 = k & ~1, k1 = k | 1;
-                g2 = ANCHOR ? pair_geom2(dup2(P.x), dup2(P.y), dup2(P.z), dup2(V.x), dup2(V.y), dup2(V.z),
-                                         make_float2(hx[k0], hx[k1]), make_float2(hy[k0], hy[k1]),
-                                         make_float2(hz[k0], hz[k1]), make_float2(vx[k0], vx[k1]),
-                                         make_float2(vy[k0], vy[k1]), make_float2(vz[k0], vz[k1]), eps2v)
-                            : pair_geom2_ds(dup2(P.x), dup2(P.y), dup2(P.z), dup2(L.x), dup2(L.y),
-                                            dup2(L.z), dup2(V.x), dup2(V.y), dup2(V.z),
-                                            make_float2(hx[k0], hx[k1]), make_float2(hy[k0], hy[k1]),
-                                            make_float2(hz[k0], hz[k1]), make_float2(lx[k0], lx[k1]),
-                                            make_float2(ly[k0], ly[k1]), make_float2(lz[k0], lz[k1]),
-                                            make_float2(vx[k0], vx[k1]), make_float2(vy[k0], vy[k1]),
-                                            make_float2(vz[k0], vz[k1]), eps2v);
+                const JPair2 J = load_jpair2<ANCHOR>(cb, TJP, jl);
+                g2 = geom2_of<ANCHOR>(J, k >> 1, hx, hy, hz, lx, ly, lz, vx, vy, vz, eps2v);
                 r2k = (k & 1) ? g2.r2.y : g2.r2.x;
+                mj = J.m.x;
               } else {
+                const float4 P = cb[jl];
+                const float4 V = cb[TJP + jl];
+                const float4 L = ANCHOR ? make_float4(0.f, 0.f, 0.f, 0.f) : cb[2 * TJP + jl];
                 gg = ANCHOR ? pair_geom(P.x, P.y, P.z, V.x, V.y, V.z, -hx[k], -hy[k], -hz[k], -vx[k], -vy[k],
                                         -vz[k], w.eps2f)
                             : pair_geom_ds(P.x, P.y, P.z, L.x, L.y, L.z, V.x, V.y, V.z, -hx[k], -hy[k],
                                            -hz[k], -lx[k], -ly[k], -lz[k], -vx[k], -vy[k], -vz[k], w.eps2f);
                 r2k = gg.r2;
+                mj = P.w;
               }
               if (!(r2k < r2g[k])) continue;
               const int ti = s_ti[k * NT + tid];
@@ -581,10 +692,10 @@ __global__ void __launch_bounds__(NT) reg_force_tile(JSet js, Work w, int n_iblo
               } else {
                 const float rr = rsqrtf(r2k);
                 if constexpr (PACK)
-                  pair_accum2(g2, dup2(P.w), (k & 1) ? make_float2(0.0f, rr) : make_float2(rr, 0.0f),
+                  pair_accum2(g2, dup2(mj), (k & 1) ? make_float2(0.0f, rr) : make_float2(rr, 0.0f),
                               p2[k >> 1]);
                 else
-                  pair_accum(gg, P.w, rr, p[k]);
+                  pair_accum(gg, mj, rr, p[k]);
               }
             }
           }
@@ -614,7 +725,7 @@ __global__ void __launch_bounds__(NT) reg_force_tile(JSet js, Work w, int n_iblo
     for (int k = 0; k < IPT; ++k) {
       const int row = s_row[k * NT + tid];
       if (row < 0) continue;
-      double *dst = w.part + ((size_t)ch * w.m + row) * 6;
+      double *dst = w.part + ((size_t)row * w.s_stride + ch) * 6;
 #pragma unroll
       for (int c = 0; c < 6; ++c)
         dst[c] = (double)ksm[(k * 12 + c) * NT + tid] - (double)ksm[(k * 12 + 6 + c) * NT + tid];
@@ -713,7 +824,7 @@ __global__ void __launch_bounds__(128) reg_force_jmajor(JSet js, Work w, int L) 
         for (int o = 16; o > 0; o >>= 1) s[q] += __shfl_xor_sync(FULL, s[q], o);
       }
       if (lane == 0) {
-        double *dst = w.part + ((size_t)c * w.m + row[k]) * 6;
+        double *dst = w.part + ((size_t)row[k] * w.s_stride + c) * 6;
 #pragma unroll
         for (int q = 0; q < 6; ++q) dst[q] = s[q];
       }
@@ -734,10 +845,13 @@ __global__ void finalize_rows(JSet js, Work w, Outputs o, int sort_cap) {
   const int lane = threadIdx.x & 31;
   int *buf = fin_smem + (threadIdx.x >> 5) * sort_cap;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < w.m; r += nwarps) {
+  const int m_rows = w.m_dev ? *w.m_dev : w.m;
+  for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < m_rows; r += nwarps) {
     double s[6] = {0, 0, 0, 0, 0, 0};
-    for (int c = lane; c < w.n_chunks; c += 32) {
-      const double *src = w.part + ((size_t)c * w.m + r) * 6;
+    const int nch = w.row_nchunks ? w.row_nchunks[r] : w.n_chunks;
+    const int joff = w.row_joff ? w.row_joff[r] : 0;
+    for (int c = lane; c < nch; c += 32) {
+      const double *src = w.part + ((size_t)r * w.s_stride + c) * 6;
 #pragma unroll
       for (int q = 0; q < 6; ++q) s[q] += src[q];
     }
@@ -770,7 +884,7 @@ __global__ void finalize_rows(JSet js, Work w, Outputs o, int sort_cap) {
         __syncwarp();
       }
     }
-    for (int k = lane; k < nl; k += 32) out[k] = buf[k];
+    for (int k = lane; k < nl; k += 32) out[k] = buf[k] - joff;
     __syncwarp();
 
     const int t = o.targets[r];
@@ -909,57 +1023,86 @@ void launch_morton_order(cudaStream_t s, int m, const int *targets, const JSet &
   gather_order<<<blocks, 256, 0, s>>>(m, targets, rows_alt, order_t, order_o);
 }
 
-template <int NT, int IPT, bool ANCHOR, bool PACK>
-static int tile_occupancy_impl() {
+// ------------------------------------------------------------------ tile variants
+// Each instantiated shape of reg_force_tile: (threads, targets per thread,
+// anchor/double-single offsets, packed FP32x2 arithmetic, j unroll, minimum
+// resident CTAs per SM as a register cap).
+struct TileVariant {
+  int nt, ipt, anchor, pack, unr, minb;
+  int (*occupancy)();
+  void (*launch)(cudaStream_t, int, const JSet &, const Work &, int);
+};
+
+template <int NT, int IPT, bool ANCHOR, bool PACK, int UNR, int MINB>
+static int tile_occ() {
   constexpr int TJ = 128, NST = 3;
-  auto k = reg_force_tile<NT, IPT, TJ, NST, ANCHOR, PACK>;
-  const size_t sm = TileLayout<NT, IPT, TJ, NST, ANCHOR>::bytes;
+  auto k = reg_force_tile<NT, IPT, TJ, NST, ANCHOR, PACK, UNR, MINB>;
+  const size_t sm = TileLayout<NT, IPT, TJ, NST, ANCHOR, PACK>::bytes;
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   int blocks = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k, NT, sm);
   return blocks;
 }
 
-template <int NT, int IPT, bool ANCHOR, bool PACK>
-static void tile_launch_impl(cudaStream_t s, int grid, const JSet &js, const Work &w, int n_iblocks) {
+template <int NT, int IPT, bool ANCHOR, bool PACK, int UNR, int MINB>
+static void tile_run(cudaStream_t s, int grid, const JSet &js, const Work &w, int n_iblocks) {
   constexpr int TJ = 128, NST = 3;
-  auto k = reg_force_tile<NT, IPT, TJ, NST, ANCHOR, PACK>;
-  const size_t sm = TileLayout<NT, IPT, TJ, NST, ANCHOR>::bytes;
-  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  auto k = reg_force_tile<NT, IPT, TJ, NST, ANCHOR, PACK, UNR, MINB>;
+  const size_t sm = TileLayout<NT, IPT, TJ, NST, ANCHOR, PACK>::bytes;
   k<<<grid, NT, sm, s>>>(js, w, n_iblocks);
 }
 
-// Instantiated shapes: scalar (PACK = false) 128x{1,2,4}, 256x2; packed 128x{2,4}, 256x{2,4}.
-#define ABYSS_TILE_SWITCH(NT_, IPT_, ANCHOR_, PACK_, CALL)                                      \
-  do {                                                                                          \
-    if (!(PACK_)) {                                                                             \
-      if (NT_ == 128 && IPT_ == 1) { if (ANCHOR_) CALL(128, 1, true, false); else CALL(128, 1, false, false); } \
-      else if (NT_ == 128 && IPT_ == 2) { if (ANCHOR_) CALL(128, 2, true, false); else CALL(128, 2, false, false); } \
-      else if (NT_ == 128 && IPT_ == 4) { if (ANCHOR_) CALL(128, 4, true, false); else CALL(128, 4, false, false); } \
-      else if (NT_ == 256 && IPT_ == 2) { if (ANCHOR_) CALL(256, 2, true, false); else CALL(256, 2, false, false); } \
-      else return -1;                                                                           \
-    } else {                                                                                    \
-      if (NT_ == 128 && IPT_ == 2) { if (ANCHOR_) CALL(128, 2, true, true); else CALL(128, 2, false, true); } \
-      else if (NT_ == 128 && IPT_ == 4) { if (ANCHOR_) CALL(128, 4, true, true); else CALL(128, 4, false, true); } \
-      else if (NT_ == 256 && IPT_ == 2) { if (ANCHOR_) CALL(256, 2, true, true); else CALL(256, 2, false, true); } \
-      else if (NT_ == 256 && IPT_ == 4) { if (ANCHOR_) CALL(256, 4, true, true); else CALL(256, 4, false, true); } \
-      else return -1;                                                                           \
-    }                                                                                           \
-  } while (0)
+#define TV(NT, IPT, A, P, U, M) \
+  {NT, IPT, A, P, U, M, &tile_occ<NT, IPT, A, P, U, M>, &tile_run<NT, IPT, A, P, U, M>}
+#define TV2(NT, IPT, P, U, M) TV(NT, IPT, true, P, U, M), TV(NT, IPT, false, P, U, M)
 
-int tile_occupancy(int nt, int ipt, bool anchor, bool pack) {
-  int r = 0;
-#define OCC_CALL(a, b, c, d) r = tile_occupancy_impl<a, b, c, d>()
-  ABYSS_TILE_SWITCH(nt, ipt, anchor, pack, OCC_CALL);
-#undef OCC_CALL
-  return r;
+static const TileVariant kTileVariants[] = {
+    // scalar pair arithmetic
+    TV2(128, 1, false, 2, 1), TV2(128, 2, false, 2, 1), TV2(128, 4, false, 2, 1), TV2(256, 2, false, 2, 1),
+    // packed FP32x2 pair arithmetic
+    TV2(128, 2, true, 2, 1), TV2(128, 2, true, 2, 4), TV2(128, 4, true, 1, 1), TV2(128, 4, true, 2, 1),
+    TV2(128, 4, true, 2, 3), TV2(128, 4, true, 1, 4), TV2(256, 2, true, 2, 1), TV2(256, 4, true, 1, 2),
+    TV2(256, 4, true, 2, 1),
+};
+#undef TV2
+#undef TV
+
+// First variant matching the request; unroll/min_blocks of 0 match anything.
+static const TileVariant *find_variant(int nt, int ipt, bool anchor, bool pack, int unr, int minb) {
+  for (const TileVariant &v : kTileVariants)
+    if (v.nt == nt && v.ipt == ipt && v.anchor == (int)anchor && v.pack == (int)pack &&
+        (unr == 0 || v.unr == unr) && (minb == 0 || v.minb == minb))
+      return &v;
+  return nullptr;
 }
 
-int launch_tile(cudaStream_t s, int nt, int ipt, bool anchor, bool pack, int grid, const JSet &js,
-                const Work &w, int n_iblocks) {
-#define LAUNCH_CALL(a, b, c, d) tile_launch_impl<a, b, c, d>(s, grid, js, w, n_iblocks)
-  ABYSS_TILE_SWITCH(nt, ipt, anchor, pack, LAUNCH_CALL);
-#undef LAUNCH_CALL
+int tile_occupancy(int nt, int ipt, bool anchor, bool pack, int unr, int minb) {
+  const TileVariant *v = find_variant(nt, ipt, anchor, pack, unr, minb);
+  if (!v) return -1;
+  const int occ = v->occupancy();
+  // the dynamic smem attribute is set on the first query; check it stuck
+  return cudaGetLastError() == cudaSuccess ? occ : -1;
+}
+
+int launch_tile(cudaStream_t s, int nt, int ipt, bool anchor, bool pack, int unr, int minb, int grid,
+                const JSet &js, const Work &w, int n_iblocks) {
+  const TileVariant *v = find_variant(nt, ipt, anchor, pack, unr, minb);
+  if (!v) return -1;
+  v->launch(s, grid, js, w, n_iblocks);
+  return 0;
+}
+
+int tile_variant_count() { return (int)(sizeof(kTileVariants) / sizeof(kTileVariants[0])); }
+
+int tile_variant_shape(int i, int *shape6) {
+  if (i < 0 || i >= tile_variant_count()) return -1;
+  const TileVariant &v = kTileVariants[i];
+  shape6[0] = v.nt;
+  shape6[1] = v.ipt;
+  shape6[2] = v.anchor;
+  shape6[3] = v.pack;
+  shape6[4] = v.unr;
+  shape6[5] = v.minb;
   return 0;
 }
 
@@ -985,6 +1128,25 @@ void launch_finalize(cudaStream_t s, const JSet &js, const Work &w, const Output
     cudaFuncSetAttribute(finalize_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const int blocks = max(1, min((w.m + warps_per_block - 1) / warps_per_block, sm_count * 32));
   finalize_rows<<<blocks, 32 * warps_per_block, smem, s>>>(js, w, o, P);
+}
+
+void launch_predict_multi(cudaStream_t s, int n, const int *cid, const int *active,
+                          const double *new_time, const double *time_scale, const double *x,
+                          const double *v, const double *a0, const double *a1, const double *t0,
+                          const double *mass, double *px, double *py, double *pz, double *pvx,
+                          double *pvy, double *pvz, float4 *vm, int sm_count) {
+  const int blocks = max(1, min((n + 255) / 256, sm_count * 8));
+  predict_multi<<<blocks, 256, 0, s>>>(n, cid, active, new_time, time_scale, x, v, a0, a1, t0, mass, px,
+                                       py, pz, pvx, pvy, pvz, vm);
+}
+
+void launch_finalize_grid(cudaStream_t s, const JSet &js, const Work &w, const Outputs &o, int blocks) {
+  int P = 32;
+  while (P < w.cap) P <<= 1;
+  const size_t smem = (size_t)4 * P * sizeof(int);
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(finalize_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  finalize_rows<<<blocks, 128, smem, s>>>(js, w, o, P);
 }
 
 void launch_energy(cudaStream_t s, int n, const double *x, const double *v, const double *mass,

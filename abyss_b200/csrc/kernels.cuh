@@ -22,12 +22,27 @@ size_t morton_temp_bytes(int m_cap);
 void launch_morton_order(cudaStream_t s, int m, const int *targets, const JSet &js, int *bbox,
                          uint32_t *keys, uint32_t *keys_alt, int *rows, int *rows_alt,
                          void *cub_tmp, size_t cub_bytes, int *order_t, int *order_o, int sm_count);
-int tile_occupancy(int nt, int ipt, bool anchor, bool pack);
-int launch_tile(cudaStream_t s, int nt, int ipt, bool anchor, bool pack, int grid, const JSet &js,
-                const Work &w, int n_iblocks);
+int tile_occupancy(int nt, int ipt, bool anchor, bool pack, int unr, int minb);
+int launch_tile(cudaStream_t s, int nt, int ipt, bool anchor, bool pack, int unr, int minb, int grid,
+                const JSet &js, const Work &w, int n_iblocks);
+int tile_variant_count();
+int tile_variant_shape(int i, int *shape6);
 int launch_jmajor(cudaStream_t s, int mi, const JSet &js, const Work &w, int L);
 void launch_finalize(cudaStream_t s, const JSet &js, const Work &w, const Outputs &o, int sm_count);
+void launch_predict_multi(cudaStream_t s, int n, const int *cid, const int *active,
+                          const double *new_time, const double *time_scale, const double *x,
+                          const double *v, const double *a0, const double *a1, const double *t0,
+                          const double *mass, double *px, double *py, double *pz, double *pvx,
+                          double *pvy, double *pvz, float4 *vm, int sm_count);
+void launch_finalize_grid(cudaStream_t s, const JSet &js, const Work &w, const Outputs &o, int blocks);
 void launch_energy(cudaStream_t s, int n, const double *x, const double *v, const double *mass,
                    double eps2, double *e_row);
 
+}  // namespace abyss
+
+struct abyss_ctx;
+namespace abyss {
+cudaStream_t ctx_stream(abyss_ctx *c);
+int ctx_device(abyss_ctx *c);
+int ctx_sm_count(abyss_ctx *c);
 }  // namespace abyss

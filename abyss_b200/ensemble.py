@@ -1,0 +1,110 @@
+"""Batched regular force over many clusters (include/abyss_ens.h)."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import Tuning, ptr, _ip, _fp, _dp, _vp
+from .regforce import ForceResult, RegularForce, _f64
+
+BATCHED, GRAPH, PLAIN = 0, 1, 2
+
+
+def _bind(L):
+    if getattr(L, "_ens_bound", False):
+        return
+    L.abyss_ens_create.argtypes = [_vp, C.c_int, _ip, C.c_int, C.POINTER(_vp)]
+    L.abyss_ens_destroy.argtypes = [_vp]
+    L.abyss_ens_device_bytes.argtypes = [_vp]
+    L.abyss_ens_device_bytes.restype = C.c_longlong
+    L.abyss_ens_upload_state.argtypes = [_vp, C.c_int] + [_dp] * 7
+    L.abyss_ens_set_wave.argtypes = [_vp, C.c_int, _ip, _dp, _dp, _ip, _ip]
+    L.abyss_ens_launch.argtypes = [_vp, C.c_double, C.c_int, C.POINTER(Tuning)]
+    L.abyss_ens_fetch.argtypes = [_vp, _dp, _dp, _dp, _dp, _ip, _ip, _ip]
+    L.abyss_ens_last_ms.argtypes = [_vp, _fp]
+    L.abyss_ens_last_stats.argtypes = [_vp, _ip, _ip, _ip]
+    L._ens_bound = True
+
+
+class Ensemble:
+    """K clusters resident on one GPU; regular force for waves of (cluster, targets)."""
+
+    def __init__(self, rf: RegularForce, sizes, list_cap: int = 256):
+        self._L = _lib.lib()
+        _bind(self._L)
+        self.rf = rf
+        self.sizes = np.ascontiguousarray(sizes, np.int32)
+        self.cap = int(list_cap)
+        h = C.c_void_p()
+        rc = self._L.abyss_ens_create(rf._h, int(self.sizes.shape[0]), ptr(self.sizes, _ip), self.cap,
+                                      C.byref(h))
+        if rc != 0:
+            raise _lib.AbyssError(rc, "abyss_ens_create failed")
+        self._h = h
+        self.rows = 0
+
+    def _check(self, rc, allow_overflow=False):
+        if rc < 0 or (rc > 0 and not allow_overflow):
+            raise _lib.AbyssError(rc, "ensemble call failed")
+        return rc
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._L.abyss_ens_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def device_bytes(self) -> int:
+        return int(self._L.abyss_ens_device_bytes(self._h))
+
+    def upload_state(self, k, x, v, a0, a1, t0, mass, r2nb):
+        n = int(self.sizes[k])
+        arrs = [_f64(x, (n, 3)), _f64(v, (n, 3)), _f64(a0, (n, 3)), _f64(a1, (n, 3)), _f64(t0), _f64(mass),
+                _f64(r2nb)]
+        self._check(self._L.abyss_ens_upload_state(self._h, int(k), *[ptr(a) for a in arrs]))
+
+    def set_wave(self, clusters, new_time, time_scale, targets):
+        """targets: list of cluster-local index arrays, one per listed cluster."""
+        cl = np.ascontiguousarray(clusters, np.int32)
+        nt = np.ascontiguousarray(new_time, np.float64)
+        sc = np.ascontiguousarray(time_scale, np.float64)
+        mp = np.array([len(t) for t in targets], np.int32)
+        tg = np.ascontiguousarray(np.concatenate([np.asarray(t, np.int32) for t in targets]), np.int32)
+        self._check(self._L.abyss_ens_set_wave(self._h, int(cl.shape[0]), ptr(cl, _ip), ptr(nt), ptr(sc),
+                                               ptr(mp, _ip), ptr(tg, _ip)))
+        self.rows = int(mp.sum())
+        self.row_splits = np.concatenate([[0], np.cumsum(mp)])
+
+    def launch(self, eps2: float = 0.0, mode: int = BATCHED, tuning: dict | None = None):
+        tu = Tuning(**tuning) if tuning else None
+        self._check(self._L.abyss_ens_launch(self._h, float(eps2), int(mode),
+                                             C.byref(tu) if tu is not None else None))
+
+    def fetch(self) -> ForceResult:
+        m = self.rows
+        out = ForceResult(np.zeros((m, 3)), np.zeros((m, 3)), np.zeros((m, 3)), np.zeros((m, 3)),
+                          np.zeros(m, np.int32), np.zeros((m, self.cap), np.int32))
+        ovf = C.c_int(0)
+        self._check(self._L.abyss_ens_fetch(self._h, ptr(out.acc_reg), ptr(out.jerk_reg), ptr(out.acc_irr),
+                                            ptr(out.jerk_irr), ptr(out.nnb, _ip), ptr(out.list, _ip),
+                                            C.byref(ovf)), allow_overflow=True)
+        out.overflow_rows = int(ovf.value)
+        return out
+
+    def last_ms(self) -> float:
+        ms = np.zeros(1, np.float32)
+        self._check(self._L.abyss_ens_last_ms(self._h, ptr(ms, _fp)))
+        return float(ms[0])
+
+    def last_stats(self) -> dict:
+        r, i, l = C.c_int(0), C.c_int(0), C.c_int(0)
+        self._check(self._L.abyss_ens_last_stats(self._h, C.byref(r), C.byref(i), C.byref(l)))
+        return {"rows": r.value, "items": i.value, "launches": l.value}

@@ -1,0 +1,60 @@
+/* abyss_ens.h -- batched regular force over many independent clusters
+ * (libabyss_reg.so).
+ *
+ * The reference integrates one cluster per run and calls its GPU regular force
+ * once per regular block (src_mpi/RootRoutines.cpp:1026-1075).  An ensemble
+ * holds K clusters of uneven size resident on one GPU; a "wave" is one regular
+ * block of any subset of them (each cluster with its own time and its own
+ * active set).  A wave runs as one device prediction, ONE persistent launch of
+ * the tile kernel over a work list of (cluster, target block, j-chunk) items and
+ * one finalize pass; with ABYSS_ENS_GRAPH those three are replayed from a CUDA
+ * graph captured once.  ABYSS_ENS_PLAIN runs the same kernels one cluster per
+ * launch, the baseline the batched form is measured against.
+ *
+ * Indices are cluster-local (0 <= target < n_k), as are the returned lists.
+ * Rows of the outputs follow the order of the wave's clusters and targets.
+ */
+#ifndef ABYSS_ENS_H
+#define ABYSS_ENS_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+struct abyss_ctx;
+struct abyss_tuning;
+typedef struct abyss_ens abyss_ens;
+
+#define ABYSS_ENS_BATCHED 0  /* one launch per wave */
+#define ABYSS_ENS_GRAPH 1    /* the batched wave replayed from a captured CUDA graph */
+#define ABYSS_ENS_PLAIN 2    /* one launch per cluster (baseline) */
+
+/* n_clusters clusters of n_per_cluster[k] particles; list_cap = neighbour-list
+ * capacity per target.  Device memory for every particle being a target is
+ * reserved up front (state, outputs and work buffers), so waves never allocate. */
+int abyss_ens_create(struct abyss_ctx *ctx, int n_clusters, const int *n_per_cluster, int list_cap,
+                     abyss_ens **out);
+int abyss_ens_destroy(abyss_ens *e);
+/* Device bytes the ensemble holds (for admission control). */
+long long abyss_ens_device_bytes(const abyss_ens *e);
+/* Un-predicted FP64 state of cluster k, as abyss_upload_state. */
+int abyss_ens_upload_state(abyss_ens *e, int k, const double *x, const double *v, const double *a0,
+                           const double *a1, const double *t0, const double *mass,
+                           const double *r2nb);
+/* Define the next wave: nk clusters, each predicted to new_time[i] with
+ * time_scale[i] and m_per[i] targets (concatenated in targets_local). */
+int abyss_ens_set_wave(abyss_ens *e, int nk, const int *clusters, const double *new_time,
+                       const double *time_scale, const int *m_per, const int *targets_local);
+/* Run the wave (mode = ABYSS_ENS_BATCHED, _GRAPH or _PLAIN); asynchronous. */
+int abyss_ens_launch(abyss_ens *e, double eps2, int mode, const struct abyss_tuning *tuning);
+/* Wait and copy the wave's results (rows in wave order); any pointer may be NULL. */
+int abyss_ens_fetch(abyss_ens *e, double *acc_reg, double *jerk_reg, double *acc_irr,
+                    double *jerk_irr, int *nnb, int *list, int *overflow_rows);
+/* GPU milliseconds of the last launch (CUDA events around the wave). */
+int abyss_ens_last_ms(abyss_ens *e, float *ms);
+/* Rows, work items and kernel launches of the last wave. */
+int abyss_ens_last_stats(const abyss_ens *e, int *rows, int *items, int *launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

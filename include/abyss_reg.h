@@ -43,13 +43,21 @@ typedef struct abyss_ctx abyss_ctx;
 /* Launch shape.  Zero fields are chosen by the library (or by a tuning table
  * installed with abyss_set_tuning_table). */
 typedef struct abyss_tuning {
-  int kernel;  /* 1 = tile kernel (i in registers, j-tiles by TMA), 2 = j-major kernel */
+  int kernel;  /* 1 = tile kernel (i in registers, j-tiles by TMA), 2 = j-major kernel,
+                  3 = tile kernel with packed FP32x2 pair arithmetic */
   int mode;    /* tile kernel: 1 = anchor offsets on spatially ordered targets, 2 = double-single */
   int threads; /* tile kernel: 128 or 256 */
   int ipt;     /* tile: targets per thread 1, 2, 4;  j-major: targets per pass 1, 2, 4, 8 */
   int j_split; /* j-chunks per target (0 = auto) */
   int grid;    /* tile kernel persistent grid size (0 = auto) */
+  int unroll;  /* tile kernel: j per warp vote, 1 or 2 (0 = first available) */
+  int min_blocks; /* tile kernel: register cap as resident CTAs per SM (0 = first available) */
 } abyss_tuning;
+
+/* Number of compiled tile-kernel shapes and the shape of entry i as
+ * (threads, ipt, anchor, packed, unroll, min_blocks); kernel = 3 when packed. */
+int abyss_tile_variants(void);
+int abyss_tile_variant(int i, int *shape6);
 
 /* Replaces the reference's _InitializeDevice/_OpenDevice state
  * (src_mpi/cuda/cuda_my_acceleration.cu:782-882, 886-903) with an explicit

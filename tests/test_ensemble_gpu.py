@@ -1,0 +1,112 @@
+"""Batched ensemble: many clusters of uneven N and uneven active sets per wave.
+
+* every cluster's rows match the FP64 oracle (lists exact, forces within the
+  bar of tests/test_regforce_gpu.py);
+* the batched launch, its CUDA-graph replay and the one-cluster-per-launch form
+  give bit-identical results (a cluster's result does not depend on the mix);
+* bad waves are refused with a status, and the ensemble stays usable.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from abyss_b200 import ic
+from abyss_b200.ensemble import BATCHED, GRAPH, PLAIN, Ensemble
+from abyss_b200.regforce import RegularForce
+from tests.test_regforce_gpu import check
+
+pytestmark = pytest.mark.gpu
+EPS2 = 1e-8
+
+
+@pytest.fixture(scope="module")
+def rf():
+    r = RegularForce(0)
+    yield r
+    r.close()
+
+
+def make_ensemble(rf, k=24, seed=4):
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(256), np.log(4096), k)).astype(int)
+    clusters = [ic.plummer(int(n), 4000 + i, k_nb=24) for i, n in enumerate(sizes)]
+    e = Ensemble(rf, sizes, list_cap=128)
+    for i, c in enumerate(clusters):
+        a = np.zeros((c.n, 3))
+        e.upload_state(i, c.x, c.v, a, a, np.zeros(c.n), c.m, c.r2nb)
+    return e, clusters
+
+
+def random_wave(rng, clusters):
+    k = len(clusters)
+    chosen = np.sort(rng.choice(k, max(1, k // 2), replace=False))
+    targets = []
+    for i in chosen:
+        n = clusters[i].n
+        frac = 2.0 ** -rng.integers(0, 6)
+        m = max(1, int(n * frac))
+        targets.append(np.sort(rng.choice(n, m, replace=False)).astype(np.int32))
+    return chosen, targets
+
+
+def test_batched_matches_oracle_and_plain(rf):
+    e, clusters = make_ensemble(rf)
+    rng = np.random.default_rng(9)
+    for wave in range(3):
+        chosen, targets = random_wave(rng, clusters)
+        e.set_wave(chosen, np.zeros(len(chosen)), np.ones(len(chosen)), targets)
+        results = {}
+        for mode in (BATCHED, GRAPH, PLAIN, GRAPH):
+            e.launch(EPS2, mode)
+            results[mode] = e.fetch()
+        b, g, p = results[BATCHED], results[GRAPH], results[PLAIN]
+        for f in ("acc_reg", "jerk_reg", "acc_irr", "jerk_irr", "nnb", "list"):
+            assert np.array_equal(getattr(b, f), getattr(g, f)), f"graph differs in {f}"
+            assert np.array_equal(getattr(b, f), getattr(p, f)), f"plain differs in {f}"
+        for idx, ci in enumerate(chosen):
+            c = clusters[ci]
+            r0, r1 = e.row_splits[idx], e.row_splits[idx + 1]
+            t = targets[idx]
+            ref = oracle.reg_force(c.x, c.v, c.m, c.r2nb, EPS2, t, 128)
+            sub = type(b)(b.acc_reg[r0:r1], b.jerk_reg[r0:r1], b.acc_irr[r0:r1], b.jerk_irr[r0:r1],
+                          b.nnb[r0:r1], b.list[r0:r1])
+            check(sub, ref, f"wave{wave}/cluster{ci}", oracle.reg_scale(c.x, c.v, c.m, c.r2nb, EPS2, t))
+
+
+def test_cluster_result_same_alone_and_in_mix(rf):
+    e, clusters = make_ensemble(rf, k=12, seed=5)
+    rng = np.random.default_rng(2)
+    chosen, targets = random_wave(rng, clusters)
+    e.set_wave(chosen, np.zeros(len(chosen)), np.ones(len(chosen)), targets)
+    e.launch(EPS2, GRAPH)
+    mix = e.fetch()
+    for idx, ci in enumerate(chosen):
+        c = clusters[ci]
+        e.set_wave([ci], [0.0], [1.0], [targets[idx]])
+        e.launch(EPS2, BATCHED)
+        alone = e.fetch()
+        lo = sum(len(t) for t in targets[:idx])
+        hi = lo + len(targets[idx])
+        assert np.array_equal(alone.list, mix.list[lo:hi])
+        assert np.array_equal(alone.nnb, mix.nnb[lo:hi])
+        in_mix = dict(acc_reg=mix.acc_reg[lo:hi], jerk_reg=mix.jerk_reg[lo:hi], acc_irr=mix.acc_irr[lo:hi],
+                      jerk_irr=mix.jerk_irr[lo:hi], nnb=mix.nnb[lo:hi], list=mix.list[lo:hi])
+        # the j-split may differ between the two waves; the difference stays
+        # inside the same per-target bound as the oracle comparison
+        check(alone, in_mix, f"alone-vs-mix/cluster{ci}",
+              oracle.reg_scale(c.x, c.v, c.m, c.r2nb, EPS2, targets[idx]))
+
+
+def test_bad_waves_are_refused(rf):
+    from abyss_b200._lib import AbyssError
+
+    e, clusters = make_ensemble(rf, k=4, seed=6)
+    with pytest.raises(AbyssError):
+        e.set_wave([0, 0], [0.0, 0.0], [1.0, 1.0], [np.array([1]), np.array([2])])  # repeated cluster
+    with pytest.raises(AbyssError):
+        e.set_wave([7], [0.0], [1.0], [np.array([1])])  # no such cluster
+    with pytest.raises(AbyssError):
+        e.set_wave([1], [0.0], [1.0], [np.array([clusters[1].n])])  # index out of range
+    e.set_wave([1], [0.0], [1.0], [np.array([0, 1, 2])])
+    e.launch(EPS2, BATCHED)
+    assert e.fetch().acc_reg.shape == (3, 3)
