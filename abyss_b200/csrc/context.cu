@@ -351,13 +351,25 @@ static abyss_tuning plan_for(abyss_ctx *c, int m, const abyss_tuning *user) {
         break;
       }
   }
-  if (t.kernel == 0) t.kernel = (m <= 64) ? 2 : 1;
+  // Built-in rule (measured on B200, King W0=6, N = 2^20): lanes over j for
+  // tiny active sets; otherwise the packed tile kernel, with anchor offsets on
+  // Morton-ordered targets once the active set is dense enough for them to be
+  // accurate, double-single offsets below that.
+  if (t.kernel == 0) t.kernel = (m <= 64) ? 2 : 3;
   if (t.kernel == 2) {
     if (t.ipt == 0) t.ipt = m <= 1 ? 1 : m <= 2 ? 2 : m <= 4 ? 4 : 8;
   } else if (t.kernel == 3) {
     if (t.mode == 0) t.mode = (m >= 16384) ? 1 : 2;
-    if (t.threads == 0) t.threads = 128;
-    if (t.ipt == 0) t.ipt = 2;
+    if (t.mode == 1) {
+      if (t.threads == 0) t.threads = 256;
+      if (t.ipt == 0) t.ipt = 4;
+      if (t.unroll == 0 && t.threads == 256 && t.ipt == 4) t.unroll = 1;
+      if (t.min_blocks == 0 && t.threads == 256 && t.ipt == 4) t.min_blocks = 2;
+    } else {
+      if (t.threads == 0) t.threads = 128;
+      if (t.ipt == 0) t.ipt = 2;
+      if (t.min_blocks == 0 && t.threads == 128 && t.ipt == 2) t.min_blocks = 4;
+    }
   } else {
     if (t.mode == 0) t.mode = (m >= 4096) ? 1 : 2;
     if (t.threads == 0) t.threads = 128;
@@ -402,6 +414,8 @@ int abyss_launch(abyss_ctx *c, double eps2, int list_cap, const abyss_tuning *tu
     L = chunk;
     S = (n + chunk - 1) / chunk;
     grid = std::min(grid, n_iblocks * S);
+    // TMA bulk copies start at multiples of the chunk length: keep it even
+    if (L % 2 != 0) return fail(c, ABYSS_ERR_STATE, "launch: j-chunk length must be even");
   } else {
     return fail(c, ABYSS_ERR_ARG, "launch: unknown kernel");
   }

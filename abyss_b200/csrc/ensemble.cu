@@ -186,10 +186,13 @@ int abyss_ens_create(abyss_ctx *ctx, int n_clusters, const int *n_per_cluster, i
   e->cap = list_cap;
   e->n_k.assign(n_per_cluster, n_per_cluster + n_clusters);
   e->off_k.resize(n_clusters);
+  // Every cluster starts on a 32-particle boundary: the force kernel's TMA bulk
+  // copies need 16-byte aligned sources (an even index for the FP64 arrays).
+  // The gaps hold padding particles that belong to no cluster (id -1).
   long long tot = 0;
   for (int k = 0; k < n_clusters; ++k) {
     e->off_k[k] = (int)tot;
-    tot += n_per_cluster[k];
+    tot += (n_per_cluster[k] + 31) / 32 * 32;
   }
   if (tot > (1ll << 30)) {
     delete e;
@@ -228,7 +231,7 @@ int abyss_ens_create(abyss_ctx *ctx, int n_clusters, const int *n_per_cluster, i
     return err == cudaErrorMemoryAllocation ? ABYSS_ERR_OOM : ABYSS_ERR_CUDA;
   }
   // cluster id per particle, identity rows
-  std::vector<int> cid(n), iota(n);
+  std::vector<int> cid(n, -1), iota(n);
   for (int k = 0; k < n_clusters; ++k)
     std::fill(cid.begin() + e->off_k[k], cid.begin() + e->off_k[k] + n_per_cluster[k], k);
   std::iota(iota.begin(), iota.end(), 0);
@@ -349,6 +352,8 @@ int abyss_ens_set_wave(abyss_ens *e, int nk, const int *clusters, const double *
     row += m;
     tp += m;
   }
+  for (const WorkItem &it : e->h_items)
+    if (it.j0 % 2 != 0) return efail(e, ABYSS_ERR_STATE, "set_wave: j-range not 16-byte aligned");
   // longest items first: the work queue then drains evenly
   std::stable_sort(e->h_items.begin(), e->h_items.end(), [](const WorkItem &a, const WorkItem &b) {
     return (long long)a.t_count * (a.j1 - a.j0) > (long long)b.t_count * (b.j1 - b.j0);

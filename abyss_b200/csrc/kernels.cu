@@ -83,7 +83,7 @@ __global__ void predict_multi(int n, const int *__restrict__ cid, const int *__r
                               double *__restrict__ pvz, float4 *__restrict__ vm) {
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
     const int k = cid[j];
-    if (!active[k]) continue;
+    if (k < 0 || !active[k]) continue;  // padding between clusters, or an idle cluster
     const double dt = __dmul_rn(__dsub_rn(new_time[k], t0[j]), time_scale[k]);
     double p[3], q[3];
 #pragma unroll
@@ -296,6 +296,8 @@ struct __align__(16) JStage {
 template <int TJ>
 __device__ __forceinline__ void issue_tile(JStage<TJ> *st, uint64_t *bar, const JSet &js, int jt0,
                                            int j1) {
+  // Callers guarantee an even jt0 (16-byte aligned FP64 sources); the host
+  // checks every j-range before a launch.
   const int cnt = min(TJ, j1 - jt0);
   const uint32_t cc = (uint32_t)((cnt + 1) & ~1);  // even count: 16-byte multiples
   const uint32_t b8 = cc * 8u, b16 = cc * 16u;
