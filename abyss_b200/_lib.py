@@ -130,6 +130,10 @@ def lib():
     L.abyss_ac_energy.argtypes = [_vp, _dp]
     L.abyss_ac_get_stats.argtypes = [_vp, C.POINTER(ACStats)]
     L.abyss_ac_last_regular.argtypes = [_vp, _ip, _ip, _dp, _dp, _dp, _dp, _dp, _ip, _ip, C.c_int]
+    L.abyss_ac_begin_block.argtypes = [_vp, _ip, _dp, _dp, _ip]
+    L.abyss_ac_block_targets.argtypes = [_vp, _ip]
+    L.abyss_ac_block_state.argtypes = [_vp] + [_dp] * 7
+    L.abyss_ac_end_block.argtypes = [_vp, _dp, _dp, _dp, _dp, _ip, _ip, C.c_int, _ip]
     L.abyss_ac_last_error.argtypes = [_vp]
     L.abyss_ac_last_error.restype = C.c_char_p
     _LIB = L

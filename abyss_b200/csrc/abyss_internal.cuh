@@ -69,6 +69,7 @@ struct Work {
   const int *m_dev;          // number of rows, read on the device
   const int *row_nchunks;    // chunks per row (else n_chunks)
   const int *row_joff;       // first particle of the row's cluster (lists are cluster-local)
+  const int *row_jlen;       // particles of the row's cluster (else js.n)
 };
 
 struct Outputs {
@@ -77,6 +78,7 @@ struct Outputs {
   int *nnb;             // [m]
   int *list;            // [m][cap]
   int *overflow_rows;   // number of rows whose list exceeded cap
+  int *ovf_list;        // [m] those rows, for the re-list pass
 };
 
 // ---------------------------------------------------------------- PTX helpers

@@ -74,7 +74,7 @@ struct abyss_ctx {
   DevBuf<char> cub_tmp;
   size_t cub_bytes = 0;
   // per-launch work and outputs
-  DevBuf<int> lcnt, lst, status, ovf, items;
+  DevBuf<int> lcnt, lst, status, ovf, items, ovf_list;
   DevBuf<double> part;
   DevBuf<double> acc_reg, jerk_reg, acc_irr, jerk_irr;
   DevBuf<int> nnb, list;
@@ -197,7 +197,7 @@ int abyss_destroy(abyss_ctx *c) {
   for (auto *b : dbl) b->release();
   DevBuf<int> *ints[] = {&c->targets, &c->order_t, &c->order_o, &c->iota, &c->rows, &c->rows_alt,
                          &c->bbox, &c->lcnt, &c->lst, &c->status, &c->ovf, &c->nnb, &c->list,
-                         &c->items};
+                         &c->items, &c->ovf_list};
   for (auto *b : ints) b->release();
   c->vm.release();
   c->keys.release();
@@ -426,6 +426,7 @@ int abyss_launch(abyss_ctx *c, double eps2, int list_cap, const abyss_tuning *tu
   CK(c->lst.ensure((size_t)m * list_cap), "alloc lst");
   CK(c->part.ensure((size_t)S * m * 6), "alloc part");
   CK(c->items.ensure(1), "alloc items");
+  CK(c->ovf_list.ensure((size_t)m), "alloc overflow list");
   CK(cudaMemsetAsync(c->status.p, 0, sizeof(int), c->stream), "clear status");
   CK(cudaMemsetAsync(c->ovf.p, 0, sizeof(int), c->stream), "clear ovf");
   CK(cudaMemsetAsync(c->items.p, 0, sizeof(int), c->stream), "clear work queue");
@@ -450,6 +451,7 @@ int abyss_launch(abyss_ctx *c, double eps2, int list_cap, const abyss_tuning *tu
   w.m_dev = nullptr;
   w.row_nchunks = nullptr;
   w.row_joff = nullptr;
+  w.row_jlen = nullptr;
 
   if (c->profiling) CK(cudaEventRecord(c->ev[0], c->stream), "event");
   if ((t.kernel == 1 || t.kernel == 3) && t.mode == 1) {
@@ -492,6 +494,7 @@ int abyss_launch(abyss_ctx *c, double eps2, int list_cap, const abyss_tuning *tu
   o.nnb = c->nnb.p;
   o.list = c->list.p;
   o.overflow_rows = c->ovf.p;
+  o.ovf_list = c->ovf_list.p;
   launch_finalize(c->stream, js, w, o, c->sm_count);
   CK(cudaGetLastError(), "finalize launch");
   if (c->profiling) CK(cudaEventRecord(c->ev[3], c->stream), "event");

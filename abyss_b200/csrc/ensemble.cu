@@ -12,6 +12,7 @@
 // be captured once into a CUDA graph and replayed for every wave.
 #include <algorithm>
 #include <cstring>
+#include <map>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -46,8 +47,9 @@ struct abyss_ens {
   abyss_ctx *ctx = nullptr;
   cudaStream_t stream = nullptr;
   int device = 0, sm_count = 148;
-  int nc = 0, n_total = 0, cap = 0;
-  std::vector<int> n_k, off_k;
+  int nc = 0, n_total = 0, cap = 0;   // nc = cluster slots, n_total = particle capacity
+  std::vector<int> n_k, off_k;          // n_k = 0: free slot
+  std::map<int, int> free_ranges;       // particle offset -> length, 32-aligned
   long long bytes = 0;
   // state and predicted j-set
   Buf<double> x, v, a0, a1, t0, mass, r2nb, px, py, pz, pvx, pvy, pvz;
@@ -55,15 +57,15 @@ struct abyss_ens {
   Buf<int> cid, active;
   Buf<double> new_time, scale;
   // wave
-  Buf<int> order_t, order_o, row_nch, row_joff, counts;  // counts: [0] rows, [1] items
+  Buf<int> order_t, order_o, row_nch, row_joff, row_jlen, counts;  // counts: [0] rows, [1] items
   Buf<WorkItem> items;
   size_t items_cap = 0;
   // work and outputs
-  Buf<int> lcnt, lst, status, ovf, qhead, list, nnb;
+  Buf<int> lcnt, lst, status, ovf, qhead, list, nnb, ovf_list;
   Buf<double> part, acc_reg, jerk_reg, acc_irr, jerk_irr;
   // host wave description
   int rows = 0, n_items = 0, launches = 0;
-  std::vector<int> h_order, h_nch, h_joff, h_active;
+  std::vector<int> h_order, h_nch, h_joff, h_jlen, h_active;
   std::vector<double> h_time, h_scale;
   std::vector<WorkItem> h_items;
   std::vector<int> wave_clusters, wave_rows_begin, wave_m;
@@ -133,6 +135,7 @@ void make_work(abyss_ens *e, double eps2, int row_begin, const WorkItem *items, 
   w.m_dev = m_dev;
   w.row_nchunks = e->row_nch.p + row_begin;
   w.row_joff = e->row_joff.p + row_begin;
+  w.row_jlen = e->row_jlen.p + row_begin;
   o.targets = e->order_t.p + row_begin;
   o.acc_reg = e->acc_reg.p + 3 * (size_t)row_begin;
   o.jerk_reg = e->jerk_reg.p + 3 * (size_t)row_begin;
@@ -141,6 +144,7 @@ void make_work(abyss_ens *e, double eps2, int row_begin, const WorkItem *items, 
   o.nnb = e->nnb.p + row_begin;
   o.list = e->list.p + (size_t)row_begin * e->cap;
   o.overflow_rows = e->ovf.p;
+  o.ovf_list = e->ovf_list.p + row_begin;
 }
 
 // The batched wave: reset, predict, one tile launch, finalize.  Everything
@@ -170,43 +174,27 @@ int enqueue_batched(abyss_ens *e, double eps2) {
 
 extern "C" {
 
-int abyss_ens_create(abyss_ctx *ctx, int n_clusters, const int *n_per_cluster, int list_cap,
-                     abyss_ens **out) {
-  if (!ctx || n_clusters <= 0 || !n_per_cluster || list_cap <= 0 || list_cap > 8192 || !out)
-    return ABYSS_ERR_ARG;
-  for (int k = 0; k < n_clusters; ++k)
-    if (n_per_cluster[k] < 2) return ABYSS_ERR_ARG;
+int abyss_ens_create_arena(abyss_ctx *ctx, int capacity, int max_clusters, int list_cap, abyss_ens **out) {
+  if (!ctx || capacity < 2 || max_clusters <= 0 || list_cap <= 0 || list_cap > 8192 || !out) return ABYSS_ERR_ARG;
   abyss_ens *e = new abyss_ens;
   e->ctx = ctx;
   e->stream = ctx_stream(ctx);
   e->device = ctx_device(ctx);
   e->sm_count = ctx_sm_count(ctx);
   cudaSetDevice(e->device);
-  e->nc = n_clusters;
+  e->nc = max_clusters;
   e->cap = list_cap;
-  e->n_k.assign(n_per_cluster, n_per_cluster + n_clusters);
-  e->off_k.resize(n_clusters);
-  // Every cluster starts on a 32-particle boundary: the force kernel's TMA bulk
-  // copies need 16-byte aligned sources (an even index for the FP64 arrays).
-  // The gaps hold padding particles that belong to no cluster (id -1).
-  long long tot = 0;
-  for (int k = 0; k < n_clusters; ++k) {
-    e->off_k[k] = (int)tot;
-    tot += (n_per_cluster[k] + 31) / 32 * 32;
-  }
-  if (tot > (1ll << 30)) {
-    delete e;
-    return ABYSS_ERR_ARG;
-  }
-  e->n_total = (int)tot;
+  e->n_total = (capacity + 31) / 32 * 32;
+  e->n_k.assign(max_clusters, 0);
+  e->off_k.assign(max_clusters, 0);
+  e->free_ranges[0] = e->n_total;
   const size_t n = e->n_total;
   e->shape.kernel = 3;
   e->shape.mode = 2;
   e->shape.threads = 128;
   e->shape.ipt = 2;
-  size_t items_cap = 0;
-  for (int k = 0; k < n_clusters; ++k) items_cap += (size_t)((n_per_cluster[k] + 127) / 128) * kSMax;
-  e->items_cap = items_cap;
+  e->shape.min_blocks = 4;
+  e->items_cap = ((size_t)n / 128 + (size_t)max_clusters) * kSMax;
   cudaError_t err = cudaSuccess;
   auto A = [&](auto &b, size_t count) {
     if (err == cudaSuccess) {
@@ -217,9 +205,10 @@ int abyss_ens_create(abyss_ctx *ctx, int n_clusters, const int *n_per_cluster, i
   A(e->x, 3 * n); A(e->v, 3 * n); A(e->a0, 3 * n); A(e->a1, 3 * n);
   A(e->t0, n); A(e->mass, n + 2); A(e->r2nb, n + 2);
   A(e->px, n + 2); A(e->py, n + 2); A(e->pz, n + 2); A(e->pvx, n + 2); A(e->pvy, n + 2); A(e->pvz, n + 2);
-  A(e->vm, n + 2); A(e->cid, n); A(e->active, n_clusters); A(e->new_time, n_clusters); A(e->scale, n_clusters);
-  A(e->order_t, n); A(e->order_o, n); A(e->row_nch, n); A(e->row_joff, n); A(e->counts, 2);
-  A(e->items, 2 * items_cap);  // the batched list, then per-cluster lists of the plain mode
+  A(e->vm, n + 2); A(e->cid, n); A(e->active, max_clusters); A(e->new_time, max_clusters); A(e->scale, max_clusters);
+  A(e->order_t, n); A(e->order_o, n); A(e->row_nch, n); A(e->row_joff, n); A(e->row_jlen, n); A(e->counts, 2);
+  A(e->ovf_list, n);
+  A(e->items, 2 * e->items_cap);  // the batched list, then per-cluster lists of the plain mode
   A(e->lcnt, n); A(e->lst, n * (size_t)list_cap); A(e->status, 1); A(e->ovf, 1); A(e->qhead, 1);
   A(e->list, n * (size_t)list_cap); A(e->nnb, n);
   A(e->part, n * (size_t)kSMax * 6);
@@ -230,23 +219,108 @@ int abyss_ens_create(abyss_ctx *ctx, int n_clusters, const int *n_per_cluster, i
     abyss_ens_destroy(e);
     return err == cudaErrorMemoryAllocation ? ABYSS_ERR_OOM : ABYSS_ERR_CUDA;
   }
-  // cluster id per particle, identity rows
-  std::vector<int> cid(n, -1), iota(n);
-  for (int k = 0; k < n_clusters; ++k)
-    std::fill(cid.begin() + e->off_k[k], cid.begin() + e->off_k[k] + n_per_cluster[k], k);
+  // every particle slot starts unowned (cluster id -1), rows map to themselves
+  std::vector<int> iota(n);
   std::iota(iota.begin(), iota.end(), 0);
-  cudaMemcpy(e->cid.p, cid.data(), n * 4, cudaMemcpyHostToDevice);
+  cudaMemset(e->cid.p, 0xff, n * sizeof(int));
   cudaMemcpy(e->order_o.p, iota.data(), n * 4, cudaMemcpyHostToDevice);
-  cudaMemset(e->active.p, 0, sizeof(int) * n_clusters);
-  e->h_active.assign(n_clusters, 0);
-  e->h_time.assign(n_clusters, 0.0);
-  e->h_scale.assign(n_clusters, 1.0);
+  cudaMemset(e->active.p, 0, sizeof(int) * max_clusters);
+  e->h_active.assign(max_clusters, 0);
+  e->h_time.assign(max_clusters, 0.0);
+  e->h_scale.assign(max_clusters, 1.0);
   const int occ = tile_occupancy(e->shape.threads, e->shape.ipt, e->shape.mode == 1, e->shape.kernel == 3,
                                  e->shape.unroll, e->shape.min_blocks);
   e->grid = std::max(1, occ) * e->sm_count;
   if (cudaDeviceSynchronize() != cudaSuccess) {
     abyss_ens_destroy(e);
     return ABYSS_ERR_CUDA;
+  }
+  *out = e;
+  return ABYSS_OK;
+}
+
+int abyss_ens_attach(abyss_ens *e, int n, int *k_out) {
+  if (!e || n < 2 || !k_out) return ABYSS_ERR_ARG;
+  cudaSetDevice(e->device);
+  int k = -1;
+  for (int i = 0; i < e->nc; ++i)
+    if (e->n_k[i] == 0) {
+      k = i;
+      break;
+    }
+  if (k < 0) return efail(e, ABYSS_ERR_OOM, "attach: no free cluster slot");
+  // Every cluster starts on a 32-particle boundary: the force kernel's TMA bulk
+  // copies need 16-byte aligned sources (an even index for the FP64 arrays).
+  const int len = (n + 31) / 32 * 32;
+  auto it = e->free_ranges.begin();
+  for (; it != e->free_ranges.end(); ++it)
+    if (it->second >= len) break;
+  if (it == e->free_ranges.end()) return efail(e, ABYSS_ERR_OOM, "attach: no room for the cluster");
+  const int off = it->first, rest = it->second - len;
+  e->free_ranges.erase(it);
+  if (rest > 0) e->free_ranges[off + len] = rest;
+  std::vector<int> cid(len, -1);
+  std::fill(cid.begin(), cid.begin() + n, k);
+  ECK(cudaMemcpyAsync(e->cid.p + off, cid.data(), 4 * (size_t)len, cudaMemcpyHostToDevice, e->stream), "H2D cid");
+  ECK(cudaStreamSynchronize(e->stream), "attach");
+  e->n_k[k] = n;
+  e->off_k[k] = off;
+  *k_out = k;
+  return ABYSS_OK;
+}
+
+int abyss_ens_detach(abyss_ens *e, int k) {
+  if (!e || k < 0 || k >= e->nc || e->n_k[k] == 0) return ABYSS_ERR_ARG;
+  cudaSetDevice(e->device);
+  const int off = e->off_k[k], len = (e->n_k[k] + 31) / 32 * 32;
+  ECK(cudaMemsetAsync(e->cid.p + off, 0xff, 4 * (size_t)len, e->stream), "clear cid");
+  ECK(cudaStreamSynchronize(e->stream), "detach");
+  e->n_k[k] = 0;
+  e->h_active[k] = 0;
+  // return the range and merge it with free neighbours
+  auto it = e->free_ranges.emplace(off, len).first;
+  auto nx = std::next(it);
+  if (nx != e->free_ranges.end() && it->first + it->second == nx->first) {
+    it->second += nx->second;
+    e->free_ranges.erase(nx);
+  }
+  if (it != e->free_ranges.begin()) {
+    auto pv = std::prev(it);
+    if (pv->first + pv->second == it->first) {
+      pv->second += it->second;
+      e->free_ranges.erase(it);
+    }
+  }
+  return ABYSS_OK;
+}
+
+int abyss_ens_free_particles(const abyss_ens *e) {
+  if (!e) return ABYSS_ERR_ARG;
+  int best = 0;
+  for (const auto &r : e->free_ranges) best = std::max(best, r.second);
+  return best;
+}
+
+int abyss_ens_create(abyss_ctx *ctx, int n_clusters, const int *n_per_cluster, int list_cap,
+                     abyss_ens **out) {
+  if (!ctx || n_clusters <= 0 || !n_per_cluster || list_cap <= 0 || list_cap > 8192 || !out)
+    return ABYSS_ERR_ARG;
+  long long tot = 0;
+  for (int k = 0; k < n_clusters; ++k) {
+    if (n_per_cluster[k] < 2) return ABYSS_ERR_ARG;
+    tot += (n_per_cluster[k] + 31) / 32 * 32;
+  }
+  if (tot > (1ll << 30)) return ABYSS_ERR_ARG;
+  abyss_ens *e = nullptr;
+  int rc = abyss_ens_create_arena(ctx, (int)tot, n_clusters, list_cap, &e);
+  if (rc != ABYSS_OK) return rc;
+  for (int k = 0; k < n_clusters; ++k) {
+    int slot = -1;
+    rc = abyss_ens_attach(e, n_per_cluster[k], &slot);
+    if (rc != ABYSS_OK || slot != k) {
+      abyss_ens_destroy(e);
+      return rc != ABYSS_OK ? rc : ABYSS_ERR_STATE;
+    }
   }
   *out = e;
   return ABYSS_OK;
@@ -262,7 +336,8 @@ int abyss_ens_destroy(abyss_ens *e) {
                       &e->pvx, &e->pvy, &e->pvz, &e->new_time, &e->scale, &e->part, &e->acc_reg,
                       &e->jerk_reg, &e->acc_irr, &e->jerk_irr};
   for (auto *b : d) b->release();
-  Buf<int> *i[] = {&e->cid, &e->active, &e->order_t, &e->order_o, &e->row_nch, &e->row_joff, &e->counts,
+  Buf<int> *i[] = {&e->cid, &e->active, &e->order_t, &e->order_o, &e->row_nch, &e->row_joff, &e->row_jlen,
+                   &e->ovf_list, &e->counts,
                    &e->lcnt, &e->lst, &e->status, &e->ovf, &e->qhead, &e->list, &e->nnb};
   for (auto *b : i) b->release();
   e->vm.release();
@@ -277,7 +352,8 @@ long long abyss_ens_device_bytes(const abyss_ens *e) { return e ? e->bytes : 0; 
 
 int abyss_ens_upload_state(abyss_ens *e, int k, const double *x, const double *v, const double *a0,
                            const double *a1, const double *t0, const double *mass, const double *r2nb) {
-  if (!e || k < 0 || k >= e->nc || !x || !v || !a0 || !a1 || !t0 || !mass || !r2nb) return ABYSS_ERR_ARG;
+  if (!e || k < 0 || k >= e->nc || e->n_k[k] == 0 || !x || !v || !a0 || !a1 || !t0 || !mass || !r2nb)
+    return ABYSS_ERR_ARG;
   cudaSetDevice(e->device);
   const size_t off = e->off_k[k], n = e->n_k[k];
   cudaStream_t s = e->stream;
@@ -302,30 +378,30 @@ int abyss_ens_set_wave(abyss_ens *e, int nk, const int *clusters, const double *
   e->h_order.clear();
   e->h_nch.clear();
   e->h_joff.clear();
+  e->h_jlen.clear();
   e->h_items.clear();
   e->wave_clusters.assign(clusters, clusters + nk);
   e->wave_rows_begin.assign(nk, 0);
   e->wave_m.assign(m_per, m_per + nk);
   e->cluster_items.assign(nk, {});
   std::fill(e->h_active.begin(), e->h_active.end(), 0);
-  // spread the work over at least ~8 items per CTA in total
-  long long tot_blocks = 0;
-  for (int i = 0; i < nk; ++i) tot_blocks += (m_per[i] + per_block - 1) / per_block;
-  const long long want_items = 8ll * e->grid;
-  int split = (int)std::min<long long>(kSMax, std::max<long long>(1, (want_items + tot_blocks - 1) / std::max(1ll, tot_blocks)));
+  // A cluster's j-chunking depends on its own size only (chunks of at least
+  // 2048 particles, at most kSMax of them), so its rows are summed in the same
+  // order whatever else is in the wave: a cluster's result is the same alone
+  // and in any mix, bit for bit.
   const int *tp = targets_local;
   int row = 0;
   for (int i = 0; i < nk; ++i) {
     const int k = clusters[i];
-    if (k < 0 || k >= e->nc || seen[k]) return efail(e, ABYSS_ERR_ARG, "set_wave: bad or repeated cluster");
+    if (k < 0 || k >= e->nc || e->n_k[k] == 0 || seen[k])
+      return efail(e, ABYSS_ERR_ARG, "set_wave: bad, detached or repeated cluster");
     seen[k] = 1;
     const int m = m_per[i], nkp = e->n_k[k], off = e->off_k[k];
     if (m <= 0 || m > nkp) return efail(e, ABYSS_ERR_ARG, "set_wave: bad target count");
     e->h_active[k] = 1;
     e->h_time[k] = new_time[i];
     e->h_scale[k] = time_scale[i];
-    // j-chunks: split (rounded to tiles) but never shorter than two tiles
-    int S = std::max(1, std::min(split, (nkp + 2 * kTJ - 1) / (2 * kTJ)));
+    int S = std::max(1, std::min(kSMax, (nkp + 2047) / 2048));
     int chunk = ((nkp + S - 1) / S + kTJ - 1) / kTJ * kTJ;
     S = (nkp + chunk - 1) / chunk;
     e->wave_rows_begin[i] = row;
@@ -335,6 +411,7 @@ int abyss_ens_set_wave(abyss_ens *e, int nk, const int *clusters, const double *
       e->h_order.push_back(off + t);
       e->h_nch.push_back(S);
       e->h_joff.push_back(off);
+      e->h_jlen.push_back(nkp);
     }
     for (int b = 0; b < m; b += per_block)
       for (int c = 0; c < S; ++c) {
@@ -366,6 +443,7 @@ int abyss_ens_set_wave(abyss_ens *e, int nk, const int *clusters, const double *
   ECK(cudaMemcpyAsync(e->order_t.p, e->h_order.data(), 4 * (size_t)row, cudaMemcpyHostToDevice, s), "H2D order");
   ECK(cudaMemcpyAsync(e->row_nch.p, e->h_nch.data(), 4 * (size_t)row, cudaMemcpyHostToDevice, s), "H2D nch");
   ECK(cudaMemcpyAsync(e->row_joff.p, e->h_joff.data(), 4 * (size_t)row, cudaMemcpyHostToDevice, s), "H2D joff");
+  ECK(cudaMemcpyAsync(e->row_jlen.p, e->h_jlen.data(), 4 * (size_t)row, cudaMemcpyHostToDevice, s), "H2D jlen");
   ECK(cudaMemcpyAsync(e->items.p, e->h_items.data(), sizeof(WorkItem) * e->h_items.size(),
                       cudaMemcpyHostToDevice, s), "H2D items");
   ECK(cudaMemcpyAsync(e->counts.p, counts, sizeof(counts), cudaMemcpyHostToDevice, s), "H2D counts");
@@ -433,6 +511,7 @@ int abyss_ens_launch(abyss_ens *e, double eps2, int mode, const abyss_tuning *tu
     ECK(cudaMemsetAsync(e->lcnt.p, 0, sizeof(int) * (size_t)e->rows, s), "reset list counts");
     JSet js = jset_of(e);
     e->launches = 0;
+    int ovf_total = 0;
     for (size_t i = 0; i < e->wave_clusters.size(); ++i) {
       const int k = e->wave_clusters[i];
       const int rb = e->wave_rows_begin[i], m = e->wave_m[i];
@@ -453,6 +532,7 @@ int abyss_ens_launch(abyss_ens *e, double eps2, int mode, const abyss_tuning *tu
           "H2D items");
       ECK(cudaMemcpyAsync(d_cnt, cnts, sizeof(cnts), cudaMemcpyHostToDevice, s), "H2D counts");
       ECK(cudaMemsetAsync(e->qhead.p, 0, sizeof(int), s), "reset queue");
+      ECK(cudaMemsetAsync(e->ovf.p, 0, sizeof(int), s), "reset overflow");  // per-cluster re-list count
       Work w;
       Outputs o;
       make_work(e, eps2, rb, d_items, d_cnt + 1, d_cnt, m, w, o);
@@ -465,8 +545,13 @@ int abyss_ens_launch(abyss_ens *e, double eps2, int mode, const abyss_tuning *tu
       // the counts buffer is restored for later batched waves
       const int all[2] = {e->rows, e->n_items};
       ECK(cudaMemcpyAsync(d_cnt, all, sizeof(all), cudaMemcpyHostToDevice, s), "H2D counts");
+      int ovf_k = 0;
+      ECK(cudaMemcpyAsync(&ovf_k, e->ovf.p, sizeof(int), cudaMemcpyDeviceToHost, s), "D2H overflow");
       ECK(cudaStreamSynchronize(s), "plain cluster");  // host arrays reused per cluster
+      ovf_total += ovf_k;
     }
+    ECK(cudaMemcpyAsync(e->ovf.p, &ovf_total, sizeof(int), cudaMemcpyHostToDevice, s), "H2D overflow");
+    ECK(cudaStreamSynchronize(s), "plain wave");
     ECK(cudaGetLastError(), "plain launches");
   } else {
     return efail(e, ABYSS_ERR_ARG, "launch: unknown mode");

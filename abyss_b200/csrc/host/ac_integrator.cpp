@@ -89,6 +89,9 @@ struct abyss_ac {
   std::vector<int> last_targets, last_nnb, last_list;
   std::vector<double> last_px, last_pv, last_r2, last_acc, last_jerk;
   int last_cap = 0;
+  // split form: the regular block begun and not yet ended
+  bool in_block = false;
+  std::vector<int> block_targets;
 };
 
 namespace {
@@ -690,6 +693,13 @@ void regular_correct_one(const abyss_ac *ac, int i, const double *acc, const dou
   out.move = true;
 }
 
+// The host half of a regular block once the force is known: corrector and
+// commit for every target (results in target order, lists [m][cap]).
+int finish_regular(abyss_ac *ac, const std::vector<int> &targets, const std::vector<double> &acc,
+                   const std::vector<double> &jerk, const std::vector<double> &airr,
+                   const std::vector<double> &jirr, const std::vector<int> &nnb, const std::vector<int> &lst,
+                   int cap);
+
 int regular_block(abyss_ac *ac, const std::vector<int> &targets) {
   const double new_time = ac->next_reg_block * ac->time_step;
   std::vector<double> acc, jerk, airr, jirr;
@@ -701,8 +711,14 @@ int regular_block(abyss_ac *ac, const std::vector<int> &targets) {
     if (rc == ABYSS_OK) break;
     if (rc != 2 || attempt > 40) return rc < 0 ? rc : ABYSS_ERR_STATE;
   }
+  return finish_regular(ac, targets, acc, jerk, airr, jirr, nnb, lst, ac->p.nb_max);
+}
+
+int finish_regular(abyss_ac *ac, const std::vector<int> &targets, const std::vector<double> &acc,
+                   const std::vector<double> &jerk, const std::vector<double> &airr,
+                   const std::vector<double> &jirr, const std::vector<int> &nnb, const std::vector<int> &lst,
+                   int cap) {
   const int m = (int)targets.size();
-  const int cap = ac->p.nb_max;
   ac->st.pairs += (double)m * ac->n;
   // keep the last call for parity checks
   ac->last_targets = targets;
@@ -803,15 +819,10 @@ int abyss_ac_destroy(abyss_ac *ac) {
   return ABYSS_OK;
 }
 
-int abyss_ac_advance_block(abyss_ac *ac, int *done) {
-  if (!ac) return ABYSS_ERR_ARG;
-  set_threads(ac);
-  if (ac->done || ac->next_reg_block * ac->time_step >= 1) {
-    ac->done = true;
-    if (done) *done = 1;
-    return ABYSS_OK;
-  }
-  // updateNextRegTime (RootRoutines.cpp:1310-1338)
+namespace {
+// updateNextRegTime (RootRoutines.cpp:1310-1338): the next regular block time
+// and its particles, in ascending index.
+std::vector<int> next_regular_block(abyss_ac *ac) {
   ULL tmin = ac->block_max;
   std::vector<int> targets;
   for (int i = 0; i < ac->n; ++i) {
@@ -825,6 +836,23 @@ int abyss_ac_advance_block(abyss_ac *ac, int *done) {
     }
   }
   ac->next_reg_block = tmin;
+  return targets;
+}
+}  // namespace
+
+int abyss_ac_advance_block(abyss_ac *ac, int *done) {
+  if (!ac) return ABYSS_ERR_ARG;
+  if (ac->in_block) {
+    ac->err = "advance_block: a split block is open";
+    return ABYSS_ERR_STATE;
+  }
+  set_threads(ac);
+  if (ac->done || ac->next_reg_block * ac->time_step >= 1) {
+    ac->done = true;
+    if (done) *done = 1;
+    return ABYSS_OK;
+  }
+  std::vector<int> targets = next_regular_block(ac);
   int rc = irregular_levels(ac);
   if (rc != ABYSS_OK) return rc;
   try {
@@ -833,6 +861,97 @@ int abyss_ac_advance_block(abyss_ac *ac, int *done) {
     ac->err = e.what();
     rc = ABYSS_ERR_STATE;
   }
+  if (rc != ABYSS_OK) return rc;
+  if (ac->next_reg_block * ac->time_step >= 1) ac->done = true;
+  if (done) *done = ac->done ? 1 : 0;
+  return ABYSS_OK;
+}
+
+int abyss_ac_begin_block(abyss_ac *ac, int *m, double *new_time, double *time_scale, int *done) {
+  if (!ac || !m) return ABYSS_ERR_ARG;
+  if (ac->in_block) {
+    ac->err = "begin_block: a block is already open";
+    return ABYSS_ERR_STATE;
+  }
+  set_threads(ac);
+  if (ac->done || ac->next_reg_block * ac->time_step >= 1) {
+    ac->done = true;
+    *m = 0;
+    if (done) *done = 1;
+    return ABYSS_OK;
+  }
+  ac->block_targets = next_regular_block(ac);
+  int rc;
+  try {
+    rc = irregular_levels(ac);
+  } catch (const std::exception &e) {
+    ac->err = e.what();
+    rc = ABYSS_ERR_STATE;
+  }
+  if (rc != ABYSS_OK) return rc;
+  ac->in_block = true;
+  *m = (int)ac->block_targets.size();
+  if (new_time) *new_time = ac->next_reg_block * ac->time_step;
+  if (time_scale) *time_scale = ac->scale;
+  if (done) *done = 0;
+  return ABYSS_OK;
+}
+
+int abyss_ac_block_targets(const abyss_ac *ac, int *targets) {
+  if (!ac || !targets || !ac->in_block) return ABYSS_ERR_ARG;
+  std::copy(ac->block_targets.begin(), ac->block_targets.end(), targets);
+  return ABYSS_OK;
+}
+
+int abyss_ac_block_state(const abyss_ac *ac, double *x, double *v, double *a0, double *a1, double *t0,
+                         double *mass, double *r2nb) {
+  if (!ac || !x || !v || !a0 || !a1 || !t0 || !mass || !r2nb) return ABYSS_ERR_ARG;
+  for (int j = 0; j < ac->n; ++j) {
+    const Star &p = ac->s[j];
+    for (int d = 0; d < 3; ++d) {
+      x[3 * (size_t)j + d] = p.x[d];
+      v[3 * (size_t)j + d] = p.v[d];
+      a0[3 * (size_t)j + d] = p.a_tot[d][0];
+      a1[3 * (size_t)j + d] = p.a_tot[d][1];
+    }
+    t0[j] = p.nb.empty() ? p.t_reg : p.t_irr;  // CalculateRegularAcceleration.cpp:371-374
+    mass[j] = p.m;
+    r2nb[j] = p.r2nb;
+  }
+  return ABYSS_OK;
+}
+
+int abyss_ac_end_block(abyss_ac *ac, const double *acc, const double *jerk, const double *acc_irr,
+                       const double *jerk_irr, const int *nnb, const int *list, int list_cap, int *done) {
+  if (!ac || !acc || !jerk || !acc_irr || !jerk_irr || !nnb || !list || list_cap <= 0) return ABYSS_ERR_ARG;
+  if (!ac->in_block) {
+    ac->err = "end_block: no block is open";
+    return ABYSS_ERR_STATE;
+  }
+  set_threads(ac);
+  const int m = (int)ac->block_targets.size();
+  // a list that did not fit: shrink those radii, commit nothing, ask for a redo
+  bool over = false;
+  for (int k = 0; k < m; ++k)
+    if (nnb[k] > list_cap) {
+      ac->s[ac->block_targets[k]].r2nb *= 0.8;
+      over = true;
+    }
+  if (over) {
+    ac->st.radius_retries++;
+    return ABYSS_WARN_OVERFLOW;
+  }
+  std::vector<double> va(acc, acc + 3 * (size_t)m), vj(jerk, jerk + 3 * (size_t)m),
+      vai(acc_irr, acc_irr + 3 * (size_t)m), vji(jerk_irr, jerk_irr + 3 * (size_t)m);
+  std::vector<int> vn(nnb, nnb + m), vl(list, list + (size_t)m * list_cap);
+  int rc;
+  try {
+    rc = finish_regular(ac, ac->block_targets, va, vj, vai, vji, vn, vl, list_cap);
+  } catch (const std::exception &e) {
+    ac->err = e.what();
+    rc = ABYSS_ERR_STATE;
+  }
+  ac->in_block = false;
   if (rc != ABYSS_OK) return rc;
   if (ac->next_reg_block * ac->time_step >= 1) ac->done = true;
   if (done) *done = ac->done ? 1 : 0;

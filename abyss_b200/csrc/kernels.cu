@@ -296,16 +296,26 @@ struct __align__(16) JStage {
 template <int TJ>
 __device__ __forceinline__ void issue_tile(JStage<TJ> *st, uint64_t *bar, const JSet &js, int jt0,
                                            int j1) {
-  // Callers guarantee an even jt0 (16-byte aligned FP64 sources); the host
-  // checks every j-range before a launch.
+  // The even part of the tile moves by TMA bulk copies (16-byte aligned FP64
+  // sources: callers keep jt0 even, and the host checks every j-range); an odd
+  // last element is loaded by this thread before the arrive, whose release
+  // ordering makes it visible to the waiting threads.  Nothing past j1 is read.
   const int cnt = min(TJ, j1 - jt0);
-  const uint32_t cc = (uint32_t)((cnt + 1) & ~1);  // even count: 16-byte multiples
-  const uint32_t b8 = cc * 8u, b16 = cc * 16u;
+  const int ce = cnt & ~1;
+  if (cnt & 1) {
+    st->x[ce] = js.px[jt0 + ce];
+    st->y[ce] = js.py[jt0 + ce];
+    st->z[ce] = js.pz[jt0 + ce];
+    st->vm[ce] = js.vm[jt0 + ce];
+  }
+  const uint32_t b8 = (uint32_t)ce * 8u, b16 = (uint32_t)ce * 16u;
   mbar_arrive_expect_tx(bar, 3u * b8 + b16);
-  bulk_g2s(st->x, js.px + jt0, b8, bar);
-  bulk_g2s(st->y, js.py + jt0, b8, bar);
-  bulk_g2s(st->z, js.pz + jt0, b8, bar);
-  bulk_g2s(st->vm, js.vm + jt0, b16, bar);
+  if (ce > 0) {
+    bulk_g2s(st->x, js.px + jt0, b8, bar);
+    bulk_g2s(st->y, js.py + jt0, b8, bar);
+    bulk_g2s(st->z, js.pz + jt0, b8, bar);
+    bulk_g2s(st->vm, js.vm + jt0, b16, bar);
+  }
 }
 
 // Packed (FP32x2) pair arithmetic: sm_100's __fadd2_rn / __fmul2_rn / __ffma2_rn
@@ -927,11 +937,80 @@ __global__ void finalize_rows(JSet js, Work w, Outputs o, int sort_cap) {
       }
       o.nnb[r] = total;
       if (total > w.cap) {
-        atomicAdd(o.overflow_rows, 1);
+        const int q = atomicAdd(o.overflow_rows, 1);
+        o.ovf_list[q] = r;
         atomicOr(w.status, kErrOverflow);
       }
     }
     __syncwarp();
+  }
+}
+
+// ============================================================ re-list
+// Rows whose neighbours did not fit in cap were appended in chunk order and kept
+// an arbitrary subset.  One warp per such row scans the row's j-range in
+// ascending order with the exact FP64 test, keeps the first cap neighbours
+// (ballot + popc placement) and recomputes the irregular part over all of them,
+// so an overflowed row reads like the reference's truncated CPU list.
+__global__ void relist_rows(JSet js, Work w, Outputs o) {
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const unsigned lt_mask = (1u << lane) - 1u;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const int nrows = *o.overflow_rows;
+  for (int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < nrows; q += nwarps) {
+    const int r = o.ovf_list[q];
+    const int t = o.targets[r];
+    const int joff = w.row_joff ? w.row_joff[r] : 0;
+    const int j1 = joff + (w.row_jlen ? w.row_jlen[r] : js.n);
+    const double xi = js.px[t], yi = js.py[t], zi = js.pz[t];
+    const double vxi = js.pvx[t], vyi = js.pvy[t], vzi = js.pvz[t];
+    const double R2 = js.r2nb[t];
+    int *out = o.list + (size_t)r * w.cap;
+    int base = 0;
+    double a[6] = {0, 0, 0, 0, 0, 0};
+    for (int jb = joff; jb < j1; jb += 32) {
+      const int j = jb + lane;
+      bool isnb = false;
+      double x[3] = {0, 0, 0}, r2 = 0.0;
+      if (j < j1 && j != t) {
+        x[0] = __dsub_rn(js.px[j], xi);
+        x[1] = __dsub_rn(js.py[j], yi);
+        x[2] = __dsub_rn(js.pz[j], zi);
+        r2 = __dmul_rn(x[0], x[0]);
+        r2 = __dadd_rn(r2, __dmul_rn(x[1], x[1]));
+        r2 = __dadd_rn(r2, __dmul_rn(x[2], x[2]));
+        isnb = r2 < R2;
+      }
+      const unsigned mask = __ballot_sync(FULL, isnb);
+      if (isnb) {
+        const int pos = base + __popc(mask & lt_mask);
+        if (pos < w.cap) out[pos] = j - joff;
+        const double v[3] = {__dsub_rn(js.pvx[j], vxi), __dsub_rn(js.pvy[j], vyi), __dsub_rn(js.pvz[j], vzi)};
+        double vx = 0.0;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) vx = __dadd_rn(vx, __dmul_rn(v[d], x[d]));
+        const double r2s = __dadd_rn(r2, w.eps2);
+        const double m_r3 = __ddiv_rn(__ddiv_rn(js.mass[j], r2s), __dsqrt_rn(r2s));
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          a[d] = __dadd_rn(a[d], __dmul_rn(m_r3, x[d]));
+          const double corr = __ddiv_rn(__dmul_rn(__dmul_rn(3.0, x[d]), vx), r2s);
+          a[3 + d] = __dadd_rn(a[3 + d], __dmul_rn(m_r3, __dsub_rn(v[d], corr)));
+        }
+      }
+      base += __popc(mask);
+    }
+#pragma unroll
+    for (int k = 0; k < 6; ++k)
+      for (int off = 16; off > 0; off >>= 1) a[k] += __shfl_xor_sync(FULL, a[k], off);
+    if (lane == 0) {
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        o.acc_irr[3 * r + d] = a[d];
+        o.jerk_irr[3 * r + d] = a[3 + d];
+      }
+    }
   }
 }
 
@@ -1130,6 +1209,7 @@ void launch_finalize(cudaStream_t s, const JSet &js, const Work &w, const Output
     cudaFuncSetAttribute(finalize_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const int blocks = max(1, min((w.m + warps_per_block - 1) / warps_per_block, sm_count * 32));
   finalize_rows<<<blocks, 32 * warps_per_block, smem, s>>>(js, w, o, P);
+  relist_rows<<<sm_count * 4, 128, 0, s>>>(js, w, o);
 }
 
 void launch_predict_multi(cudaStream_t s, int n, const int *cid, const int *active,
@@ -1149,6 +1229,7 @@ void launch_finalize_grid(cudaStream_t s, const JSet &js, const Work &w, const O
   if (smem > 48 * 1024)
     cudaFuncSetAttribute(finalize_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   finalize_rows<<<blocks, 128, smem, s>>>(js, w, o, P);
+  relist_rows<<<blocks, 128, 0, s>>>(js, w, o);
 }
 
 void launch_energy(cudaStream_t s, int n, const double *x, const double *v, const double *mass,

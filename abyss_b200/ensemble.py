@@ -25,25 +25,54 @@ def _bind(L):
     L.abyss_ens_fetch.argtypes = [_vp, _dp, _dp, _dp, _dp, _ip, _ip, _ip]
     L.abyss_ens_last_ms.argtypes = [_vp, _fp]
     L.abyss_ens_last_stats.argtypes = [_vp, _ip, _ip, _ip]
+    L.abyss_ens_create_arena.argtypes = [_vp, C.c_int, C.c_int, C.c_int, C.POINTER(_vp)]
+    L.abyss_ens_attach.argtypes = [_vp, C.c_int, _ip]
+    L.abyss_ens_detach.argtypes = [_vp, C.c_int]
+    L.abyss_ens_free_particles.argtypes = [_vp]
     L._ens_bound = True
 
 
 class Ensemble:
     """K clusters resident on one GPU; regular force for waves of (cluster, targets)."""
 
-    def __init__(self, rf: RegularForce, sizes, list_cap: int = 256):
+    def __init__(self, rf: RegularForce, sizes=None, list_cap: int = 256, capacity: int = 0,
+                 max_clusters: int = 0):
+        """Fixed clusters of the given sizes, or (sizes=None) an empty arena with room
+        for `capacity` particles in at most `max_clusters` clusters."""
         self._L = _lib.lib()
         _bind(self._L)
         self.rf = rf
-        self.sizes = np.ascontiguousarray(sizes, np.int32)
         self.cap = int(list_cap)
         h = C.c_void_p()
-        rc = self._L.abyss_ens_create(rf._h, int(self.sizes.shape[0]), ptr(self.sizes, _ip), self.cap,
-                                      C.byref(h))
+        if sizes is not None:
+            self.sizes = np.ascontiguousarray(sizes, np.int32)
+            rc = self._L.abyss_ens_create(rf._h, int(self.sizes.shape[0]), ptr(self.sizes, _ip), self.cap,
+                                          C.byref(h))
+        else:
+            self.sizes = np.zeros(int(max_clusters), np.int32)
+            rc = self._L.abyss_ens_create_arena(rf._h, int(capacity), int(max_clusters), self.cap, C.byref(h))
         if rc != 0:
             raise _lib.AbyssError(rc, "abyss_ens_create failed")
         self._h = h
         self.rows = 0
+
+    def attach(self, n: int):
+        """Place a cluster of n particles; returns its id, or None when it does not fit."""
+        k = C.c_int(-1)
+        rc = self._L.abyss_ens_attach(self._h, int(n), C.byref(k))
+        if rc == _lib.ABYSS_ERR_OOM:
+            return None
+        self._check(rc)
+        self.sizes[k.value] = n
+        return int(k.value)
+
+    def detach(self, k: int):
+        self._check(self._L.abyss_ens_detach(self._h, int(k)))
+        self.sizes[k] = 0
+
+    @property
+    def free_particles(self) -> int:
+        return int(self._L.abyss_ens_free_particles(self._h))
 
     def _check(self, rc, allow_overflow=False):
         if rc < 0 or (rc > 0 and not allow_overflow):

@@ -57,6 +57,43 @@ class ACIntegrator:
         self._check(self._L.abyss_ac_advance_block(self._h, C.byref(done)))
         return bool(done.value)
 
+    # ---- split form: the regular force of the block comes from elsewhere
+    def begin_block(self):
+        """Irregular levels up to the next regular block; returns (targets, new_time,
+        time_scale) or None when the run is done."""
+        m = C.c_int(0)
+        nt = C.c_double(0.0)
+        sc = C.c_double(1.0)
+        done = C.c_int(0)
+        self._check(self._L.abyss_ac_begin_block(self._h, C.byref(m), C.byref(nt), C.byref(sc), C.byref(done)))
+        if done.value or m.value == 0:
+            return None
+        t = np.zeros(m.value, np.int32)
+        self._check(self._L.abyss_ac_block_targets(self._h, ptr(t, _ip)))
+        return t, float(nt.value), float(sc.value)
+
+    def block_state(self):
+        n = self.n
+        arrs = dict(x=np.zeros((n, 3)), v=np.zeros((n, 3)), a0=np.zeros((n, 3)), a1=np.zeros((n, 3)),
+                    t0=np.zeros(n), mass=np.zeros(n), r2nb=np.zeros(n))
+        self._check(self._L.abyss_ac_block_state(self._h, *[ptr(arrs[k]) for k in
+                                                             ("x", "v", "a0", "a1", "t0", "mass", "r2nb")]))
+        return arrs
+
+    def end_block(self, acc, jerk, acc_irr, jerk_irr, nnb, lst) -> str:
+        """Commit the block; returns 'ok', 'done' or 'redo' (a list overflowed: the
+        radii were shrunk, fetch block_state again and recompute)."""
+        a = [np.ascontiguousarray(x, np.float64) for x in (acc, jerk, acc_irr, jerk_irr)]
+        nb = np.ascontiguousarray(nnb, np.int32)
+        ls = np.ascontiguousarray(lst, np.int32)
+        done = C.c_int(0)
+        rc = self._L.abyss_ac_end_block(self._h, *[ptr(x) for x in a], ptr(nb, _ip), ptr(ls, _ip),
+                                        int(ls.shape[1]), C.byref(done))
+        if rc == _lib.ABYSS_WARN_OVERFLOW:
+            return "redo"
+        self._check(rc)
+        return "done" if done.value else "ok"
+
     def run(self, t_code: float = 1.0):
         self._check(self._L.abyss_ac_run(self._h, float(t_code)))
 

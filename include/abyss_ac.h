@@ -52,6 +52,25 @@ int abyss_ac_destroy(abyss_ac *ac);
 /* Advance through the next regular block (its irregular levels first, then the
  * regular step).  *done = 1 once code time 1 is reached. */
 int abyss_ac_advance_block(abyss_ac *ac, int *done);
+/* Split form of abyss_ac_advance_block, for callers that batch the regular
+ * force of many integrators into one launch (abyss_ens.h):
+ *   begin_block   runs the irregular levels up to the next regular block and
+ *                 opens it: m targets at new_time (code time), time_scale;
+ *   block_targets the block's targets [m] (ascending particle index);
+ *   block_state   the un-predicted state to upload for the force: x, v, a0, a1
+ *                 [n][3], t0, mass, r2nb [n];
+ *   end_block     hands over the regular force of the targets (rows in target
+ *                 order, as abyss_fetch returns them) and commits the block.
+ * When a target's list did not fit in list_cap, end_block shrinks that
+ * target's radius, commits nothing and returns ABYSS_WARN_OVERFLOW: fetch the
+ * state again, redo the force and call end_block again. */
+int abyss_ac_begin_block(abyss_ac *ac, int *m, double *new_time, double *time_scale, int *done);
+int abyss_ac_block_targets(const abyss_ac *ac, int *targets);
+int abyss_ac_block_state(const abyss_ac *ac, double *x, double *v, double *a0, double *a1, double *t0,
+                         double *mass, double *r2nb);
+int abyss_ac_end_block(abyss_ac *ac, const double *acc, const double *jerk, const double *acc_irr,
+                       const double *jerk_irr, const int *nnb, const int *list, int list_cap, int *done);
+
 /* Advance until code time >= t_code (<= 1). */
 int abyss_ac_run(abyss_ac *ac, double t_code);
 /* Current code time (the last regular block time reached). */

@@ -34,6 +34,17 @@ typedef struct abyss_ens abyss_ens;
 int abyss_ens_create(struct abyss_ctx *ctx, int n_clusters, const int *n_per_cluster, int list_cap,
                      abyss_ens **out);
 int abyss_ens_destroy(abyss_ens *e);
+/* An empty ensemble with room for `capacity` particles in at most max_clusters
+ * clusters (all device memory reserved here).  Clusters then come and go: */
+int abyss_ens_create_arena(struct abyss_ctx *ctx, int capacity, int max_clusters, int list_cap,
+                           abyss_ens **out);
+/* Place a cluster of n particles (first fit, 32-particle aligned); *k is its id.
+ * ABYSS_ERR_OOM when no slot or no contiguous room is free (admission refused). */
+int abyss_ens_attach(abyss_ens *e, int n, int *k);
+/* Release cluster k's slot and particle range. */
+int abyss_ens_detach(abyss_ens *e, int k);
+/* Largest contiguous free particle range. */
+int abyss_ens_free_particles(const abyss_ens *e);
 /* Device bytes the ensemble holds (for admission control). */
 long long abyss_ens_device_bytes(const abyss_ens *e);
 /* Un-predicted FP64 state of cluster k, as abyss_upload_state. */

@@ -3,7 +3,7 @@
 * every cluster's rows match the FP64 oracle (lists exact, forces within the
   bar of tests/test_regforce_gpu.py);
 * the batched launch, its CUDA-graph replay and the one-cluster-per-launch form
-  give bit-identical results (a cluster's result does not depend on the mix);
+  give bit-identical results, and so does a cluster alone versus in a mix;
 * bad waves are refused with a status, and the ensemble stays usable.
 """
 import numpy as np
@@ -87,14 +87,9 @@ def test_cluster_result_same_alone_and_in_mix(rf):
         alone = e.fetch()
         lo = sum(len(t) for t in targets[:idx])
         hi = lo + len(targets[idx])
-        assert np.array_equal(alone.list, mix.list[lo:hi])
-        assert np.array_equal(alone.nnb, mix.nnb[lo:hi])
-        in_mix = dict(acc_reg=mix.acc_reg[lo:hi], jerk_reg=mix.jerk_reg[lo:hi], acc_irr=mix.acc_irr[lo:hi],
-                      jerk_irr=mix.jerk_irr[lo:hi], nnb=mix.nnb[lo:hi], list=mix.list[lo:hi])
-        # the j-split may differ between the two waves; the difference stays
-        # inside the same per-target bound as the oracle comparison
-        check(alone, in_mix, f"alone-vs-mix/cluster{ci}",
-              oracle.reg_scale(c.x, c.v, c.m, c.r2nb, EPS2, targets[idx]))
+        # a cluster's chunking depends on its own size only: bit-identical
+        for f in ("acc_reg", "jerk_reg", "acc_irr", "jerk_irr", "nnb", "list"):
+            assert np.array_equal(getattr(alone, f), getattr(mix, f)[lo:hi]), f"cluster {ci}: {f}"
 
 
 def test_bad_waves_are_refused(rf):
