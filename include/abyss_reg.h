@@ -121,6 +121,27 @@ int abyss_last_timing(abyss_ctx *ctx, float *ms3);
  * the first entry with m <= m_max wins.  k = 0 restores the built-in rule. */
 int abyss_set_tuning_table(abyss_ctx *ctx, int k, const int *m_max, const abyss_tuning *entries);
 
+/* Regular force for callers that cannot allocate device memory (no counterpart
+ * in the reference).  For hosts whose GPU memory is owned by another allocator,
+ * held to a hard budget, or on a path where cudaMalloc/cudaFree may not run:
+ * the caller passes device buffers for inputs (predicted j-set px, py, pz,
+ * pvx, pvy, pvz, mass, r2nb [n]; vm [n][4] = (vx, vy, vz, m) as float; targets
+ * [m]) and outputs (acc/jerk [m][3], nnb [m], list [m][list_cap]); every
+ * intermediate buffer is a fixed array inside the library and nothing is
+ * allocated.  Limits: m <= 4096, list_cap <= 256; larger sizes are rejected
+ * with ABYSS_ERR_ARG and a message on stderr.  px, py, pz, vm must be 16-byte
+ * aligned.  The array is shared by all calls on a device and keeps the last
+ * call's contents; calls that overlap on the GPU race on it and must be
+ * serialized by the caller.  Work runs on `stream` (a cudaStream_t, may be 0)
+ * and the call returns when it has finished.  The first call on a device sets
+ * the array up.  Returns ABYSS_OK, ABYSS_WARN_OVERFLOW or an ABYSS_ERR_* code. */
+int abyss_regular_force_noalloc(int n, const double *px, const double *py, const double *pz,
+                                const float *vm, const double *pvx, const double *pvy,
+                                const double *pvz, const double *mass, const double *r2nb, int m,
+                                const int *targets, double eps2, int list_cap, double *acc_reg,
+                                double *jerk_reg, double *acc_irr, double *jerk_irr, int *nnb,
+                                int *list, void *stream);
+
 /* FP64 total energy (kinetic + softened potential) of n particles. */
 int abyss_energy(abyss_ctx *ctx, int n, const double *x, const double *v, const double *mass,
                  double eps2, double *energy);
