@@ -373,28 +373,26 @@ __device__ __forceinline__ void pair_accum2(const PairGeom2 &g, float2 mj, float
   p[5] = __ffma2_rn(mr3, __ffma2_rn(al, g.dz, g.dvz), p[5]);
 }
 
-// A j-particle in the packed compute buffer: every value duplicated, so each
-// half of a float4 record is a ready float2 operand.
+// A j-particle as packed operands: each value of the compute buffer's float4
+// records broadcast to both halves of a float2.
 struct JPair2 {
   float2 x, y, z, m, vx, vy, vz, lx, ly, lz;
 };
 
 template <bool ANCHOR>
-__device__ __forceinline__ JPair2 load_jpair2(const float4 *cb, int TJP, int jl) {
+__device__ __forceinline__ JPair2 jpair2_of(const float4 &P, const float4 &V, const float4 &L) {
   JPair2 J;
-  const float4 A = cb[jl], B = cb[TJP + jl], C = cb[2 * TJP + jl], D = cb[3 * TJP + jl];
-  J.x = make_float2(A.x, A.y);
-  J.y = make_float2(A.z, A.w);
-  J.z = make_float2(B.x, B.y);
-  J.m = make_float2(B.z, B.w);
-  J.vx = make_float2(C.x, C.y);
-  J.vy = make_float2(C.z, C.w);
-  J.vz = make_float2(D.x, D.y);
+  J.x = dup2(P.x);
+  J.y = dup2(P.y);
+  J.z = dup2(P.z);
+  J.m = dup2(P.w);
+  J.vx = dup2(V.x);
+  J.vy = dup2(V.y);
+  J.vz = dup2(V.z);
   if (!ANCHOR) {
-    const float4 E = cb[4 * TJP + jl], F = cb[5 * TJP + jl];
-    J.lx = make_float2(E.x, E.y);
-    J.ly = make_float2(E.z, E.w);
-    J.lz = make_float2(F.x, F.y);
+    J.lx = dup2(L.x);
+    J.ly = dup2(L.y);
+    J.lz = dup2(L.z);
   } else {
     J.lx = J.ly = J.lz = make_float2(0.f, 0.f);
   }
@@ -423,10 +421,8 @@ __device__ __forceinline__ PairGeom2 geom2_of(const JPair2 &J, int q, const floa
 template <int NT, int IPT, int TJ, int NST, bool ANCHOR, bool PACK>
 struct TileLayout {
   static constexpr int TJP = TJ + 4;           // compute buffer incl. pad entries
-  // float4 records per j.  Scalar: (x,y,z,m) (vx,vy,vz,-) [+ (xl,yl,zl,-)].
-  // Packed: every value duplicated so that each half of a float4 is a ready
-  // float2 operand: (x,x,y,y) (z,z,m,m) (vx,vx,vy,vy) (vz,vz,-,-) [+ (xl,xl,yl,yl) (zl,zl,-,-)].
-  static constexpr int CW = PACK ? (ANCHOR ? 4 : 6) : (ANCHOR ? 2 : 3);
+  // float4 records per j: (x,y,z,m) (vx,vy,vz,-) [+ (xl,yl,zl,-) with double-single].
+  static constexpr int CW = ANCHOR ? 2 : 3;
   static constexpr size_t stage = 0;
   static constexpr size_t cbuf = stage + NST * sizeof(JStage<TJ>);
   static constexpr size_t kahan = cbuf + 2 * CW * TJP * sizeof(float4);  // float [IPT*12][NT]
@@ -451,8 +447,11 @@ __global__ void __launch_bounds__(NT, MINB) reg_force_tile(JSet js, Work w, int 
   using LY = TileLayout<NT, IPT, TJ, NST, ANCHOR, PACK>;
   constexpr int TJP = LY::TJP;
   constexpr int CW = LY::CW;
-  constexpr int PP = PACK ? IPT / 2 : 1;
-  static_assert(!PACK || IPT % 2 == 0, "packed arithmetic holds targets in pairs");
+  // With PACK, targets 0 .. NPK-1 run in pairs on FP32x2 instructions and an odd
+  // last target on scalar ones; without, every target is scalar.
+  constexpr int NPK = PACK ? 2 * (IPT / 2) : 0;
+  constexpr int PP = NPK > 0 ? NPK / 2 : 1;
+  static_assert(32 % UNR == 0 && UNR <= 4, "a 32-j group is whole unroll steps; pad covers UNR - 1");
   extern __shared__ __align__(128) unsigned char smem_raw[];
   JStage<TJ> *st = reinterpret_cast<JStage<TJ> *>(smem_raw + LY::stage);
   float4 *cbuf = reinterpret_cast<float4 *>(smem_raw + LY::cbuf);
@@ -588,20 +587,9 @@ __global__ void __launch_bounds__(NT, MINB) reg_force_tile(JSet js, Work w, int 
           lyj = (float)(Y - (double)fy);
           lzj = (float)(Z - (double)fz);
         }
-        if constexpr (PACK) {
-          cb[jj] = make_float4(fx, fx, fy, fy);
-          cb[TJP + jj] = make_float4(fz, fz, vmj.w, vmj.w);
-          cb[2 * TJP + jj] = make_float4(vmj.x, vmj.x, vmj.y, vmj.y);
-          cb[3 * TJP + jj] = make_float4(vmj.z, vmj.z, 0.0f, 0.0f);
-          if (!ANCHOR) {
-            cb[4 * TJP + jj] = make_float4(lxj, lxj, lyj, lyj);
-            cb[5 * TJP + jj] = make_float4(lzj, lzj, 0.0f, 0.0f);
-          }
-        } else {
-          cb[jj] = make_float4(fx, fy, fz, vmj.w);
-          cb[TJP + jj] = make_float4(vmj.x, vmj.y, vmj.z, 0.0f);
-          if (!ANCHOR) cb[2 * TJP + jj] = make_float4(lxj, lyj, lzj, 0.0f);
-        }
+        cb[jj] = make_float4(fx, fy, fz, vmj.w);
+        cb[TJP + jj] = make_float4(vmj.x, vmj.y, vmj.z, 0.0f);
+        if (!ANCHOR) cb[2 * TJP + jj] = make_float4(lxj, lyj, lzj, 0.0f);
       }
       if (!__syncthreads_and(ok)) {
         if (tid == 0) {
@@ -628,29 +616,39 @@ __global__ void __launch_bounds__(NT, MINB) reg_force_tile(JSet js, Work w, int 
 #pragma unroll
         for (int c = 0; c < 6; ++c) p2[q][c] = make_float2(0.0f, 0.0f);
 
-      for (int jj = 0; jj < cnt; jj += UNR) {
-        bool any = false;
+      // Fast path, 32 j at a time: every pair is accumulated with candidates
+      // (pairs inside the guard band of R_nb) masked to 0, and each thread sets
+      // bit l of cbits when j = g0 + l gave it a candidate.  No branch depends on
+      // the data, so the j iterations schedule freely.  Up to UNR - 1 pad entries
+      // past cnt may be visited: they are far away and massless, never
+      // candidates, and contribute exactly 0.
+      for (int g0 = 0; g0 < cnt; g0 += 32) {
+        const int gl = min(32, cnt - g0);
+        unsigned cbits = 0u;
+        for (int l = 0; l < gl; l += UNR) {
 #pragma unroll
-        for (int u = 0; u < UNR; ++u) {
-          if constexpr (PACK) {
-            const JPair2 J = load_jpair2<ANCHOR>(cb, TJP, jj + u);
+          for (int u = 0; u < UNR; ++u) {
+            const int jl = g0 + l + u;
+            bool any = false;
+            const float4 P = cb[jl];
+            const float4 V = cb[TJP + jl];
+            const float4 L = ANCHOR ? make_float4(0.f, 0.f, 0.f, 0.f) : cb[2 * TJP + jl];
+            if constexpr (NPK > 0) {
+              const JPair2 J = jpair2_of<ANCHOR>(P, V, L);
 #pragma unroll
-            for (int q = 0; q < PP; ++q) {
-              const PairGeom2 g = geom2_of<ANCHOR>(J, q, hx, hy, hz, lx, ly, lz, vx, vy, vz, eps2v);
-              const bool c0 = g.r2.x < r2g[2 * q];
-              const bool c1 = g.r2.y < r2g[2 * q + 1];
-              float2 ri;
-              ri.x = c0 ? 0.0f : rsqrtf(g.r2.x);
-              ri.y = c1 ? 0.0f : rsqrtf(g.r2.y);
-              any |= (c0 | c1);
-              pair_accum2(g, J.m, ri, p2[q]);
+              for (int q = 0; q < NPK / 2; ++q) {
+                const PairGeom2 g = geom2_of<ANCHOR>(J, q, hx, hy, hz, lx, ly, lz, vx, vy, vz, eps2v);
+                const bool c0 = g.r2.x < r2g[2 * q];
+                const bool c1 = g.r2.y < r2g[2 * q + 1];
+                float2 ri;
+                ri.x = c0 ? 0.0f : rsqrtf(g.r2.x);
+                ri.y = c1 ? 0.0f : rsqrtf(g.r2.y);
+                any |= (c0 | c1);
+                pair_accum2(g, J.m, ri, p2[q]);
+              }
             }
-          } else {
-            const float4 P = cb[jj + u];
-            const float4 V = cb[TJP + jj + u];
-            const float4 L = ANCHOR ? make_float4(0.f, 0.f, 0.f, 0.f) : cb[2 * TJP + jj + u];
 #pragma unroll
-            for (int k = 0; k < IPT; ++k) {
+            for (int k = NPK; k < IPT; ++k) {
               const PairGeom gg =
                   ANCHOR ? pair_geom(P.x, P.y, P.z, V.x, V.y, V.z, -hx[k], -hy[k], -hz[k], -vx[k], -vy[k],
                                      -vz[k], w.eps2f)
@@ -662,53 +660,52 @@ __global__ void __launch_bounds__(NT, MINB) reg_force_tile(JSet js, Work w, int 
               any |= cand;
               pair_accum(gg, P.w, rinv, p[k]);
             }
+            cbits |= (unsigned)any << (l + u);
           }
         }
-        if (__any_sync(FULL, any)) {
-          // Slow path: candidates are re-decided with the FP64 test.
+        // Slow path: every j of the group that gave any thread of the warp a
+        // candidate is re-decided with the FP64 test (a warp-uniform loop over
+        // the set bits, in ascending j).
+        unsigned wbits = __reduce_or_sync(FULL, cbits);
+        while (wbits) {
+          const int jl = g0 + __ffs(wbits) - 1;
+          wbits &= wbits - 1u;
+          if (jl >= cnt) break;
+          const int jg = jt0 + jl;
+          const float4 P = cb[jl];
+          const float4 V = cb[TJP + jl];
+          const float4 L = ANCHOR ? make_float4(0.f, 0.f, 0.f, 0.f) : cb[2 * TJP + jl];
+          const float mj = P.w;
 #pragma unroll
-          for (int u = 0; u < UNR; ++u) {
-            const int jl = jj + u;
-            if (jl >= cnt) continue;
-            const int jg = jt0 + jl;
-#pragma unroll
-            for (int k = 0; k < IPT; ++k) {
-              float r2k;
-              PairGeom2 g2;
-              PairGeom gg;
-              float mj;
-              if constexpr (PACK) {
-                const JPair2 J = load_jpair2<ANCHOR>(cb, TJP, jl);
-                g2 = geom2_of<ANCHOR>(J, k >> 1, hx, hy, hz, lx, ly, lz, vx, vy, vz, eps2v);
-                r2k = (k & 1) ? g2.r2.y : g2.r2.x;
-                mj = J.m.x;
-              } else {
-                const float4 P = cb[jl];
-                const float4 V = cb[TJP + jl];
-                const float4 L = ANCHOR ? make_float4(0.f, 0.f, 0.f, 0.f) : cb[2 * TJP + jl];
-                gg = ANCHOR ? pair_geom(P.x, P.y, P.z, V.x, V.y, V.z, -hx[k], -hy[k], -hz[k], -vx[k], -vy[k],
-                                        -vz[k], w.eps2f)
-                            : pair_geom_ds(P.x, P.y, P.z, L.x, L.y, L.z, V.x, V.y, V.z, -hx[k], -hy[k],
-                                           -hz[k], -lx[k], -ly[k], -lz[k], -vx[k], -vy[k], -vz[k], w.eps2f);
-                r2k = gg.r2;
-                mj = P.w;
-              }
-              if (!(r2k < r2g[k])) continue;
-              const int ti = s_ti[k * NT + tid];
-              if (jg == ti) continue;
-              const double r2e = exact_r2(js.px[ti], js.py[ti], js.pz[ti], js.px[jg], js.py[jg], js.pz[jg]);
-              if (r2e < js.r2nb[ti]) {
-                const int row = s_row[k * NT + tid];
-                const int pos = atomicAdd(&w.lcnt[row], 1);
-                if (pos < w.cap) w.lst[(size_t)row * w.cap + pos] = jg;
-              } else {
-                const float rr = rsqrtf(r2k);
-                if constexpr (PACK)
-                  pair_accum2(g2, dup2(mj), (k & 1) ? make_float2(0.0f, rr) : make_float2(rr, 0.0f),
-                              p2[k >> 1]);
-                else
-                  pair_accum(gg, mj, rr, p[k]);
-              }
+          for (int k = 0; k < IPT; ++k) {
+            float r2k;
+            PairGeom2 g2;
+            PairGeom gg;
+            if (k < NPK) {
+              g2 = geom2_of<ANCHOR>(jpair2_of<ANCHOR>(P, V, L), k >> 1, hx, hy, hz, lx, ly, lz, vx, vy, vz,
+                                    eps2v);
+              r2k = (k & 1) ? g2.r2.y : g2.r2.x;
+            } else {
+              gg = ANCHOR ? pair_geom(P.x, P.y, P.z, V.x, V.y, V.z, -hx[k], -hy[k], -hz[k], -vx[k], -vy[k],
+                                      -vz[k], w.eps2f)
+                          : pair_geom_ds(P.x, P.y, P.z, L.x, L.y, L.z, V.x, V.y, V.z, -hx[k], -hy[k], -hz[k],
+                                         -lx[k], -ly[k], -lz[k], -vx[k], -vy[k], -vz[k], w.eps2f);
+              r2k = gg.r2;
+            }
+            if (!(r2k < r2g[k])) continue;
+            const int ti = s_ti[k * NT + tid];
+            if (jg == ti) continue;
+            const double r2e = exact_r2(js.px[ti], js.py[ti], js.pz[ti], js.px[jg], js.py[jg], js.pz[jg]);
+            if (r2e < js.r2nb[ti]) {
+              const int row = s_row[k * NT + tid];
+              const int pos = atomicAdd(&w.lcnt[row], 1);
+              if (pos < w.cap) w.lst[(size_t)row * w.cap + pos] = jg;
+            } else {
+              const float rr = rsqrtf(r2k);
+              if (k < NPK)
+                pair_accum2(g2, dup2(mj), (k & 1) ? make_float2(0.0f, rr) : make_float2(rr, 0.0f), p2[k >> 1]);
+              else
+                pair_accum(gg, mj, rr, p[k]);
             }
           }
         }
@@ -719,7 +716,7 @@ __global__ void __launch_bounds__(NT, MINB) reg_force_tile(JSet js, Work w, int 
 #pragma unroll
         for (int c = 0; c < 6; ++c) {
           float pv;
-          if constexpr (PACK)
+          if (k < NPK)
             pv = (k & 1) ? p2[k >> 1][c].y : p2[k >> 1][c].x;
           else
             pv = p[k][c];
@@ -1140,10 +1137,11 @@ static void tile_run(cudaStream_t s, int grid, const JSet &js, const Work &w, in
 static const TileVariant kTileVariants[] = {
     // scalar pair arithmetic
     TV2(128, 1, false, 2, 1), TV2(128, 2, false, 2, 1), TV2(128, 4, false, 2, 1), TV2(256, 2, false, 2, 1),
-    // packed FP32x2 pair arithmetic
+    // packed FP32x2 pair arithmetic (odd ipt: the last target of a thread on scalar arithmetic)
     TV2(128, 2, true, 2, 1), TV2(128, 2, true, 2, 4), TV2(128, 4, true, 1, 1), TV2(128, 4, true, 2, 1),
     TV2(128, 4, true, 2, 3), TV2(128, 4, true, 1, 4), TV2(256, 2, true, 2, 1), TV2(256, 4, true, 1, 2),
-    TV2(256, 4, true, 2, 1),
+    TV2(256, 4, true, 2, 1), TV2(128, 2, true, 1, 5), TV2(128, 2, true, 4, 4), TV2(128, 4, true, 2, 4),
+    TV2(256, 4, true, 2, 2), TV2(128, 8, true, 1, 2), TV2(128, 6, true, 1, 2), TV2(128, 3, true, 2, 4),
 };
 #undef TV2
 #undef TV

@@ -34,6 +34,9 @@ PACKED = dict(kernel=3, mode=2)
 SHAPES = [
     ("packed-ds-128x2", dict(kernel=3, mode=2, threads=128, ipt=2)),
     ("packed-ds-256x4", dict(kernel=3, mode=2, threads=256, ipt=4)),
+    ("packed-ds-128x4-u2", dict(kernel=3, mode=2, threads=128, ipt=4, unroll=2, min_blocks=4)),
+    ("packed-ds-128x3", dict(kernel=3, mode=2, threads=128, ipt=3)),
+    ("packed-ds-128x8", dict(kernel=3, mode=2, threads=128, ipt=8)),
     ("packed-anchor-128x2", dict(kernel=3, mode=1, threads=128, ipt=2)),
     ("tile-ds-128x1", dict(kernel=1, mode=2, threads=128, ipt=1)),
     ("tile-ds-128x2", dict(kernel=1, mode=2, threads=128, ipt=2)),
@@ -211,7 +214,8 @@ def test_bad_arguments_are_reported_not_trapped(rf):
 
 
 @pytest.mark.parametrize("kernel,threads,ipt", [(1, 128, 2), (1, 128, 4), (1, 256, 2), (3, 128, 2),
-                                                (3, 128, 4), (3, 256, 2), (3, 256, 4)])
+                                                (3, 128, 3), (3, 128, 4), (3, 256, 2), (3, 256, 4),
+                                                (3, 128, 6), (3, 128, 8)])
 def test_anchor_mode_on_dense_active_set(rf, kernel, threads, ipt):
     """Anchor offsets are accurate when a block's targets are spatially compact,
     which the library arranges by Morton-ordering large active sets."""
