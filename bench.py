@@ -140,6 +140,21 @@ class ClockSampler:
                 "samples": len(self.samples)}
 
 
+# DRAM bytes of one force launch of the default workload (N = m = 2^20) with the
+# default anchor plan, from one ncu capture (dram__bytes_read.sum 734.35 MB +
+# dram__bytes_write.sum 997.66 MB).  The kernel is FP32-bound; these bytes are
+# reported beside the FP32 roofline, not against HBM.
+CAPTURED_TRAFFIC = {"n": 1 << 20, "m": 1 << 20, "kernel": 3, "mode": 1, "threads": 128, "ipt": 8,
+                    "bytes": 734.35e6 + 997.66e6}
+
+
+def captured_traffic(n, m, plan):
+    c = CAPTURED_TRAFFIC
+    if n == c["n"] and m == c["m"] and all(plan.get(k) == c[k] for k in ("kernel", "mode", "threads", "ipt")):
+        return c["bytes"]
+    return None
+
+
 def measured_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -369,7 +384,9 @@ def run_ours(args, world, rank, local, pg):
     clk = clocks.get("sm_mhz")
     roofline = {
         "bound": "fp32", "achieved": achieved_tf, "peak": peak_tf, "unit": "TFLOP/s",
-        "frac": achieved_tf / peak_tf, "traffic": None,
+        "frac": achieved_tf / peak_tf, "traffic": captured_traffic(n, m, plan),
+        "traffic_unit": "bytes per force launch (ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
+                        "launch of this workload and plan; null for any other)",
         "note": (f"FP32 CUDA-core pipe: 2 x {sm_count} SMs x 128 lanes x {max_mhz:.0f} MHz "
                  f"(sm_max_mhz of MEASURED_PEAKS.json, {peak_src}); 40 flop/pair; force kernel "
                  f"{f_ms:.1f} ms per launch by CUDA events on the launching stream"),
