@@ -22,7 +22,9 @@ number density (N n(r) 4/3 pi R^3 = k), which is only right on average.
 """
 from __future__ import annotations
 
+import functools
 import math
+import threading
 from dataclasses import dataclass
 
 import numpy as np
@@ -87,7 +89,9 @@ def _r2_exact_k(x: np.ndarray, k: int) -> np.ndarray:
 
     tree = cKDTree(x)
     k = min(k, x.shape[0] - 2)
-    d, _ = tree.query(x, k=k + 2, workers=-1)
+    # all host cores for large clusters; one for small ones, which callers build
+    # many at a time on their own threads
+    d, _ = tree.query(x, k=k + 2, workers=-1 if x.shape[0] >= 65536 else 1)
     # self is d[:, 0]; place R between the k-th and (k+1)-th neighbour
     lo = d[:, k] ** 2
     hi = d[:, k + 1] ** 2
@@ -142,7 +146,19 @@ def plummer(n: int, seed: int, rmax_a: float = 10.0, masses: str = "equal",
     return Cluster(pos, vel, m, r2nb, name=f"plummer_n{n}_s{seed}")
 
 
-def _king_profile(w0: float, npts: int = 4000):
+_KING_LOCK = threading.Lock()
+
+
+def _king_profile(w0: float):
+    """King's profile for W0, computed once per W0 and shared (read-only arrays).
+    The lock makes concurrent first requests for one W0 wait for a single
+    computation instead of each repeating it."""
+    with _KING_LOCK:
+        return _king_profile_solve(float(w0))
+
+
+@functools.lru_cache(maxsize=16)
+def _king_profile_solve(w0: float, npts: int = 4000):
     """Integrate King's equation in units r0 = sigma = G = 1 (rho0 = 9 / 4 pi).
 
     Returns radius grid, W(r), cumulative mass M(r), density rho(r), tidal radius.
@@ -193,7 +209,9 @@ def _king_profile(w0: float, npts: int = 4000):
     # cumulative mass by trapezoid on 4 pi r^2 rho
     shell = 4.0 * math.pi * rs * rs * rho
     mass = np.concatenate([[0.0], np.cumsum(0.5 * (shell[1:] + shell[:-1]) * np.diff(rs))])
-    return rs, ws, mass, rho, rs[-1]
+    for a in (rs, ws, mass, rho):
+        a.setflags(write=False)
+    return rs, ws, mass, rho, float(rs[-1])
 
 
 def king(n: int, seed: int, w0: float = 6.0, masses: str = "equal",

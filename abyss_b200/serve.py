@@ -1,6 +1,6 @@
 """Serving loop: many cluster integrations on one GPU with continuous batching.
 
-A request asks for one cluster (Plummer, or King of a given W0; N particles;
+A request carries one cluster (Plummer, or King of a given W0; N particles;
 Kroupa IMF) to be integrated with the Ahmad-Cohen scheme to code time 1.
 The server keeps every admitted cluster's state resident in one ensemble arena
 on the GPU and runs rounds:
@@ -8,13 +8,16 @@ on the GPU and runs rounds:
   1. admit   waiting requests while the arena has a free slot and a contiguous
              particle range for them (admission by device-memory footprint;
              a request that does not fit waits, the loop never allocates);
+             their initial conditions and integrator set-up run on host
+             threads, each through a regular-force context of its own;
   2. begin   every active integration runs its irregular levels up to its next
              regular block (host threads, in parallel);
   3. wave    the regular forces of all open blocks -- each cluster at its own
              time, with its own active set -- run as ONE replayed CUDA graph
              (prediction, one persistent force launch, finalize);
   4. end     every integration applies its corrector (host threads);
-  5. retire  finished integrations report energy drift, free their range.
+  5. retire  finished integrations report energy drift (host threads) and free
+             their range.
 
 Requests arriving while others are on the GPU join the next round: their work
 shares the device with the ones already running (continuous batching).  A
@@ -26,6 +29,8 @@ from __future__ import annotations
 
 import argparse
 import json
+import queue
+import threading
 import time
 from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass, field
@@ -56,9 +61,14 @@ class Request:
     e1: float = 0.0
     blocks: int = 0
     pending: tuple | None = None   # open block: (targets, new_time, time_scale)
+    cluster: object = None         # the payload: initial conditions (built on admission if None)
+    state: dict | None = None      # its un-predicted state, to upload
+    ctx_lock: object = None        # lock of the context the integrator was set up on
     result: dict = field(default_factory=dict)
 
     def make_cluster(self):
+        if self.cluster is not None:
+            return self.cluster
         if self.model == "plummer":
             return ic.plummer(self.n, self.seed, masses="kroupa", k_nb=self.k_nb)
         return ic.king(self.n, self.seed, float(self.model[4:]), masses="kroupa", k_nb=self.k_nb)
@@ -72,7 +82,15 @@ class Server:
         self.eps2 = eps2
         self.eta_reg, self.eta_irr = eta_reg, eta_irr
         self.list_cap = list_cap
-        self.pool = ThreadPoolExecutor(max_workers=max(1, host_threads))
+        nthreads = max(1, host_threads)
+        self.pool = ThreadPoolExecutor(max_workers=nthreads)
+        # Integrator set-up (its initial force on the GPU) and energies run on
+        # host threads, each through a context of its own: a context serves one
+        # caller at a time, which its lock enforces.
+        self.ctx_free: queue.Queue = queue.Queue()
+        self.ctxs = [(RegularForce(device), threading.Lock()) for _ in range(nthreads)]
+        for c in self.ctxs:
+            self.ctx_free.put(c)
         self.waiting: list[Request] = []
         self.active: list[Request] = []
         self.done: list[Request] = []
@@ -80,6 +98,9 @@ class Server:
         self.rounds = 0
         self.wave_ms = 0.0
         self.peak_active = 0
+        self.phase_s = dict(admit=0.0, begin=0.0, upload=0.0, wave=0.0, end=0.0, retire=0.0)
+        self.build_s = dict(cluster=0.0, wait_ctx=0.0, init=0.0, energy=0.0)
+        self.stat_lock = threading.Lock()
 
     def now(self) -> float:
         return time.perf_counter() - self.t0
@@ -89,14 +110,42 @@ class Server:
         for r in self.active:
             r.ac.close()
         self.ens.close()
+        for rf, _ in self.ctxs:
+            rf.close()
         self.rf.close()
 
     # ------------------------------------------------------------ admission
     def submit(self, req: Request):
         self.waiting.append(req)
 
+    def _build(self, r: Request):
+        """Initial conditions, integrator set-up and initial energy of one request."""
+        t0 = time.perf_counter()
+        c = r.make_cluster()
+        t1 = time.perf_counter()
+        ctx = self.ctx_free.get()
+        try:
+            rf, lock = ctx
+            with lock:
+                t2 = time.perf_counter()
+                r.ac = ACIntegrator(rf, c.x, c.v, c.m, c.r2nb, eps2=self.eps2, eta_reg=self.eta_reg,
+                                    eta_irr=self.eta_irr, fix_nb=r.k_nb, nb_max=self.list_cap, t_end=r.t_end,
+                                    threads=1)
+                t3 = time.perf_counter()
+                r.e0 = r.ac.energy()
+                t4 = time.perf_counter()
+            r.ctx_lock = lock
+            r.cluster = None
+        finally:
+            self.ctx_free.put(ctx)
+        with self.stat_lock:  # thread-seconds spent per part of the set-up
+            self.build_s["cluster"] += t1 - t0
+            self.build_s["wait_ctx"] += t2 - t1
+            self.build_s["init"] += t3 - t2
+            self.build_s["energy"] += t4 - t3
+
     def _admit(self):
-        still = []
+        still, batch = [], []
         for r in self.waiting:
             if r.arrival > self.now():
                 still.append(r)
@@ -105,38 +154,51 @@ class Server:
             if slot is None:
                 still.append(r)  # not enough device room yet: wait for a retirement
                 continue
-            c = r.make_cluster()
             r.slot = slot
-            r.ac = ACIntegrator(self.rf, c.x, c.v, c.m, c.r2nb, eps2=self.eps2, eta_reg=self.eta_reg,
-                                eta_irr=self.eta_irr, fix_nb=r.k_nb, nb_max=self.list_cap, t_end=r.t_end,
-                                threads=1)
-            r.e0 = r.ac.energy()
-            r.admitted = self.now()
-            self.active.append(r)
+            batch.append(r)
         self.waiting = still
+        if batch:
+            list(self.pool.map(self._build, batch))
+            for r in batch:
+                r.admitted = self.now()
+                self.active.append(r)
 
     # ------------------------------------------------------------ one round
+    def _begin(self, r: Request):
+        """Irregular levels up to the next regular block, then the block's state."""
+        if r.pending is None:
+            r.pending = r.ac.begin_block()
+        r.state = r.ac.block_state() if r.pending is not None else None
+
     def round(self):
+        ph = self.phase_s
+        t = time.perf_counter()
         self._admit()
+        ph["admit"] += time.perf_counter() - t
         self.peak_active = max(self.peak_active, len(self.active))
         if not self.active:
             return
-        # begin: irregular levels up to each integration's next regular block
-        need = [r for r in self.active if r.pending is None]
-        for r, res in zip(need, self.pool.map(lambda q: q.ac.begin_block(), need)):
-            r.pending = res
+        t = time.perf_counter()
+        list(self.pool.map(self._begin, self.active))
+        ph["begin"] += time.perf_counter() - t
         finished = [r for r in self.active if r.pending is None]
         live = [r for r in self.active if r.pending is not None]
         if live:
-            states = list(self.pool.map(lambda q: q.ac.block_state(), live))
-            for r, st in zip(live, states):
+            t = time.perf_counter()
+            for r in live:
+                st = r.state
                 self.ens.upload_state(r.slot, st["x"], st["v"], st["a0"], st["a1"], st["t0"], st["mass"], st["r2nb"])
+                r.state = None
+            ph["upload"] += time.perf_counter() - t
+            t = time.perf_counter()
             self.ens.set_wave([r.slot for r in live], [r.pending[1] for r in live], [r.pending[2] for r in live],
                               [r.pending[0] for r in live])
             self.ens.launch(self.eps2, GRAPH)
             out = self.ens.fetch()
             self.wave_ms += self.ens.last_ms()
+            ph["wave"] += time.perf_counter() - t
             sp = self.ens.row_splits
+            t = time.perf_counter()
 
             def end(i):
                 r = live[i]
@@ -152,22 +214,27 @@ class Server:
                 r.blocks += 1
                 if status == "done":
                     finished.append(r)
-        for r in finished:
-            self._retire(r)
+            ph["end"] += time.perf_counter() - t
+        t = time.perf_counter()
+        if finished:
+            list(self.pool.map(self._finish, finished))
+            for r in finished:
+                self.ens.detach(r.slot)
+                self.active.remove(r)
+                self.done.append(r)
+        ph["retire"] += time.perf_counter() - t
         self.rounds += 1
 
-    def _retire(self, r: Request):
-        r.e1 = r.ac.energy()
+    def _finish(self, r: Request):
+        """Final energy and positions of a finished integration; frees it."""
+        with r.ctx_lock:
+            r.e1 = r.ac.energy()
         r.finished = self.now()
         r.result = dict(rid=r.rid, n=r.n, model=r.model, dE_over_E=abs((r.e1 - r.e0) / r.e0), blocks=r.blocks,
                         latency_s=r.finished - r.arrival, queue_s=r.admitted - r.arrival)
-        st = r.ac.state()
-        r.result["x_final"] = st["x"]
+        r.result["x_final"] = r.ac.state()["x"]
         r.ac.close()
         r.ac = None
-        self.ens.detach(r.slot)
-        self.active.remove(r)
-        self.done.append(r)
 
     def run_until_idle(self, max_seconds: float = 1e9):
         while (self.waiting or self.active) and self.now() < max_seconds:
@@ -197,8 +264,11 @@ def serve(rate: float = 200.0, duration: float = 2.0, nmin: int = 256, nmax: int
     """Run a Poisson stream through the server (or, with serial=True, one request at
     a time through the same code) and report latency percentiles and throughput."""
     reqs = poisson_requests(rate, duration, nmin, nmax, seed=seed, t_end=t_end)
+    # a request arrives with its particles: build the payloads before the clock starts
+    for r in reqs:
+        r.cluster = r.make_cluster()
     if serial:
-        done = serve_serial(reqs, host_threads)
+        done, phases = serve_serial(reqs, host_threads)
         rounds, wave_ms, peak = 0, 0.0, 1
         srv = None
     else:
@@ -207,6 +277,7 @@ def serve(rate: float = 200.0, duration: float = 2.0, nmin: int = 256, nmax: int
             srv.submit(r)
         srv.run_until_idle()
         done, rounds, wave_ms, peak = srv.done, srv.rounds, srv.wave_ms, srv.peak_active
+        phases = dict(srv.phase_s, build_thread_s=dict(srv.build_s))
         srv.close()
     wall = max(r.finished for r in done) if done else 0.0
     lat = np.array([r.result["latency_s"] for r in done])
@@ -217,7 +288,7 @@ def serve(rate: float = 200.0, duration: float = 2.0, nmin: int = 256, nmax: int
                p99_latency_s=float(np.percentile(lat, 99)) if len(lat) else None,
                max_dE_over_E=float(de.max()) if len(de) else None,
                median_dE_over_E=float(np.median(de)) if len(de) else None,
-               rounds=rounds, gpu_wave_ms=wave_ms, peak_active=peak,
+               rounds=rounds, gpu_wave_ms=wave_ms, peak_active=peak, phase_s=phases,
                config=dict(rate=rate, duration=duration, nmin=nmin, nmax=nmax, t_end=t_end, capacity=capacity,
                            seed=seed, serial=serial))
     return res, done
@@ -230,16 +301,23 @@ def serve_serial(reqs, host_threads: int = 16):
     rf = RegularForce(0)
     t0 = time.perf_counter()
     done = []
+    phases = dict(cluster=0.0, init=0.0, run=0.0)
     for r in sorted(reqs, key=lambda q: q.arrival):
         wait = r.arrival - (time.perf_counter() - t0)
         if wait > 0:
             time.sleep(wait)
         r.admitted = time.perf_counter() - t0
+        t = time.perf_counter()
         c = r.make_cluster()
+        phases["cluster"] += time.perf_counter() - t
+        t = time.perf_counter()
         ac = ACIntegrator(rf, c.x, c.v, c.m, c.r2nb, eps2=1e-8, eta_reg=0.02, eta_irr=0.01, fix_nb=r.k_nb,
                           nb_max=128, t_end=r.t_end, threads=host_threads)
         r.e0 = ac.energy()
+        phases["init"] += time.perf_counter() - t
+        t = time.perf_counter()
         ac.run(1.0)
+        phases["run"] += time.perf_counter() - t
         r.e1 = ac.energy()
         r.finished = time.perf_counter() - t0
         r.result = dict(rid=r.rid, n=r.n, model=r.model, dE_over_E=abs((r.e1 - r.e0) / r.e0),
@@ -247,7 +325,7 @@ def serve_serial(reqs, host_threads: int = 16):
         ac.close()
         done.append(r)
     rf.close()
-    return done
+    return done, phases
 
 
 def main():
