@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="abyss", choices=["abyss", "reference"])
+    ap.add_argument("--impl", default="abyss", choices=["abyss", "reference", "reference_gpu"])
     ap.add_argument("--n", type=int, default=N_DEFAULT)
     ap.add_argument("--no-sweep", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -259,6 +259,21 @@ def run_reference(args, world, rank, local, pg):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------------ reference GPU kernel
+REF_GPU_UNAVAILABLE = (
+    "the reference's GPU regular force (src_mpi/cuda, float build) made an illegal memory access on "
+    "B200 at N = 2^20 and is not run again: its per-chunk list buffer is sized GridDimY * NNB_per_block * "
+    "target_size = 64 * 128 * 2^20 = 2^33 ints in an int argument (cuda_my_acceleration.cu:695, "
+    "cuda_routines.h:124), which wraps to 0, so compute_forces writes its lists outside any allocation")
+
+
+def run_reference_gpu(args, world, rank, local, pg):
+    """The reference's own GPU kernel as a baseline: unavailable (see the reason)."""
+    if rank != 0:
+        return
+    print(json.dumps({"impl": "reference_gpu", "unavailable": REF_GPU_UNAVAILABLE}), flush=True)
+
+
 # ------------------------------------------------------------------ our arm
 def run_ours(args, world, rank, local, pg):
     import torch
@@ -429,6 +444,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, world, rank, local, pg)
+        elif args.impl == "reference_gpu":
+            run_reference_gpu(args, world, rank, local, pg)
         else:
             run_ours(args, world, rank, local, pg)
     finally:
