@@ -96,6 +96,7 @@ def lib():
     L.abyss_last_timing.argtypes = [_vp, _fp]
     L.abyss_set_tuning_table.argtypes = [_vp, C.c_int, _ip, C.POINTER(Tuning)]
     L.abyss_energy.argtypes = [_vp, C.c_int, _dp, _dp, _dp, C.c_double, _dp]
+    L.abyss_init_derivs23.argtypes = [_vp, C.c_int] + [_dp] * 6 + [C.c_double] + [_dp] * 4
     L.abyss_tile_variant.argtypes = [C.c_int, _ip]
     # reference-compatible drop-in
     L.InitializeDevice.argtypes = [_ip]

@@ -88,6 +88,7 @@ struct abyss_ctx {
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   // scratch for energies
   DevBuf<double> e_x, e_v, e_m, e_row;
+  DevBuf<double> i_a0, i_a1, i_r2, i_out;  // initialisation derivatives
 };
 
 static int fail(abyss_ctx *c, int code, const std::string &msg) {
@@ -193,7 +194,8 @@ int abyss_destroy(abyss_ctx *c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   DevBuf<double> *dbl[] = {&c->x, &c->v, &c->a0, &c->a1, &c->t0, &c->mass, &c->r2nb, &c->px, &c->py,
                            &c->pz, &c->pvx, &c->pvy, &c->pvz, &c->part, &c->acc_reg, &c->jerk_reg,
-                           &c->acc_irr, &c->jerk_irr, &c->e_x, &c->e_v, &c->e_m, &c->e_row};
+                           &c->acc_irr, &c->jerk_irr, &c->e_x, &c->e_v, &c->e_m, &c->e_row,
+                           &c->i_a0, &c->i_a1, &c->i_r2, &c->i_out};
   for (auto *b : dbl) b->release();
   DevBuf<int> *ints[] = {&c->targets, &c->order_t, &c->order_o, &c->iota, &c->rows, &c->rows_alt,
                          &c->bbox, &c->lcnt, &c->lst, &c->status, &c->ovf, &c->nnb, &c->list,
@@ -606,6 +608,44 @@ int abyss_energy(abyss_ctx *c, int n, const double *x, const double *v, const do
   double e = 0.0;
   for (int i = 0; i < n; ++i) e += rows[i];
   *energy = e;
+  return ABYSS_OK;
+}
+
+int abyss_init_derivs23(abyss_ctx *c, int n, const double *x, const double *v, const double *mass,
+                        const double *r2nb, const double *a0, const double *a1, double eps2,
+                        double *reg2, double *reg3, double *irr2, double *irr3) {
+  if (!c || n <= 0 || !x || !v || !mass || !r2nb || !a0 || !a1 || !reg2 || !reg3 || !irr2 || !irr3)
+    return fail(c, ABYSS_ERR_ARG, "init_derivs23: bad args");
+  if (!(eps2 >= 0.0)) return fail(c, ABYSS_ERR_ARG, "init_derivs23: eps2 must be >= 0");
+  cudaSetDevice(c->device);
+  const size_t n3 = (size_t)3 * n;
+  CK(c->e_x.ensure(n3), "alloc");
+  CK(c->e_v.ensure(n3), "alloc");
+  CK(c->e_m.ensure(n), "alloc");
+  CK(c->i_a0.ensure(n3), "alloc");
+  CK(c->i_a1.ensure(n3), "alloc");
+  CK(c->i_r2.ensure(n), "alloc");
+  CK(c->i_out.ensure((size_t)12 * n), "alloc");
+  CK(cudaMemcpyAsync(c->e_x.p, x, 8 * n3, cudaMemcpyHostToDevice, c->stream), "H2D");
+  CK(cudaMemcpyAsync(c->e_v.p, v, 8 * n3, cudaMemcpyHostToDevice, c->stream), "H2D");
+  CK(cudaMemcpyAsync(c->e_m.p, mass, (size_t)8 * n, cudaMemcpyHostToDevice, c->stream), "H2D");
+  CK(cudaMemcpyAsync(c->i_a0.p, a0, 8 * n3, cudaMemcpyHostToDevice, c->stream), "H2D");
+  CK(cudaMemcpyAsync(c->i_a1.p, a1, 8 * n3, cudaMemcpyHostToDevice, c->stream), "H2D");
+  CK(cudaMemcpyAsync(c->i_r2.p, r2nb, (size_t)8 * n, cudaMemcpyHostToDevice, c->stream), "H2D");
+  launch_init_derivs23(c->stream, n, c->e_x.p, c->e_v.p, c->i_a0.p, c->i_a1.p, c->e_m.p, c->i_r2.p, eps2,
+                       c->i_out.p);
+  CK(cudaGetLastError(), "init_derivs23 launch");
+  std::vector<double> out((size_t)12 * n);
+  CK(cudaMemcpyAsync(out.data(), c->i_out.p, (size_t)96 * n, cudaMemcpyDeviceToHost, c->stream), "D2H");
+  CK(cudaStreamSynchronize(c->stream), "synchronize");
+  for (int i = 0; i < n; ++i)
+    for (int d = 0; d < 3; ++d) {
+      const double *o = &out[(size_t)12 * i];
+      reg2[3 * (size_t)i + d] = o[d];
+      reg3[3 * (size_t)i + d] = o[3 + d];
+      irr2[3 * (size_t)i + d] = o[6 + d];
+      irr3[3 * (size_t)i + d] = o[9 + d];
+    }
   return ABYSS_OK;
 }
 

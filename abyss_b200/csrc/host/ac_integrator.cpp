@@ -327,77 +327,42 @@ int upload_and_predict(abyss_ac *ac, double new_time) {
   return rc;
 }
 
-// Initialize.cpp:102-185 (CalculateAcceleration23) with softened r^2, for all i.
-void init_acc23(abyss_ac *ac) {
+// Initialize.cpp:102-185 (CalculateAcceleration23) with softened r^2, for all i,
+// on the device (abyss_init_derivs23: the same sequential FP64 sums, bit for bit).
+int init_acc23(abyss_ac *ac) {
   const int n = ac->n;
-  const double eps2 = ac->p.eps2;
-  std::vector<std::array<double, 24>> out(n);
-#pragma omp parallel for schedule(dynamic, 16)
+  std::vector<double> x(3 * (size_t)n), v(3 * (size_t)n), m(n), r2(n), a0(3 * (size_t)n), a1(3 * (size_t)n);
   for (int i = 0; i < n; ++i) {
-    const Star &p1 = ac->s[i];
-    double reg2[3] = {0, 0, 0}, reg3[3] = {0, 0, 0}, irr2[3] = {0, 0, 0}, irr3[3] = {0, 0, 0};
-    double a1[3], a1dot[3];
+    const Star &p = ac->s[i];
     for (int d = 0; d < 3; ++d) {
-      a1[d] = p1.a_tot[d][0];
-      a1dot[d] = p1.a_tot[d][1];
+      x[3 * (size_t)i + d] = p.x[d];
+      v[3 * (size_t)i + d] = p.v[d];
+      a0[3 * (size_t)i + d] = p.a_tot[d][0];
+      a1[3 * (size_t)i + d] = p.a_tot[d][1];
     }
-    for (int j = 0; j < n; ++j) {
-      if (j == i) continue;
-      const Star &p2 = ac->s[j];
-      double x[3], v[3], a21[3], a21dot[3];
-      double r2u = 0, vr = 0, v2 = 0, rdf_r2 = 0, vdf_r2 = 0, rdfdot_r2 = 0;
-      for (int d = 0; d < 3; ++d) {
-        x[d] = p2.x[d] - p1.x[d];
-        v[d] = p2.v[d] - p1.v[d];
-        r2u += x[d] * x[d];
-        vr += v[d] * x[d];
-        v2 += v[d] * v[d];
-      }
-      const double r2 = r2u + eps2;
-      const double r3 = r2 * std::sqrt(r2);
-      const double m_r3 = p2.m / r3;
-      for (int d = 0; d < 3; ++d) {
-        a21[d] = m_r3 * x[d];
-        a21dot[d] = m_r3 * (v[d] - 3 * x[d] * vr / r2);
-        rdf_r2 += x[d] * (a1[d] - p2.a_tot[d][0]) / r2;
-        vdf_r2 += v[d] * (a1[d] - p2.a_tot[d][0]) / r2;
-        rdfdot_r2 += x[d] * (a1dot[d] - p2.a_tot[d][1]) / r2;
-      }
-      const double a = vr / r2;
-      const double b = v2 / r2 + rdf_r2 + a * a;
-      const double c = 3 * vdf_r2 + rdfdot_r2 + a * (3 * b - 4 * a * a);
-      const bool reg = !(r2u < p1.r2nb);  // the regular-step neighbour rule
-      for (int d = 0; d < 3; ++d) {
-        const double adot2 = -p2.m * (a1[d] - p2.a_tot[d][0]) / r3 - 6 * a * a21dot[d] - 3 * b * a21[d];
-        const double adot3 =
-            -p2.m * (a1dot[d] - p2.a_tot[d][1]) / r3 - 9 * a * adot2 - 9 * b * a21dot[d] - 3 * c * a21[d];
-        if (reg) {
-          reg2[d] += adot2;
-          reg3[d] += adot3;
-        } else {
-          irr2[d] += adot2;
-          irr3[d] += adot3;
-        }
-      }
-    }
-    for (int d = 0; d < 3; ++d) {
-      out[i][d] = reg2[d];
-      out[i][3 + d] = reg3[d];
-      out[i][6 + d] = irr2[d];
-      out[i][9 + d] = irr3[d];
-    }
+    m[i] = p.m;
+    r2[i] = p.r2nb;
+  }
+  std::vector<double> reg2(3 * (size_t)n), reg3(3 * (size_t)n), irr2(3 * (size_t)n), irr3(3 * (size_t)n);
+  const int rc = abyss_init_derivs23(ac->ctx, n, x.data(), v.data(), m.data(), r2.data(), a0.data(), a1.data(),
+                                     ac->p.eps2, reg2.data(), reg3.data(), irr2.data(), irr3.data());
+  if (rc != ABYSS_OK) {
+    ac->err = std::string("init_derivs23: ") + abyss_last_error(ac->ctx);
+    return rc;
   }
   for (int i = 0; i < n; ++i) {
     Star &p = ac->s[i];
     for (int d = 0; d < 3; ++d) {
-      p.a_reg[d][2] = out[i][d];
-      p.a_reg[d][3] = out[i][3 + d];
-      p.a_irr[d][2] = out[i][6 + d];
-      p.a_irr[d][3] = out[i][9 + d];
+      const size_t k = 3 * (size_t)i + d;
+      p.a_reg[d][2] = reg2[k];
+      p.a_reg[d][3] = reg3[k];
+      p.a_irr[d][2] = irr2[k];
+      p.a_irr[d][3] = irr3[k];
       p.a_tot[d][2] = p.a_reg[d][2] + p.a_irr[d][2];
       p.a_tot[d][3] = p.a_reg[d][3] + p.a_irr[d][3];
     }
   }
+  return ABYSS_OK;
 }
 
 // Initialize.cpp:199-230 (initializeTimeStep).
@@ -453,7 +418,10 @@ int initialise(abyss_ac *ac, const double *r2nb) {
     }
     p.nb.assign(lst.begin() + (size_t)i * cap, lst.begin() + (size_t)i * cap + nnb[i]);
   }
-  init_acc23(ac);  // InitAcc2
+  {  // InitAcc2
+    const int rc = init_acc23(ac);
+    if (rc != ABYSS_OK) return rc;
+  }
   for (int i = 0; i < n; ++i) init_time_step(ac, ac->s[i]);  // InitTime
   // time-step correction and time_block (RootRoutines.cpp:240-270)
   int min_level = 0;

@@ -37,6 +37,10 @@ void launch_predict_multi(cudaStream_t s, int n, const int *cid, const int *acti
 void launch_finalize_grid(cudaStream_t s, const JSet &js, const Work &w, const Outputs &o, int blocks);
 void launch_energy(cudaStream_t s, int n, const double *x, const double *v, const double *mass,
                    double eps2, double *e_row);
+// init_derivs.cu: out [n][12] = (reg2, reg3, irr2, irr3) x 3 dimensions
+void launch_init_derivs23(cudaStream_t s, int n, const double *x, const double *v, const double *a0,
+                          const double *a1, const double *mass, const double *r2nb, double eps2,
+                          double *out);
 
 }  // namespace abyss
 

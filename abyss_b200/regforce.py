@@ -176,6 +176,16 @@ class RegularForce:
             arr[i] = Tuning(**d)
         self._check(self._L.abyss_set_tuning_table(self._h, k, ptr(mm, _ip), arr))
 
+    def init_derivs23(self, x, v, mass, r2nb, a0, a1, eps2: float = 0.0) -> dict:
+        """Second and third acceleration derivatives at a common time, split into
+        regular and irregular parts (include/abyss_reg.h abyss_init_derivs23)."""
+        n = int(np.asarray(mass).shape[0])
+        ins = [_f64(x, (n, 3)), _f64(v, (n, 3)), _f64(mass), _f64(r2nb), _f64(a0, (n, 3)), _f64(a1, (n, 3))]
+        out = {k: np.zeros((n, 3)) for k in ("reg2", "reg3", "irr2", "irr3")}
+        self._check(self._L.abyss_init_derivs23(self._h, n, *[ptr(a) for a in ins], float(eps2),
+                                                *[ptr(out[k]) for k in ("reg2", "reg3", "irr2", "irr3")]))
+        return out
+
     def energy(self, x, v, mass, eps2: float = 0.0) -> float:
         n = int(np.asarray(mass).shape[0])
         e = C.c_double(0.0)

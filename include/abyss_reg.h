@@ -142,6 +142,19 @@ int abyss_regular_force_noalloc(int n, const double *px, const double *py, const
                                 double *jerk_reg, double *acc_irr, double *jerk_irr, int *nnb,
                                 int *list, void *stream);
 
+/* Second and third time derivatives of the acceleration of n particles at one
+ * common time: the initialisation pass of the scheme (the reference's
+ * CalculateAcceleration23, src_mpi/Particle/Initialize.cpp:102-185, run there
+ * on the host for every particle).  Split into regular (r^2 >= R^2, unsoftened
+ * r^2) and irregular parts; eps2 is added to r^2 in the force terms.  FP64 on
+ * the device, one target per thread summing j in ascending order in the
+ * reference's operation order, so each value equals that sequential loop bit
+ * for bit.  Host arrays: x, v, a0 (acceleration), a1 (jerk) [n][3], mass and
+ * r2nb [n]; outputs [n][3].  Synchronous. */
+int abyss_init_derivs23(abyss_ctx *ctx, int n, const double *x, const double *v, const double *mass,
+                        const double *r2nb, const double *a0, const double *a1, double eps2,
+                        double *reg2, double *reg3, double *irr2, double *irr3);
+
 /* FP64 total energy (kinetic + softened potential) of n particles. */
 int abyss_energy(abyss_ctx *ctx, int n, const double *x, const double *v, const double *mass,
                  double eps2, double *energy);

@@ -63,6 +63,7 @@ def lib():
         L.oracle_reg_scale.argtypes = [C.c_int, _dp, _dp, _dp, _dp, C.c_double, C.c_int, _ip, _dp, _dp,
                                        C.c_int]
         L.oracle_energy.restype = C.c_double
+        L.oracle_init_derivs23.argtypes = [C.c_int] + [_dp] * 6 + [C.c_double, C.c_int, _ip] + [_dp] * 4 + [C.c_int]
         _LIB = L
     return _LIB
 
@@ -177,3 +178,14 @@ def hermite_correct(pos, vel, a_reg_old, a_new, adot_new, a_tmp, adot_tmp, dt):
 def energy(x, v, m, eps2, nthreads=0):
     return lib().oracle_energy(x.shape[0], _p(np.ascontiguousarray(x)), _p(np.ascontiguousarray(v)),
                                _p(np.ascontiguousarray(m)), eps2, nthreads)
+
+
+def init_derivs23(x, v, m, r2nb, a0, a1, eps2, targets, nthreads=0):
+    """Second and third acceleration derivatives, split (CalculateAcceleration23)."""
+    f = lambda a: np.ascontiguousarray(a, np.float64)
+    x, v, m, r2nb, a0, a1 = map(f, (x, v, m, r2nb, a0, a1))
+    t = np.ascontiguousarray(targets, np.int32)
+    out = [np.zeros((t.shape[0], 3)) for _ in range(4)]
+    lib().oracle_init_derivs23(x.shape[0], _p(x), _p(v), _p(m), _p(r2nb), _p(a0), _p(a1), eps2, t.shape[0],
+                               _p(t, _ip), *[_p(o) for o in out], nthreads)
+    return dict(reg2=out[0], reg3=out[1], irr2=out[2], irr3=out[3])

@@ -236,3 +236,67 @@ void oracle_reg_scale(int n, const double *px, const double *pv, const double *m
         jerk_abs[k] = sj;
     }
 }
+
+/* CalculateAcceleration23, src_mpi/Particle/Initialize.cpp:102-185: the same
+ * expressions in the same order (a21, a21dot, rdf_r2, vdf_r2, rdfdot_r2, then
+ * a, b, c, then adot2, adot3 per dimension). */
+void oracle_init_derivs23(int n, const double *x, const double *v, const double *mass,
+                          const double *r2nb, const double *a0, const double *a1, double eps2,
+                          int nt, const int *targets, double *reg2, double *reg3, double *irr2,
+                          double *irr3, int nthreads) {
+    set_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int k = 0; k < nt; ++k) {
+        const int i = targets[k];
+        double r2o[3] = {0, 0, 0}, r3o[3] = {0, 0, 0}, i2o[3] = {0, 0, 0}, i3o[3] = {0, 0, 0};
+        double a1i[3], a1doti[3];
+        for (int d = 0; d < 3; ++d) {
+            a1i[d] = a0[3 * i + d];
+            a1doti[d] = a1[3 * i + d];
+        }
+        for (int j = 0; j < n; ++j) {
+            if (j == i) continue;
+            double xx[3], vv[3], a21[3], a21dot[3];
+            double r2u = 0.0, vr = 0.0, v2 = 0.0, rdf_r2 = 0.0, vdf_r2 = 0.0, rdfdot_r2 = 0.0;
+            for (int d = 0; d < 3; ++d) {
+                xx[d] = x[3 * j + d] - x[3 * i + d];
+                vv[d] = v[3 * j + d] - v[3 * i + d];
+                r2u += xx[d] * xx[d];
+                vr += vv[d] * xx[d];
+                v2 += vv[d] * vv[d];
+            }
+            const double r2 = r2u + eps2;
+            const double r3 = r2 * sqrt(r2);
+            const double m_r3 = mass[j] / r3;
+            for (int d = 0; d < 3; ++d) {
+                a21[d] = m_r3 * xx[d];
+                a21dot[d] = m_r3 * (vv[d] - 3 * xx[d] * vr / r2);
+                rdf_r2 += xx[d] * (a1i[d] - a0[3 * j + d]) / r2;
+                vdf_r2 += vv[d] * (a1i[d] - a0[3 * j + d]) / r2;
+                rdfdot_r2 += xx[d] * (a1doti[d] - a1[3 * j + d]) / r2;
+            }
+            const double a = vr / r2;
+            const double b = v2 / r2 + rdf_r2 + a * a;
+            const double c = 3 * vdf_r2 + rdfdot_r2 + a * (3 * b - 4 * a * a);
+            const int reg = !(r2u < r2nb[i]);
+            for (int d = 0; d < 3; ++d) {
+                const double adot2 = -mass[j] * (a1i[d] - a0[3 * j + d]) / r3 - 6 * a * a21dot[d] - 3 * b * a21[d];
+                const double adot3 = -mass[j] * (a1doti[d] - a1[3 * j + d]) / r3 - 9 * a * adot2 -
+                                     9 * b * a21dot[d] - 3 * c * a21[d];
+                if (reg) {
+                    r2o[d] += adot2;
+                    r3o[d] += adot3;
+                } else {
+                    i2o[d] += adot2;
+                    i3o[d] += adot3;
+                }
+            }
+        }
+        for (int d = 0; d < 3; ++d) {
+            reg2[3 * k + d] = r2o[d];
+            reg3[3 * k + d] = r3o[d];
+            irr2[3 * k + d] = i2o[d];
+            irr3[3 * k + d] = i3o[d];
+        }
+    }
+}

@@ -74,6 +74,17 @@ void oracle_reg_scale(int n, const double *px, const double *pv, const double *m
                       double *acc_abs, double *jerk_abs, int nthreads);
 
 /* Total energy T + W (FP64, softened potential) of n particles. */
+/* Second and third derivatives of the acceleration at a common time, split into
+ * regular (r^2 >= R^2, unsoftened) and irregular parts: CalculateAcceleration23
+ * (src_mpi/Particle/Initialize.cpp:102-185) in its operation order, j ascending,
+ * with eps2 added to r^2 in the force terms.  x, v, a0, a1: [n][3]; targets
+ * [nt]; outputs [nt][3].  With eps2 = 0 it equals the reference except for a
+ * pair at exactly r^2 = R^2 (the reference counts it irregular). */
+void oracle_init_derivs23(int n, const double *x, const double *v, const double *mass,
+                          const double *r2nb, const double *a0, const double *a1, double eps2,
+                          int nt, const int *targets, double *reg2, double *reg3, double *irr2,
+                          double *irr3, int nthreads);
+
 double oracle_energy(int n, const double *x, const double *v, const double *mass,
                      double eps2, int nthreads);
 
