@@ -32,7 +32,10 @@ struct DevBuf {
     if (p) cudaFree(p);
     p = nullptr;
     cap = 0;
-    size_t want = std::max<size_t>(n, 1);
+    // a buffer that has to grow grows by at least half again, so a context
+    // that sees slowly rising sizes reallocates (and synchronizes the device
+    // in cudaFree) only a few times
+    size_t want = std::max<size_t>(std::max<size_t>(n, 1), cap + cap / 2);
     want = (want + kPad - 1) / kPad * kPad;
     cudaError_t e = cudaMalloc((void **)&p, want * sizeof(T));
     if (e != cudaSuccess) {
@@ -228,8 +231,26 @@ int abyss_reserve(abyss_ctx *c, int n, int m, int list_cap) {
   cudaSetDevice(c->device);
   int rc;
   if ((rc = ensure_jset(c, n)) != ABYSS_OK) return rc;
-  if ((rc = ensure_targets(c, std::max(m, 1))) != ABYSS_OK) return rc;
-  if ((rc = ensure_outputs(c, std::max(m, 1), std::max(list_cap, 1))) != ABYSS_OK) return rc;
+  const int m1 = std::max(m, 1), cap1 = std::max(list_cap, 1);
+  if ((rc = ensure_targets(c, m1)) != ABYSS_OK) return rc;
+  if ((rc = ensure_outputs(c, m1, cap1)) != ABYSS_OK) return rc;
+  // un-predicted state, energy and initialisation buffers for n particles
+  const size_t n3 = (size_t)3 * std::max(n, 1);
+  DevBuf<double> *st[] = {&c->x, &c->v, &c->a0, &c->a1, &c->e_x, &c->e_v, &c->i_a0, &c->i_a1};
+  for (auto *b : st) CK(b->ensure(n3), "alloc state");
+  DevBuf<double> *st1[] = {&c->t0, &c->e_m, &c->e_row, &c->i_r2};
+  for (auto *b : st1) CK(b->ensure(std::max(n, 1)), "alloc state");
+  CK(c->i_out.ensure((size_t)12 * std::max(n, 1)), "alloc init");
+  // work buffers of the tile kernel: chunk partials for at most the chunk count
+  // a launch plan can choose (<= n / 1024 chunks, and <= 32 items per CTA of a
+  // grid of at most 8 CTAs per SM over i-blocks of >= 128 targets)
+  const int s_items = (int)((32LL * 8 * c->sm_count) / std::max(1, (m1 + 127) / 128)) + 1;
+  const int s_max = std::max(1, std::min((std::max(n, 1) + 1023) / 1024, s_items));
+  CK(c->lcnt.ensure((size_t)m1), "alloc lcnt");
+  CK(c->lst.ensure((size_t)m1 * cap1), "alloc lst");
+  CK(c->part.ensure((size_t)s_max * m1 * 6), "alloc part");
+  CK(c->items.ensure(1), "alloc items");
+  CK(c->ovf_list.ensure((size_t)m1), "alloc overflow list");
   return ABYSS_OK;
 }
 

@@ -79,6 +79,16 @@ struct abyss_ens {
   abyss_tuning graph_shape{};
   double graph_eps2 = -1.0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // pinned host staging of the state arrays, laid out like the device arena
+  // (15 doubles per particle: x, v, a0, a1 [3] each, t0, mass, r2nb)
+  double *stage = nullptr;
+  int chunk_j = 2048;  // j per chunk of a cluster (>= 128): its chunk count is ceil(n_k / chunk_j), <= kSMax
+  // pinned host staging of a wave's description (set_wave) and of its results
+  // (fetch_view), so that neither goes through pageable copies
+  unsigned char *wstage = nullptr;
+  size_t wstage_bytes = 0;
+  unsigned char *ostage = nullptr;
+  size_t ostage_bytes = 0;
   std::string err;
 };
 
@@ -344,11 +354,99 @@ int abyss_ens_destroy(abyss_ens *e) {
   e->items.release();
   if (e->ev0) cudaEventDestroy(e->ev0);
   if (e->ev1) cudaEventDestroy(e->ev1);
+  if (e->stage) cudaFreeHost(e->stage);
+  if (e->wstage) cudaFreeHost(e->wstage);
+  if (e->ostage) cudaFreeHost(e->ostage);
   delete e;
   return ABYSS_OK;
 }
 
 long long abyss_ens_device_bytes(const abyss_ens *e) { return e ? e->bytes : 0; }
+
+int abyss_ens_list_cap(const abyss_ens *e) { return e ? e->cap : 0; }
+
+int abyss_ens_set_chunk(abyss_ens *e, int j_per_chunk) {
+  if (!e || j_per_chunk < kTJ) return ABYSS_ERR_ARG;
+  e->chunk_j = j_per_chunk;
+  return ABYSS_OK;
+}
+
+int abyss_ens_stage(abyss_ens *e, int k, double **x, double **v, double **a0, double **a1, double **t0,
+                    double **mass, double **r2nb) {
+  if (!e || k < 0 || k >= e->nc || e->n_k[k] == 0 || !x || !v || !a0 || !a1 || !t0 || !mass || !r2nb)
+    return ABYSS_ERR_ARG;
+  if (!e->stage) return efail(e, ABYSS_ERR_STATE, "stage: call abyss_ens_stage_reserve first");
+  const size_t N = (size_t)e->n_total, off = e->off_k[k];
+  double *b = e->stage;
+  *x = b + 3 * off;
+  *v = b + 3 * N + 3 * off;
+  *a0 = b + 6 * N + 3 * off;
+  *a1 = b + 9 * N + 3 * off;
+  *t0 = b + 12 * N + off;
+  *mass = b + 13 * N + off;
+  *r2nb = b + 14 * N + off;
+  return ABYSS_OK;
+}
+
+int abyss_ens_stage_reserve(abyss_ens *e) {
+  if (!e) return ABYSS_ERR_ARG;
+  if (e->stage) return ABYSS_OK;
+  cudaSetDevice(e->device);
+  ECK(cudaMallocHost((void **)&e->stage, (size_t)15 * e->n_total * sizeof(double)), "pinned staging");
+  return ABYSS_OK;
+}
+
+int abyss_ens_upload_staged(abyss_ens *e, int nk, const int *clusters) {
+  if (!e || nk < 0 || (nk > 0 && !clusters)) return ABYSS_ERR_ARG;
+  if (!e->stage) return efail(e, ABYSS_ERR_STATE, "upload_staged: nothing staged");
+  if (nk == 0) return ABYSS_OK;
+  std::vector<char> listed(e->nc, 0);
+  for (int i = 0; i < nk; ++i) {
+    const int k = clusters[i];
+    if (k < 0 || k >= e->nc || e->n_k[k] == 0) return efail(e, ABYSS_ERR_ARG, "upload_staged: bad cluster");
+    listed[k] = 1;
+  }
+  // walk every placed cluster in arena order; a run of listed clusters is copied
+  // in one go (free gaps inside it are copied too), and an unlisted cluster ends
+  // the run, so its device state is never touched
+  std::vector<std::pair<int, int>> placed;  // (offset, cluster)
+  for (int k = 0; k < e->nc; ++k)
+    if (e->n_k[k] > 0) placed.emplace_back(e->off_k[k], k);
+  std::sort(placed.begin(), placed.end());
+  cudaSetDevice(e->device);
+  cudaStream_t s = e->stream;
+  const size_t N = (size_t)e->n_total;
+  const double *b = e->stage;
+  auto copy = [&](size_t lo, size_t hi) -> int {
+    const size_t n = hi - lo;
+    ECK(cudaMemcpyAsync(e->x.p + 3 * lo, b + 3 * lo, 24 * n, cudaMemcpyHostToDevice, s), "H2D x");
+    ECK(cudaMemcpyAsync(e->v.p + 3 * lo, b + 3 * N + 3 * lo, 24 * n, cudaMemcpyHostToDevice, s), "H2D v");
+    ECK(cudaMemcpyAsync(e->a0.p + 3 * lo, b + 6 * N + 3 * lo, 24 * n, cudaMemcpyHostToDevice, s), "H2D a0");
+    ECK(cudaMemcpyAsync(e->a1.p + 3 * lo, b + 9 * N + 3 * lo, 24 * n, cudaMemcpyHostToDevice, s), "H2D a1");
+    ECK(cudaMemcpyAsync(e->t0.p + lo, b + 12 * N + lo, 8 * n, cudaMemcpyHostToDevice, s), "H2D t0");
+    ECK(cudaMemcpyAsync(e->mass.p + lo, b + 13 * N + lo, 8 * n, cudaMemcpyHostToDevice, s), "H2D mass");
+    ECK(cudaMemcpyAsync(e->r2nb.p + lo, b + 14 * N + lo, 8 * n, cudaMemcpyHostToDevice, s), "H2D r2nb");
+    return ABYSS_OK;
+  };
+  bool open = false;
+  size_t lo = 0, hi = 0;
+  for (const auto &pk : placed) {
+    const int k = pk.second;
+    if (listed[k]) {
+      if (!open) {
+        lo = (size_t)e->off_k[k];
+        open = true;
+      }
+      hi = (size_t)e->off_k[k] + e->n_k[k];
+    } else if (open) {
+      const int rc = copy(lo, hi);
+      if (rc != ABYSS_OK) return rc;
+      open = false;
+    }
+  }
+  if (open) return copy(lo, hi);
+  return ABYSS_OK;
+}
 
 int abyss_ens_upload_state(abyss_ens *e, int k, const double *x, const double *v, const double *a0,
                            const double *a1, const double *t0, const double *mass, const double *r2nb) {
@@ -386,9 +484,9 @@ int abyss_ens_set_wave(abyss_ens *e, int nk, const int *clusters, const double *
   e->cluster_items.assign(nk, {});
   std::fill(e->h_active.begin(), e->h_active.end(), 0);
   // A cluster's j-chunking depends on its own size only (chunks of at least
-  // 2048 particles, at most kSMax of them), so its rows are summed in the same
-  // order whatever else is in the wave: a cluster's result is the same alone
-  // and in any mix, bit for bit.
+  // chunk_j particles, at most kSMax of them), so its rows are summed in the
+  // same order whatever else is in the wave: a cluster's result is the same
+  // alone and in any mix, bit for bit.
   const int *tp = targets_local;
   int row = 0;
   for (int i = 0; i < nk; ++i) {
@@ -401,7 +499,7 @@ int abyss_ens_set_wave(abyss_ens *e, int nk, const int *clusters, const double *
     e->h_active[k] = 1;
     e->h_time[k] = new_time[i];
     e->h_scale[k] = time_scale[i];
-    int S = std::max(1, std::min(kSMax, (nkp + 2047) / 2048));
+    int S = std::max(1, std::min(kSMax, (nkp + e->chunk_j - 1) / e->chunk_j));
     int chunk = ((nkp + S - 1) / S + kTJ - 1) / kTJ * kTJ;
     S = (nkp + chunk - 1) / chunk;
     e->wave_rows_begin[i] = row;
@@ -439,18 +537,43 @@ int abyss_ens_set_wave(abyss_ens *e, int nk, const int *clusters, const double *
   e->rows = row;
   e->n_items = (int)e->h_items.size();
   cudaStream_t s = e->stream;
+  // the previous wave's copies read the pinned staging: let them finish first
+  ECK(cudaStreamSynchronize(s), "set_wave");
   const int counts[2] = {e->rows, e->n_items};
-  ECK(cudaMemcpyAsync(e->order_t.p, e->h_order.data(), 4 * (size_t)row, cudaMemcpyHostToDevice, s), "H2D order");
-  ECK(cudaMemcpyAsync(e->row_nch.p, e->h_nch.data(), 4 * (size_t)row, cudaMemcpyHostToDevice, s), "H2D nch");
-  ECK(cudaMemcpyAsync(e->row_joff.p, e->h_joff.data(), 4 * (size_t)row, cudaMemcpyHostToDevice, s), "H2D joff");
-  ECK(cudaMemcpyAsync(e->row_jlen.p, e->h_jlen.data(), 4 * (size_t)row, cudaMemcpyHostToDevice, s), "H2D jlen");
-  ECK(cudaMemcpyAsync(e->items.p, e->h_items.data(), sizeof(WorkItem) * e->h_items.size(),
-                      cudaMemcpyHostToDevice, s), "H2D items");
-  ECK(cudaMemcpyAsync(e->counts.p, counts, sizeof(counts), cudaMemcpyHostToDevice, s), "H2D counts");
-  ECK(cudaMemcpyAsync(e->active.p, e->h_active.data(), 4 * (size_t)e->nc, cudaMemcpyHostToDevice, s), "H2D active");
-  ECK(cudaMemcpyAsync(e->new_time.p, e->h_time.data(), 8 * (size_t)e->nc, cudaMemcpyHostToDevice, s), "H2D times");
-  ECK(cudaMemcpyAsync(e->scale.p, e->h_scale.data(), 8 * (size_t)e->nc, cudaMemcpyHostToDevice, s), "H2D scales");
-  ECK(cudaStreamSynchronize(s), "set_wave");  // host vectors may change after return
+  struct Piece {
+    void *dst;
+    const void *src;
+    size_t bytes;
+  };
+  const Piece pieces[] = {
+      {e->order_t.p, e->h_order.data(), 4 * (size_t)row},
+      {e->row_nch.p, e->h_nch.data(), 4 * (size_t)row},
+      {e->row_joff.p, e->h_joff.data(), 4 * (size_t)row},
+      {e->row_jlen.p, e->h_jlen.data(), 4 * (size_t)row},
+      {e->items.p, e->h_items.data(), sizeof(WorkItem) * e->h_items.size()},
+      {e->counts.p, counts, sizeof(counts)},
+      {e->active.p, e->h_active.data(), 4 * (size_t)e->nc},
+      {e->new_time.p, e->h_time.data(), 8 * (size_t)e->nc},
+      {e->scale.p, e->h_scale.data(), 8 * (size_t)e->nc},
+  };
+  size_t total = 0;
+  for (const Piece &q : pieces) total += (q.bytes + 15) / 16 * 16;
+  if (total > e->wstage_bytes) {
+    if (e->wstage) cudaFreeHost(e->wstage);
+    e->wstage = nullptr;
+    e->wstage_bytes = 0;
+    const size_t want = std::max(total, (size_t)1 << 20) * 3 / 2;
+    ECK(cudaMallocHost((void **)&e->wstage, want), "pinned wave staging");
+    e->wstage_bytes = want;
+  }
+  size_t at = 0;
+  for (const Piece &q : pieces) {
+    if (q.bytes) {
+      std::memcpy(e->wstage + at, q.src, q.bytes);
+      ECK(cudaMemcpyAsync(q.dst, e->wstage + at, q.bytes, cudaMemcpyHostToDevice, s), "H2D wave");
+    }
+    at += (q.bytes + 15) / 16 * 16;
+  }
   return ABYSS_OK;
 }
 
@@ -558,6 +681,47 @@ int abyss_ens_launch(abyss_ens *e, double eps2, int mode, const abyss_tuning *tu
   }
   ECK(cudaEventRecord(e->ev1, s), "event");
   return ABYSS_OK;
+}
+
+int abyss_ens_fetch_view(abyss_ens *e, const double **acc_reg, const double **jerk_reg, const double **acc_irr,
+                         const double **jerk_irr, const int **nnb, const int **list, int *overflow_rows) {
+  if (!e || !acc_reg || !jerk_reg || !acc_irr || !jerk_irr || !nnb || !list) return ABYSS_ERR_ARG;
+  cudaSetDevice(e->device);
+  cudaStream_t s = e->stream;
+  const size_t m = e->rows, cap = (size_t)e->cap;
+  const size_t need = 16 + 4 * 24 * m + 4 * m + 4 * m * cap + 64;
+  if (need > e->ostage_bytes) {
+    ECK(cudaStreamSynchronize(s), "fetch_view");
+    if (e->ostage) cudaFreeHost(e->ostage);
+    e->ostage = nullptr;
+    e->ostage_bytes = 0;
+    const size_t want = std::max(need, (size_t)1 << 20) * 3 / 2;
+    ECK(cudaMallocHost((void **)&e->ostage, want), "pinned result staging");
+    e->ostage_bytes = want;
+  }
+  unsigned char *b = e->ostage;
+  int *st = reinterpret_cast<int *>(b);
+  double *d = reinterpret_cast<double *>(b + 16);
+  int *nb = reinterpret_cast<int *>(b + 16 + 4 * 24 * m);
+  int *ls = nb + m;
+  ECK(cudaMemcpyAsync(st, e->status.p, 4, cudaMemcpyDeviceToHost, s), "D2H");
+  ECK(cudaMemcpyAsync(st + 1, e->ovf.p, 4, cudaMemcpyDeviceToHost, s), "D2H");
+  ECK(cudaMemcpyAsync(d, e->acc_reg.p, 24 * m, cudaMemcpyDeviceToHost, s), "D2H");
+  ECK(cudaMemcpyAsync(d + 3 * m, e->jerk_reg.p, 24 * m, cudaMemcpyDeviceToHost, s), "D2H");
+  ECK(cudaMemcpyAsync(d + 6 * m, e->acc_irr.p, 24 * m, cudaMemcpyDeviceToHost, s), "D2H");
+  ECK(cudaMemcpyAsync(d + 9 * m, e->jerk_irr.p, 24 * m, cudaMemcpyDeviceToHost, s), "D2H");
+  ECK(cudaMemcpyAsync(nb, e->nnb.p, 4 * m, cudaMemcpyDeviceToHost, s), "D2H");
+  ECK(cudaMemcpyAsync(ls, e->list.p, 4 * m * cap, cudaMemcpyDeviceToHost, s), "D2H");
+  ECK(cudaStreamSynchronize(s), "fetch_view");
+  *acc_reg = d;
+  *jerk_reg = d + 3 * m;
+  *acc_irr = d + 6 * m;
+  *jerk_irr = d + 9 * m;
+  *nnb = nb;
+  *list = ls;
+  if (overflow_rows) *overflow_rows = st[1];
+  if (st[0] & kErrTimeout) return efail(e, ABYSS_ERR_TIMEOUT, "device wait timed out");
+  return st[1] > 0 ? ABYSS_WARN_OVERFLOW : ABYSS_OK;
 }
 
 int abyss_ens_fetch(abyss_ens *e, double *acc_reg, double *jerk_reg, double *acc_irr, double *jerk_irr,

@@ -26,6 +26,10 @@
 #include <array>
 #include <chrono>
 #include <cmath>
+#include <condition_variable>
+#include <deque>
+#include <mutex>
+#include <thread>
 #include <cstring>
 #include <map>
 #include <stdexcept>
@@ -37,6 +41,7 @@
 #endif
 
 #include "../../../include/abyss_ac.h"
+#include "../../../include/abyss_ens.h"
 #include "../../../include/abyss_reg.h"
 
 namespace {
@@ -780,6 +785,230 @@ int abyss_ac_create(abyss_ctx *ctx, const abyss_ac_params *p, int n, const doubl
   }
   *out = ac;
   return ABYSS_OK;
+}
+
+namespace {
+
+// Shared state of one abyss_ac_serve_run call.
+struct ServeRun {
+  abyss_ens *e = nullptr;
+  abyss_ac *const *acs = nullptr;
+  const int *slots = nullptr;
+  int k = 0, cap = 0;
+  std::mutex mu;
+  std::condition_variable cv_host, cv_gpu;
+  std::deque<int> host_q;         // integrations with host work to do
+  std::vector<int> gpu_ready;     // integrations whose open block is staged
+  std::vector<char> has_result;   // a wave result waits for end_block
+  std::vector<std::vector<double>> res_d;  // acc, jerk, acc_irr, jerk_irr [4][3m]
+  std::vector<std::vector<int>> res_n, res_l;
+  int busy = 0;                   // workers inside an integration
+  double worker_s = 0.0;          // busy time summed over workers
+  int finished = 0;               // integrations that reached code time 1
+  bool stop = false, quit = false;
+  int *status = nullptr, *blocks = nullptr;
+};
+
+// One host worker: takes an integration, commits its returned block if it has
+// one, then (unless stopping) opens its next block and stages it for the GPU.
+void serve_worker(ServeRun *R) {
+  for (;;) {
+    int i;
+    {
+      std::unique_lock<std::mutex> lk(R->mu);
+      R->cv_host.wait(lk, [&] { return R->quit || !R->host_q.empty(); });
+      if (R->host_q.empty()) return;
+      i = R->host_q.front();
+      R->host_q.pop_front();
+      ++R->busy;
+    }
+    const double tw = now_s();
+    abyss_ac *ac = R->acs[i];
+    int st = R->status[i];
+    bool queue_gpu = false, fin = false;
+    if (R->has_result[i]) {
+      const auto &d = R->res_d[i];
+      const size_t m3 = d.size() / 4;
+      int done = 0;
+      const int r = abyss_ac_end_block(ac, d.data(), d.data() + m3, d.data() + 2 * m3, d.data() + 3 * m3,
+                                       R->res_n[i].data(), R->res_l[i].data(), R->cap, &done);
+      R->has_result[i] = 0;
+      if (r == ABYSS_WARN_OVERFLOW) {
+        st = ABYSS_ROUND_REDO;
+      } else if (r != ABYSS_OK) {
+        st = r;
+      } else {
+        ++R->blocks[i];
+        st = done ? ABYSS_ROUND_ADVANCED_DONE : ABYSS_ROUND_ADVANCED;
+        fin = done != 0;
+      }
+    }
+    bool stopping;
+    {
+      std::lock_guard<std::mutex> lk(R->mu);
+      stopping = R->stop;
+    }
+    if (st >= 0 && !fin && !stopping) {
+      if (!ac->in_block) {
+        int m = 0, done = 0;
+        double nt = 0.0, sc = 1.0;
+        const int r = abyss_ac_begin_block(ac, &m, &nt, &sc, &done);
+        if (r != ABYSS_OK) {
+          st = r;
+        } else if (done || m == 0) {
+          st = ABYSS_ROUND_FINISHED;
+          fin = true;
+        }
+      }
+      if (st >= 0 && !fin) {
+        double *x, *v, *a0, *a1, *t0, *ms, *r2;
+        int r = abyss_ens_stage(R->e, R->slots[i], &x, &v, &a0, &a1, &t0, &ms, &r2);
+        if (r == ABYSS_OK) r = abyss_ac_block_state(ac, x, v, a0, a1, t0, ms, r2);
+        if (r != ABYSS_OK)
+          st = r;
+        else
+          queue_gpu = true;
+      }
+    }
+    {
+      std::lock_guard<std::mutex> lk(R->mu);
+      R->status[i] = st;
+      if (fin) ++R->finished;
+      if (queue_gpu) R->gpu_ready.push_back(i);
+      --R->busy;
+      R->worker_s += now_s() - tw;
+    }
+    R->cv_gpu.notify_one();
+  }
+}
+
+}  // namespace
+
+int abyss_ac_serve_run(abyss_ens *e, int k, abyss_ac *const *acs, const int *slots, double eps2, int mode,
+                       int threads, double budget_ms, int stop_after, int *status, int *blocks, float *gpu_ms,
+                       int *waves, abyss_serve_stats *stats) {
+  if (!e || k < 0 || (k > 0 && (!acs || !slots || !status || !blocks))) return ABYSS_ERR_ARG;
+  if (gpu_ms) *gpu_ms = 0.0f;
+  if (waves) *waves = 0;
+  if (k == 0) return ABYSS_OK;
+  for (int i = 0; i < k; ++i)
+    if (!acs[i]) return ABYSS_ERR_ARG;
+  int rc = abyss_ens_stage_reserve(e);
+  if (rc != ABYSS_OK) return rc;
+  ServeRun R;
+  R.e = e;
+  R.acs = acs;
+  R.slots = slots;
+  R.k = k;
+  R.cap = abyss_ens_list_cap(e);
+  R.status = status;
+  R.blocks = blocks;
+  R.has_result.assign(k, 0);
+  R.res_d.resize(k);
+  R.res_n.resize(k);
+  R.res_l.resize(k);
+  for (int i = 0; i < k; ++i) {
+    status[i] = ABYSS_ROUND_ADVANCED;
+    blocks[i] = 0;
+    R.host_q.push_back(i);
+  }
+  const int nth = std::max(1, threads > 0 ? threads : (int)std::thread::hardware_concurrency());
+  std::vector<std::thread> pool;
+  for (int t = 0; t < nth; ++t) pool.emplace_back(serve_worker, &R);
+  const double t0 = now_s();
+  const int want_fin = stop_after > 0 ? std::min(stop_after, k) : k;
+  int err = ABYSS_OK;
+  abyss_serve_stats S{};
+  // the dispatcher: every staged block goes into the next wave, one wave at a time
+  for (;;) {
+    std::vector<int> wave;
+    double tp = now_s();
+    {
+      std::unique_lock<std::mutex> lk(R.mu);
+      R.cv_gpu.wait(lk, [&] {
+        return !R.gpu_ready.empty() || (R.busy == 0 && R.host_q.empty());
+      });
+      if (R.gpu_ready.empty()) break;  // every worker idle and nothing queued: all done or stopped
+      wave.swap(R.gpu_ready);
+    }
+    S.idle_s += now_s() - tp;
+    tp = now_s();
+    std::vector<int> cl, mper, tg;
+    std::vector<double> tm, scl;
+    for (int i : wave) {
+      const abyss_ac *ac = acs[i];
+      cl.push_back(slots[i]);
+      tm.push_back(ac->next_reg_block * ac->time_step);
+      scl.push_back(ac->scale);
+      mper.push_back((int)ac->block_targets.size());
+      tg.insert(tg.end(), ac->block_targets.begin(), ac->block_targets.end());
+    }
+    const int nl = (int)wave.size();
+    rc = abyss_ens_upload_staged(e, nl, cl.data());
+    if (rc == ABYSS_OK) rc = abyss_ens_set_wave(e, nl, cl.data(), tm.data(), scl.data(), mper.data(), tg.data());
+    if (rc == ABYSS_OK) rc = abyss_ens_launch(e, eps2, mode, nullptr);
+    S.prep_s += now_s() - tp;
+    tp = now_s();
+    const size_t rows = tg.size();
+    S.rows += (long long)rows;
+    const double *acc = nullptr, *jerk = nullptr, *airr = nullptr, *jirr = nullptr;
+    const int *nnb = nullptr, *lst = nullptr;
+    if (rc == ABYSS_OK) {
+      int ovf = 0;
+      rc = abyss_ens_fetch_view(e, &acc, &jerk, &airr, &jirr, &nnb, &lst, &ovf);
+      if (rc == ABYSS_WARN_OVERFLOW) rc = ABYSS_OK;  // end_block handles each overflowed block
+    }
+    if (rc != ABYSS_OK) {
+      err = rc;
+      std::lock_guard<std::mutex> lk(R.mu);
+      R.stop = true;
+      R.quit = true;
+      R.host_q.clear();
+      break;
+    }
+    S.wait_s += now_s() - tp;
+    tp = now_s();
+    float ms = 0.0f;
+    abyss_ens_last_ms(e, &ms);
+    if (gpu_ms) *gpu_ms += ms;
+    if (waves) ++*waves;
+    // the wave's integrations are idle until their rows are handed back, so
+    // their result buffers are filled without the lock
+    size_t r0 = 0;
+    for (int b = 0; b < nl; ++b) {
+      const int i = wave[b];
+      const size_t m = mper[b];
+      auto &d = R.res_d[i];
+      d.resize(12 * m);
+      std::copy(acc + 3 * r0, acc + 3 * (r0 + m), d.begin());
+      std::copy(jerk + 3 * r0, jerk + 3 * (r0 + m), d.begin() + 3 * m);
+      std::copy(airr + 3 * r0, airr + 3 * (r0 + m), d.begin() + 6 * m);
+      std::copy(jirr + 3 * r0, jirr + 3 * (r0 + m), d.begin() + 9 * m);
+      R.res_n[i].assign(nnb + r0, nnb + r0 + m);
+      R.res_l[i].assign(lst + r0 * R.cap, lst + (r0 + m) * R.cap);
+      R.has_result[i] = 1;
+      r0 += m;
+    }
+    {
+      std::lock_guard<std::mutex> lk(R.mu);
+      for (int i : wave) R.host_q.push_back(i);
+      if (R.finished >= want_fin || (budget_ms > 0 && (now_s() - t0) * 1e3 >= budget_ms)) R.stop = true;
+    }
+    R.cv_host.notify_all();
+    S.hand_s += now_s() - tp;
+  }
+  {
+    std::lock_guard<std::mutex> lk(R.mu);
+    R.quit = true;
+  }
+  R.cv_host.notify_all();
+  for (auto &t : pool) t.join();
+  if (stats) {
+    S.wall_s = now_s() - t0;
+    S.worker_s = R.worker_s;
+    *stats = S;
+  }
+  return err;
 }
 
 int abyss_ac_destroy(abyss_ac *ac) {

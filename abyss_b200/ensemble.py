@@ -29,6 +29,11 @@ def _bind(L):
     L.abyss_ens_attach.argtypes = [_vp, C.c_int, _ip]
     L.abyss_ens_detach.argtypes = [_vp, C.c_int]
     L.abyss_ens_free_particles.argtypes = [_vp]
+    L.abyss_ens_stage_reserve.argtypes = [_vp]
+    L.abyss_ens_stage.argtypes = [_vp, C.c_int] + [C.POINTER(_dp)] * 7
+    L.abyss_ens_upload_staged.argtypes = [_vp, C.c_int, _ip]
+    L.abyss_ens_list_cap.argtypes = [_vp]
+    L.abyss_ens_set_chunk.argtypes = [_vp, C.c_int]
     L._ens_bound = True
 
 
@@ -99,6 +104,25 @@ class Ensemble:
         arrs = [_f64(x, (n, 3)), _f64(v, (n, 3)), _f64(a0, (n, 3)), _f64(a1, (n, 3)), _f64(t0), _f64(mass),
                 _f64(r2nb)]
         self._check(self._L.abyss_ens_upload_state(self._h, int(k), *[ptr(a) for a in arrs]))
+
+    def stage(self, k: int) -> dict:
+        """Cluster k's seven state arrays in the ensemble's pinned staging, as
+        writable numpy views (x, v, a0, a1 [n][3]; t0, mass, r2nb [n])."""
+        self._check(self._L.abyss_ens_stage_reserve(self._h))
+        n = int(self.sizes[k])
+        ptrs = [_dp() for _ in range(7)]
+        self._check(self._L.abyss_ens_stage(self._h, int(k), *[C.byref(p) for p in ptrs]))
+        shapes = [(n, 3)] * 4 + [(n,)] * 3
+        names = ("x", "v", "a0", "a1", "t0", "mass", "r2nb")
+        return {nm: np.ctypeslib.as_array(p, shape=sh) for nm, p, sh in zip(names, ptrs, shapes)}
+
+    def set_chunk(self, j_per_chunk: int):
+        """j per chunk of a cluster's work items (its chunk count depends on its size only)."""
+        self._check(self._L.abyss_ens_set_chunk(self._h, int(j_per_chunk)))
+
+    def upload_staged(self, clusters):
+        cl = np.ascontiguousarray(clusters, np.int32)
+        self._check(self._L.abyss_ens_upload_staged(self._h, int(cl.shape[0]), ptr(cl, _ip)))
 
     def set_wave(self, clusters, new_time, time_scale, targets):
         """targets: list of cluster-local index arrays, one per listed cluster."""

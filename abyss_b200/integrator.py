@@ -41,6 +41,9 @@ class ACIntegrator:
         if rc != 0:
             raise _lib.AbyssError(rc, self._L.abyss_ac_last_error(self._h).decode())
 
+    def last_error(self) -> str:
+        return self._L.abyss_ac_last_error(self._h).decode()
+
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:
             self._L.abyss_ac_destroy(self._h)

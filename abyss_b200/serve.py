@@ -10,13 +10,15 @@ on the GPU and runs rounds:
              a request that does not fit waits, the loop never allocates);
              their initial conditions and integrator set-up run on host
              threads, each through a regular-force context of its own;
-  2. begin   every active integration runs its irregular levels up to its next
-             regular block (host threads, in parallel);
-  3. wave    the regular forces of all open blocks -- each cluster at its own
-             time, with its own active set -- run as ONE replayed CUDA graph
-             (prediction, one persistent force launch, finalize);
-  4. end     every integration applies its corrector (host threads);
-  5. retire  finished integrations report energy drift (host threads) and free
+  2. run     for a slice of wall time the admitted integrations advance on
+             their own: host workers run each one's irregular levels up to its
+             next regular block and queue the block, the GPU runs every queued
+             block -- each cluster at its own time, with its own active set --
+             as back-to-back waves of ONE replayed CUDA graph (prediction, one
+             persistent force launch, finalize), and a worker applies the
+             corrector as soon as a block's rows are back and opens the next
+             block (one native call, abyss_ac_serve_run);
+  3. retire  finished integrations report energy drift (host threads) and free
              their range.
 
 Requests arriving while others are on the GPU join the next round: their work
@@ -37,10 +39,30 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import ic
+import ctypes as C
+
+from . import _lib, ic
+from ._lib import AbyssError, _ip, ptr
 from .ensemble import GRAPH, Ensemble
 from .integrator import ACIntegrator
 from .regforce import RegularForce
+
+
+ROUND_ADVANCED, ROUND_ADVANCED_DONE, ROUND_FINISHED, ROUND_REDO = 0, 1, 2, 3  # include/abyss_ac.h
+
+
+class ServeStats(C.Structure):
+    _fields_ = [("wall_s", C.c_double), ("prep_s", C.c_double), ("wait_s", C.c_double), ("hand_s", C.c_double),
+                ("idle_s", C.c_double), ("worker_s", C.c_double), ("rows", C.c_longlong)]
+
+
+def _bind(L):
+    if getattr(L, "_serve_bound", False):
+        return
+    L.abyss_ac_serve_run.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_void_p), _ip, C.c_double, C.c_int,
+                                     C.c_int, C.c_double, C.c_int, _ip, _ip, C.POINTER(C.c_float),
+                                     C.POINTER(C.c_int), C.POINTER(ServeStats)]
+    L._serve_bound = True
 
 
 @dataclass
@@ -76,19 +98,30 @@ class Request:
 
 class Server:
     def __init__(self, device: int = 0, capacity: int = 1 << 21, max_clusters: int = 512, list_cap: int = 128,
-                 eps2: float = 1e-8, eta_reg: float = 0.02, eta_irr: float = 0.01, host_threads: int = 16):
+                 eps2: float = 1e-8, eta_reg: float = 0.02, eta_irr: float = 0.01, host_threads: int = 16,
+                 slice_ms: float = 20.0, max_n: int = 16384, chunk_j: int = 256):
         self.rf = RegularForce(device)
         self.ens = Ensemble(self.rf, None, list_cap=list_cap, capacity=capacity, max_clusters=max_clusters)
+        # short j-chunks: a serving wave is small and latency-bound, so its work
+        # is spread over as many CTAs as possible
+        self.ens.set_chunk(chunk_j)
         self.eps2 = eps2
         self.eta_reg, self.eta_irr = eta_reg, eta_irr
         self.list_cap = list_cap
         nthreads = max(1, host_threads)
+        self.host_threads = nthreads
+        self._L = _lib.lib()
+        _bind(self._L)
         self.pool = ThreadPoolExecutor(max_workers=nthreads)
         # Integrator set-up (its initial force on the GPU) and energies run on
         # host threads, each through a context of its own: a context serves one
         # caller at a time, which its lock enforces.
         self.ctx_free: queue.Queue = queue.Queue()
         self.ctxs = [(RegularForce(device), threading.Lock()) for _ in range(nthreads)]
+        # every buffer a set-up of up to max_n particles uses, allocated now: a
+        # context that grew while waves run would stall the device in cudaFree
+        for rf, _ in self.ctxs:
+            rf.reserve(max_n, max_n, list_cap)
         for c in self.ctxs:
             self.ctx_free.put(c)
         self.waiting: list[Request] = []
@@ -97,8 +130,12 @@ class Server:
         self.t0 = time.perf_counter()
         self.rounds = 0
         self.wave_ms = 0.0
+        self.waves = 0
+        self._st = ServeStats()
+        self.run_stats = {f: 0 for f, _ in ServeStats._fields_}
+        self.slice_ms = float(slice_ms)
         self.peak_active = 0
-        self.phase_s = dict(admit=0.0, begin=0.0, upload=0.0, wave=0.0, end=0.0, retire=0.0)
+        self.phase_s = dict(admit=0.0, round=0.0, retire=0.0)
         self.build_s = dict(cluster=0.0, wait_ctx=0.0, init=0.0, energy=0.0)
         self.stat_lock = threading.Lock()
 
@@ -164,12 +201,6 @@ class Server:
                 self.active.append(r)
 
     # ------------------------------------------------------------ one round
-    def _begin(self, r: Request):
-        """Irregular levels up to the next regular block, then the block's state."""
-        if r.pending is None:
-            r.pending = r.ac.begin_block()
-        r.state = r.ac.block_state() if r.pending is not None else None
-
     def round(self):
         ph = self.phase_s
         t = time.perf_counter()
@@ -178,43 +209,34 @@ class Server:
         self.peak_active = max(self.peak_active, len(self.active))
         if not self.active:
             return
+        # the integrations advance asynchronously for a slice of wall time: host
+        # workers run irregular levels and correctors, the GPU runs every queued
+        # regular block in back-to-back waves (include/abyss_ac.h abyss_ac_serve_run)
         t = time.perf_counter()
-        list(self.pool.map(self._begin, self.active))
-        ph["begin"] += time.perf_counter() - t
-        finished = [r for r in self.active if r.pending is None]
-        live = [r for r in self.active if r.pending is not None]
-        if live:
-            t = time.perf_counter()
-            for r in live:
-                st = r.state
-                self.ens.upload_state(r.slot, st["x"], st["v"], st["a0"], st["a1"], st["t0"], st["mass"], st["r2nb"])
-                r.state = None
-            ph["upload"] += time.perf_counter() - t
-            t = time.perf_counter()
-            self.ens.set_wave([r.slot for r in live], [r.pending[1] for r in live], [r.pending[2] for r in live],
-                              [r.pending[0] for r in live])
-            self.ens.launch(self.eps2, GRAPH)
-            out = self.ens.fetch()
-            self.wave_ms += self.ens.last_ms()
-            ph["wave"] += time.perf_counter() - t
-            sp = self.ens.row_splits
-            t = time.perf_counter()
-
-            def end(i):
-                r = live[i]
-                a, b = sp[i], sp[i + 1]
-                return r.ac.end_block(out.acc_reg[a:b], out.jerk_reg[a:b], out.acc_irr[a:b], out.jerk_irr[a:b],
-                                      out.nnb[a:b], out.list[a:b])
-
-            for i, status in enumerate(self.pool.map(end, range(len(live)))):
-                r = live[i]
-                if status == "redo":
-                    continue  # radii shrunk; the block is recomputed next round
-                r.pending = None
-                r.blocks += 1
-                if status == "done":
-                    finished.append(r)
-            ph["end"] += time.perf_counter() - t
+        k = len(self.active)
+        acs = (C.c_void_p * k)(*[r.ac._h.value for r in self.active])
+        slots = np.array([r.slot for r in self.active], np.int32)
+        status = np.zeros(k, np.int32)
+        blocks = np.zeros(k, np.int32)
+        ms = C.c_float(0.0)
+        nw = C.c_int(0)
+        rc = self._L.abyss_ac_serve_run(self.ens._h, k, acs, ptr(slots, _ip), self.eps2, GRAPH, self.host_threads,
+                                        self.slice_ms, 0, ptr(status, _ip), ptr(blocks, _ip), C.byref(ms),
+                                        C.byref(nw), C.byref(self._st))
+        for f, _ in ServeStats._fields_:
+            self.run_stats[f] += getattr(self._st, f)
+        if rc != 0:
+            raise AbyssError(rc, "serve run failed")
+        self.wave_ms += float(ms.value)
+        self.waves += int(nw.value)
+        ph["round"] += time.perf_counter() - t
+        finished = []
+        for r, st, nb in zip(self.active, status, blocks):
+            if st < 0:
+                raise AbyssError(int(st), f"request {r.rid}: " + r.ac.last_error())
+            r.blocks += int(nb)
+            if st in (ROUND_ADVANCED_DONE, ROUND_FINISHED):
+                finished.append(r)
         t = time.perf_counter()
         if finished:
             list(self.pool.map(self._finish, finished))
@@ -260,7 +282,8 @@ def poisson_requests(rate: float, duration: float, nmin: int, nmax: int, seed: i
 
 
 def serve(rate: float = 200.0, duration: float = 2.0, nmin: int = 256, nmax: int = 2048, t_end: float = 0.0625,
-          capacity: int = 1 << 21, seed: int = 5, host_threads: int = 16, serial: bool = False):
+          capacity: int = 1 << 21, seed: int = 5, host_threads: int = 16, serial: bool = False,
+          chunk_j: int = 256):
     """Run a Poisson stream through the server (or, with serial=True, one request at
     a time through the same code) and report latency percentiles and throughput."""
     reqs = poisson_requests(rate, duration, nmin, nmax, seed=seed, t_end=t_end)
@@ -272,12 +295,12 @@ def serve(rate: float = 200.0, duration: float = 2.0, nmin: int = 256, nmax: int
         rounds, wave_ms, peak = 0, 0.0, 1
         srv = None
     else:
-        srv = Server(capacity=capacity, host_threads=host_threads)
+        srv = Server(capacity=capacity, host_threads=host_threads, max_n=nmax, chunk_j=chunk_j)
         for r in reqs:
             srv.submit(r)
         srv.run_until_idle()
         done, rounds, wave_ms, peak = srv.done, srv.rounds, srv.wave_ms, srv.peak_active
-        phases = dict(srv.phase_s, build_thread_s=dict(srv.build_s))
+        phases = dict(srv.phase_s, build_thread_s=dict(srv.build_s), waves=srv.waves, run=dict(srv.run_stats))
         srv.close()
     wall = max(r.finished for r in done) if done else 0.0
     lat = np.array([r.result["latency_s"] for r in done])

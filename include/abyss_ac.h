@@ -71,6 +71,43 @@ int abyss_ac_block_state(const abyss_ac *ac, double *x, double *v, double *a0, d
 int abyss_ac_end_block(abyss_ac *ac, const double *acc, const double *jerk, const double *acc_irr,
                        const double *jerk_irr, const int *nnb, const int *list, int list_cap, int *done);
 
+/* Serving loop over k integrations whose regular forces share the ensemble e
+ * (include/abyss_ens.h); integration i owns cluster slots[i] and must have
+ * been created with threads = 1.  `threads` host workers advance the
+ * integrations independently, block by block: a worker runs an integration's
+ * irregular levels up to its next regular block, writes the block's state into
+ * the ensemble's pinned staging and queues it; the calling thread runs every
+ * queued block as one ensemble wave (mode ABYSS_ENS_BATCHED or _GRAPH), one wave
+ * at a time, back to back, and hands each block's rows back to a worker, which
+ * applies the corrector and opens the next block at once.  No integration waits
+ * for another's host work, and each one's results do not depend on which
+ * blocks shared its waves.
+ * The call returns once stop_after integrations (0 = all) have reached code
+ * time 1, or after the wave that ends past budget_ms of wall time (<= 0: no
+ * budget); blocks in flight are committed first, and an integration whose
+ * block was queued but not run keeps it open for the next call.
+ * status[i]: one of the codes below, or a negative ABYSS_ERR_* code;
+ * blocks[i]: regular blocks it committed in this call.  *gpu_ms: GPU time of
+ * the waves, *waves: their count, *stats: where the time went (any of the three
+ * may be NULL). */
+#define ABYSS_ROUND_ADVANCED 0       /* between blocks, or a block open */
+#define ABYSS_ROUND_ADVANCED_DONE 1  /* its last block was committed: code time 1 reached */
+#define ABYSS_ROUND_FINISHED 2       /* nothing to do: code time 1 had been reached */
+#define ABYSS_ROUND_REDO 3           /* a list overflowed: radii shrunk, the block runs again */
+struct abyss_ens;
+typedef struct abyss_serve_stats {
+  double wall_s;      /* the whole call */
+  double prep_s;      /* dispatcher: staged upload, wave set-up, launch */
+  double wait_s;      /* dispatcher: waiting for a wave's results */
+  double hand_s;      /* dispatcher: handing rows back to the workers */
+  double idle_s;      /* dispatcher: no block queued */
+  double worker_s;    /* host workers: busy time, summed over workers */
+  long long rows;     /* targets over all waves */
+} abyss_serve_stats;
+int abyss_ac_serve_run(struct abyss_ens *e, int k, abyss_ac *const *acs, const int *slots, double eps2,
+                       int mode, int threads, double budget_ms, int stop_after, int *status, int *blocks,
+                       float *gpu_ms, int *waves, abyss_serve_stats *stats);
+
 /* Advance until code time >= t_code (<= 1). */
 int abyss_ac_run(abyss_ac *ac, double t_code);
 /* Current code time (the last regular block time reached). */

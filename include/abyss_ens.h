@@ -45,12 +45,33 @@ int abyss_ens_attach(abyss_ens *e, int n, int *k);
 int abyss_ens_detach(abyss_ens *e, int k);
 /* Largest contiguous free particle range. */
 int abyss_ens_free_particles(const abyss_ens *e);
+/* j-particles per chunk of the work list (>= 128; default 2048): cluster k is
+ * split into min(16, ceil(n_k / j_per_chunk)) j-chunks in every wave.  Small
+ * chunks spread a wave of small clusters over more of the GPU (lower latency
+ * per wave); the split depends on n_k alone, so results stay the same alone
+ * and in any mix.  Results change with this setting at the FP32 rounding level. */
+int abyss_ens_set_chunk(abyss_ens *e, int j_per_chunk);
+/* Neighbour-list capacity per target (the row stride of fetched lists). */
+int abyss_ens_list_cap(const abyss_ens *e);
 /* Device bytes the ensemble holds (for admission control). */
 long long abyss_ens_device_bytes(const abyss_ens *e);
 /* Un-predicted FP64 state of cluster k, as abyss_upload_state. */
 int abyss_ens_upload_state(abyss_ens *e, int k, const double *x, const double *v, const double *a0,
                            const double *a1, const double *t0, const double *mass,
                            const double *r2nb);
+/* Staged upload, for callers that refresh many clusters per wave: after
+ * abyss_ens_stage_reserve (pinned host memory for the whole arena, 120 B per
+ * particle of capacity), abyss_ens_stage gives cluster k's seven state arrays
+ * inside it (same layout as abyss_ens_upload_state; the caller writes them, from
+ * any thread), and abyss_ens_upload_staged queues the copies of the listed
+ * clusters on the ensemble's stream, merged into one copy per array for each
+ * run of listed clusters that are adjacent in the arena.  Clusters not listed
+ * are not written.  The staged memory must not change until the next wave has
+ * been launched and fetched. */
+int abyss_ens_stage_reserve(abyss_ens *e);
+int abyss_ens_stage(abyss_ens *e, int k, double **x, double **v, double **a0, double **a1, double **t0,
+                    double **mass, double **r2nb);
+int abyss_ens_upload_staged(abyss_ens *e, int nk, const int *clusters);
 /* Define the next wave: nk clusters, each predicted to new_time[i] with
  * time_scale[i] and m_per[i] targets (concatenated in targets_local). */
 int abyss_ens_set_wave(abyss_ens *e, int nk, const int *clusters, const double *new_time,
@@ -60,6 +81,11 @@ int abyss_ens_launch(abyss_ens *e, double eps2, int mode, const struct abyss_tun
 /* Wait and copy the wave's results (rows in wave order); any pointer may be NULL. */
 int abyss_ens_fetch(abyss_ens *e, double *acc_reg, double *jerk_reg, double *acc_irr,
                     double *jerk_irr, int *nnb, int *list, int *overflow_rows);
+/* As abyss_ens_fetch, without copies into caller memory: the results land in
+ * pinned host memory owned by the ensemble and the pointers returned stay valid
+ * until the next abyss_ens_fetch_view or abyss_ens_destroy. */
+int abyss_ens_fetch_view(abyss_ens *e, const double **acc_reg, const double **jerk_reg, const double **acc_irr,
+                         const double **jerk_irr, const int **nnb, const int **list, int *overflow_rows);
 /* GPU milliseconds of the last launch (CUDA events around the wave). */
 int abyss_ens_last_ms(abyss_ens *e, float *ms);
 /* Rows, work items and kernel launches of the last wave. */

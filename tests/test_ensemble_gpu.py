@@ -105,3 +105,34 @@ def test_bad_waves_are_refused(rf):
     e.set_wave([1], [0.0], [1.0], [np.array([0, 1, 2])])
     e.launch(EPS2, BATCHED)
     assert e.fetch().acc_reg.shape == (3, 3)
+
+
+def test_staged_upload_matches_and_leaves_unlisted_clusters(rf):
+    """Staged uploads give the same wave results as per-cluster uploads, and a
+    cluster that is not listed keeps its device state even when it lies between
+    listed ones (its staging was never written)."""
+    e, clusters = make_ensemble(rf, k=6, seed=7)
+    rng = np.random.default_rng(3)
+    allk = np.arange(len(clusters))
+    targets = [np.sort(rng.choice(c.n, max(1, c.n // 3), replace=False)).astype(np.int32) for c in clusters]
+    e.set_wave(allk, np.zeros(len(allk)), np.ones(len(allk)), targets)
+    e.launch(EPS2, GRAPH)
+    want = e.fetch()
+    # clusters 0, 2, 4 restaged (same state); 1, 3, 5 keep their device state
+    for k in (0, 2, 4):
+        st = e.stage(k)
+        c = clusters[k]
+        st["x"][:] = c.x
+        st["v"][:] = c.v
+        st["a0"][:] = 0.0
+        st["a1"][:] = 0.0
+        st["t0"][:] = 0.0
+        st["mass"][:] = c.m
+        st["r2nb"][:] = c.r2nb
+    e.upload_staged([0, 2, 4])
+    e.set_wave(allk, np.zeros(len(allk)), np.ones(len(allk)), targets)
+    e.launch(EPS2, GRAPH)
+    got = e.fetch()
+    for f in ("acc_reg", "jerk_reg", "acc_irr", "jerk_irr", "nnb", "list"):
+        assert np.array_equal(getattr(got, f), getattr(want, f)), f
+    e.close()
