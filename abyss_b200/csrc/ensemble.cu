@@ -89,7 +89,36 @@ struct abyss_ens {
   size_t wstage_bytes = 0;
   unsigned char *ostage = nullptr;
   size_t ostage_bytes = 0;
+  cudaEvent_t desc_ev = nullptr;  // the wave description's copies out of wstage are done
+  bool desc_pending = false;
+  // Two waves can be in flight (abyss_ens_submit / abyss_ens_collect): every
+  // per-wave buffer above has a twin in `other`, and switching slots swaps
+  // them, so the code above always works on the current slot.
+  struct Slot *other = nullptr;
+  int cur = 0;            // slot number the fields above belong to
+  int busy[2] = {0, 0};   // slot s holds a submitted wave not yet collected
   std::string err;
+};
+
+// The per-wave state of an ensemble that is not current (see abyss_ens::other).
+struct Slot {
+  Buf<int> active, order_t, row_nch, row_joff, row_jlen, counts, lcnt, lst, status, ovf, qhead, list, nnb, ovf_list;
+  Buf<WorkItem> items;
+  Buf<double> new_time, scale, part, acc_reg, jerk_reg, acc_irr, jerk_irr;
+  int rows = 0, n_items = 0, launches = 0;
+  std::vector<int> h_order, h_nch, h_joff, h_jlen, h_active;
+  std::vector<double> h_time, h_scale;
+  std::vector<WorkItem> h_items;
+  std::vector<int> wave_clusters, wave_rows_begin, wave_m;
+  std::vector<std::vector<WorkItem>> cluster_items;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  abyss_tuning graph_shape{};
+  double graph_eps2 = -1.0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, desc_ev = nullptr;
+  bool desc_pending = false;
+  unsigned char *wstage = nullptr, *ostage = nullptr;
+  size_t wstage_bytes = 0, ostage_bytes = 0;
 };
 
 namespace {
@@ -97,6 +126,61 @@ namespace {
 int efail(abyss_ens *e, int code, const std::string &m) {
   if (e) e->err = m;
   return code;
+}
+
+// Make the other slot current (its buffers must exist: abyss_ens_pipeline).
+void swap_slot(abyss_ens *e) {
+  Slot &o = *e->other;
+  std::swap(e->active, o.active);
+  std::swap(e->order_t, o.order_t);
+  std::swap(e->row_nch, o.row_nch);
+  std::swap(e->row_joff, o.row_joff);
+  std::swap(e->row_jlen, o.row_jlen);
+  std::swap(e->counts, o.counts);
+  std::swap(e->items, o.items);
+  std::swap(e->lcnt, o.lcnt);
+  std::swap(e->lst, o.lst);
+  std::swap(e->status, o.status);
+  std::swap(e->ovf, o.ovf);
+  std::swap(e->qhead, o.qhead);
+  std::swap(e->list, o.list);
+  std::swap(e->nnb, o.nnb);
+  std::swap(e->ovf_list, o.ovf_list);
+  std::swap(e->new_time, o.new_time);
+  std::swap(e->scale, o.scale);
+  std::swap(e->part, o.part);
+  std::swap(e->acc_reg, o.acc_reg);
+  std::swap(e->jerk_reg, o.jerk_reg);
+  std::swap(e->acc_irr, o.acc_irr);
+  std::swap(e->jerk_irr, o.jerk_irr);
+  std::swap(e->rows, o.rows);
+  std::swap(e->n_items, o.n_items);
+  std::swap(e->launches, o.launches);
+  std::swap(e->h_order, o.h_order);
+  std::swap(e->h_nch, o.h_nch);
+  std::swap(e->h_joff, o.h_joff);
+  std::swap(e->h_jlen, o.h_jlen);
+  std::swap(e->h_active, o.h_active);
+  std::swap(e->h_time, o.h_time);
+  std::swap(e->h_scale, o.h_scale);
+  std::swap(e->h_items, o.h_items);
+  std::swap(e->wave_clusters, o.wave_clusters);
+  std::swap(e->wave_rows_begin, o.wave_rows_begin);
+  std::swap(e->wave_m, o.wave_m);
+  std::swap(e->cluster_items, o.cluster_items);
+  std::swap(e->graph, o.graph);
+  std::swap(e->graph_exec, o.graph_exec);
+  std::swap(e->graph_shape, o.graph_shape);
+  std::swap(e->graph_eps2, o.graph_eps2);
+  std::swap(e->ev0, o.ev0);
+  std::swap(e->ev1, o.ev1);
+  std::swap(e->desc_ev, o.desc_ev);
+  std::swap(e->desc_pending, o.desc_pending);
+  std::swap(e->wstage, o.wstage);
+  std::swap(e->ostage, o.ostage);
+  std::swap(e->wstage_bytes, o.wstage_bytes);
+  std::swap(e->ostage_bytes, o.ostage_bytes);
+  e->cur ^= 1;
 }
 
 #define ECK(expr, what)                                                                          \
@@ -225,6 +309,7 @@ int abyss_ens_create_arena(abyss_ctx *ctx, int capacity, int max_clusters, int l
   A(e->acc_reg, 3 * n); A(e->jerk_reg, 3 * n); A(e->acc_irr, 3 * n); A(e->jerk_irr, 3 * n);
   if (err == cudaSuccess) err = cudaEventCreate(&e->ev0);
   if (err == cudaSuccess) err = cudaEventCreate(&e->ev1);
+  if (err == cudaSuccess) err = cudaEventCreateWithFlags(&e->desc_ev, cudaEventDisableTiming);
   if (err != cudaSuccess) {
     abyss_ens_destroy(e);
     return err == cudaErrorMemoryAllocation ? ABYSS_ERR_OOM : ABYSS_ERR_CUDA;
@@ -357,6 +442,24 @@ int abyss_ens_destroy(abyss_ens *e) {
   if (e->stage) cudaFreeHost(e->stage);
   if (e->wstage) cudaFreeHost(e->wstage);
   if (e->ostage) cudaFreeHost(e->ostage);
+  if (e->desc_ev) cudaEventDestroy(e->desc_ev);
+  if (e->other) {
+    Slot &o = *e->other;
+    Buf<int> *bi[] = {&o.active, &o.order_t, &o.row_nch, &o.row_joff, &o.row_jlen, &o.counts, &o.lcnt,
+                      &o.lst, &o.status, &o.ovf, &o.qhead, &o.list, &o.nnb, &o.ovf_list};
+    for (auto *b : bi) b->release();
+    o.items.release();
+    Buf<double> *bd[] = {&o.new_time, &o.scale, &o.part, &o.acc_reg, &o.jerk_reg, &o.acc_irr, &o.jerk_irr};
+    for (auto *b : bd) b->release();
+    if (o.graph_exec) cudaGraphExecDestroy(o.graph_exec);
+    if (o.graph) cudaGraphDestroy(o.graph);
+    cudaEvent_t ev[] = {o.ev0, o.ev1, o.desc_ev};
+    for (auto v : ev)
+      if (v) cudaEventDestroy(v);
+    if (o.wstage) cudaFreeHost(o.wstage);
+    if (o.ostage) cudaFreeHost(o.ostage);
+    delete e->other;
+  }
   delete e;
   return ABYSS_OK;
 }
@@ -470,6 +573,7 @@ int abyss_ens_set_wave(abyss_ens *e, int nk, const int *clusters, const double *
                        const double *time_scale, const int *m_per, const int *targets_local) {
   if (!e || nk <= 0 || !clusters || !new_time || !time_scale || !m_per || !targets_local)
     return efail(e, ABYSS_ERR_ARG, "set_wave: bad arguments");
+  if (e->busy[e->cur]) return efail(e, ABYSS_ERR_STATE, "set_wave: a submitted wave is not collected yet");
   cudaSetDevice(e->device);
   std::vector<char> seen(e->nc, 0);
   const int per_block = e->shape.threads * e->shape.ipt;
@@ -537,8 +641,9 @@ int abyss_ens_set_wave(abyss_ens *e, int nk, const int *clusters, const double *
   e->rows = row;
   e->n_items = (int)e->h_items.size();
   cudaStream_t s = e->stream;
-  // the previous wave's copies read the pinned staging: let them finish first
-  ECK(cudaStreamSynchronize(s), "set_wave");
+  // this slot's previous description copies read the pinned staging: let them
+  // finish first (a wave of the other slot may still run)
+  if (e->desc_pending) ECK(cudaEventSynchronize(e->desc_ev), "set_wave");
   const int counts[2] = {e->rows, e->n_items};
   struct Piece {
     void *dst;
@@ -559,7 +664,7 @@ int abyss_ens_set_wave(abyss_ens *e, int nk, const int *clusters, const double *
   size_t total = 0;
   for (const Piece &q : pieces) total += (q.bytes + 15) / 16 * 16;
   if (total > e->wstage_bytes) {
-    if (e->wstage) cudaFreeHost(e->wstage);
+    if (e->wstage) cudaFreeHost(e->wstage);  // its copies are done (desc_ev above)
     e->wstage = nullptr;
     e->wstage_bytes = 0;
     const size_t want = std::max(total, (size_t)1 << 20) * 3 / 2;
@@ -574,12 +679,15 @@ int abyss_ens_set_wave(abyss_ens *e, int nk, const int *clusters, const double *
     }
     at += (q.bytes + 15) / 16 * 16;
   }
+  ECK(cudaEventRecord(e->desc_ev, s), "event");
+  e->desc_pending = true;
   return ABYSS_OK;
 }
 
 int abyss_ens_launch(abyss_ens *e, double eps2, int mode, const abyss_tuning *tuning) {
   if (!e || !(eps2 >= 0.0)) return efail(e, ABYSS_ERR_ARG, "launch: bad arguments");
   if (e->rows <= 0) return efail(e, ABYSS_ERR_STATE, "launch: no wave set");
+  if (e->busy[e->cur]) return efail(e, ABYSS_ERR_STATE, "launch: a submitted wave is not collected yet");
   cudaSetDevice(e->device);
   cudaStream_t s = e->stream;
   if (tuning && tuning->kernel != 0) {
@@ -686,6 +794,7 @@ int abyss_ens_launch(abyss_ens *e, double eps2, int mode, const abyss_tuning *tu
 int abyss_ens_fetch_view(abyss_ens *e, const double **acc_reg, const double **jerk_reg, const double **acc_irr,
                          const double **jerk_irr, const int **nnb, const int **list, int *overflow_rows) {
   if (!e || !acc_reg || !jerk_reg || !acc_irr || !jerk_irr || !nnb || !list) return ABYSS_ERR_ARG;
+  if (e->busy[e->cur]) return efail(e, ABYSS_ERR_STATE, "fetch: use abyss_ens_collect for a submitted wave");
   cudaSetDevice(e->device);
   cudaStream_t s = e->stream;
   const size_t m = e->rows, cap = (size_t)e->cap;
@@ -724,9 +833,132 @@ int abyss_ens_fetch_view(abyss_ens *e, const double **acc_reg, const double **je
   return st[1] > 0 ? ABYSS_WARN_OVERFLOW : ABYSS_OK;
 }
 
+int abyss_ens_pipeline(abyss_ens *e) {
+  if (!e) return ABYSS_ERR_ARG;
+  if (e->other) return ABYSS_OK;
+  cudaSetDevice(e->device);
+  e->other = new Slot;
+  Slot &o = *e->other;
+  const size_t n = e->n_total, nc = e->nc, cap = e->cap;
+  cudaError_t err = cudaSuccess;
+  auto A = [&](auto &b, size_t count) {
+    if (err == cudaSuccess) {
+      err = b.alloc(count);
+      e->bytes += (long long)b.n * (long long)sizeof(*b.p);
+    }
+  };
+  A(o.active, nc); A(o.new_time, nc); A(o.scale, nc);
+  A(o.order_t, n); A(o.row_nch, n); A(o.row_joff, n); A(o.row_jlen, n); A(o.counts, 2);
+  A(o.ovf_list, n); A(o.items, 2 * e->items_cap);
+  A(o.lcnt, n); A(o.lst, n * cap); A(o.status, 1); A(o.ovf, 1); A(o.qhead, 1);
+  A(o.list, n * cap); A(o.nnb, n);
+  A(o.part, n * (size_t)kSMax * 6);
+  A(o.acc_reg, 3 * n); A(o.jerk_reg, 3 * n); A(o.acc_irr, 3 * n); A(o.jerk_irr, 3 * n);
+  if (err == cudaSuccess) err = cudaEventCreate(&o.ev0);
+  if (err == cudaSuccess) err = cudaEventCreate(&o.ev1);
+  if (err == cudaSuccess) err = cudaEventCreateWithFlags(&o.desc_ev, cudaEventDisableTiming);
+  if (err == cudaSuccess) err = cudaMemsetAsync(o.active.p, 0, sizeof(int) * nc, e->stream);
+  if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
+  o.h_active.assign(nc, 0);
+  o.h_time.assign(nc, 0.0);
+  o.h_scale.assign(nc, 1.0);
+  if (err != cudaSuccess)
+    return efail(e, err == cudaErrorMemoryAllocation ? ABYSS_ERR_OOM : ABYSS_ERR_CUDA,
+                 std::string("pipeline: ") + cudaGetErrorString(err));
+  return ABYSS_OK;
+}
+
+int abyss_ens_submit(abyss_ens *e, int nk, const int *clusters, const double *new_time, const double *time_scale,
+                     const int *m_per, const int *targets_local, double eps2, int mode, int *ticket) {
+  if (!e || !ticket || (mode != ABYSS_ENS_BATCHED && mode != ABYSS_ENS_GRAPH))
+    return efail(e, ABYSS_ERR_ARG, "submit: bad arguments");
+  int rc = abyss_ens_pipeline(e);
+  if (rc != ABYSS_OK) return rc;
+  // a free slot: the current one, else the other
+  if (e->busy[e->cur]) {
+    if (e->busy[e->cur ^ 1]) return efail(e, ABYSS_ERR_STATE, "submit: two waves are in flight already");
+    swap_slot(e);
+  }
+  cudaSetDevice(e->device);
+  if ((rc = abyss_ens_upload_staged(e, nk, clusters)) != ABYSS_OK) return rc;
+  if ((rc = abyss_ens_set_wave(e, nk, clusters, new_time, time_scale, m_per, targets_local)) != ABYSS_OK) return rc;
+  if ((rc = abyss_ens_launch(e, eps2, mode, nullptr)) != ABYSS_OK) return rc;
+  // queue the results' copies into this slot's pinned staging behind the wave
+  cudaStream_t s = e->stream;
+  const size_t m = e->rows, cap = (size_t)e->cap;
+  const size_t need = 16 + 4 * 24 * m + 4 * m + 4 * m * cap + 64;
+  if (need > e->ostage_bytes) {
+    ECK(cudaStreamSynchronize(s), "submit");
+    if (e->ostage) cudaFreeHost(e->ostage);
+    e->ostage = nullptr;
+    e->ostage_bytes = 0;
+    const size_t want = std::max(need, (size_t)1 << 20) * 3 / 2;
+    ECK(cudaMallocHost((void **)&e->ostage, want), "pinned result staging");
+    e->ostage_bytes = want;
+  }
+  unsigned char *b = e->ostage;
+  int *st = reinterpret_cast<int *>(b);
+  double *d = reinterpret_cast<double *>(b + 16);
+  int *nb = reinterpret_cast<int *>(b + 16 + 4 * 24 * m);
+  ECK(cudaMemcpyAsync(st, e->status.p, 4, cudaMemcpyDeviceToHost, s), "D2H");
+  ECK(cudaMemcpyAsync(st + 1, e->ovf.p, 4, cudaMemcpyDeviceToHost, s), "D2H");
+  ECK(cudaMemcpyAsync(d, e->acc_reg.p, 24 * m, cudaMemcpyDeviceToHost, s), "D2H");
+  ECK(cudaMemcpyAsync(d + 3 * m, e->jerk_reg.p, 24 * m, cudaMemcpyDeviceToHost, s), "D2H");
+  ECK(cudaMemcpyAsync(d + 6 * m, e->acc_irr.p, 24 * m, cudaMemcpyDeviceToHost, s), "D2H");
+  ECK(cudaMemcpyAsync(d + 9 * m, e->jerk_irr.p, 24 * m, cudaMemcpyDeviceToHost, s), "D2H");
+  ECK(cudaMemcpyAsync(nb, e->nnb.p, 4 * m, cudaMemcpyDeviceToHost, s), "D2H");
+  ECK(cudaMemcpyAsync(nb + m, e->list.p, 4 * m * cap, cudaMemcpyDeviceToHost, s), "D2H");
+  ECK(cudaEventRecord(e->desc_ev, s), "event");  // also marks the result copies
+  e->busy[e->cur] = 1;
+  *ticket = e->cur;
+  return ABYSS_OK;
+}
+
+int abyss_ens_ready(abyss_ens *e, int ticket) {
+  if (!e || ticket < 0 || ticket > 1 || !e->other || !e->busy[ticket]) return ABYSS_ERR_ARG;
+  cudaSetDevice(e->device);
+  const cudaEvent_t ev = e->cur == ticket ? e->desc_ev : e->other->desc_ev;
+  const cudaError_t q = cudaEventQuery(ev);
+  if (q == cudaSuccess) return 1;
+  if (q == cudaErrorNotReady) return 0;
+  return efail(e, ABYSS_ERR_CUDA, std::string("ready: ") + cudaGetErrorString(q));
+}
+
+int abyss_ens_collect(abyss_ens *e, int ticket, const double **acc_reg, const double **jerk_reg,
+                      const double **acc_irr, const double **jerk_irr, const int **nnb, const int **list,
+                      int *rows, float *gpu_ms) {
+  if (!e || ticket < 0 || ticket > 1 || !e->other || !e->busy[ticket] || !acc_reg || !jerk_reg || !acc_irr ||
+      !jerk_irr || !nnb || !list || !rows)
+    return efail(e, ABYSS_ERR_ARG, "collect: bad ticket or arguments");
+  if (e->cur != ticket) swap_slot(e);
+  cudaSetDevice(e->device);
+  ECK(cudaEventSynchronize(e->desc_ev), "collect");
+  e->desc_pending = false;
+  e->busy[ticket] = 0;
+  const size_t m = e->rows;
+  unsigned char *b = e->ostage;
+  const int *st = reinterpret_cast<const int *>(b);
+  const double *d = reinterpret_cast<const double *>(b + 16);
+  const int *nb = reinterpret_cast<const int *>(b + 16 + 4 * 24 * m);
+  *acc_reg = d;
+  *jerk_reg = d + 3 * m;
+  *acc_irr = d + 6 * m;
+  *jerk_irr = d + 9 * m;
+  *nnb = nb;
+  *list = nb + m;
+  *rows = (int)m;
+  if (gpu_ms) {
+    *gpu_ms = 0.0f;
+    ECK(cudaEventElapsedTime(gpu_ms, e->ev0, e->ev1), "event time");
+  }
+  if (st[0] & kErrTimeout) return efail(e, ABYSS_ERR_TIMEOUT, "device wait timed out");
+  return st[1] > 0 ? ABYSS_WARN_OVERFLOW : ABYSS_OK;
+}
+
 int abyss_ens_fetch(abyss_ens *e, double *acc_reg, double *jerk_reg, double *acc_irr, double *jerk_irr,
                     int *nnb, int *list, int *overflow_rows) {
   if (!e) return ABYSS_ERR_ARG;
+  if (e->busy[e->cur]) return efail(e, ABYSS_ERR_STATE, "fetch: use abyss_ens_collect for a submitted wave");
   cudaSetDevice(e->device);
   cudaStream_t s = e->stream;
   const size_t m = e->rows;

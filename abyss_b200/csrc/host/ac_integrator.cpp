@@ -919,65 +919,89 @@ int abyss_ac_serve_run(abyss_ens *e, int k, abyss_ac *const *acs, const int *slo
   const int want_fin = stop_after > 0 ? std::min(stop_after, k) : k;
   int err = ABYSS_OK;
   abyss_serve_stats S{};
-  // the dispatcher: every staged block goes into the next wave, one wave at a time
+  // The dispatcher: every staged block goes into the next wave.  Two waves can
+  // be in flight: while the GPU runs one, the next is uploaded and launched
+  // behind it, or the last one's rows are handed back.
+  struct Flight {
+    int ticket;
+    std::vector<int> wave, mper;
+  };
+  std::deque<Flight> infl;
   for (;;) {
     std::vector<int> wave;
+    bool collect = false;
     double tp = now_s();
     {
       std::unique_lock<std::mutex> lk(R.mu);
-      R.cv_gpu.wait(lk, [&] {
-        return !R.gpu_ready.empty() || (R.busy == 0 && R.host_q.empty());
-      });
-      if (R.gpu_ready.empty()) break;  // every worker idle and nothing queued: all done or stopped
-      wave.swap(R.gpu_ready);
+      for (;;) {
+        if (!R.gpu_ready.empty() && infl.size() < 2) {
+          wave.swap(R.gpu_ready);
+          break;
+        }
+        if (!infl.empty()) {
+          lk.unlock();
+          const int r = abyss_ens_ready(e, infl.front().ticket);
+          lk.lock();
+          if (r != 0) {  // finished (or failed: collect reports it)
+            collect = true;
+            break;
+          }
+          R.cv_gpu.wait_for(lk, std::chrono::microseconds(20));
+          continue;
+        }
+        if (R.busy == 0 && R.host_q.empty()) break;  // all done or stopped
+        R.cv_gpu.wait(lk);
+      }
     }
     S.idle_s += now_s() - tp;
+    if (wave.empty() && !collect) break;
     tp = now_s();
-    std::vector<int> cl, mper, tg;
-    std::vector<double> tm, scl;
-    for (int i : wave) {
-      const abyss_ac *ac = acs[i];
-      cl.push_back(slots[i]);
-      tm.push_back(ac->next_reg_block * ac->time_step);
-      scl.push_back(ac->scale);
-      mper.push_back((int)ac->block_targets.size());
-      tg.insert(tg.end(), ac->block_targets.begin(), ac->block_targets.end());
+    if (!wave.empty()) {
+      std::vector<int> cl, mper, tg;
+      std::vector<double> tm, scl;
+      for (int i : wave) {
+        const abyss_ac *ac = acs[i];
+        cl.push_back(slots[i]);
+        tm.push_back(ac->next_reg_block * ac->time_step);
+        scl.push_back(ac->scale);
+        mper.push_back((int)ac->block_targets.size());
+        tg.insert(tg.end(), ac->block_targets.begin(), ac->block_targets.end());
+      }
+      int ticket = -1;
+      rc = abyss_ens_submit(e, (int)wave.size(), cl.data(), tm.data(), scl.data(), mper.data(), tg.data(), eps2,
+                            mode, &ticket);
+      S.prep_s += now_s() - tp;
+      if (rc != ABYSS_OK) {
+        err = rc;
+        break;
+      }
+      S.rows += (long long)tg.size();
+      infl.push_back(Flight{ticket, std::move(wave), std::move(mper)});
+      continue;
     }
-    const int nl = (int)wave.size();
-    rc = abyss_ens_upload_staged(e, nl, cl.data());
-    if (rc == ABYSS_OK) rc = abyss_ens_set_wave(e, nl, cl.data(), tm.data(), scl.data(), mper.data(), tg.data());
-    if (rc == ABYSS_OK) rc = abyss_ens_launch(e, eps2, mode, nullptr);
-    S.prep_s += now_s() - tp;
-    tp = now_s();
-    const size_t rows = tg.size();
-    S.rows += (long long)rows;
-    const double *acc = nullptr, *jerk = nullptr, *airr = nullptr, *jirr = nullptr;
-    const int *nnb = nullptr, *lst = nullptr;
-    if (rc == ABYSS_OK) {
-      int ovf = 0;
-      rc = abyss_ens_fetch_view(e, &acc, &jerk, &airr, &jirr, &nnb, &lst, &ovf);
-      if (rc == ABYSS_WARN_OVERFLOW) rc = ABYSS_OK;  // end_block handles each overflowed block
-    }
+    // hand the oldest wave's rows back to the workers
+    Flight f = std::move(infl.front());
+    infl.pop_front();
+    const double *acc, *jerk, *airr, *jirr;
+    const int *nnb, *lst;
+    int rows = 0;
+    float ms = 0.0f;
+    rc = abyss_ens_collect(e, f.ticket, &acc, &jerk, &airr, &jirr, &nnb, &lst, &rows, &ms);
+    if (rc == ABYSS_WARN_OVERFLOW) rc = ABYSS_OK;  // end_block handles each overflowed block
+    S.wait_s += now_s() - tp;
     if (rc != ABYSS_OK) {
       err = rc;
-      std::lock_guard<std::mutex> lk(R.mu);
-      R.stop = true;
-      R.quit = true;
-      R.host_q.clear();
       break;
     }
-    S.wait_s += now_s() - tp;
     tp = now_s();
-    float ms = 0.0f;
-    abyss_ens_last_ms(e, &ms);
     if (gpu_ms) *gpu_ms += ms;
     if (waves) ++*waves;
     // the wave's integrations are idle until their rows are handed back, so
     // their result buffers are filled without the lock
     size_t r0 = 0;
-    for (int b = 0; b < nl; ++b) {
-      const int i = wave[b];
-      const size_t m = mper[b];
+    for (size_t b = 0; b < f.wave.size(); ++b) {
+      const int i = f.wave[b];
+      const size_t m = f.mper[b];
       auto &d = R.res_d[i];
       d.resize(12 * m);
       std::copy(acc + 3 * r0, acc + 3 * (r0 + m), d.begin());
@@ -991,11 +1015,23 @@ int abyss_ac_serve_run(abyss_ens *e, int k, abyss_ac *const *acs, const int *slo
     }
     {
       std::lock_guard<std::mutex> lk(R.mu);
-      for (int i : wave) R.host_q.push_back(i);
+      for (int i : f.wave) R.host_q.push_back(i);
       if (R.finished >= want_fin || (budget_ms > 0 && (now_s() - t0) * 1e3 >= budget_ms)) R.stop = true;
     }
     R.cv_host.notify_all();
     S.hand_s += now_s() - tp;
+  }
+  if (err != ABYSS_OK) {
+    // drain what is in flight so that the ensemble is usable again
+    for (const Flight &f : infl) {
+      const double *a, *b2, *c2, *d2;
+      const int *n2, *l2;
+      int rows = 0;
+      (void)abyss_ens_collect(e, f.ticket, &a, &b2, &c2, &d2, &n2, &l2, &rows, nullptr);
+    }
+    std::lock_guard<std::mutex> lk(R.mu);
+    R.stop = true;
+    R.host_q.clear();
   }
   {
     std::lock_guard<std::mutex> lk(R.mu);

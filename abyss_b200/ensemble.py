@@ -34,6 +34,9 @@ def _bind(L):
     L.abyss_ens_upload_staged.argtypes = [_vp, C.c_int, _ip]
     L.abyss_ens_list_cap.argtypes = [_vp]
     L.abyss_ens_set_chunk.argtypes = [_vp, C.c_int]
+    L.abyss_ens_submit.argtypes = [_vp, C.c_int, _ip, _dp, _dp, _ip, _ip, C.c_double, C.c_int, _ip]
+    L.abyss_ens_ready.argtypes = [_vp, C.c_int]
+    L.abyss_ens_collect.argtypes = [_vp, C.c_int] + [C.POINTER(_dp)] * 4 + [C.POINTER(_ip)] * 2 + [_ip, _fp]
     L._ens_bound = True
 
 
@@ -115,6 +118,35 @@ class Ensemble:
         shapes = [(n, 3)] * 4 + [(n,)] * 3
         names = ("x", "v", "a0", "a1", "t0", "mass", "r2nb")
         return {nm: np.ctypeslib.as_array(p, shape=sh) for nm, p, sh in zip(names, ptrs, shapes)}
+
+    def submit(self, clusters, new_time, time_scale, targets, eps2: float = 0.0, mode: int = GRAPH) -> int:
+        """Launch a wave of staged clusters without waiting (at most two in flight);
+        returns its ticket for collect()."""
+        cl = np.ascontiguousarray(clusters, np.int32)
+        nt = np.ascontiguousarray(new_time, np.float64)
+        sc = np.ascontiguousarray(time_scale, np.float64)
+        mp = np.array([len(t) for t in targets], np.int32)
+        tg = np.ascontiguousarray(np.concatenate([np.asarray(t, np.int32) for t in targets]), np.int32)
+        ticket = C.c_int(-1)
+        self._check(self._L.abyss_ens_submit(self._h, int(cl.shape[0]), ptr(cl, _ip), ptr(nt), ptr(sc),
+                                              ptr(mp, _ip), ptr(tg, _ip), float(eps2), int(mode),
+                                              C.byref(ticket)))
+        return int(ticket.value)
+
+    def collect(self, ticket: int) -> ForceResult:
+        """Wait for a submitted wave; its rows, copied out of the pinned staging."""
+        p = [_dp() for _ in range(4)]
+        q = [_ip() for _ in range(2)]
+        rows = C.c_int(0)
+        ms = np.zeros(1, np.float32)
+        rc = self._L.abyss_ens_collect(self._h, int(ticket), *[C.byref(x) for x in p], *[C.byref(x) for x in q],
+                                       C.byref(rows), ptr(ms, _fp))
+        self._check(rc, allow_overflow=True)
+        m = int(rows.value)
+        arr = [np.ctypeslib.as_array(x, shape=(m, 3)).copy() for x in p]
+        nnb = np.ctypeslib.as_array(q[0], shape=(m,)).copy()
+        lst = np.ctypeslib.as_array(q[1], shape=(m, self.cap)).copy()
+        return ForceResult(arr[0], arr[1], arr[2], arr[3], nnb, lst)
 
     def set_chunk(self, j_per_chunk: int):
         """j per chunk of a cluster's work items (its chunk count depends on its size only)."""

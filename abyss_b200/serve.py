@@ -125,6 +125,8 @@ class Server:
         for c in self.ctxs:
             self.ctx_free.put(c)
         self.waiting: list[Request] = []
+        self.building: list = []  # (request, future of its set-up)
+        self.retiring: list = []  # (request, future of its final energy and state)
         self.active: list[Request] = []
         self.done: list[Request] = []
         self.t0 = time.perf_counter()
@@ -143,7 +145,11 @@ class Server:
         return time.perf_counter() - self.t0
 
     def close(self):
+        self._reap(wait=True)
         self.pool.shutdown()
+        for r, _ in self.building:
+            if r.ac is not None:
+                r.ac.close()
         for r in self.active:
             r.ac.close()
         self.ens.close()
@@ -182,7 +188,11 @@ class Server:
             self.build_s["energy"] += t4 - t3
 
     def _admit(self):
-        still, batch = [], []
+        """Requests that have arrived get an arena slot (main thread, between
+        runs: the ensemble is not in use then) and their set-up is started on
+        the host pool; set-ups that have finished join the active set.  Set-ups
+        run while the integrations already admitted are being served."""
+        still = []
         for r in self.waiting:
             if r.arrival > self.now():
                 still.append(r)
@@ -192,13 +202,22 @@ class Server:
                 still.append(r)  # not enough device room yet: wait for a retirement
                 continue
             r.slot = slot
-            batch.append(r)
+            self.building.append((r, self.pool.submit(self._build, r)))
         self.waiting = still
-        if batch:
-            list(self.pool.map(self._build, batch))
-            for r in batch:
+        pending = []
+        for r, fut in self.building:
+            if fut.done():
+                fut.result()  # re-raises a failed set-up
                 r.admitted = self.now()
                 self.active.append(r)
+            else:
+                pending.append((r, fut))
+        self.building = pending
+        if not self.active and self.building:  # nothing to serve meanwhile: wait for one set-up
+            r, fut = self.building.pop(0)
+            fut.result()
+            r.admitted = self.now()
+            self.active.append(r)
 
     # ------------------------------------------------------------ one round
     def round(self):
@@ -238,14 +257,25 @@ class Server:
             if st in (ROUND_ADVANCED_DONE, ROUND_FINISHED):
                 finished.append(r)
         t = time.perf_counter()
-        if finished:
-            list(self.pool.map(self._finish, finished))
-            for r in finished:
-                self.ens.detach(r.slot)
-                self.active.remove(r)
-                self.done.append(r)
+        # a finished integration no longer touches the ensemble: its range is
+        # freed now, its final energy and state are taken on the host pool
+        for r in finished:
+            self.ens.detach(r.slot)
+            self.active.remove(r)
+            self.retiring.append((r, self.pool.submit(self._finish, r)))
+        self._reap()
         ph["retire"] += time.perf_counter() - t
         self.rounds += 1
+
+    def _reap(self, wait: bool = False):
+        still = []
+        for r, fut in self.retiring:
+            if wait or fut.done():
+                fut.result()
+                self.done.append(r)
+            else:
+                still.append((r, fut))
+        self.retiring = still
 
     def _finish(self, r: Request):
         """Final energy and positions of a finished integration; frees it."""
@@ -259,10 +289,11 @@ class Server:
         r.ac = None
 
     def run_until_idle(self, max_seconds: float = 1e9):
-        while (self.waiting or self.active) and self.now() < max_seconds:
+        while (self.waiting or self.building or self.active) and self.now() < max_seconds:
             if not self.active and self.waiting and all(r.arrival > self.now() for r in self.waiting):
                 time.sleep(max(0.0, min(r.arrival for r in self.waiting) - self.now()))
             self.round()
+        self._reap(wait=True)
 
 
 def poisson_requests(rate: float, duration: float, nmin: int, nmax: int, seed: int = 5, t_end: float = 1.0,
@@ -283,7 +314,7 @@ def poisson_requests(rate: float, duration: float, nmin: int, nmax: int, seed: i
 
 def serve(rate: float = 200.0, duration: float = 2.0, nmin: int = 256, nmax: int = 2048, t_end: float = 0.0625,
           capacity: int = 1 << 21, seed: int = 5, host_threads: int = 16, serial: bool = False,
-          chunk_j: int = 256):
+          chunk_j: int = 256, slice_ms: float = 20.0):
     """Run a Poisson stream through the server (or, with serial=True, one request at
     a time through the same code) and report latency percentiles and throughput."""
     reqs = poisson_requests(rate, duration, nmin, nmax, seed=seed, t_end=t_end)
@@ -295,7 +326,7 @@ def serve(rate: float = 200.0, duration: float = 2.0, nmin: int = 256, nmax: int
         rounds, wave_ms, peak = 0, 0.0, 1
         srv = None
     else:
-        srv = Server(capacity=capacity, host_threads=host_threads, max_n=nmax, chunk_j=chunk_j)
+        srv = Server(capacity=capacity, host_threads=host_threads, max_n=nmax, chunk_j=chunk_j, slice_ms=slice_ms)
         for r in reqs:
             srv.submit(r)
         srv.run_until_idle()

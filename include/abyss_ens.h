@@ -86,6 +86,25 @@ int abyss_ens_fetch(abyss_ens *e, double *acc_reg, double *jerk_reg, double *acc
  * until the next abyss_ens_fetch_view or abyss_ens_destroy. */
 int abyss_ens_fetch_view(abyss_ens *e, const double **acc_reg, const double **jerk_reg, const double **acc_irr,
                          const double **jerk_irr, const int **nnb, const int **list, int *overflow_rows);
+/* Two waves in flight.  abyss_ens_submit uploads the listed clusters' staged
+ * state, describes the wave, launches it (mode ABYSS_ENS_BATCHED or _GRAPH) and
+ * queues the copies of its results, all asynchronously, and returns a ticket;
+ * abyss_ens_collect(ticket) waits for that wave and returns its rows (in wave
+ * order) in pinned memory that stays valid until that ticket's slot is
+ * submitted to again.  At most two waves may be submitted and not collected;
+ * the GPU runs them in submission order, while the caller prepares the next or
+ * consumes the last.  A cluster must not be in two uncollected waves.  The
+ * first submit allocates a second set of wave buffers (abyss_ens_pipeline may
+ * do it earlier).  While a wave is uncollected, set_wave, launch and fetch
+ * refuse to touch its slot. */
+int abyss_ens_pipeline(abyss_ens *e);
+int abyss_ens_submit(abyss_ens *e, int nk, const int *clusters, const double *new_time, const double *time_scale,
+                     const int *m_per, const int *targets_local, double eps2, int mode, int *ticket);
+/* 1 when the wave of `ticket` and its result copies have finished, 0 if not yet. */
+int abyss_ens_ready(abyss_ens *e, int ticket);
+int abyss_ens_collect(abyss_ens *e, int ticket, const double **acc_reg, const double **jerk_reg,
+                      const double **acc_irr, const double **jerk_irr, const int **nnb, const int **list,
+                      int *rows, float *gpu_ms);
 /* GPU milliseconds of the last launch (CUDA events around the wave). */
 int abyss_ens_last_ms(abyss_ens *e, float *ms);
 /* Rows, work items and kernel launches of the last wave. */

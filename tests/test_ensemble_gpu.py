@@ -136,3 +136,35 @@ def test_staged_upload_matches_and_leaves_unlisted_clusters(rf):
     for f in ("acc_reg", "jerk_reg", "acc_irr", "jerk_irr", "nnb", "list"):
         assert np.array_equal(getattr(got, f), getattr(want, f)), f
     e.close()
+
+
+def test_two_waves_in_flight_match_blocking_waves(rf):
+    """Two submitted waves (disjoint clusters, staged state) give the same rows
+    as the same waves run one at a time with set_wave/launch/fetch."""
+    e, clusters = make_ensemble(rf, k=8, seed=11)
+    rng = np.random.default_rng(5)
+    waves = [np.array([0, 2, 3, 6]), np.array([1, 4, 5, 7])]
+    targets = {k: np.sort(rng.choice(c.n, max(1, c.n // 4), replace=False)).astype(np.int32)
+               for k, c in enumerate(clusters)}
+    want = []
+    for w in waves:
+        e.set_wave(w, np.zeros(len(w)), np.ones(len(w)), [targets[k] for k in w])
+        e.launch(EPS2, GRAPH)
+        want.append(e.fetch())
+    for k, c in enumerate(clusters):  # the same state, through the staging
+        st = e.stage(k)
+        st["x"][:] = c.x
+        st["v"][:] = c.v
+        st["a0"][:] = 0.0
+        st["a1"][:] = 0.0
+        st["t0"][:] = 0.0
+        st["mass"][:] = c.m
+        st["r2nb"][:] = c.r2nb
+    for rep in range(2):
+        tickets = [e.submit(w, np.zeros(len(w)), np.ones(len(w)), [targets[k] for k in w], EPS2, GRAPH)
+                   for w in waves]
+        got = [e.collect(t) for t in tickets]
+        for g, w in zip(got, want):
+            for f in ("acc_reg", "jerk_reg", "acc_irr", "jerk_irr", "nnb", "list"):
+                assert np.array_equal(getattr(g, f), getattr(w, f)), (rep, f)
+    e.close()
