@@ -97,6 +97,12 @@ def lib():
     L.abyss_set_tuning_table.argtypes = [_vp, C.c_int, _ip, C.POINTER(Tuning)]
     L.abyss_energy.argtypes = [_vp, C.c_int, _dp, _dp, _dp, C.c_double, _dp]
     L.abyss_init_derivs23.argtypes = [_vp, C.c_int] + [_dp] * 6 + [C.c_double] + [_dp] * 4
+    # state I/O (include/abyss_io.h)
+    L.abyss_read_reference_ic.argtypes = [C.c_char_p, _ip, _dp, _dp, _dp]
+    L.abyss_ac_write_snapshot.argtypes = [_vp, C.c_char_p, C.c_double, C.c_double]
+    L.abyss_ac_save.argtypes = [_vp, C.c_char_p]
+    L.abyss_ac_load.argtypes = [_vp, C.c_char_p, C.c_int, C.POINTER(_vp)]
+    L.abyss_ac_info.argtypes = [_vp, _ip, C.POINTER(ACParams)]
     L.abyss_tile_variant.argtypes = [C.c_int, _ip]
     # reference-compatible drop-in
     L.InitializeDevice.argtypes = [_ip]

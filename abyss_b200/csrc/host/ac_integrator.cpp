@@ -26,8 +26,12 @@
 #include <array>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <condition_variable>
 #include <deque>
+#include <fstream>
+#include <iomanip>
+#include <sstream>
 #include <mutex>
 #include <thread>
 #include <cstring>
@@ -42,6 +46,7 @@
 
 #include "../../../include/abyss_ac.h"
 #include "../../../include/abyss_ens.h"
+#include "../../../include/abyss_io.h"
 #include "../../../include/abyss_reg.h"
 
 namespace {
@@ -1261,6 +1266,13 @@ int abyss_ac_last_regular(const abyss_ac *ac, int *m, int *targets, double *px, 
 
 const char *abyss_ac_last_error(const abyss_ac *ac) { return ac ? ac->err.c_str() : "null integrator"; }
 
+int abyss_ac_info(const abyss_ac *ac, int *n, abyss_ac_params *p) {
+  if (!ac) return ABYSS_ERR_ARG;
+  if (n) *n = ac->n;
+  if (p) *p = ac->p;
+  return ABYSS_OK;
+}
+
 }  // extern "C"
 
 // ------------------------------------------------------------------ host rules
@@ -1342,6 +1354,176 @@ int abyss_host_regular_correct(int n, const double *x, const double *v, const do
   commit_derivatives(acc, jerk, acc_irr, jerk_irr, a2, a3, n_new, a_reg, a_irr, at);
   std::memcpy(a_reg_out, a_reg, sizeof(a_reg));
   std::memcpy(a_tot_out, at, sizeof(at));
+  return ABYSS_OK;
+}
+
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ state I/O
+
+namespace {
+
+constexpr char kCkptMagic[8] = {'A', 'B', 'Y', 'S', 'S', 'A', 'C', 'K'};
+constexpr unsigned kCkptVersion = 1;
+
+// Units of the reference's text files (src_mpi/def.h:51-60 and
+// particle.h:204-214): input positions in kpc, velocities in km/s, masses in
+// 1e9 Msun; output in pc, km/s and Msun; code units are G = 1.
+constexpr double kPc = 3.08567758149137e18;
+constexpr double kYr = 3.1536e7;
+constexpr double kPositionUnit = 4.0;       // pc
+constexpr double kVelocityUnit = 4e-10;     // pc / yr
+constexpr double kMassUnit = 0.0001424198;  // Msun
+
+template <class T>
+void put(std::ofstream &f, const T &v) {
+  f.write(reinterpret_cast<const char *>(&v), sizeof(T));
+}
+template <class T>
+bool get(std::ifstream &f, T &v) {
+  return (bool)f.read(reinterpret_cast<char *>(&v), sizeof(T));
+}
+
+}  // namespace
+
+extern "C" {
+
+int abyss_ac_save(const abyss_ac *ac, const char *path) {
+  if (!ac || !path) return ABYSS_ERR_ARG;
+  if (ac->in_block) return ABYSS_ERR_STATE;  // only between regular blocks
+  std::ofstream f(path, std::ios::binary | std::ios::trunc);
+  if (!f) return ABYSS_ERR_ARG;
+  f.write(kCkptMagic, sizeof(kCkptMagic));
+  put(f, kCkptVersion);
+  put(f, (unsigned)sizeof(Star::a_tot));
+  put(f, ac->n);
+  put(f, ac->p);
+  put(f, ac->scale);
+  put(f, ac->time_block);
+  put(f, ac->block_max);
+  put(f, ac->time_step);
+  put(f, ac->next_reg_block);
+  put(f, (int)ac->done);
+  put(f, ac->st);
+  for (const Star &p : ac->s) {
+    put(f, p.x);
+    put(f, p.v);
+    put(f, p.m);
+    put(f, p.a_tot);
+    put(f, p.a_reg);
+    put(f, p.a_irr);
+    put(f, p.r2nb);
+    put(f, p.t_reg);
+    put(f, p.t_irr);
+    put(f, p.dt_reg);
+    put(f, p.dt_irr);
+    const ULL u[6] = {p.cur_reg, p.cur_irr, p.new_cur_irr, p.next_irr, p.tb_reg, p.tb_irr};
+    put(f, u);
+    put(f, p.lv_reg);
+    put(f, p.lv_irr);
+    put(f, (int)p.nb.size());
+    if (!p.nb.empty()) f.write(reinterpret_cast<const char *>(p.nb.data()), sizeof(int) * p.nb.size());
+  }
+  f.write(kCkptMagic, sizeof(kCkptMagic));  // trailer: the file is complete
+  return f ? ABYSS_OK : ABYSS_ERR_STATE;
+}
+
+int abyss_ac_load(abyss_ctx *ctx, const char *path, int threads, abyss_ac **out) {
+  if (!ctx || !path || !out) return ABYSS_ERR_ARG;
+  std::ifstream f(path, std::ios::binary);
+  if (!f) return ABYSS_ERR_ARG;
+  char magic[8];
+  unsigned version = 0, dsz = 0;
+  int n = 0;
+  if (!f.read(magic, 8) || std::memcmp(magic, kCkptMagic, 8) != 0) return ABYSS_ERR_STATE;
+  if (!get(f, version) || version != kCkptVersion || !get(f, dsz) || dsz != sizeof(Star::a_tot)) return ABYSS_ERR_STATE;
+  if (!get(f, n) || n < 2) return ABYSS_ERR_STATE;
+  abyss_ac *ac = new abyss_ac;
+  ac->ctx = ctx;
+  ac->n = n;
+  int done = 0;
+  bool ok = get(f, ac->p) && get(f, ac->scale) && get(f, ac->time_block) && get(f, ac->block_max) &&
+            get(f, ac->time_step) && get(f, ac->next_reg_block) && get(f, done) && get(f, ac->st);
+  ac->done = done != 0;
+  ac->p.threads = threads;
+  if (ok) ac->s.resize(n);
+  for (int i = 0; ok && i < n; ++i) {
+    Star &p = ac->s[i];
+    ULL u[6];
+    int nn = 0;
+    ok = get(f, p.x) && get(f, p.v) && get(f, p.m) && get(f, p.a_tot) && get(f, p.a_reg) && get(f, p.a_irr) &&
+         get(f, p.r2nb) && get(f, p.t_reg) && get(f, p.t_irr) && get(f, p.dt_reg) && get(f, p.dt_irr) &&
+         get(f, u) && get(f, p.lv_reg) && get(f, p.lv_irr) && get(f, nn) && nn >= 0 && nn <= n;
+    if (!ok) break;
+    p.cur_reg = u[0];
+    p.cur_irr = u[1];
+    p.new_cur_irr = u[2];
+    p.next_irr = u[3];
+    p.tb_reg = u[4];
+    p.tb_irr = u[5];
+    p.nb.resize(nn);
+    if (nn > 0) ok = (bool)f.read(reinterpret_cast<char *>(p.nb.data()), sizeof(int) * (size_t)nn);
+    for (int j : p.nb)
+      if (j < 0 || j >= n) ok = false;
+  }
+  if (ok) ok = f.read(magic, 8) && std::memcmp(magic, kCkptMagic, 8) == 0;
+  if (!ok) {
+    delete ac;
+    return ABYSS_ERR_STATE;
+  }
+  *out = ac;
+  return ABYSS_OK;
+}
+
+int abyss_ac_write_snapshot(const abyss_ac *ac, const char *path, double output_time, double output_time_step) {
+  if (!ac || !path) return ABYSS_ERR_ARG;
+  std::ofstream f(path, std::ios::trunc);
+  if (!f) return ABYSS_ERR_ARG;
+  const double now = ac->next_reg_block * ac->time_step;  // code time of the state
+  const int w = 18;
+  f << now * ac->scale * 1e10 / 1e6 << " Myr, " << "\n";
+  f << output_time << ", " << output_time_step << ", " << now << "\n";
+  f << std::left << std::setw(w) << "PID" << std::setw(w) << "Mass (Msun)" << std::setw(w) << "X (pc)"
+    << std::setw(w) << "Y (pc)" << std::setw(w) << "Z (pc)" << std::setw(w) << "Vx (km/s)" << std::setw(w)
+    << "Vy (km/s)" << std::setw(w) << "Vz (km/s)" << "\n";
+  auto kms = [](double u) { return u * kVelocityUnit / kYr * kPc / 1e5; };  // ReadWrite.cpp:257-264 order
+  for (int i = 0; i < ac->n; ++i) {
+    const Star &p = ac->s[i];
+    double pos[3], vel[3];
+    predict(p, now - p.t_irr, ac->scale, pos, vel);
+    f << std::left << std::fixed << std::setprecision(8) << std::setw(w) << i << std::setw(w) << p.m * kMassUnit
+      << std::setw(w) << pos[0] * kPositionUnit << std::setw(w) << pos[1] * kPositionUnit << std::setw(w)
+      << pos[2] * kPositionUnit << std::setw(w) << kms(vel[0]) << std::setw(w) << kms(vel[1]) << std::setw(w)
+      << kms(vel[2]) << '\n';
+  }
+  return f ? ABYSS_OK : ABYSS_ERR_STATE;
+}
+
+int abyss_read_reference_ic(const char *path, int *n, double *x, double *v, double *mass) {
+  if (!path || !n) return ABYSS_ERR_ARG;
+  std::ifstream f(path);
+  if (!f) return ABYSS_ERR_ARG;
+  std::string line;
+  int row = 0;
+  while (std::getline(f, line)) {
+    if (x && v && mass) {
+      if (row >= *n) return ABYSS_ERR_ARG;
+      double d[7] = {0, 0, 0, 0, 0, 0, 0};
+      std::istringstream iss(line);
+      double val;
+      int col = 0;
+      while (col < 7 && iss >> val) d[col++] = val;
+      for (int k = 0; k < 3; ++k) {
+        x[3 * (size_t)row + k] = d[k] * 1000 / kPositionUnit;
+        v[3 * (size_t)row + k] = d[3 + k] * (1e5 * kYr / kPc) / kVelocityUnit;
+      }
+      mass[row] = d[6] * 1e9 / kMassUnit;
+    }
+    ++row;
+  }
+  if (x && v && mass && row != *n) return ABYSS_ERR_ARG;
+  *n = row;
   return ABYSS_OK;
 }
 

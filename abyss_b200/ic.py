@@ -260,3 +260,27 @@ def king(n: int, seed: int, w0: float = 6.0, masses: str = "equal",
         dens_model = np.interp(r, rs, rho) / mtot * n  # number density in model units
         r2nb = _r2_from_density(r * lam, dens_model / lam ** 3, k_nb)
     return Cluster(pos, vel, m, r2nb, name=f"king{w0:g}_n{n}_s{seed}")
+
+
+def read_reference(path: str, k_nb: float = 32.0) -> Cluster:
+    """A cluster from an input file in the reference's text format (x y z in kpc,
+    vx vy vz in km/s, mass in 1e9 Msun per line; include/abyss_io.h), in code
+    units, with neighbour radii for k_nb neighbours."""
+    import ctypes as C
+
+    from . import _lib
+
+    L = _lib.lib()
+    n = C.c_int(0)
+    rc = L.abyss_read_reference_ic(str(path).encode(), C.byref(n), None, None, None)
+    if rc != 0:
+        raise _lib.AbyssError(rc, f"cannot read {path}")
+    x = np.zeros((n.value, 3))
+    v = np.zeros((n.value, 3))
+    m = np.zeros(n.value)
+    dp = C.POINTER(C.c_double)
+    rc = L.abyss_read_reference_ic(str(path).encode(), C.byref(n), x.ctypes.data_as(dp), v.ctypes.data_as(dp),
+                                   m.ctypes.data_as(dp))
+    if rc != 0:
+        raise _lib.AbyssError(rc, f"cannot read {path}")
+    return Cluster(x, v, m, _r2_exact_k(x, int(k_nb)), name=f"reference_ic_{n.value}")

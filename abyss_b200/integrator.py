@@ -41,6 +41,34 @@ class ACIntegrator:
         if rc != 0:
             raise _lib.AbyssError(rc, self._L.abyss_ac_last_error(self._h).decode())
 
+    @classmethod
+    def load(cls, rf: RegularForce, path: str, threads: int = 0) -> "ACIntegrator":
+        """An integration restored from a checkpoint written by save() (include/abyss_io.h)."""
+        self = cls.__new__(cls)
+        self._L = _lib.lib()
+        self.rf = rf
+        h = C.c_void_p()
+        rc = self._L.abyss_ac_load(rf._h, str(path).encode(), int(threads), C.byref(h))
+        if rc != 0:
+            raise _lib.AbyssError(rc, f"abyss_ac_load failed for {path}")
+        self._h = h
+        n = C.c_int(0)
+        self.params = ACParams()
+        self._check(self._L.abyss_ac_info(self._h, C.byref(n), C.byref(self.params)))
+        self.n = int(n.value)
+        self.nb_max = int(self.params.nb_max)
+        self.m = None
+        return self
+
+    def save(self, path: str):
+        """Checkpoint between regular blocks (include/abyss_io.h abyss_ac_save)."""
+        self._check(self._L.abyss_ac_save(self._h, str(path).encode()))
+
+    def write_snapshot(self, path: str, output_time: float = 0.0, output_time_step: float = 0.0):
+        """The state as a snapshot in the reference's text format."""
+        self._check(self._L.abyss_ac_write_snapshot(self._h, str(path).encode(), float(output_time),
+                                                    float(output_time_step)))
+
     def last_error(self) -> str:
         return self._L.abyss_ac_last_error(self._h).decode()
 

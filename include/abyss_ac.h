@@ -124,6 +124,8 @@ int abyss_ac_last_regular(const abyss_ac *ac, int *m, int *targets, double *px, 
                           double *r2nb, double *acc_reg, double *jerk_reg, int *nnb, int *list,
                           int list_cap);
 const char *abyss_ac_last_error(const abyss_ac *ac);
+/* Particle count and parameters of an integration (either may be NULL). */
+int abyss_ac_info(const abyss_ac *ac, int *n, abyss_ac_params *p);
 
 #ifdef __cplusplus
 }

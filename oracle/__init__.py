@@ -105,6 +105,7 @@ def ref():
         L.ref_new_time_step_irr.restype = C.c_double
         L.ref_block_time_step.argtypes = [C.c_double, _ip, C.POINTER(C.c_ulonglong), _dp]
         L.ref_eta.restype = C.c_double
+        L.ref_particle_from_row.argtypes = [_dp, _dp, _dp, _dp]
         _REF = L
     return _REF
 

@@ -79,6 +79,21 @@ int ref_alloc(int n) {
     return 0;
 }
 
+// One line of the reference's input file through its own Particle::initialize
+// and normalizeParticle (particle.h:139-147,204-214): code-unit x, v, mass.
+void ref_particle_from_row(const double *row7, double *x, double *v, double *mass) {
+    Particle p;
+    double d[7];
+    std::memcpy(d, row7, sizeof(d));
+    p.initialize(d, 0);
+    p.normalizeParticle();
+    for (int k = 0; k < 3; ++k) {
+        x[k] = p.Position[k];
+        v[k] = p.Velocity[k];
+    }
+    *mass = p.Mass;
+}
+
 void ref_free(void) {
     delete[] particles;
     delete global_variable;
