@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--n", type=int, default=N_DEFAULT)
     ap.add_argument("--no-sweep", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the batched-ensemble, serving and energy measurements after the timed region")
     return ap.parse_args()
 
 
@@ -425,17 +427,63 @@ def run_ours(args, world, rank, local, pg):
         "clocks": clocks,
         "sweep": sweep,
     }
+    rf.close()
     if rank == 0 and world == 1 and not args.no_cpu:
+        import oracle
+
         threads = host_threads()
         sample = 2048
-        v, el = cpu_port_baseline(c, sample, threads)
-        line["cpu_baseline"] = {"value": v, "unit": "Gpairs/s", "cores": threads, "kind": "port",
-                                "sample": f"{sample} evenly spaced targets x all {n} j "
-                                          f"({el:.1f} s, FP64 restatement of "
-                                          "ComputeAcceleration.cpp:235-299)"}
+        if oracle.ref_available() and host_mem_gb() > n * 16616 / 1e9 * 1.2 + 8:
+            v, el = cpu_reference_baseline(c, sample, threads)
+            kind, what = "reference", "Particle::computeAccelerationReg of the reference, oracle/_ref"
+        else:
+            v, el = cpu_port_baseline(c, sample, threads)
+            kind, what = "port", "FP64 restatement of ComputeAcceleration.cpp:235-299"
+        line["cpu_baseline"] = {"value": v, "unit": "Gpairs/s", "cores": threads, "kind": kind,
+                                "sample": f"{sample} evenly spaced targets x all {n} j ({el:.1f} s, {what})"}
+    if rank == 0 and world == 1 and not args.no_extras:
+        line["extras"] = extras(local)
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def extras(device: int) -> dict:
+    """The rest of the headline metric, measured after the timed region on the
+    same GPU: batched-ensemble throughput against one cluster per launch, the
+    serving loop against serial plain integrations (throughput, p50/p99), and
+    the energy drift of a full integration."""
+    from abyss_b200 import bench_ensemble, runs, serve, workloads
+    from abyss_b200.regforce import RegularForce
+
+    out = {}
+    rf = RegularForce(device)
+    clusters = workloads.ensemble(k=512)
+    waves = workloads.ensemble_waves(clusters, 6)
+    ens = bench_ensemble.measure(rf, clusters, waves)
     rf.close()
+    out["batched_ensemble"] = {
+        "workload": "512 Plummer clusters, N log-uniform in [256, 16384], 6 waves of regular blocks",
+        "cluster_blocks_per_s_graph": ens["graph"]["cluster_blocks_per_s"],
+        "cluster_blocks_per_s_plain": ens["plain"]["cluster_blocks_per_s"],
+        "gpairs_s_graph": ens["graph"]["gpairs_s"], "graph_vs_plain": ens["graph_vs_plain"]}
+    kw = dict(rate=2000.0, duration=0.25, nmin=256, nmax=2048, t_end=0.0625)
+    res = {}
+    for serial in (False, True):
+        r, _ = serve.serve(**kw, serial=serial)
+        res["serial" if serial else "continuous"] = r
+    c, sp = res["continuous"], res["serial"]
+    out["serving"] = {
+        "workload": "Poisson 2000 requests/s for 0.25 s (seed 5), Plummer or King W0 3/6/9, Kroupa IMF, "
+                    "N log-uniform in [256, 2048], each integrated to t = 1/16",
+        "requests": c["requests"], "clusters_per_s": c["clusters_per_s"],
+        "clusters_per_s_serial_plain": sp["clusters_per_s"], "vs_serial_plain": c["clusters_per_s"] / sp["clusters_per_s"],
+        "p50_latency_s": c["p50_latency_s"], "p99_latency_s": c["p99_latency_s"],
+        "p50_latency_s_serial_plain": sp["p50_latency_s"], "p99_latency_s_serial_plain": sp["p99_latency_s"],
+        "median_dE_over_E": c["median_dE_over_E"], "max_dE_over_E": c["max_dE_over_E"]}
+    c1 = runs.run("c1")
+    out["energy_c1"] = {"workload": "Plummer N = 1024, eps = 1e-4, to t = 10", "dE_over_E": c1["dE_over_E"],
+                        "regular_blocks": c1["stats"]["blocks"], "wall_s": c1["wall_s"]}
+    return out
 
 
 def main():
