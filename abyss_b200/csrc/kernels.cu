@@ -859,6 +859,9 @@ __global__ void finalize_rows(JSet js, Work w, Outputs o, int sort_cap) {
     double s[6] = {0, 0, 0, 0, 0, 0};
     const int nch = w.row_nchunks ? w.row_nchunks[r] : w.n_chunks;
     const int joff = w.row_joff ? w.row_joff[r] : 0;
+    // unrolled so that the loads of several chunks are in flight at once; the
+    // additions keep their order (chunk c, c + 32, ...), so the sum is unchanged
+#pragma unroll 8
     for (int c = lane; c < nch; c += 32) {
       const double *src = w.part + ((size_t)r * w.s_stride + c) * 6;
 #pragma unroll
