@@ -149,17 +149,35 @@ void block_step(const abyss_ac *ac, double dt, int &level, ULL &block, double &s
 }
 
 // UpdateParticle.cpp:151-241 (calculateTimeStepIrr).
+// The irregular step of a particle from its fields (a_tot, a_irr are the
+// particle's new derivatives); lv_irr, dt_irr, tb_irr are updated in place.
+void time_step_irr_of(const abyss_ac *ac, bool has_nb, const double (&a_tot)[3][4], const double (&a_irr)[3][4],
+                      ULL new_cur_irr, ULL cur_reg, ULL tb_reg, int lv_reg, int &lv_irr, double &dt_irr,
+                      ULL &tb_irr);
+
 void time_step_irr(const abyss_ac *ac, Star &p) {
-  if (p.nb.empty()) {
-    p.lv_irr = p.lv_reg;
-    p.dt_irr = static_cast<double>(std::pow(2, p.lv_reg));
-    p.tb_irr = static_cast<ULL>(std::pow(2, p.lv_reg - ac->time_block));
+  time_step_irr_of(ac, !p.nb.empty(), p.a_tot, p.a_irr, p.new_cur_irr, p.cur_reg, p.tb_reg, p.lv_reg, p.lv_irr,
+                   p.dt_irr, p.tb_irr);
+}
+
+void time_step_irr_of(const abyss_ac *ac, bool has_nb, const double (&a_tot)[3][4], const double (&a_irr)[3][4],
+                      ULL new_cur_irr, ULL cur_reg, ULL tb_reg, int lv_reg, int &lv_irr, double &dt_irr,
+                      ULL &tb_irr) {
+  struct {
+    ULL new_cur_irr, cur_reg, tb_reg, tb_irr;
+    int lv_reg, lv_irr;
+    double dt_irr;
+  } p{new_cur_irr, cur_reg, tb_reg, tb_irr, lv_reg, lv_irr, dt_irr};
+  if (!has_nb) {
+    lv_irr = p.lv_reg;
+    dt_irr = static_cast<double>(std::pow(2, p.lv_reg));
+    tb_irr = static_cast<ULL>(std::pow(2, p.lv_reg - ac->time_block));
     return;
   }
   int lv;
   ULL tb;
   double stp;
-  block_step(ac, new_step_irr(p.a_tot, p.a_irr, ac->p.eta_irr), lv, tb, stp);
+  block_step(ac, new_step_irr(a_tot, a_irr, ac->p.eta_irr), lv, tb, stp);
   if (lv > p.lv_irr) {
     if (std::fmod((double)p.new_cur_irr, 2.0 * (double)p.tb_irr) == 0) {
       lv = p.lv_irr + 1;
@@ -185,10 +203,10 @@ void time_step_irr(const abyss_ac *ac, Star &p) {
     lv--;
     tb = (ULL)(tb * 0.5);
   }
-  p.lv_irr = std::max(ac->time_block, lv);
-  p.dt_irr = static_cast<double>(std::pow(2, p.lv_irr));
-  p.tb_irr = static_cast<ULL>(std::pow(2, p.lv_irr - ac->time_block));
-  if (p.dt_irr > 1) throw std::runtime_error("irregular time step exceeds the run");
+  lv_irr = std::max(ac->time_block, lv);
+  dt_irr = static_cast<double>(std::pow(2, lv_irr));
+  tb_irr = static_cast<ULL>(std::pow(2, lv_irr - ac->time_block));
+  if (dt_irr > 1) throw std::runtime_error("irregular time step exceeds the run");
 }
 
 // UpdateParticle.cpp:314-407 (calculateTimeStepReg).
@@ -531,20 +549,22 @@ int irregular_levels(abyss_ac *ac) {
     for (int k = 0; k < (int)P.size(); ++k) {
       irregular_one(ac, P[k], pend[k]);
       // NewCurrentBlockIrr and the new irregular step use this particle's new
-      // derivatives (WorkerRoutines.cpp:46-64); computed here on a copy.
-      Star tmp = ac->s[P[k]];
-      std::memcpy(tmp.a_tot, pend[k].a_tot, sizeof(tmp.a_tot));
-      std::memcpy(tmp.a_irr, pend[k].a_irr, sizeof(tmp.a_irr));
-      tmp.new_cur_irr = tmp.cur_irr + tmp.tb_irr;
+      // derivatives (WorkerRoutines.cpp:46-64), without touching its state.
+      const Star &sp = ac->s[P[k]];
+      int lv_irr = sp.lv_irr;
+      double dt_irr = sp.dt_irr;
+      ULL tb_irr = sp.tb_irr;
+      const ULL new_cur = sp.cur_irr + sp.tb_irr;
       try {
-        time_step_irr(ac, tmp);
+        time_step_irr_of(ac, !sp.nb.empty(), pend[k].a_tot, pend[k].a_irr, new_cur, sp.cur_reg, sp.tb_reg,
+                         sp.lv_reg, lv_irr, dt_irr, tb_irr);
       } catch (const std::exception &) {
         bad++;
       }
-      pend[k].lv_irr = tmp.lv_irr;
-      pend[k].dt_irr = tmp.dt_irr;
-      pend[k].tb_irr = tmp.tb_irr;
-      pend[k].new_cur_irr = tmp.new_cur_irr;
+      pend[k].lv_irr = lv_irr;
+      pend[k].dt_irr = dt_irr;
+      pend[k].tb_irr = tb_irr;
+      pend[k].new_cur_irr = new_cur;
     }
     if (bad) {
       ac->err = "irregular time step out of range";
@@ -587,16 +607,41 @@ template <class Pred, class Mass>
 void neighbour_change(const int *old_nb, int n_old, const int *new_nb, int n_new, Pred pred,
                       Mass mass, double eps2, const double pos[3], const double vel[3],
                       double a_tmp[3], double adot_tmp[3]) {
-  std::unordered_set<int> old_set(old_nb, old_nb + n_old);
-  std::unordered_set<int> new_set(new_nb, new_nb + n_new);
+  // lost[k]: old_nb[k] is not in the new list; gained[k]: new_nb[k] is not in
+  // the old one.  Lists kept by this library are ascending, and a linear merge
+  // marks them; other lists go through hash sets.
+  thread_local std::vector<char> lost, gained;
+  lost.assign(n_old, 0);
+  gained.assign(n_new, 0);
+  const bool sorted_old = std::is_sorted(old_nb, old_nb + n_old);
+  const bool sorted_new = std::is_sorted(new_nb, new_nb + n_new);
+  if (sorted_old && sorted_new) {
+    int a = 0, b = 0;
+    while (a < n_old || b < n_new) {
+      if (b >= n_new || (a < n_old && old_nb[a] < new_nb[b])) {
+        lost[a++] = 1;
+      } else if (a >= n_old || new_nb[b] < old_nb[a]) {
+        gained[b++] = 1;
+      } else {
+        const int v = old_nb[a];  // in both (repeats advance together)
+        while (a < n_old && old_nb[a] == v) ++a;
+        while (b < n_new && new_nb[b] == v) ++b;
+      }
+    }
+  } else {
+    std::unordered_set<int> old_set(old_nb, old_nb + n_old);
+    std::unordered_set<int> new_set(new_nb, new_nb + n_new);
+    for (int k = 0; k < n_old; ++k) lost[k] = !new_set.count(old_nb[k]);
+    for (int k = 0; k < n_new; ++k) gained[k] = !old_set.count(new_nb[k]);
+  }
   const int size = std::max(n_old, n_new);
   for (int k = 0; k < size; ++k) {
-    if (k < n_old && !new_set.count(old_nb[k])) {
+    if (k < n_old && lost[k]) {
       double pj[3], vj[3];
       pred(old_nb[k], pj, vj);
       pair_force(pos, vel, pj, vj, mass(old_nb[k]), eps2, a_tmp, adot_tmp, -1.0);
     }
-    if (k < n_new && !old_set.count(new_nb[k])) {
+    if (k < n_new && gained[k]) {
       double pj[3], vj[3];
       pred(new_nb[k], pj, vj);
       pair_force(pos, vel, pj, vj, mass(new_nb[k]), eps2, a_tmp, adot_tmp, +1.0);
