@@ -48,10 +48,17 @@
 #include "../../../include/abyss_ens.h"
 #include "../../../include/abyss_io.h"
 #include "../../../include/abyss_reg.h"
+namespace abyss_host {
+// host/pair_terms.cpp
+void irregular_terms(int nn, const double *X, const double *V, const double *A0, const double *A1, const double *T,
+                     const double *M, const double *pos, const double *vel, double new_time, double scale,
+                     double eps2, double *ta, double *tj);
+}  // namespace abyss_host
 
 namespace {
 
 typedef unsigned long long ULL;
+
 
 double now_s() {
   using namespace std::chrono;
@@ -492,24 +499,36 @@ void irregular_one(const abyss_ac *ac, int i, Pending &out) {
   const double dt = p.dt_irr * ac->scale;
   double pos[3], vel[3], a_tmp[3] = {0, 0, 0}, adot_tmp[3] = {0, 0, 0};
   predict(p, p.dt_irr, ac->scale, pos, vel);
-  for (int j : p.nb) {
-    const Star &q = ac->s[j];
-    double pj[3], vj[3];
-    predict(q, new_time - q.t_irr, ac->scale, pj, vj);
-    double x[3], v[3], r2 = 0.0, vx = 0.0;
+  // the neighbours' state gathered, their terms computed independently (SIMD),
+  // then added in neighbour order: the same sums as the one-pass loop
+  const int nn = (int)p.nb.size();
+  thread_local std::vector<double> X, V, A0, A1, T, M, ta, tj;
+  X.resize(3 * (size_t)nn);
+  V.resize(3 * (size_t)nn);
+  A0.resize(3 * (size_t)nn);
+  A1.resize(3 * (size_t)nn);
+  T.resize(nn);
+  M.resize(nn);
+  ta.resize(3 * (size_t)nn);
+  tj.resize(3 * (size_t)nn);
+  for (int k = 0; k < nn; ++k) {
+    const Star &q = ac->s[p.nb[k]];
     for (int d = 0; d < 3; ++d) {
-      x[d] = pj[d] - pos[d];
-      v[d] = vj[d] - vel[d];
-      r2 += x[d] * x[d];
-      vx += v[d] * x[d];
+      X[3 * k + d] = q.x[d];
+      V[3 * k + d] = q.v[d];
+      A0[3 * k + d] = q.a_tot[d][0];
+      A1[3 * k + d] = q.a_tot[d][1];
     }
-    const double r2s = r2 + ac->p.eps2;
-    const double m_r3 = q.m / (r2s * std::sqrt(r2s));
-    for (int d = 0; d < 3; ++d) {
-      a_tmp[d] += m_r3 * x[d];
-      adot_tmp[d] += m_r3 * (v[d] - 3 * x[d] * vx / r2s);
-    }
+    T[k] = q.t_irr;
+    M[k] = q.m;
   }
+  abyss_host::irregular_terms(nn, X.data(), V.data(), A0.data(), A1.data(), T.data(), M.data(), pos, vel, new_time,
+                              ac->scale, ac->p.eps2, ta.data(), tj.data());
+  for (int k = 0; k < nn; ++k)
+    for (int d = 0; d < 3; ++d) {
+      a_tmp[d] += ta[3 * k + d];
+      adot_tmp[d] += tj[3 * k + d];
+    }
   const double dt_ex = (new_time - p.t_reg) * ac->scale;
   const double dt2 = dt * dt, dt3 = dt2 * dt, dt4 = dt3 * dt, dt5 = dt4 * dt;
   for (int d = 0; d < 3; ++d) {
@@ -540,56 +559,77 @@ int irregular_levels(abyss_ac *ac) {
   std::vector<Pending> pend;
   while (!levels.empty()) {
     auto it = levels.begin();
+    // The level's particles are computed from the pre-level state and committed
+    // one by one, so their order changes nothing.
     std::vector<int> P = std::move(it->second);
     levels.erase(it);
-    std::sort(P.begin(), P.end());
     pend.resize(P.size());
     int bad = 0;
-#pragma omp parallel for schedule(dynamic, 8) reduction(+ : bad)
-    for (int k = 0; k < (int)P.size(); ++k) {
-      irregular_one(ac, P[k], pend[k]);
-      // NewCurrentBlockIrr and the new irregular step use this particle's new
-      // derivatives (WorkerRoutines.cpp:46-64), without touching its state.
-      const Star &sp = ac->s[P[k]];
-      int lv_irr = sp.lv_irr;
-      double dt_irr = sp.dt_irr;
-      ULL tb_irr = sp.tb_irr;
-      const ULL new_cur = sp.cur_irr + sp.tb_irr;
-      try {
-        time_step_irr_of(ac, !sp.nb.empty(), pend[k].a_tot, pend[k].a_irr, new_cur, sp.cur_reg, sp.tb_reg,
-                         sp.lv_reg, lv_irr, dt_irr, tb_irr);
-      } catch (const std::exception &) {
-        bad++;
+    const bool par = P.size() >= 32;  // small levels: a thread team costs more than it saves
+    // one thread team per level: every particle's step from the pre-level state,
+    // then (after the loop's barrier) every commit
+#pragma omp parallel if (par)
+    {
+#pragma omp for schedule(dynamic, 8) reduction(+ : bad)
+      for (int k = 0; k < (int)P.size(); ++k) {
+        irregular_one(ac, P[k], pend[k]);
+        // NewCurrentBlockIrr and the new irregular step use this particle's new
+        // derivatives (WorkerRoutines.cpp:46-64), without touching its state.
+        const Star &sp = ac->s[P[k]];
+        int lv_irr = sp.lv_irr;
+        double dt_irr = sp.dt_irr;
+        ULL tb_irr = sp.tb_irr;
+        const ULL new_cur = sp.cur_irr + sp.tb_irr;
+        try {
+          time_step_irr_of(ac, !sp.nb.empty(), pend[k].a_tot, pend[k].a_irr, new_cur, sp.cur_reg, sp.tb_reg,
+                           sp.lv_reg, lv_irr, dt_irr, tb_irr);
+        } catch (const std::exception &) {
+          bad++;
+        }
+        pend[k].lv_irr = lv_irr;
+        pend[k].dt_irr = dt_irr;
+        pend[k].tb_irr = tb_irr;
+        pend[k].new_cur_irr = new_cur;
       }
-      pend[k].lv_irr = lv_irr;
-      pend[k].dt_irr = dt_irr;
-      pend[k].tb_irr = tb_irr;
-      pend[k].new_cur_irr = new_cur;
+      // phase two: commit (IrrForce results + IrrUpdate, WorkerRoutines.cpp:76-87);
+      // on a failed step nothing is committed
+#pragma omp for schedule(static)
+      for (int k = 0; k < (int)P.size(); ++k) {
+        if (bad) continue;
+        Star &p = ac->s[P[k]];
+        const Pending &q = pend[k];
+        p.lv_irr = q.lv_irr;
+        p.dt_irr = q.dt_irr;
+        p.tb_irr = q.tb_irr;
+        p.new_cur_irr = q.new_cur_irr;
+        std::memcpy(p.a_tot, q.a_tot, sizeof(p.a_tot));
+        std::memcpy(p.a_irr, q.a_irr, sizeof(p.a_irr));
+        p.next_irr = p.new_cur_irr + p.tb_irr;
+        if (!p.nb.empty() && q.move) {
+          for (int d = 0; d < 3; ++d) {
+            p.x[d] = q.new_x[d];
+            p.v[d] = q.new_v[d];
+          }
+        }
+        p.cur_irr = p.new_cur_irr;
+        p.t_irr = p.cur_irr * ac->time_step;
+      }
     }
     if (bad) {
       ac->err = "irregular time step out of range";
       return ABYSS_ERR_STATE;
     }
-    // phase two: commit (IrrForce results + IrrUpdate, WorkerRoutines.cpp:76-87)
-    for (size_t k = 0; k < P.size(); ++k) {
-      Star &p = ac->s[P[k]];
-      const Pending &q = pend[k];
-      p.lv_irr = q.lv_irr;
-      p.dt_irr = q.dt_irr;
-      p.tb_irr = q.tb_irr;
-      p.new_cur_irr = q.new_cur_irr;
-      std::memcpy(p.a_tot, q.a_tot, sizeof(p.a_tot));
-      std::memcpy(p.a_irr, q.a_irr, sizeof(p.a_irr));
-      p.next_irr = p.new_cur_irr + p.tb_irr;
-      if (!p.nb.empty() && q.move) {
-        for (int d = 0; d < 3; ++d) {
-          p.x[d] = q.new_x[d];
-          p.v[d] = q.new_v[d];
-        }
+    // file each particle under its next irregular level (most share one)
+    ULL last_key = 0;
+    std::vector<int> *last = nullptr;
+    for (int i : P) {
+      const ULL key = ac->s[i].next_irr;
+      if (key > ac->next_reg_block) continue;
+      if (!last || key != last_key) {
+        last = &levels[key];
+        last_key = key;
       }
-      p.cur_irr = p.new_cur_irr;
-      p.t_irr = p.cur_irr * ac->time_step;
-      if (p.next_irr <= ac->next_reg_block) levels[p.next_irr].push_back(P[k]);
+      last->push_back(i);
     }
     ac->st.irr_levels++;
     ac->st.irr_steps += (long long)P.size();
