@@ -157,6 +157,15 @@ def captured_traffic(n, m, plan):
     return None
 
 
+def launches_per_step(plan) -> int:
+    """Kernels one device step launches (all compiled into libabyss_reg.so):
+    predict_jset; for anchor offsets the Morton ordering (target_bbox,
+    target_morton, CUB radix sort: histogram, exclusive sum, 4 onesweep passes,
+    gather_order); the force kernel; finalize_rows and relist_rows."""
+    order = 9 if plan.get("mode") == 1 and plan.get("kernel") in (1, 3) else 0
+    return 1 + order + 1 + 2
+
+
 def measured_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -423,7 +432,7 @@ def run_ours(args, world, rank, local, pg):
         "roofline": roofline,
         "e2e": {"value": e2e_value, "unit": "Gpairs/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
-        "gpu_launches": 6 * args.steps,
+        "gpu_launches": launches_per_step(plan) * args.steps,
         "clocks": clocks,
         "sweep": sweep,
     }

@@ -181,6 +181,9 @@ def test_no_neighbours_and_all_neighbours(rf):
         assert np.all(res.nnb == c.n - 1)
         assert np.array_equal(res.list, ref["list"])
         assert np.abs(res.acc_reg).max() == 0.0 and np.abs(res.jerk_reg).max() == 0.0
+        # the irregular part of an overflowed row sums all its neighbours, not the first list_cap
+        assert row_rel_err(res.acc_irr, ref["acc_irr"]).max() <= IRR_TOL, tu
+        assert row_rel_err(res.jerk_irr, ref["jerk_irr"]).max() <= IRR_TOL, tu
 
 
 @pytest.mark.parametrize("n", [2, 3, 5, 127, 129, 255, 257])
