@@ -81,6 +81,7 @@ def lib():
     L.abyss_stream.argtypes = [_vp]
     L.abyss_stream.restype = _vp
     L.abyss_synchronize.argtypes = [_vp]
+    L.abyss_set_wait.argtypes = [_vp, C.c_int]
     L.abyss_reserve.argtypes = [_vp, C.c_int, C.c_int, C.c_int]
     L.abyss_upload_state.argtypes = [_vp, C.c_int] + [_dp] * 7
     L.abyss_predict.argtypes = [_vp, C.c_double, C.c_double]

@@ -9,9 +9,11 @@
 //   [target ordering] -> force kernel (tile or j-major) -> finalize
 // all enqueued on the context stream.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <initializer_list>
 #include <string>
 #include <vector>
 
@@ -29,14 +31,14 @@ struct DevBuf {
   size_t cap = 0;  // elements
   cudaError_t ensure(size_t n) {
     if (n <= cap && p) return cudaSuccess;
-    if (p) cudaFree(p);
-    p = nullptr;
-    cap = 0;
     // a buffer that has to grow grows by at least half again, so a context
     // that sees slowly rising sizes reallocates (and synchronizes the device
     // in cudaFree) only a few times
     size_t want = std::max<size_t>(std::max<size_t>(n, 1), cap + cap / 2);
     want = (want + kPad - 1) / kPad * kPad;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
     cudaError_t e = cudaMalloc((void **)&p, want * sizeof(T));
     if (e != cudaSuccess) {
       p = nullptr;
@@ -51,6 +53,38 @@ struct DevBuf {
     cap = 0;
   }
 };
+
+// Pinned host memory for the copies of one call between pageable caller
+// memory and the device.  The driver copies pageable memory through its own
+// staging, which serialises such copies across host threads and waits for the
+// device; copies through a context's own pinned buffer are plain DMA.
+struct HostStage {
+  unsigned char *p = nullptr;
+  size_t cap = 0;  // bytes
+  cudaError_t ensure(size_t bytes) {
+    if (bytes <= cap && p) return cudaSuccess;
+    const size_t want = std::max(bytes, cap + cap / 2);
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+    cudaError_t e = cudaHostAlloc((void **)&p, want, cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      return e;
+    }
+    cap = want;
+    return cudaSuccess;
+  }
+  void release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+  }
+};
+
+// Pageable copies larger than this go the driver's way, which overlaps its
+// host-side staging with the DMA.
+constexpr size_t kStageMax = (size_t)16 << 20;
 
 struct Table {
   std::vector<int> m_max;
@@ -89,6 +123,13 @@ struct abyss_ctx {
   // profiling
   bool profiling = false;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  // host waits: < 0 stream synchronisation, else spin this long, then block
+  int wait_spin_us = -1;
+  cudaEvent_t ev_wait = nullptr;  // cudaEventBlockingSync
+  // pinned staging of pageable caller memory: inputs, and results; ev_hin
+  // marks the end of the last copies out of `hin`
+  HostStage hin, hout;
+  cudaEvent_t ev_hin = nullptr;
   // scratch for energies
   DevBuf<double> e_x, e_v, e_m, e_row;
   DevBuf<double> i_a0, i_a1, i_r2, i_out;  // initialisation derivatives
@@ -103,6 +144,133 @@ static int cuda_fail(abyss_ctx *c, cudaError_t e, const char *what) {
   return fail(c, e == cudaErrorMemoryAllocation ? ABYSS_ERR_OOM : ABYSS_ERR_CUDA,
               std::string(what) + ": " + cudaGetErrorString(e));
 }
+
+// Wait on the host for everything queued on the context stream.  By default
+// this is the stream synchronisation, whose waiting thread keeps its core (it
+// spins while the process has no more threads than cores).  With a wait policy
+// (abyss_set_wait) the thread polls for at most wait_spin_us and then sleeps in
+// a blocking event wait, leaving its core to other host threads while the GPU
+// is busy with other work.
+static cudaError_t ctx_wait(abyss_ctx *c) {
+  if (c->wait_spin_us < 0 || !c->ev_wait) return cudaStreamSynchronize(c->stream);
+  cudaError_t e = cudaEventRecord(c->ev_wait, c->stream);
+  if (e != cudaSuccess) return e;
+  const auto t0 = std::chrono::steady_clock::now();
+  const auto spin = std::chrono::microseconds(c->wait_spin_us);
+  for (;;) {
+    e = cudaEventQuery(c->ev_wait);
+    if (e != cudaErrorNotReady) return e;
+    if (std::chrono::steady_clock::now() - t0 >= spin) break;
+  }
+  return cudaEventSynchronize(c->ev_wait);
+}
+
+// Wait for `ev` (created with cudaEventBlockingSync) by the context's policy.
+static cudaError_t wait_event(abyss_ctx *c, cudaEvent_t ev) {
+  const auto t0 = std::chrono::steady_clock::now();
+  const auto spin = std::chrono::microseconds(std::max(c->wait_spin_us, 0));
+  for (;;) {
+    const cudaError_t e = cudaEventQuery(ev);
+    if (e != cudaErrorNotReady) return e;
+    if (c->wait_spin_us >= 0 && std::chrono::steady_clock::now() - t0 >= spin) break;
+  }
+  return cudaEventSynchronize(ev);
+}
+
+static bool host_pinned(const void *p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+static size_t round16(size_t b) { return (b + 15) & ~(size_t)15; }
+
+// One host<->device copy of a call.
+struct Xfer {
+  void *dst;
+  const void *src;
+  size_t bytes;
+};
+
+// Queue the host-to-device copies of one call.  Pinned sources are copied
+// directly; pageable ones (up to kStageMax in all) through `hin`, after the
+// copies that last read it have finished.
+static cudaError_t h2d(abyss_ctx *c, std::initializer_list<Xfer> xs) {
+  if (xs.size() > 16) return cudaErrorInvalidValue;
+  bool stage[16];
+  size_t need = 0, k = 0;
+  for (const Xfer &x : xs) {
+    stage[k] = x.bytes > 0 && !host_pinned(x.src);
+    if (stage[k]) need += round16(x.bytes);
+    ++k;
+  }
+  const bool staged = need > 0 && need <= kStageMax;
+  if (staged) {
+    cudaError_t e = wait_event(c, c->ev_hin);
+    if (e == cudaSuccess) e = c->hin.ensure(need);
+    if (e != cudaSuccess) return e;
+  }
+  size_t off = 0;
+  k = 0;
+  for (const Xfer &x : xs) {
+    const void *src = x.src;
+    if (staged && stage[k]) {
+      std::memcpy(c->hin.p + off, x.src, x.bytes);
+      src = c->hin.p + off;
+      off += round16(x.bytes);
+    }
+    ++k;
+    if (x.bytes == 0) continue;
+    const cudaError_t e = cudaMemcpyAsync(x.dst, src, x.bytes, cudaMemcpyHostToDevice, c->stream);
+    if (e != cudaSuccess) return e;
+  }
+  return staged ? cudaEventRecord(c->ev_hin, c->stream) : cudaSuccess;
+}
+
+// The device-to-host copies of one call: queue() them (pageable destinations,
+// up to kStageMax in all, into `hout`), wait for the stream, then finish()
+// copies the staged bytes to their destinations.
+struct D2H {
+  std::vector<Xfer> out;  // staged: dst = caller memory, src = hout
+  cudaError_t queue(abyss_ctx *c, std::initializer_list<Xfer> xs) {
+    if (xs.size() > 16) return cudaErrorInvalidValue;
+    size_t need = 0;
+    bool stage[16];
+    size_t k = 0;
+    for (const Xfer &x : xs) {
+      stage[k] = x.bytes > 0 && !host_pinned(x.dst);
+      if (stage[k]) need += round16(x.bytes);
+      ++k;
+    }
+    const bool staged = need > 0 && need <= kStageMax;
+    if (staged) {
+      // the previous call's results were read out before it returned
+      cudaError_t e = c->hout.ensure(need);
+      if (e != cudaSuccess) return e;
+    }
+    size_t off = 0;
+    k = 0;
+    for (const Xfer &x : xs) {
+      void *dst = x.dst;
+      if (staged && stage[k]) {
+        dst = c->hout.p + off;
+        out.push_back(Xfer{x.dst, dst, x.bytes});
+        off += round16(x.bytes);
+      }
+      ++k;
+      if (x.bytes == 0) continue;
+      const cudaError_t e = cudaMemcpyAsync(dst, x.src, x.bytes, cudaMemcpyDeviceToHost, c->stream);
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  }
+  void finish() {
+    for (const Xfer &x : out) std::memcpy(x.dst, x.src, x.bytes);
+  }
+};
 
 #define CK(expr, what)                                  \
   do {                                                  \
@@ -183,6 +351,8 @@ int abyss_create(int device, abyss_ctx **out) {
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
   for (int i = 0; i < 4 && e == cudaSuccess; ++i) e = cudaEventCreate(&c->ev[i]);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_hin, cudaEventBlockingSync | cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventRecord(c->ev_hin, c->stream);
   if (e != cudaSuccess) {
     delete c;
     return ABYSS_ERR_CUDA;
@@ -210,6 +380,10 @@ int abyss_destroy(abyss_ctx *c) {
   c->cub_tmp.release();
   for (auto &e : c->ev)
     if (e) cudaEventDestroy(e);
+  if (c->ev_wait) cudaEventDestroy(c->ev_wait);
+  if (c->ev_hin) cudaEventDestroy(c->ev_hin);
+  c->hin.release();
+  c->hout.release();
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return ABYSS_OK;
@@ -222,7 +396,16 @@ void *abyss_stream(abyss_ctx *c) { return c ? (void *)c->stream : nullptr; }
 int abyss_synchronize(abyss_ctx *c) {
   if (!c) return ABYSS_ERR_ARG;
   cudaSetDevice(c->device);
-  CK(cudaStreamSynchronize(c->stream), "synchronize");
+  CK(ctx_wait(c), "synchronize");
+  return ABYSS_OK;
+}
+
+int abyss_set_wait(abyss_ctx *c, int spin_us) {
+  if (!c) return ABYSS_ERR_ARG;
+  cudaSetDevice(c->device);
+  if (spin_us >= 0 && !c->ev_wait)
+    CK(cudaEventCreateWithFlags(&c->ev_wait, cudaEventBlockingSync | cudaEventDisableTiming), "wait event");
+  c->wait_spin_us = spin_us < 0 ? -1 : spin_us;
   return ABYSS_OK;
 }
 
@@ -251,6 +434,15 @@ int abyss_reserve(abyss_ctx *c, int n, int m, int list_cap) {
   CK(c->part.ensure((size_t)s_max * m1 * 6), "alloc part");
   CK(c->items.ensure(1), "alloc items");
   CK(c->ovf_list.ensure((size_t)m1), "alloc overflow list");
+  // pinned staging for pageable callers: the state upload (15 doubles per
+  // particle) and the targets; the results (12 doubles and 1 + list_cap ints
+  // per target) or the initialisation derivatives (12 doubles per particle)
+  const size_t n1 = std::max(n, 1);
+  const size_t in_b = 15 * 8 * n1 + 4 * (size_t)m1 + 16 * 16;
+  const size_t out_b = std::max(96 * n1, (96 + 4 + 4 * (size_t)cap1) * m1) + 16 * 16;
+  CK(wait_event(c, c->ev_hin), "staging");
+  CK(c->hin.ensure(std::min(in_b, kStageMax)), "pinned staging");
+  CK(c->hout.ensure(std::min(out_b, kStageMax)), "pinned staging");
   return ABYSS_OK;
 }
 
@@ -268,13 +460,9 @@ int abyss_upload_state(abyss_ctx *c, int n, const double *x, const double *v, co
   CK(c->a0.ensure(v3), "alloc a0");
   CK(c->a1.ensure(v3), "alloc a1");
   CK(c->t0.ensure(n), "alloc t0");
-  CK(cudaMemcpyAsync(c->x.p, x, v3 * 8, cudaMemcpyHostToDevice, c->stream), "H2D x");
-  CK(cudaMemcpyAsync(c->v.p, v, v3 * 8, cudaMemcpyHostToDevice, c->stream), "H2D v");
-  CK(cudaMemcpyAsync(c->a0.p, a0, v3 * 8, cudaMemcpyHostToDevice, c->stream), "H2D a0");
-  CK(cudaMemcpyAsync(c->a1.p, a1, v3 * 8, cudaMemcpyHostToDevice, c->stream), "H2D a1");
-  CK(cudaMemcpyAsync(c->t0.p, t0, (size_t)n * 8, cudaMemcpyHostToDevice, c->stream), "H2D t0");
-  CK(cudaMemcpyAsync(c->mass.p, mass, (size_t)n * 8, cudaMemcpyHostToDevice, c->stream), "H2D mass");
-  CK(cudaMemcpyAsync(c->r2nb.p, r2nb, (size_t)n * 8, cudaMemcpyHostToDevice, c->stream), "H2D r2nb");
+  CK(h2d(c, {{c->x.p, x, v3 * 8}, {c->v.p, v, v3 * 8}, {c->a0.p, a0, v3 * 8}, {c->a1.p, a1, v3 * 8},
+             {c->t0.p, t0, (size_t)n * 8}, {c->mass.p, mass, (size_t)n * 8}, {c->r2nb.p, r2nb, (size_t)n * 8}}),
+     "H2D state");
   c->n = n;
   c->have_state = true;
   c->have_jset = false;
@@ -304,10 +492,9 @@ int abyss_upload_predicted(abyss_ctx *c, int n, const double *px, const double *
   const size_t v3 = (size_t)3 * n;
   CK(c->x.ensure(v3), "alloc x");
   CK(c->v.ensure(v3), "alloc v");
-  CK(cudaMemcpyAsync(c->x.p, px, v3 * 8, cudaMemcpyHostToDevice, c->stream), "H2D px");
-  CK(cudaMemcpyAsync(c->v.p, pv, v3 * 8, cudaMemcpyHostToDevice, c->stream), "H2D pv");
-  CK(cudaMemcpyAsync(c->mass.p, mass, (size_t)n * 8, cudaMemcpyHostToDevice, c->stream), "H2D mass");
-  CK(cudaMemcpyAsync(c->r2nb.p, r2nb, (size_t)n * 8, cudaMemcpyHostToDevice, c->stream), "H2D r2nb");
+  CK(h2d(c, {{c->x.p, px, v3 * 8}, {c->v.p, pv, v3 * 8}, {c->mass.p, mass, (size_t)n * 8},
+             {c->r2nb.p, r2nb, (size_t)n * 8}}),
+     "H2D predicted");
   launch_unpack_predicted(c->stream, n, c->x.p, c->v.p, c->mass.p, c->px.p, c->py.p, c->pz.p,
                           c->pvx.p, c->pvy.p, c->pvz.p, c->vm.p, c->sm_count);
   CK(cudaGetLastError(), "unpack launch");
@@ -326,10 +513,13 @@ int abyss_read_predicted(abyss_ctx *c, double *px, double *pv, float *vm4) {
   double *dst[6] = {tmp.data(), tmp.data() + n, tmp.data() + 2 * n,
                     tmp.data() + 3 * n, tmp.data() + 4 * n, tmp.data() + 5 * n};
   const double *src[6] = {c->px.p, c->py.p, c->pz.p, c->pvx.p, c->pvy.p, c->pvz.p};
-  for (int k = 0; k < 6; ++k)
-    CK(cudaMemcpyAsync(dst[k], src[k], n * 8, cudaMemcpyDeviceToHost, c->stream), "D2H predicted");
-  if (vm4) CK(cudaMemcpyAsync(vm4, c->vm.p, n * 16, cudaMemcpyDeviceToHost, c->stream), "D2H vm");
-  CK(cudaStreamSynchronize(c->stream), "synchronize");
+  D2H out;
+  CK(out.queue(c, {{dst[0], src[0], n * 8}, {dst[1], src[1], n * 8}, {dst[2], src[2], n * 8},
+                   {dst[3], src[3], n * 8}, {dst[4], src[4], n * 8}, {dst[5], src[5], n * 8},
+                   {vm4, c->vm.p, vm4 ? n * 16 : 0}}),
+     "D2H predicted");
+  CK(ctx_wait(c), "synchronize");
+  out.finish();
   for (size_t j = 0; j < n; ++j)
     for (int d = 0; d < 3; ++d) {
       if (px) px[3 * j + d] = dst[d][j];
@@ -349,8 +539,7 @@ int abyss_set_targets(abyss_ctx *c, int m, const int *targets) {
   cudaSetDevice(c->device);
   int rc = ensure_targets(c, m);
   if (rc != ABYSS_OK) return rc;
-  CK(cudaMemcpyAsync(c->targets.p, targets, (size_t)m * 4, cudaMemcpyHostToDevice, c->stream),
-     "H2D targets");
+  CK(h2d(c, {{c->targets.p, targets, (size_t)m * 4}}), "H2D targets");
   c->m = m;
   return ABYSS_OK;
 }
@@ -542,18 +731,18 @@ int abyss_fetch(abyss_ctx *c, double *acc_reg, double *jerk_reg, double *acc_irr
   cudaSetDevice(c->device);
   const size_t m = c->launched_m;
   int st = 0, ovf = 0;
-  CK(cudaMemcpyAsync(&st, c->status.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "D2H status");
-  CK(cudaMemcpyAsync(&ovf, c->ovf.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "D2H ovf");
-  if (acc_reg) CK(cudaMemcpyAsync(acc_reg, c->acc_reg.p, m * 24, cudaMemcpyDeviceToHost, c->stream), "D2H");
-  if (jerk_reg) CK(cudaMemcpyAsync(jerk_reg, c->jerk_reg.p, m * 24, cudaMemcpyDeviceToHost, c->stream), "D2H");
-  if (acc_irr) CK(cudaMemcpyAsync(acc_irr, c->acc_irr.p, m * 24, cudaMemcpyDeviceToHost, c->stream), "D2H");
-  if (jerk_irr) CK(cudaMemcpyAsync(jerk_irr, c->jerk_irr.p, m * 24, cudaMemcpyDeviceToHost, c->stream), "D2H");
-  if (nnb) CK(cudaMemcpyAsync(nnb, c->nnb.p, m * 4, cudaMemcpyDeviceToHost, c->stream), "D2H");
-  if (list)
-    CK(cudaMemcpyAsync(list, c->list.p, m * (size_t)c->launched_cap * 4, cudaMemcpyDeviceToHost,
-                       c->stream),
-       "D2H list");
-  CK(cudaStreamSynchronize(c->stream), "synchronize");
+  D2H out;
+  CK(out.queue(c, {{&st, c->status.p, sizeof(int)},
+                   {&ovf, c->ovf.p, sizeof(int)},
+                   {acc_reg, c->acc_reg.p, acc_reg ? m * 24 : 0},
+                   {jerk_reg, c->jerk_reg.p, jerk_reg ? m * 24 : 0},
+                   {acc_irr, c->acc_irr.p, acc_irr ? m * 24 : 0},
+                   {jerk_irr, c->jerk_irr.p, jerk_irr ? m * 24 : 0},
+                   {nnb, c->nnb.p, nnb ? m * 4 : 0},
+                   {list, c->list.p, list ? m * (size_t)c->launched_cap * 4 : 0}}),
+     "D2H results");
+  CK(ctx_wait(c), "synchronize");
+  out.finish();
   if (overflow_rows) *overflow_rows = ovf;
   if (st & kErrTimeout) return fail(c, ABYSS_ERR_TIMEOUT, "device wait timed out");
   if (ovf > 0) {
@@ -598,7 +787,7 @@ int abyss_last_timing(abyss_ctx *c, float *ms3) {
   if (!c || !ms3) return ABYSS_ERR_ARG;
   if (!c->profiling) return fail(c, ABYSS_ERR_STATE, "last_timing: profiling is off");
   cudaSetDevice(c->device);
-  CK(cudaStreamSynchronize(c->stream), "synchronize");
+  CK(ctx_wait(c), "synchronize");
   for (int i = 0; i < 3; ++i) CK(cudaEventElapsedTime(&ms3[i], c->ev[i], c->ev[i + 1]), "event time");
   return ABYSS_OK;
 }
@@ -618,14 +807,15 @@ int abyss_energy(abyss_ctx *c, int n, const double *x, const double *v, const do
   CK(c->e_v.ensure((size_t)3 * n), "alloc");
   CK(c->e_m.ensure(n), "alloc");
   CK(c->e_row.ensure(n), "alloc");
-  CK(cudaMemcpyAsync(c->e_x.p, x, (size_t)24 * n, cudaMemcpyHostToDevice, c->stream), "H2D");
-  CK(cudaMemcpyAsync(c->e_v.p, v, (size_t)24 * n, cudaMemcpyHostToDevice, c->stream), "H2D");
-  CK(cudaMemcpyAsync(c->e_m.p, mass, (size_t)8 * n, cudaMemcpyHostToDevice, c->stream), "H2D");
+  CK(h2d(c, {{c->e_x.p, x, (size_t)24 * n}, {c->e_v.p, v, (size_t)24 * n}, {c->e_m.p, mass, (size_t)8 * n}}),
+     "H2D");
   launch_energy(c->stream, n, c->e_x.p, c->e_v.p, c->e_m.p, eps2, c->e_row.p);
   CK(cudaGetLastError(), "energy launch");
   std::vector<double> rows(n);
-  CK(cudaMemcpyAsync(rows.data(), c->e_row.p, (size_t)8 * n, cudaMemcpyDeviceToHost, c->stream), "D2H");
-  CK(cudaStreamSynchronize(c->stream), "synchronize");
+  D2H out;
+  CK(out.queue(c, {{rows.data(), c->e_row.p, (size_t)8 * n}}), "D2H");
+  CK(ctx_wait(c), "synchronize");
+  out.finish();
   double e = 0.0;
   for (int i = 0; i < n; ++i) e += rows[i];
   *energy = e;
@@ -647,18 +837,17 @@ int abyss_init_derivs23(abyss_ctx *c, int n, const double *x, const double *v, c
   CK(c->i_a1.ensure(n3), "alloc");
   CK(c->i_r2.ensure(n), "alloc");
   CK(c->i_out.ensure((size_t)12 * n), "alloc");
-  CK(cudaMemcpyAsync(c->e_x.p, x, 8 * n3, cudaMemcpyHostToDevice, c->stream), "H2D");
-  CK(cudaMemcpyAsync(c->e_v.p, v, 8 * n3, cudaMemcpyHostToDevice, c->stream), "H2D");
-  CK(cudaMemcpyAsync(c->e_m.p, mass, (size_t)8 * n, cudaMemcpyHostToDevice, c->stream), "H2D");
-  CK(cudaMemcpyAsync(c->i_a0.p, a0, 8 * n3, cudaMemcpyHostToDevice, c->stream), "H2D");
-  CK(cudaMemcpyAsync(c->i_a1.p, a1, 8 * n3, cudaMemcpyHostToDevice, c->stream), "H2D");
-  CK(cudaMemcpyAsync(c->i_r2.p, r2nb, (size_t)8 * n, cudaMemcpyHostToDevice, c->stream), "H2D");
+  CK(h2d(c, {{c->e_x.p, x, 8 * n3}, {c->e_v.p, v, 8 * n3}, {c->e_m.p, mass, (size_t)8 * n},
+             {c->i_a0.p, a0, 8 * n3}, {c->i_a1.p, a1, 8 * n3}, {c->i_r2.p, r2nb, (size_t)8 * n}}),
+     "H2D");
   launch_init_derivs23(c->stream, n, c->e_x.p, c->e_v.p, c->i_a0.p, c->i_a1.p, c->e_m.p, c->i_r2.p, eps2,
                        c->i_out.p);
   CK(cudaGetLastError(), "init_derivs23 launch");
   std::vector<double> out((size_t)12 * n);
-  CK(cudaMemcpyAsync(out.data(), c->i_out.p, (size_t)96 * n, cudaMemcpyDeviceToHost, c->stream), "D2H");
-  CK(cudaStreamSynchronize(c->stream), "synchronize");
+  D2H res;
+  CK(res.queue(c, {{out.data(), c->i_out.p, (size_t)96 * n}}), "D2H");
+  CK(ctx_wait(c), "synchronize");
+  res.finish();
   for (int i = 0; i < n; ++i)
     for (int d = 0; d < 3; ++d) {
       const double *o = &out[(size_t)12 * i];

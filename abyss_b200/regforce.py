@@ -88,6 +88,12 @@ class RegularForce:
     def synchronize(self):
         self._check(self._L.abyss_synchronize(self._h))
 
+    def set_wait(self, spin_us: int):
+        """How this context's calls wait for the GPU: spin_us < 0 keeps the
+        stream synchronisation (the default); spin_us >= 0 polls that long,
+        then sleeps in a blocking wait (include/abyss_reg.h abyss_set_wait)."""
+        self._check(self._L.abyss_set_wait(self._h, int(spin_us)))
+
     def reserve(self, n: int, m: int, list_cap: int):
         self._check(self._L.abyss_reserve(self._h, n, m, list_cap))
 

@@ -122,6 +122,9 @@ class Server:
         # context that grew while waves run would stall the device in cudaFree
         for rf, _ in self.ctxs:
             rf.reserve(max_n, max_n, list_cap)
+            # a set-up waits behind the waves on the GPU: it sleeps meanwhile,
+            # leaving its core to the workers instead of spinning on it
+            rf.set_wait(50)
         for c in self.ctxs:
             self.ctx_free.put(c)
         self.waiting: list[Request] = []

@@ -70,6 +70,14 @@ const char *abyss_last_error(const abyss_ctx *ctx);
 /* Opaque cudaStream_t of the context (all work of the context runs on it). */
 void *abyss_stream(abyss_ctx *ctx);
 int abyss_synchronize(abyss_ctx *ctx);
+/* How the context's calls wait for the GPU.  spin_us < 0 (the default): the
+ * stream synchronisation, whose thread keeps its core while it waits.
+ * spin_us >= 0: poll for at most spin_us microseconds, then sleep in a blocking
+ * event wait, so that a thread whose call waits behind other work on a busy GPU
+ * leaves its core to other host threads (many contexts driven from more host
+ * threads than cores).  Results do not depend on it.  No reference counterpart:
+ * the reference waits in cudaStreamSynchronize (cuda_my_acceleration.cu:242). */
+int abyss_set_wait(abyss_ctx *ctx, int spin_us);
 
 /* Pre-size buffers for n particles, m targets, list capacity list_cap
  * (replaces the grow-on-demand reallocation at cuda_my_acceleration.cu:635-727). */

@@ -234,3 +234,24 @@ def test_anchor_mode_on_dense_active_set(rf, kernel, threads, ipt):
                     res.jerk_irr[sample], res.nnb[sample], res.list[sample], plan=res.plan)
     check(sub, ref, f"king65536-anchor-k{kernel}-{threads}x{ipt}", scale)
     assert np.all(res.nnb == 80)
+
+
+def test_blocking_wait_policy_gives_the_same_results():
+    """abyss_set_wait changes how the host waits, not what is computed: with a
+    spin of 0 or 50 us before the blocking wait, every output is identical to
+    the default wait's; a negative spin restores the default."""
+    c = ic.king(4000, 9, 6.0, k_nb=40)
+    t = np.arange(0, c.n, 2, dtype=np.int32)
+    r = RegularForce(0)
+    try:
+        r.send_to_device(c.m, c.x, c.v, c.r2nb)
+        want = r.calculate_acceleration(t, eps2=1e-8, list_cap=256)
+        for spin in (0, 50, -1):
+            r.set_wait(spin)
+            r.send_to_device(c.m, c.x, c.v, c.r2nb)
+            got = r.calculate_acceleration(t, eps2=1e-8, list_cap=256)
+            for k in ("acc_reg", "jerk_reg", "acc_irr", "jerk_irr", "nnb", "list"):
+                assert np.array_equal(getattr(got, k), getattr(want, k)), (spin, k)
+            assert r.energy(c.x, c.v, c.m, 1e-8) == r.energy(c.x, c.v, c.m, 1e-8)
+    finally:
+        r.close()
