@@ -65,12 +65,14 @@ double now_s() {
   return duration<double>(steady_clock::now().time_since_epoch()).count();
 }
 
-struct Star {
-  double x[3], v[3], m;
+struct alignas(64) Star {
+  // what a neighbour's irregular step reads: x, v, m, t_irr on one cache line,
+  // a_tot[.][0..1] on the next two
+  double x[3], v[3], m, t_irr = 0;
   double a_tot[3][4], a_reg[3][4], a_irr[3][4];
   std::vector<int> nb;
   double r2nb;
-  double t_reg = 0, t_irr = 0, dt_reg = 0, dt_irr = 0;
+  double t_reg = 0, dt_reg = 0, dt_irr = 0;
   ULL cur_reg = 0, cur_irr = 0, new_cur_irr = 0, next_irr = 0, tb_reg = 0, tb_irr = 0;
   int lv_reg = 0, lv_irr = 0;
 };
@@ -511,7 +513,20 @@ void irregular_one(const abyss_ac *ac, int i, Pending &out) {
   M.resize(nn);
   ta.resize(3 * (size_t)nn);
   tj.resize(3 * (size_t)nn);
+  constexpr int kAhead = 6;  // neighbours fetched ahead of the gather
+  for (int k = 0; k < std::min(nn, kAhead); ++k) {
+    const char *q = reinterpret_cast<const char *>(&ac->s[p.nb[k]]);
+    __builtin_prefetch(q);
+    __builtin_prefetch(q + 64);
+    __builtin_prefetch(q + 128);
+  }
   for (int k = 0; k < nn; ++k) {
+    if (k + kAhead < nn) {
+      const char *q = reinterpret_cast<const char *>(&ac->s[p.nb[k + kAhead]]);
+      __builtin_prefetch(q);
+      __builtin_prefetch(q + 64);
+      __builtin_prefetch(q + 128);
+    }
     const Star &q = ac->s[p.nb[k]];
     for (int d = 0; d < 3; ++d) {
       X[3 * k + d] = q.x[d];

@@ -478,12 +478,16 @@ def extras(device: int) -> dict:
     kw = dict(rate=2000.0, duration=0.25, nmin=256, nmax=2048, t_end=0.0625)
     res = {}
     for serial in (False, True):
+        # a short stream first, untimed, for one-time costs (host threads and
+        # memory, first launches of each kernel) in either arm
+        serve.serve(**dict(kw, duration=0.05, seed=6), serial=serial)
         r, _ = serve.serve(**kw, serial=serial)
         res["serial" if serial else "continuous"] = r
     c, sp = res["continuous"], res["serial"]
     out["serving"] = {
         "workload": "Poisson 2000 requests/s for 0.25 s (seed 5), Plummer or King W0 3/6/9, Kroupa IMF, "
-                    "N log-uniform in [256, 2048], each integrated to t = 1/16",
+                    "N log-uniform in [256, 2048], each integrated to t = 1/16; each arm after an untimed "
+                    "0.05 s stream (seed 6)",
         "requests": c["requests"], "clusters_per_s": c["clusters_per_s"],
         "clusters_per_s_serial_plain": sp["clusters_per_s"], "vs_serial_plain": c["clusters_per_s"] / sp["clusters_per_s"],
         "p50_latency_s": c["p50_latency_s"], "p99_latency_s": c["p99_latency_s"],
