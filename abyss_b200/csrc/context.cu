@@ -572,13 +572,15 @@ static abyss_tuning plan_for(abyss_ctx *c, int m, const abyss_tuning *user) {
     if (t.ipt == 0) t.ipt = m <= 1 ? 1 : m <= 2 ? 2 : m <= 4 ? 4 : 8;
   } else if (t.kernel == 3) {
     if (t.mode == 0) t.mode = (m >= 16384) ? 1 : 2;
-    // measured on B200 (King W0=6, N = 2^20): anchor 128 threads x 8 targets,
-    // 2 CTAs per SM; double-single 128 x 4 with 2 j per step, 4 CTAs per SM,
-    // or 128 x 2 for active sets too small to fill 512-target blocks
+    // measured on B200 (King W0=6, N = 2^20): anchor 128 threads x 6 targets,
+    // 3 CTAs per SM (168 registers); double-single 128 x 4 with 2 j per step,
+    // 4 CTAs per SM, or 128 x 2 for active sets too small to fill 512-target
+    // blocks
     if (t.mode == 1) {
       if (t.threads == 0) t.threads = 128;
-      if (t.ipt == 0) t.ipt = 8;
-      if (t.unroll == 0 && t.threads == 128 && t.ipt == 8) t.unroll = 1;
+      if (t.ipt == 0) t.ipt = 6;
+      if (t.unroll == 0 && t.threads == 128 && (t.ipt == 6 || t.ipt == 8)) t.unroll = 1;
+      if (t.min_blocks == 0 && t.threads == 128 && t.ipt == 6) t.min_blocks = 3;
       if (t.min_blocks == 0 && t.threads == 128 && t.ipt == 8) t.min_blocks = 2;
     } else {
       if (t.threads == 0) t.threads = 128;

@@ -1144,7 +1144,7 @@ static const TileVariant kTileVariants[] = {
     TV2(128, 2, true, 2, 1), TV2(128, 2, true, 2, 4), TV2(128, 4, true, 1, 1), TV2(128, 4, true, 2, 1),
     TV2(128, 4, true, 2, 3), TV2(128, 4, true, 1, 4), TV2(256, 2, true, 2, 1), TV2(256, 4, true, 1, 2),
     TV2(256, 4, true, 2, 1), TV2(128, 2, true, 1, 5), TV2(128, 2, true, 4, 4), TV2(128, 4, true, 2, 4),
-    TV2(256, 4, true, 2, 2), TV2(128, 8, true, 1, 2), TV2(128, 6, true, 1, 2), TV2(128, 3, true, 2, 4),
+    TV2(256, 4, true, 2, 2), TV2(128, 8, true, 1, 2), TV2(128, 6, true, 1, 2), TV2(128, 3, true, 2, 4), TV(128, 6, true, true, 1, 3),
 };
 #undef TV2
 #undef TV

@@ -146,8 +146,8 @@ class ClockSampler:
 # default anchor plan, from one ncu capture (dram__bytes_read.sum 734.35 MB +
 # dram__bytes_write.sum 997.66 MB).  The kernel is FP32-bound; these bytes are
 # reported beside the FP32 roofline, not against HBM.
-CAPTURED_TRAFFIC = {"n": 1 << 20, "m": 1 << 20, "kernel": 3, "mode": 1, "threads": 128, "ipt": 8,
-                    "bytes": 734.35e6 + 997.66e6}
+CAPTURED_TRAFFIC = {"n": 1 << 20, "m": 1 << 20, "kernel": 3, "mode": 1, "threads": 128, "ipt": 6,
+                    "bytes": 791.76e6 + 1074.76e6}
 
 
 def captured_traffic(n, m, plan):
