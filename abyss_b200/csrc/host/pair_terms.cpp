@@ -5,30 +5,33 @@
 // order, so the sums are the same, bit for bit, as the one-pass loop.
 //
 // Plain C++ compiled by g++ with -ffp-contract=off (no fused multiply-add, the
-// operations exactly as written); target_clones builds AVX-512, AVX2 and
-// baseline versions and picks one for the host's CPU at load time.
+// operations exactly as written) and -fno-math-errno (sqrt as the correctly
+// rounded instruction, without the errno call that blocks vectorisation);
+// target_clones builds AVX-512, AVX2 and baseline versions and picks one for
+// the host's CPU at load time.  The loop body has no branch: the predicted
+// state is computed for every neighbour and selected, so the compiler
+// vectorises across neighbours.
 #include <cmath>
 
 namespace abyss_host {
 
 __attribute__((target_clones("avx512f", "avx2", "default")))
-void irregular_terms(int nn, const double *X, const double *V, const double *A0, const double *A1, const double *T,
-                     const double *M, const double *pos, const double *vel, double new_time, double scale,
-                     double eps2, double *ta, double *tj) {
+void irregular_terms(int nn, const double *__restrict X, const double *__restrict V, const double *__restrict A0,
+                     const double *__restrict A1, const double *__restrict T, const double *__restrict M,
+                     const double *__restrict pos, const double *__restrict vel, double new_time, double scale,
+                     double eps2, double *__restrict ta, double *__restrict tj) {
+  const double pi[3] = {pos[0], pos[1], pos[2]}, vi[3] = {vel[0], vel[1], vel[2]};
   for (int k = 0; k < nn; ++k) {
     const double dt = (new_time - T[k]) * scale;
     double x[3], v[3], r2 = 0.0, vx = 0.0;
     for (int d = 0; d < 3; ++d) {
-      double pj, vj;
-      if (dt == 0) {
-        pj = X[3 * k + d];
-        vj = V[3 * k + d];
-      } else {
-        pj = ((A1[3 * k + d] * dt / 3 + A0[3 * k + d]) * dt / 2 + V[3 * k + d]) * dt + X[3 * k + d];
-        vj = (A1[3 * k + d] * dt / 2 + A0[3 * k + d]) * dt + V[3 * k + d];
-      }
-      x[d] = pj - pos[d];
-      v[d] = vj - vel[d];
+      // a neighbour already at new_time keeps its state exactly
+      const double pp = ((A1[3 * k + d] * dt / 3 + A0[3 * k + d]) * dt / 2 + V[3 * k + d]) * dt + X[3 * k + d];
+      const double vp = (A1[3 * k + d] * dt / 2 + A0[3 * k + d]) * dt + V[3 * k + d];
+      const double pj = dt == 0 ? X[3 * k + d] : pp;
+      const double vj = dt == 0 ? V[3 * k + d] : vp;
+      x[d] = pj - pi[d];
+      v[d] = vj - vi[d];
       r2 += x[d] * x[d];
       vx += v[d] * x[d];
     }
