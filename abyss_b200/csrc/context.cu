@@ -611,10 +611,13 @@ int abyss_launch(abyss_ctx *c, double eps2, int list_cap, const abyss_tuning *tu
   if (t.kernel == 2) {
     if (t.ipt != 1 && t.ipt != 2 && t.ipt != 4 && t.ipt != 8)
       return fail(c, ABYSS_ERR_ARG, "launch: j-major ipt must be 1, 2, 4 or 8");
-    int want = t.j_split > 0 ? t.j_split : c->sm_count * 16;
-    L = (n + want - 1) / want;
-    L = std::max(32, (L + 31) / 32 * 32);
-    S = (n + L - 1) / L;
+    // j_split counts j-chunks, one block of jmajor_warps() warps each; by
+    // default as many blocks as fit on the GPU at once
+    const int nw = jmajor_warps();
+    const int want = t.j_split > 0 ? t.j_split : c->sm_count * jmajor_occupancy(t.ipt);
+    L = (n + want * nw - 1) / (want * nw);
+    L = std::max(64, (L + 63) / 64 * 64);
+    S = (n + L * nw - 1) / (L * nw);
   } else if (t.kernel == 1 || t.kernel == 3) {
     const int per_block = t.threads * t.ipt;
     n_iblocks = (m + per_block - 1) / per_block;

@@ -5,8 +5,8 @@
 //   reg_force_tile    i in registers, j-tiles through shared memory by TMA bulk
 //                     copies, FP32 pair arithmetic with Kahan-folded tile sums,
 //                     guarded FP32 neighbour test re-decided in FP64
-//   reg_force_jmajor  lanes over j for very small active sets; exact FP64
-//                     neighbour test, ballot + popc ordered list compaction
+//   reg_force_jmajor  lanes over j for very small active sets, two j per lane
+//                     in FP32x2; guarded FP32 neighbour test re-decided in FP64
 //   finalize_rows     FP64 cross-chunk sum, ordered list concatenation,
 //                     FP64 irregular part over the final list
 //
@@ -16,6 +16,7 @@
 // neighbour (irregular part, list in ascending j); every other j adds
 // m r^-3 dx to the regular acceleration and m r^-3 (dv - 3 (dx.dv) dx / r^2)
 // to the regular jerk, with r^2 softened by eps^2 in the force terms.
+#include <algorithm>
 #include <cfloat>
 #include <cstdint>
 #include <cub/cub.cuh>
@@ -743,103 +744,175 @@ __global__ void __launch_bounds__(NT, MINB) reg_force_tile(JSet js, Work w, int 
 }
 
 // ============================================================ j-major kernel
-// One warp per j-chunk of L consecutive particles; lanes take j = j0 + lane +
-// 32 k; the MI targets of a group are held by every lane.  The neighbour test is
-// the exact FP64 one; __ballot_sync + __popc give each neighbour of a 32-j
-// group its slot, reserved with one atomic per group.
+// For very small active sets: lanes over j, every lane holding the same MI
+// targets.  A block of kJmWarps warps covers one j-chunk (its partials are one
+// column of the chunk-partial array); each warp takes a contiguous sub-chunk of
+// Lw particles (a multiple of 64) and each lane two j per step, j and j + 32,
+// as the halves of FP32x2 operands with double-single differencing.  Pairs
+// inside the guard band of R_nb are masked in that fast path and re-decided by
+// their own lane with the exact FP64 test: a neighbour is appended to the
+// target's list (one atomic per neighbour), any other pair adds its unmasked
+// FP32 contribution.  Lane halves and lanes are summed in FP64 in a fixed tree,
+// warps in a fixed order, so a launch is deterministic.
+constexpr int kJmWarps = 4;
+
 template <int MI>
-__global__ void __launch_bounds__(128) reg_force_jmajor(JSet js, Work w, int L) {
+__global__ void __launch_bounds__(32 * kJmWarps) reg_force_jmajor(JSet js, Work w, int Lw) {
+  __shared__ double s_red[kJmWarps][MI][6];
   const unsigned FULL = 0xffffffffu;
-  const int lane = threadIdx.x & 31;
-  const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (c >= w.n_chunks) return;
-  const int j0 = c * L;
-  const int j1 = min(js.n, j0 + L);
-  const unsigned lt_mask = (1u << lane) - 1u;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ch = blockIdx.x;
+  const int jw0 = min(js.n, (ch * kJmWarps + warp) * Lw);
+  const int jw1 = min(js.n, jw0 + Lw);
+  const float2 eps2v = dup2(w.eps2f);
   for (int ig = 0; ig < w.m; ig += MI) {
-    double xi[MI], yi[MI], zi[MI], R2[MI];
-    float vxi[MI], vyi[MI], vzi[MI];
-    int ti[MI], row[MI];
-    float p[MI][6];
+    // targets, held negated as double-single hi/lo; r2g < 0 marks an unused slot
+    float nhx[MI], nhy[MI], nhz[MI], nlx[MI], nly[MI], nlz[MI], nvx[MI], nvy[MI], nvz[MI], r2g[MI];
 #pragma unroll
     for (int k = 0; k < MI; ++k) {
       const bool valid = ig + k < w.m;
-      const int s = valid ? ig + k : ig;
-      ti[k] = w.order_t[s];
-      row[k] = valid ? w.order_o[s] : -1;
-      xi[k] = js.px[ti[k]];
-      yi[k] = js.py[ti[k]];
-      zi[k] = js.pz[ti[k]];
-      R2[k] = js.r2nb[ti[k]];
-      const float4 vmi = js.vm[ti[k]];
-      vxi[k] = vmi.x;
-      vyi[k] = vmi.y;
-      vzi[k] = vmi.z;
-#pragma unroll
-      for (int q = 0; q < 6; ++q) p[k][q] = 0.0f;
+      const int t = w.order_t[valid ? ig + k : ig];
+      const double X = js.px[t], Y = js.py[t], Z = js.pz[t];
+      const float fx = (float)X, fy = (float)Y, fz = (float)Z;
+      nhx[k] = -fx;
+      nhy[k] = -fy;
+      nhz[k] = -fz;
+      nlx[k] = -(float)(X - (double)fx);
+      nly[k] = -(float)(Y - (double)fy);
+      nlz[k] = -(float)(Z - (double)fz);
+      const float4 vmi = js.vm[t];
+      nvx[k] = -vmi.x;
+      nvy[k] = -vmi.y;
+      nvz[k] = -vmi.z;
+      // the tile kernel's candidate threshold with double-single offsets: every
+      // FP64 neighbour (r2 < R2) passes r2f < r2g, and so does the self pair
+      const double R = sqrt(fmax(js.r2nb[t], 0.0));
+      const double Rg = R * (1.0 + 0x1p-17) + 1e-30;
+      float g = __double2float_ru(Rg * Rg + w.eps2);
+      g = fmaxf(g, nextafterf(w.eps2f, FLT_MAX));
+      r2g[k] = valid ? g : -1.0f;
     }
-    for (int jb = j0; jb < j1; jb += 32) {
-      const int j = jb + lane;
-      const bool inr = j < j1;
-      double X = 0.0, Y = 0.0, Z = 0.0;
-      float4 V = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (inr) {
-        X = js.px[j];
-        Y = js.py[j];
-        Z = js.pz[j];
-        V = js.vm[j];
+    float2 p[MI][6];
+#pragma unroll
+    for (int k = 0; k < MI; ++k)
+#pragma unroll
+      for (int c = 0; c < 6; ++c) p[k][c] = make_float2(0.0f, 0.0f);
+
+    for (int jb = jw0; jb < jw1; jb += 64) {
+      const int ja = jb + lane, jc = jb + 32 + lane;
+      const bool ina = ja < jw1, inc = jc < jw1;
+      // j records; a pad is massless and far away: never a candidate, adds 0
+      double X0 = 1e30, Y0 = 1e30, Z0 = 1e30, X1 = 1e30, Y1 = 1e30, Z1 = 1e30;
+      float4 V0 = make_float4(0.f, 0.f, 0.f, 0.f), V1 = V0;
+      if (ina) {
+        X0 = js.px[ja];
+        Y0 = js.py[ja];
+        Z0 = js.pz[ja];
+        V0 = js.vm[ja];
       }
+      if (inc) {
+        X1 = js.px[jc];
+        Y1 = js.py[jc];
+        Z1 = js.pz[jc];
+        V1 = js.vm[jc];
+      }
+      const float2 xh = make_float2((float)X0, (float)X1);
+      const float2 yh = make_float2((float)Y0, (float)Y1);
+      const float2 zh = make_float2((float)Z0, (float)Z1);
+      const float2 xl = make_float2((float)(X0 - (double)xh.x), (float)(X1 - (double)xh.y));
+      const float2 yl = make_float2((float)(Y0 - (double)yh.x), (float)(Y1 - (double)yh.y));
+      const float2 zl = make_float2((float)(Z0 - (double)zh.x), (float)(Z1 - (double)zh.y));
+      const float2 vx = make_float2(V0.x, V1.x);
+      const float2 vy = make_float2(V0.y, V1.y);
+      const float2 vz = make_float2(V0.z, V1.z);
+      const float2 mj = make_float2(V0.w, V1.w);
+      bool any = false;
 #pragma unroll
       for (int k = 0; k < MI; ++k) {
-        if (row[k] < 0) continue;  // uniform across the warp
-        const double dxd = __dsub_rn(X, xi[k]), dyd = __dsub_rn(Y, yi[k]), dzd = __dsub_rn(Z, zi[k]);
-        double r2e = __dmul_rn(dxd, dxd);
-        r2e = __dadd_rn(r2e, __dmul_rn(dyd, dyd));
-        r2e = __dadd_rn(r2e, __dmul_rn(dzd, dzd));
-        const bool self = (j == ti[k]);
-        const bool isnb = inr && !self && (r2e < R2[k]);
-        const bool isreg = inr && !self && !isnb;
-        PairGeom g;
-        g.dx = (float)dxd;
-        g.dy = (float)dyd;
-        g.dz = (float)dzd;
-        g.dvx = V.x - vxi[k];
-        g.dvy = V.y - vyi[k];
-        g.dvz = V.z - vzi[k];
-        g.r2 = (float)__dadd_rn(r2e, w.eps2);
-        g.rv = fmaf(g.dx, g.dvx, fmaf(g.dy, g.dvy, g.dz * g.dvz));
-        const float rinv = isreg ? rsqrtf(g.r2) : 0.0f;
-        pair_accum(g, V.w, rinv, p[k]);
-        const unsigned mask = __ballot_sync(FULL, isnb);
-        if (mask) {
-          const int leader = __ffs(mask) - 1;
-          int basepos = 0;
-          if (lane == leader) basepos = atomicAdd(&w.lcnt[row[k]], __popc(mask));
-          basepos = __shfl_sync(FULL, basepos, leader);
-          if (isnb) {
-            const int idx = basepos + __popc(mask & lt_mask);
-            if (idx < w.cap) w.lst[(size_t)row[k] * w.cap + idx] = j;
+        if (r2g[k] < 0.0f) continue;  // the same for every lane
+        const PairGeom2 g = pair_geom2_ds(xh, yh, zh, xl, yl, zl, vx, vy, vz, dup2(nhx[k]), dup2(nhy[k]),
+                                          dup2(nhz[k]), dup2(nlx[k]), dup2(nly[k]), dup2(nlz[k]), dup2(nvx[k]),
+                                          dup2(nvy[k]), dup2(nvz[k]), eps2v);
+        const bool c0 = g.r2.x < r2g[k];
+        const bool c1 = g.r2.y < r2g[k];
+        float2 ri;
+        ri.x = c0 ? 0.0f : rsqrtf(g.r2.x);
+        ri.y = c1 ? 0.0f : rsqrtf(g.r2.y);
+        any |= (c0 | c1);
+        pair_accum2(g, mj, ri, p[k]);
+      }
+      if (any) {
+        // slow path, this lane only: candidates re-decided with the FP64 test
+#pragma unroll
+        for (int k = 0; k < MI; ++k) {
+          if (r2g[k] < 0.0f) continue;
+          const PairGeom2 g = pair_geom2_ds(xh, yh, zh, xl, yl, zl, vx, vy, vz, dup2(nhx[k]), dup2(nhy[k]),
+                                            dup2(nhz[k]), dup2(nlx[k]), dup2(nly[k]), dup2(nlz[k]),
+                                            dup2(nvx[k]), dup2(nvy[k]), dup2(nvz[k]), eps2v);
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const float r2f = h ? g.r2.y : g.r2.x;
+            if (!(r2f < r2g[k]) || !(h ? inc : ina)) continue;
+            const int j = h ? jc : ja;
+            const int t = w.order_t[ig + k];
+            if (j == t) continue;
+            const double r2e = exact_r2(js.px[t], js.py[t], js.pz[t], js.px[j], js.py[j], js.pz[j]);
+            if (r2e < js.r2nb[t]) {
+              const int row = w.order_o[ig + k];
+              const int idx = atomicAdd(&w.lcnt[row], 1);
+              if (idx < w.cap) w.lst[(size_t)row * w.cap + idx] = j;
+            } else {
+              const float rr = rsqrtf(r2f);
+              pair_accum2(g, mj, h ? make_float2(0.0f, rr) : make_float2(rr, 0.0f), p[k]);
+            }
           }
         }
       }
     }
+    // lane halves and lanes in FP64 (fixed tree), then the block's warps in order
 #pragma unroll
     for (int k = 0; k < MI; ++k) {
-      if (row[k] < 0) continue;
-      double s[6];
 #pragma unroll
-      for (int q = 0; q < 6; ++q) {
-        s[q] = (double)p[k][q];
-        for (int o = 16; o > 0; o >>= 1) s[q] += __shfl_xor_sync(FULL, s[q], o);
-      }
-      if (lane == 0) {
-        double *dst = w.part + ((size_t)row[k] * w.s_stride + c) * 6;
-#pragma unroll
-        for (int q = 0; q < 6; ++q) dst[q] = s[q];
+      for (int c = 0; c < 6; ++c) {
+        double sum = (double)p[k][c].x + (double)p[k][c].y;
+        for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(FULL, sum, o);
+        if (lane == 0) s_red[warp][k][c] = sum;
       }
     }
+    __syncthreads();
+    if (threadIdx.x < MI * 6) {
+      const int k = threadIdx.x / 6, c = threadIdx.x - 6 * (threadIdx.x / 6);
+      if (ig + k < w.m) {
+        double sum = 0.0;
+#pragma unroll
+        for (int q = 0; q < kJmWarps; ++q) sum += s_red[q][k][c];
+        w.part[((size_t)w.order_o[ig + k] * w.s_stride + ch) * 6 + c] = sum;
+      }
+    }
+    __syncthreads();
   }
 }
+
+// ============================================================ list sort
+// The row's nl list entries (distinct j) from lrow, sorted ascending into
+// buf[0..nl) by the calling threads (tid of nthr), with buf of P >= 2 nl ints:
+// entry k is staged at buf[P/2 + k] and placed at its rank, the number of
+// entries smaller than it.  `sync` orders the staging before the ranking.
+template <class Sync>
+__device__ __forceinline__ void rank_sort(const int *lrow, int nl, int *buf, int P, int tid, int nthr, Sync sync) {
+  int *stage = buf + P / 2;
+  for (int k = tid; k < nl; k += nthr) stage[k] = lrow[k];
+  sync();
+  for (int k = tid; k < nl; k += nthr) {
+    const int e = stage[k];
+    int rank = 0;
+    for (int q = 0; q < nl; ++q) rank += stage[q] < e;
+    buf[rank] = e;
+  }
+  sync();
+}
+
+__device__ void relist_row(const JSet &js, const Work &w, const Outputs &o, int r);
 
 // ============================================================ finalize
 // One warp per output row.  Regular part: FP64 sum of the chunk partials in a
@@ -875,12 +948,16 @@ __global__ void finalize_rows(JSet js, Work w, Outputs o, int sort_cap) {
     const int nl = min(total, w.cap);
     int *lrow = w.lst + (size_t)r * w.cap;
     int *out = o.list + (size_t)r * w.cap;
-    // bitonic sort of nl entries, padded to a power of two >= 32
+    // short lists (most): rank sort; longer ones: bitonic sort of nl
+    // entries, padded to a power of two >= 32
+    const bool by_rank = 2 * nl <= sort_cap;
+    if (by_rank) rank_sort(lrow, nl, buf, sort_cap, lane, 32, []() { __syncwarp(); });
     int P = 32;
     while (P < nl) P <<= 1;
-    for (int k = lane; k < P; k += 32) buf[k] = k < nl ? lrow[k] : INT_MAX;
+    if (!by_rank)
+      for (int k = lane; k < P; k += 32) buf[k] = k < nl ? lrow[k] : INT_MAX;
     __syncwarp();
-    for (int kk = 2; kk <= P; kk <<= 1) {
+    for (int kk = 2; kk <= (by_rank ? 1 : P); kk <<= 1) {
       for (int jj = kk >> 1; jj > 0; jj >>= 1) {
         for (int i = lane; i < P; i += 32) {
           const int l = i ^ jj;
@@ -946,72 +1023,209 @@ __global__ void finalize_rows(JSet js, Work w, Outputs o, int sort_cap) {
   }
 }
 
+// One block per output row, for launches with few rows (the warp-per-row
+// kernel above leaves most of the GPU idle there and is latency-bound).  The
+// same three parts: the chunk partials summed by every thread (thread t adds
+// chunks t, t + NT, ... in order, then the thread sums are added in a fixed
+// tree), the list sorted by warp 0 as above, and the irregular part with one
+// neighbour per thread, added in a fixed tree.
+template <int NT>
+__device__ __forceinline__ void block_sum6(double (&v)[6], double (*red)[6]) {
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < 6; ++q)
+    for (int off = 16; off > 0; off >>= 1) v[q] += __shfl_xor_sync(FULL, v[q], off);
+  if (lane == 0)
+#pragma unroll
+    for (int q = 0; q < 6; ++q) red[warp][q] = v[q];
+  __syncthreads();
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      double t = 0.0;
+      for (int k = 0; k < NT / 32; ++k) t += red[k][q];
+      v[q] = t;
+    }
+  __syncthreads();
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT) finalize_rows_block(JSet js, Work w, Outputs o, int sort_cap) {
+  extern __shared__ int fin_smem[];  // the row's sort buffer
+  __shared__ double red[NT / 32][6];
+  __shared__ int s_nl, s_total;
+  const int lane = threadIdx.x & 31;
+  const int m_rows = w.m_dev ? *w.m_dev : w.m;
+  for (int r = blockIdx.x; r < m_rows; r += gridDim.x) {
+    const int nch = w.row_nchunks ? w.row_nchunks[r] : w.n_chunks;
+    const int joff = w.row_joff ? w.row_joff[r] : 0;
+    double s[6] = {0, 0, 0, 0, 0, 0};
+    for (int c = threadIdx.x; c < nch; c += NT) {
+      const double *src = w.part + ((size_t)r * w.s_stride + c) * 6;
+#pragma unroll
+      for (int q = 0; q < 6; ++q) s[q] += src[q];
+    }
+    block_sum6<NT>(s, red);
+
+    {
+      const int total = w.lcnt[r];
+      const int nl = min(total, w.cap);
+      if (threadIdx.x == 0) {
+        s_nl = nl;
+        s_total = total;
+      }
+      if (2 * nl <= sort_cap)
+        rank_sort(w.lst + (size_t)r * w.cap, nl, fin_smem, sort_cap, threadIdx.x, NT,
+                  []() { __syncthreads(); });
+    }
+    __syncthreads();
+    if (threadIdx.x < 32 && 2 * s_nl > sort_cap) {
+      const int nl = s_nl;
+      const int *lrow = w.lst + (size_t)r * w.cap;
+      int P = 32;
+      while (P < nl) P <<= 1;
+      int *buf = fin_smem;
+      for (int k = lane; k < P; k += 32) buf[k] = k < nl ? lrow[k] : INT_MAX;
+      __syncwarp();
+      for (int kk = 2; kk <= P; kk <<= 1) {
+        for (int jj = kk >> 1; jj > 0; jj >>= 1) {
+          for (int i = lane; i < P; i += 32) {
+            const int l = i ^ jj;
+            if (l > i) {
+              const int a = buf[i], b = buf[l];
+              const bool up = (i & kk) == 0;
+              if ((a > b) == up) {
+                buf[i] = b;
+                buf[l] = a;
+              }
+            }
+          }
+          __syncwarp();
+        }
+      }
+    }
+    __syncthreads();
+    const int nl = s_nl, total = s_total;
+    const int *buf = fin_smem;
+    int *out = o.list + (size_t)r * w.cap;
+    for (int k = threadIdx.x; k < nl; k += NT) out[k] = buf[k] - joff;
+
+    const int t = o.targets[r];
+    const double xi = js.px[t], yi = js.py[t], zi = js.pz[t];
+    const double vxi = js.pvx[t], vyi = js.pvy[t], vzi = js.pvz[t];
+    double a[6] = {0, 0, 0, 0, 0, 0};
+    for (int k = threadIdx.x; k < nl; k += NT) {
+      const int j = buf[k];
+      const double x[3] = {__dsub_rn(js.px[j], xi), __dsub_rn(js.py[j], yi), __dsub_rn(js.pz[j], zi)};
+      const double v[3] = {__dsub_rn(js.pvx[j], vxi), __dsub_rn(js.pvy[j], vyi), __dsub_rn(js.pvz[j], vzi)};
+      double r2 = 0.0, vx = 0.0;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        r2 = __dadd_rn(r2, __dmul_rn(x[d], x[d]));
+        vx = __dadd_rn(vx, __dmul_rn(v[d], x[d]));
+      }
+      const double r2s = __dadd_rn(r2, w.eps2);
+      const double m_r3 = __ddiv_rn(__ddiv_rn(js.mass[j], r2s), __dsqrt_rn(r2s));
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        a[d] = __dadd_rn(a[d], __dmul_rn(m_r3, x[d]));
+        const double corr = __ddiv_rn(__dmul_rn(__dmul_rn(3.0, x[d]), vx), r2s);
+        a[3 + d] = __dadd_rn(a[3 + d], __dmul_rn(m_r3, __dsub_rn(v[d], corr)));
+      }
+    }
+    block_sum6<NT>(a, red);
+
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        o.acc_reg[3 * r + d] = s[d];
+        o.jerk_reg[3 * r + d] = s[3 + d];
+        o.acc_irr[3 * r + d] = a[d];
+        o.jerk_irr[3 * r + d] = a[3 + d];
+      }
+      o.nnb[r] = total;
+      if (total > w.cap) {
+        const int q = atomicAdd(o.overflow_rows, 1);
+        o.ovf_list[q] = r;
+        atomicOr(w.status, kErrOverflow);
+      }
+    }
+    __syncthreads();
+    // an overflowed row is re-listed here, by warp 0, instead of by relist_rows
+    if (total > w.cap && threadIdx.x < 32) relist_row(js, w, o, r);
+    __syncthreads();
+  }
+}
+
 // ============================================================ re-list
 // Rows whose neighbours did not fit in cap were appended in chunk order and kept
 // an arbitrary subset.  One warp per such row scans the row's j-range in
 // ascending order with the exact FP64 test, keeps the first cap neighbours
 // (ballot + popc placement) and recomputes the irregular part over all of them,
 // so an overflowed row reads like the reference's truncated CPU list.
-__global__ void relist_rows(JSet js, Work w, Outputs o) {
+// One warp re-lists row r (see above).
+__device__ void relist_row(const JSet &js, const Work &w, const Outputs &o, int r) {
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const unsigned lt_mask = (1u << lane) - 1u;
-  const int nwarps = (gridDim.x * blockDim.x) >> 5;
-  const int nrows = *o.overflow_rows;
-  for (int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < nrows; q += nwarps) {
-    const int r = o.ovf_list[q];
-    const int t = o.targets[r];
-    const int joff = w.row_joff ? w.row_joff[r] : 0;
-    const int j1 = joff + (w.row_jlen ? w.row_jlen[r] : js.n);
-    const double xi = js.px[t], yi = js.py[t], zi = js.pz[t];
-    const double vxi = js.pvx[t], vyi = js.pvy[t], vzi = js.pvz[t];
-    const double R2 = js.r2nb[t];
-    int *out = o.list + (size_t)r * w.cap;
-    int base = 0;
-    double a[6] = {0, 0, 0, 0, 0, 0};
-    for (int jb = joff; jb < j1; jb += 32) {
-      const int j = jb + lane;
-      bool isnb = false;
-      double x[3] = {0, 0, 0}, r2 = 0.0;
-      if (j < j1 && j != t) {
-        x[0] = __dsub_rn(js.px[j], xi);
-        x[1] = __dsub_rn(js.py[j], yi);
-        x[2] = __dsub_rn(js.pz[j], zi);
-        r2 = __dmul_rn(x[0], x[0]);
-        r2 = __dadd_rn(r2, __dmul_rn(x[1], x[1]));
-        r2 = __dadd_rn(r2, __dmul_rn(x[2], x[2]));
-        isnb = r2 < R2;
-      }
-      const unsigned mask = __ballot_sync(FULL, isnb);
-      if (isnb) {
-        const int pos = base + __popc(mask & lt_mask);
-        if (pos < w.cap) out[pos] = j - joff;
-        const double v[3] = {__dsub_rn(js.pvx[j], vxi), __dsub_rn(js.pvy[j], vyi), __dsub_rn(js.pvz[j], vzi)};
-        double vx = 0.0;
-#pragma unroll
-        for (int d = 0; d < 3; ++d) vx = __dadd_rn(vx, __dmul_rn(v[d], x[d]));
-        const double r2s = __dadd_rn(r2, w.eps2);
-        const double m_r3 = __ddiv_rn(__ddiv_rn(js.mass[j], r2s), __dsqrt_rn(r2s));
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          a[d] = __dadd_rn(a[d], __dmul_rn(m_r3, x[d]));
-          const double corr = __ddiv_rn(__dmul_rn(__dmul_rn(3.0, x[d]), vx), r2s);
-          a[3 + d] = __dadd_rn(a[3 + d], __dmul_rn(m_r3, __dsub_rn(v[d], corr)));
-        }
-      }
-      base += __popc(mask);
+  const int t = o.targets[r];
+  const int joff = w.row_joff ? w.row_joff[r] : 0;
+  const int j1 = joff + (w.row_jlen ? w.row_jlen[r] : js.n);
+  const double xi = js.px[t], yi = js.py[t], zi = js.pz[t];
+  const double vxi = js.pvx[t], vyi = js.pvy[t], vzi = js.pvz[t];
+  const double R2 = js.r2nb[t];
+  int *out = o.list + (size_t)r * w.cap;
+  int base = 0;
+  double a[6] = {0, 0, 0, 0, 0, 0};
+  for (int jb = joff; jb < j1; jb += 32) {
+    const int j = jb + lane;
+    bool isnb = false;
+    double x[3] = {0, 0, 0}, r2 = 0.0;
+    if (j < j1 && j != t) {
+      x[0] = __dsub_rn(js.px[j], xi);
+      x[1] = __dsub_rn(js.py[j], yi);
+      x[2] = __dsub_rn(js.pz[j], zi);
+      r2 = __dmul_rn(x[0], x[0]);
+      r2 = __dadd_rn(r2, __dmul_rn(x[1], x[1]));
+      r2 = __dadd_rn(r2, __dmul_rn(x[2], x[2]));
+      isnb = r2 < R2;
     }
+    const unsigned mask = __ballot_sync(FULL, isnb);
+    if (isnb) {
+      const int pos = base + __popc(mask & lt_mask);
+      if (pos < w.cap) out[pos] = j - joff;
+      const double v[3] = {__dsub_rn(js.pvx[j], vxi), __dsub_rn(js.pvy[j], vyi), __dsub_rn(js.pvz[j], vzi)};
+      double vx = 0.0;
 #pragma unroll
-    for (int k = 0; k < 6; ++k)
-      for (int off = 16; off > 0; off >>= 1) a[k] += __shfl_xor_sync(FULL, a[k], off);
-    if (lane == 0) {
+      for (int d = 0; d < 3; ++d) vx = __dadd_rn(vx, __dmul_rn(v[d], x[d]));
+      const double r2s = __dadd_rn(r2, w.eps2);
+      const double m_r3 = __ddiv_rn(__ddiv_rn(js.mass[j], r2s), __dsqrt_rn(r2s));
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
-        o.acc_irr[3 * r + d] = a[d];
-        o.jerk_irr[3 * r + d] = a[3 + d];
+        a[d] = __dadd_rn(a[d], __dmul_rn(m_r3, x[d]));
+        const double corr = __ddiv_rn(__dmul_rn(__dmul_rn(3.0, x[d]), vx), r2s);
+        a[3 + d] = __dadd_rn(a[3 + d], __dmul_rn(m_r3, __dsub_rn(v[d], corr)));
       }
     }
+    base += __popc(mask);
   }
+#pragma unroll
+  for (int k = 0; k < 6; ++k)
+    for (int off = 16; off > 0; off >>= 1) a[k] += __shfl_xor_sync(FULL, a[k], off);
+  if (lane == 0) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      o.acc_irr[3 * r + d] = a[d];
+      o.jerk_irr[3 * r + d] = a[3 + d];
+    }
+  }
+}
+
+__global__ void relist_rows(JSet js, Work w, Outputs o) {
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const int nrows = *o.overflow_rows;
+  for (int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < nrows; q += nwarps) relist_row(js, w, o, o.ovf_list[q]);
 }
 
 // ============================================================ energy
@@ -1188,14 +1402,29 @@ int tile_variant_shape(int i, int *shape6) {
   return 0;
 }
 
-int launch_jmajor(cudaStream_t s, int mi, const JSet &js, const Work &w, int L) {
-  const int warps = w.n_chunks;
-  const int blocks = (warps * 32 + 127) / 128;
+int jmajor_warps() { return kJmWarps; }
+
+int jmajor_occupancy(int mi) {
+  int occ = 0;
+  cudaError_t e = cudaErrorInvalidValue;
   switch (mi) {
-    case 1: reg_force_jmajor<1><<<blocks, 128, 0, s>>>(js, w, L); break;
-    case 2: reg_force_jmajor<2><<<blocks, 128, 0, s>>>(js, w, L); break;
-    case 4: reg_force_jmajor<4><<<blocks, 128, 0, s>>>(js, w, L); break;
-    case 8: reg_force_jmajor<8><<<blocks, 128, 0, s>>>(js, w, L); break;
+    case 1: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, reg_force_jmajor<1>, 32 * kJmWarps, 0); break;
+    case 2: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, reg_force_jmajor<2>, 32 * kJmWarps, 0); break;
+    case 4: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, reg_force_jmajor<4>, 32 * kJmWarps, 0); break;
+    case 8: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, reg_force_jmajor<8>, 32 * kJmWarps, 0); break;
+    default: break;
+  }
+  return e == cudaSuccess ? std::max(occ, 1) : 1;
+}
+
+int launch_jmajor(cudaStream_t s, int mi, const JSet &js, const Work &w, int Lw) {
+  // one block per j-chunk (w.n_chunks of them), kJmWarps sub-chunks of Lw each
+  const int blocks = w.n_chunks;
+  switch (mi) {
+    case 1: reg_force_jmajor<1><<<blocks, 32 * kJmWarps, 0, s>>>(js, w, Lw); break;
+    case 2: reg_force_jmajor<2><<<blocks, 32 * kJmWarps, 0, s>>>(js, w, Lw); break;
+    case 4: reg_force_jmajor<4><<<blocks, 32 * kJmWarps, 0, s>>>(js, w, Lw); break;
+    case 8: reg_force_jmajor<8><<<blocks, 32 * kJmWarps, 0, s>>>(js, w, Lw); break;
     default: return -1;
   }
   return 0;
@@ -1204,6 +1433,14 @@ int launch_jmajor(cudaStream_t s, int mi, const JSet &js, const Work &w, int L) 
 void launch_finalize(cudaStream_t s, const JSet &js, const Work &w, const Outputs &o, int sm_count) {
   int P = 32;
   while (P < w.cap) P <<= 1;
+  if (w.m <= 2 * sm_count) {
+    // few rows: a block per row
+    const size_t smem = (size_t)P * sizeof(int);
+    if (smem > 48 * 1024)
+      cudaFuncSetAttribute(finalize_rows_block<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    finalize_rows_block<128><<<w.m, 128, smem, s>>>(js, w, o, P);
+    return;
+  }
   const int warps_per_block = 4;
   const size_t smem = (size_t)warps_per_block * P * sizeof(int);
   if (smem > 48 * 1024)

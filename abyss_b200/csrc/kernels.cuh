@@ -27,7 +27,11 @@ int launch_tile(cudaStream_t s, int nt, int ipt, bool anchor, bool pack, int unr
                 const JSet &js, const Work &w, int n_iblocks);
 int tile_variant_count();
 int tile_variant_shape(int i, int *shape6);
-int launch_jmajor(cudaStream_t s, int mi, const JSet &js, const Work &w, int L);
+// j-major force kernel: w.n_chunks blocks of jmajor_warps() warps, each warp a
+// sub-chunk of Lw particles (a multiple of 64).
+int jmajor_warps();
+int jmajor_occupancy(int mi);  // resident blocks per SM
+int launch_jmajor(cudaStream_t s, int mi, const JSet &js, const Work &w, int Lw);
 void launch_finalize(cudaStream_t s, const JSet &js, const Work &w, const Outputs &o, int sm_count);
 void launch_predict_multi(cudaStream_t s, int n, const int *cid, const int *active,
                           const double *new_time, const double *time_scale, const double *x,
