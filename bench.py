@@ -475,7 +475,7 @@ def extras(device: int) -> dict:
         "cluster_blocks_per_s_graph": ens["graph"]["cluster_blocks_per_s"],
         "cluster_blocks_per_s_plain": ens["plain"]["cluster_blocks_per_s"],
         "gpairs_s_graph": ens["graph"]["gpairs_s"], "graph_vs_plain": ens["graph_vs_plain"]}
-    kw = dict(rate=2000.0, duration=0.25, nmin=256, nmax=2048, t_end=0.0625)
+    kw = dict(rate=2000.0, duration=0.5, nmin=256, nmax=2048, t_end=0.0625)
     res = {}
     for serial in (False, True):
         # a short stream first, untimed, for one-time costs (host threads and
@@ -485,7 +485,7 @@ def extras(device: int) -> dict:
         res["serial" if serial else "continuous"] = r
     c, sp = res["continuous"], res["serial"]
     out["serving"] = {
-        "workload": "Poisson 2000 requests/s for 0.25 s (seed 5), Plummer or King W0 3/6/9, Kroupa IMF, "
+        "workload": "Poisson 2000 requests/s for 0.5 s (seed 5), Plummer or King W0 3/6/9, Kroupa IMF, "
                     "N log-uniform in [256, 2048], each integrated to t = 1/16; each arm after an untimed "
                     "0.05 s stream (seed 6)",
         "requests": c["requests"], "clusters_per_s": c["clusters_per_s"],
