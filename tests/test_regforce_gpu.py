@@ -186,6 +186,26 @@ def test_no_neighbours_and_all_neighbours(rf):
         assert row_rel_err(res.jerk_irr, ref["jerk_irr"]).max() <= IRR_TOL, tu
 
 
+@pytest.mark.parametrize("m", [1, 37, 250])
+def test_overflow_with_few_rows(rf, m):
+    """Launches of at most 2 x 148 rows finalize a row per block and re-list an
+    overflowed row inside that block: the same truncated ascending list and full
+    irregular sums as the warp-per-row path."""
+    c = ic.plummer(700, 4, k_nb=10)
+    t = np.sort(np.random.default_rng(m).choice(c.n, m, replace=False)).astype(np.int32)
+    big = np.full(c.n, 1e6)
+    rf.send_to_device(c.m, c.x, c.v, big)
+    ref = oracle.reg_force(c.x, c.v, c.m, big, 1e-8, t, 100)
+    for tu in (TILE_DS, JMAJOR, PACKED):
+        res = rf.calculate_acceleration(t, 1e-8, 100, tu)
+        assert res.overflow_rows == m, tu
+        assert np.all(res.nnb == c.n - 1), tu
+        assert np.array_equal(res.list, ref["list"]), tu
+        assert np.abs(res.acc_reg).max() == 0.0 and np.abs(res.jerk_reg).max() == 0.0
+        assert row_rel_err(res.acc_irr, ref["acc_irr"]).max() <= IRR_TOL, tu
+        assert row_rel_err(res.jerk_irr, ref["jerk_irr"]).max() <= IRR_TOL, tu
+
+
 @pytest.mark.parametrize("n", [2, 3, 5, 127, 129, 255, 257])
 def test_tiny_and_ragged_jsets(rf, n):
     c = ic.plummer(n, 100 + n, k_nb=min(4, n - 1) + 0.5)
