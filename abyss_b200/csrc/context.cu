@@ -564,10 +564,25 @@ static abyss_tuning plan_for(abyss_ctx *c, int m, const abyss_tuning *user) {
       }
   }
   // Built-in rule (measured on B200, King W0=6, N = 2^20): lanes over j for
-  // tiny active sets; otherwise the packed tile kernel, with anchor offsets on
-  // Morton-ordered targets once the active set is dense enough for them to be
-  // accurate, double-single offsets below that.
-  if (t.kernel == 0) t.kernel = (m <= 64) ? 2 : 3;
+  // tiny active sets; one target per thread on the scalar tile kernel, in
+  // blocks of 32, 64 or 128 threads, up to 192 targets; otherwise the packed
+  // tile kernel, with anchor offsets on Morton-ordered targets once the active
+  // set is dense enough for them to be accurate, double-single offsets below
+  // that.
+  if (t.kernel == 0) {
+    if (m <= 24) {
+      t.kernel = 2;
+    } else if (m <= 192 && (t.threads == 0 || t.threads == (m <= 48 ? 32 : m <= 96 ? 64 : 128)) &&
+               (t.ipt == 0 || t.ipt == 1) && (t.mode == 0 || t.mode == 2)) {
+      t.kernel = 1;
+      t.mode = 2;
+      t.threads = m <= 48 ? 32 : m <= 96 ? 64 : 128;
+      t.ipt = 1;
+      if (t.j_split == 0) t.j_split = t.threads == 32 ? 1024 : t.threads == 64 ? 4096 : 2048;
+    } else {
+      t.kernel = 3;
+    }
+  }
   if (t.kernel == 2) {
     if (t.ipt == 0) t.ipt = m <= 1 ? 1 : m <= 2 ? 2 : m <= 4 ? 4 : 8;
   } else if (t.kernel == 3) {

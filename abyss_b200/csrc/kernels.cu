@@ -1353,7 +1353,8 @@ static void tile_run(cudaStream_t s, int grid, const JSet &js, const Work &w, in
 
 static const TileVariant kTileVariants[] = {
     // scalar pair arithmetic
-    TV2(128, 1, false, 2, 1), TV2(128, 2, false, 2, 1), TV2(128, 4, false, 2, 1), TV2(256, 2, false, 2, 1),
+    TV2(32, 1, false, 2, 1), TV2(64, 1, false, 2, 1), TV2(128, 1, false, 2, 1), TV2(128, 2, false, 2, 1),
+    TV2(128, 4, false, 2, 1), TV2(256, 2, false, 2, 1),
     // packed FP32x2 pair arithmetic (odd ipt: the last target of a thread on scalar arithmetic)
     TV2(128, 2, true, 2, 1), TV2(128, 2, true, 2, 4), TV2(128, 4, true, 1, 1), TV2(128, 4, true, 2, 1),
     TV2(128, 4, true, 2, 3), TV2(128, 4, true, 1, 4), TV2(256, 2, true, 2, 1), TV2(256, 4, true, 1, 2),

@@ -38,6 +38,8 @@ SHAPES = [
     ("packed-ds-128x3", dict(kernel=3, mode=2, threads=128, ipt=3)),
     ("packed-ds-128x8", dict(kernel=3, mode=2, threads=128, ipt=8)),
     ("packed-anchor-128x2", dict(kernel=3, mode=1, threads=128, ipt=2)),
+    ("tile-ds-32x1", dict(kernel=1, mode=2, threads=32, ipt=1)),
+    ("tile-ds-64x1", dict(kernel=1, mode=2, threads=64, ipt=1)),
     ("tile-ds-128x1", dict(kernel=1, mode=2, threads=128, ipt=1)),
     ("tile-ds-128x2", dict(kernel=1, mode=2, threads=128, ipt=2)),
     ("tile-ds-256x2", dict(kernel=1, mode=2, threads=256, ipt=2)),
