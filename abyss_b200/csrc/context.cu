@@ -565,14 +565,14 @@ static abyss_tuning plan_for(abyss_ctx *c, int m, const abyss_tuning *user) {
   }
   // Built-in rule (measured on B200, King W0=6, N = 2^20): lanes over j for
   // tiny active sets; one target per thread on the scalar tile kernel, in
-  // blocks of 32, 64 or 128 threads, up to 192 targets; otherwise the packed
+  // blocks of 32, 64 or 128 threads, up to 128 targets; otherwise the packed
   // tile kernel, with anchor offsets on Morton-ordered targets once the active
   // set is dense enough for them to be accurate, double-single offsets below
   // that.
   if (t.kernel == 0) {
     if (m <= 24) {
       t.kernel = 2;
-    } else if (m <= 192 && (t.threads == 0 || t.threads == (m <= 48 ? 32 : m <= 96 ? 64 : 128)) &&
+    } else if (m <= 128 && (t.threads == 0 || t.threads == (m <= 48 ? 32 : m <= 96 ? 64 : 128)) &&
                (t.ipt == 0 || t.ipt == 1) && (t.mode == 0 || t.mode == 2)) {
       t.kernel = 1;
       t.mode = 2;
@@ -589,8 +589,9 @@ static abyss_tuning plan_for(abyss_ctx *c, int m, const abyss_tuning *user) {
     if (t.mode == 0) t.mode = (m >= 16384) ? 1 : 2;
     // measured on B200 (King W0=6, N = 2^20): anchor 128 threads x 6 targets,
     // 3 CTAs per SM (168 registers); double-single 128 x 4 with 2 j per step,
-    // 4 CTAs per SM, or 128 x 2 for active sets too small to fill 512-target
-    // blocks
+    // 4 CTAs per SM, or, for active sets too small to fill 512-target blocks,
+    // 128 x 2 with 1 j per step at 5 CTAs per SM (2048 j-chunks up to 256
+    // targets)
     if (t.mode == 1) {
       if (t.threads == 0) t.threads = 128;
       if (t.ipt == 0) t.ipt = 6;
@@ -600,9 +601,14 @@ static abyss_tuning plan_for(abyss_ctx *c, int m, const abyss_tuning *user) {
     } else {
       if (t.threads == 0) t.threads = 128;
       if (t.ipt == 0) t.ipt = (m >= 1024) ? 4 : 2;
-      const bool small4 = t.threads == 128 && (t.ipt == 2 || t.ipt == 4);
-      if (t.unroll == 0 && small4) t.unroll = 2;
-      if (t.min_blocks == 0 && small4) t.min_blocks = 4;
+      if (t.threads == 128 && t.ipt == 4) {
+        if (t.unroll == 0) t.unroll = 2;
+        if (t.min_blocks == 0) t.min_blocks = 4;
+      } else if (t.threads == 128 && t.ipt == 2 && t.unroll == 0 && t.min_blocks == 0) {
+        t.unroll = 1;
+        t.min_blocks = 5;
+        if (t.j_split == 0 && m <= 256) t.j_split = 2048;
+      }
     }
   } else {
     if (t.mode == 0) t.mode = (m >= 4096) ? 1 : 2;
