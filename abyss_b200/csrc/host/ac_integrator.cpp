@@ -89,6 +89,12 @@ struct Pending {
   ULL tb_irr = 0, new_cur_irr = 0;
 };
 
+// A neighbour's fields as its irregular step reads them, on two cache lines.
+struct alignas(64) JRec {
+  double x[3], v[3], m, t;   // position, velocity, mass, t_irr
+  double a0[3], a1[3], pad[2];  // a_tot[.][0], a_tot[.][1]
+};
+
 }  // namespace
 
 struct abyss_ac {
@@ -111,6 +117,11 @@ struct abyss_ac {
   // split form: the regular block begun and not yet ended
   bool in_block = false;
   std::vector<int> block_targets;
+  // large clusters: the neighbour fields mirrored in Morton order of the
+  // particles' positions (slot[i] is particle i's record), so that a
+  // particle's neighbours, which are near it in space, are near in memory too
+  std::vector<JRec> jrec;
+  std::vector<int> slot;
 };
 
 namespace {
@@ -487,7 +498,7 @@ int initialise(abyss_ac *ac, const double *r2nb) {
 }
 
 // ComputeAcceleration.cpp:14-190 for one particle, into `out` (phase one).
-void irregular_one(const abyss_ac *ac, int i, Pending &out) {
+void irregular_one(const abyss_ac *ac, int i, Pending &out, bool mirror) {
   const Star &p = ac->s[i];
   std::memcpy(out.a_tot, p.a_tot, sizeof(out.a_tot));
   std::memcpy(out.a_reg, p.a_reg, sizeof(out.a_reg));
@@ -513,29 +524,55 @@ void irregular_one(const abyss_ac *ac, int i, Pending &out) {
   M.resize(nn);
   ta.resize(3 * (size_t)nn);
   tj.resize(3 * (size_t)nn);
-  constexpr int kAhead = 6;  // neighbours fetched ahead of the gather
-  for (int k = 0; k < std::min(nn, kAhead); ++k) {
-    const char *q = reinterpret_cast<const char *>(&ac->s[p.nb[k]]);
-    __builtin_prefetch(q);
-    __builtin_prefetch(q + 64);
-    __builtin_prefetch(q + 128);
-  }
-  for (int k = 0; k < nn; ++k) {
-    if (k + kAhead < nn) {
-      const char *q = reinterpret_cast<const char *>(&ac->s[p.nb[k + kAhead]]);
+  constexpr int kAhead = 8;  // neighbours fetched ahead of the gather
+  if (mirror) {
+    const JRec *J = ac->jrec.data();
+    const int *sl = ac->slot.data();
+    for (int k = 0; k < std::min(nn, kAhead); ++k) {
+      const char *q = reinterpret_cast<const char *>(&J[sl[p.nb[k]]]);
+      __builtin_prefetch(q);
+      __builtin_prefetch(q + 64);
+    }
+    for (int k = 0; k < nn; ++k) {
+      if (k + kAhead < nn) {
+        const char *q = reinterpret_cast<const char *>(&J[sl[p.nb[k + kAhead]]]);
+        __builtin_prefetch(q);
+        __builtin_prefetch(q + 64);
+      }
+      const JRec &q = J[sl[p.nb[k]]];
+      for (int d = 0; d < 3; ++d) {
+        X[3 * k + d] = q.x[d];
+        V[3 * k + d] = q.v[d];
+        A0[3 * k + d] = q.a0[d];
+        A1[3 * k + d] = q.a1[d];
+      }
+      T[k] = q.t;
+      M[k] = q.m;
+    }
+  } else {
+    for (int k = 0; k < std::min(nn, kAhead); ++k) {
+      const char *q = reinterpret_cast<const char *>(&ac->s[p.nb[k]]);
       __builtin_prefetch(q);
       __builtin_prefetch(q + 64);
       __builtin_prefetch(q + 128);
     }
-    const Star &q = ac->s[p.nb[k]];
-    for (int d = 0; d < 3; ++d) {
-      X[3 * k + d] = q.x[d];
-      V[3 * k + d] = q.v[d];
-      A0[3 * k + d] = q.a_tot[d][0];
-      A1[3 * k + d] = q.a_tot[d][1];
+    for (int k = 0; k < nn; ++k) {
+      if (k + kAhead < nn) {
+        const char *q = reinterpret_cast<const char *>(&ac->s[p.nb[k + kAhead]]);
+        __builtin_prefetch(q);
+        __builtin_prefetch(q + 64);
+        __builtin_prefetch(q + 128);
+      }
+      const Star &q = ac->s[p.nb[k]];
+      for (int d = 0; d < 3; ++d) {
+        X[3 * k + d] = q.x[d];
+        V[3 * k + d] = q.v[d];
+        A0[3 * k + d] = q.a_tot[d][0];
+        A1[3 * k + d] = q.a_tot[d][1];
+      }
+      T[k] = q.t_irr;
+      M[k] = q.m;
     }
-    T[k] = q.t_irr;
-    M[k] = q.m;
   }
   abyss_host::irregular_terms(nn, X.data(), V.data(), A0.data(), A1.data(), T.data(), M.data(), pos, vel, new_time,
                               ac->scale, ac->p.eps2, ta.data(), tj.data());
@@ -566,8 +603,66 @@ void irregular_one(const abyss_ac *ac, int i, Pending &out) {
   }
 }
 
+// Clusters from this size up read neighbours from the Morton-ordered mirror;
+// smaller ones fit in cache as they are.
+constexpr int kMirrorMin = 16384;
+
+void put_rec(abyss_ac *ac, int i) {
+  const Star &p = ac->s[i];
+  JRec &r = ac->jrec[ac->slot[i]];
+  for (int d = 0; d < 3; ++d) {
+    r.x[d] = p.x[d];
+    r.v[d] = p.v[d];
+    r.a0[d] = p.a_tot[d][0];
+    r.a1[d] = p.a_tot[d][1];
+  }
+  r.m = p.m;
+  r.t = p.t_irr;
+}
+
+// Morton order (21 bits per axis over the bounding box) of the positions now.
+void build_slots(abyss_ac *ac) {
+  const int n = ac->n;
+  double lo[3] = {HUGE_VAL, HUGE_VAL, HUGE_VAL}, hi[3] = {-HUGE_VAL, -HUGE_VAL, -HUGE_VAL};
+  for (int i = 0; i < n; ++i)
+    for (int d = 0; d < 3; ++d) {
+      lo[d] = std::min(lo[d], ac->s[i].x[d]);
+      hi[d] = std::max(hi[d], ac->s[i].x[d]);
+    }
+  auto spread = [](ULL v) {
+    v &= 0x1fffffULL;
+    v = (v | v << 32) & 0x1f00000000ffffULL;
+    v = (v | v << 16) & 0x1f0000ff0000ffULL;
+    v = (v | v << 8) & 0x100f00f00f00f00fULL;
+    v = (v | v << 4) & 0x10c30c30c30c30c3ULL;
+    v = (v | v << 2) & 0x1249249249249249ULL;
+    return v;
+  };
+  std::vector<std::pair<ULL, int>> key(n);
+  for (int i = 0; i < n; ++i) {
+    ULL c[3];
+    for (int d = 0; d < 3; ++d) {
+      const double w = hi[d] > lo[d] ? (ac->s[i].x[d] - lo[d]) / (hi[d] - lo[d]) : 0.0;
+      c[d] = (ULL)(std::min(std::max(w, 0.0), 1.0) * 2097151.0);
+    }
+    key[i] = {spread(c[0]) | spread(c[1]) << 1 | spread(c[2]) << 2, i};
+  }
+  std::sort(key.begin(), key.end());
+  ac->slot.assign(n, 0);
+  for (int r = 0; r < n; ++r) ac->slot[key[r].second] = r;
+  ac->jrec.assign(n, JRec{});
+}
+
 int irregular_levels(abyss_ac *ac) {
   const double t0 = now_s();
+  // the mirror is refreshed from the particles (the state of record) at every
+  // call, and kept current by the commits below
+  const bool mirror = ac->n >= kMirrorMin;
+  if (mirror) {
+    if ((int)ac->slot.size() != ac->n) build_slots(ac);
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < ac->n; ++i) put_rec(ac, i);
+  }
   std::map<ULL, std::vector<int>> levels;
   for (int i = 0; i < ac->n; ++i)
     if (ac->s[i].next_irr <= ac->next_reg_block) levels[ac->s[i].next_irr].push_back(i);
@@ -587,7 +682,7 @@ int irregular_levels(abyss_ac *ac) {
     {
 #pragma omp for schedule(dynamic, 8) reduction(+ : bad)
       for (int k = 0; k < (int)P.size(); ++k) {
-        irregular_one(ac, P[k], pend[k]);
+        irregular_one(ac, P[k], pend[k], mirror);
         // NewCurrentBlockIrr and the new irregular step use this particle's new
         // derivatives (WorkerRoutines.cpp:46-64), without touching its state.
         const Star &sp = ac->s[P[k]];
@@ -628,6 +723,7 @@ int irregular_levels(abyss_ac *ac) {
         }
         p.cur_irr = p.new_cur_irr;
         p.t_irr = p.cur_irr * ac->time_step;
+        if (mirror) put_rec(ac, P[k]);
       }
     }
     if (bad) {
