@@ -48,12 +48,7 @@
 #include "../../../include/abyss_ens.h"
 #include "../../../include/abyss_io.h"
 #include "../../../include/abyss_reg.h"
-namespace abyss_host {
-// host/pair_terms.cpp
-void irregular_terms(int nn, const double *X, const double *V, const double *A0, const double *A1, const double *T,
-                     const double *M, const double *pos, const double *vel, double new_time, double scale,
-                     double eps2, double *ta, double *tj);
-}  // namespace abyss_host
+#include "pair_terms.h"
 
 namespace {
 
@@ -89,11 +84,7 @@ struct Pending {
   ULL tb_irr = 0, new_cur_irr = 0;
 };
 
-// A neighbour's fields as its irregular step reads them, on two cache lines.
-struct alignas(64) JRec {
-  double x[3], v[3], m, t;   // position, velocity, mass, t_irr
-  double a0[3], a1[3], pad[2];  // a_tot[.][0], a_tot[.][1]
-};
+using abyss_host::NbRec;
 
 }  // namespace
 
@@ -117,10 +108,10 @@ struct abyss_ac {
   // split form: the regular block begun and not yet ended
   bool in_block = false;
   std::vector<int> block_targets;
-  // large clusters: the neighbour fields mirrored in Morton order of the
-  // particles' positions (slot[i] is particle i's record), so that a
-  // particle's neighbours, which are near it in space, are near in memory too
-  std::vector<JRec> jrec;
+  // the neighbour fields mirrored in Morton order of the particles' positions
+  // (slot[i] is particle i's record), so that a particle's neighbours, which
+  // are near it in space, are near in memory too
+  std::vector<NbRec> jrec;
   std::vector<int> slot;
 };
 
@@ -498,7 +489,7 @@ int initialise(abyss_ac *ac, const double *r2nb) {
 }
 
 // ComputeAcceleration.cpp:14-190 for one particle, into `out` (phase one).
-void irregular_one(const abyss_ac *ac, int i, Pending &out, bool mirror) {
+void irregular_one(const abyss_ac *ac, int i, Pending &out) {
   const Star &p = ac->s[i];
   std::memcpy(out.a_tot, p.a_tot, sizeof(out.a_tot));
   std::memcpy(out.a_reg, p.a_reg, sizeof(out.a_reg));
@@ -515,67 +506,19 @@ void irregular_one(const abyss_ac *ac, int i, Pending &out, bool mirror) {
   // the neighbours' state gathered, their terms computed independently (SIMD),
   // then added in neighbour order: the same sums as the one-pass loop
   const int nn = (int)p.nb.size();
-  thread_local std::vector<double> X, V, A0, A1, T, M, ta, tj;
-  X.resize(3 * (size_t)nn);
-  V.resize(3 * (size_t)nn);
-  A0.resize(3 * (size_t)nn);
-  A1.resize(3 * (size_t)nn);
-  T.resize(nn);
-  M.resize(nn);
+  thread_local std::vector<double> ta, tj;
   ta.resize(3 * (size_t)nn);
   tj.resize(3 * (size_t)nn);
-  constexpr int kAhead = 8;  // neighbours fetched ahead of the gather
-  if (mirror) {
-    const JRec *J = ac->jrec.data();
-    const int *sl = ac->slot.data();
-    for (int k = 0; k < std::min(nn, kAhead); ++k) {
-      const char *q = reinterpret_cast<const char *>(&J[sl[p.nb[k]]]);
-      __builtin_prefetch(q);
-      __builtin_prefetch(q + 64);
-    }
-    for (int k = 0; k < nn; ++k) {
-      if (k + kAhead < nn) {
-        const char *q = reinterpret_cast<const char *>(&J[sl[p.nb[k + kAhead]]]);
-        __builtin_prefetch(q);
-        __builtin_prefetch(q + 64);
-      }
-      const JRec &q = J[sl[p.nb[k]]];
-      for (int d = 0; d < 3; ++d) {
-        X[3 * k + d] = q.x[d];
-        V[3 * k + d] = q.v[d];
-        A0[3 * k + d] = q.a0[d];
-        A1[3 * k + d] = q.a1[d];
-      }
-      T[k] = q.t;
-      M[k] = q.m;
-    }
-  } else {
-    for (int k = 0; k < std::min(nn, kAhead); ++k) {
-      const char *q = reinterpret_cast<const char *>(&ac->s[p.nb[k]]);
-      __builtin_prefetch(q);
-      __builtin_prefetch(q + 64);
-      __builtin_prefetch(q + 128);
-    }
-    for (int k = 0; k < nn; ++k) {
-      if (k + kAhead < nn) {
-        const char *q = reinterpret_cast<const char *>(&ac->s[p.nb[k + kAhead]]);
-        __builtin_prefetch(q);
-        __builtin_prefetch(q + 64);
-        __builtin_prefetch(q + 128);
-      }
-      const Star &q = ac->s[p.nb[k]];
-      for (int d = 0; d < 3; ++d) {
-        X[3 * k + d] = q.x[d];
-        V[3 * k + d] = q.v[d];
-        A0[3 * k + d] = q.a_tot[d][0];
-        A1[3 * k + d] = q.a_tot[d][1];
-      }
-      T[k] = q.t_irr;
-      M[k] = q.m;
-    }
+  // the records are fetched ahead of the terms, which gather them themselves
+  const NbRec *J = ac->jrec.data();
+  const int *sl = ac->slot.data();
+  for (int k = 0; k < nn; ++k) {
+    const char *q = reinterpret_cast<const char *>(&J[sl[p.nb[k]]]);
+    __builtin_prefetch(q);
+    __builtin_prefetch(q + 64);
   }
-  abyss_host::irregular_terms(nn, X.data(), V.data(), A0.data(), A1.data(), T.data(), M.data(), pos, vel, new_time,
-                              ac->scale, ac->p.eps2, ta.data(), tj.data());
+  abyss_host::irregular_terms(nn, p.nb.data(), sl, J, pos, vel, new_time, ac->scale, ac->p.eps2, ta.data(),
+                              tj.data());
   for (int k = 0; k < nn; ++k)
     for (int d = 0; d < 3; ++d) {
       a_tmp[d] += ta[3 * k + d];
@@ -603,13 +546,9 @@ void irregular_one(const abyss_ac *ac, int i, Pending &out, bool mirror) {
   }
 }
 
-// Clusters from this size up read neighbours from the Morton-ordered mirror;
-// smaller ones fit in cache as they are.
-constexpr int kMirrorMin = 16384;
-
 void put_rec(abyss_ac *ac, int i) {
   const Star &p = ac->s[i];
-  JRec &r = ac->jrec[ac->slot[i]];
+  NbRec &r = ac->jrec[ac->slot[i]];
   for (int d = 0; d < 3; ++d) {
     r.x[d] = p.x[d];
     r.v[d] = p.v[d];
@@ -650,19 +589,16 @@ void build_slots(abyss_ac *ac) {
   std::sort(key.begin(), key.end());
   ac->slot.assign(n, 0);
   for (int r = 0; r < n; ++r) ac->slot[key[r].second] = r;
-  ac->jrec.assign(n, JRec{});
+  ac->jrec.assign(n, NbRec{});
 }
 
 int irregular_levels(abyss_ac *ac) {
   const double t0 = now_s();
-  // the mirror is refreshed from the particles (the state of record) at every
-  // call, and kept current by the commits below
-  const bool mirror = ac->n >= kMirrorMin;
-  if (mirror) {
-    if ((int)ac->slot.size() != ac->n) build_slots(ac);
-#pragma omp parallel for schedule(static)
-    for (int i = 0; i < ac->n; ++i) put_rec(ac, i);
-  }
+  // the neighbour mirror is refreshed from the particles (the state of record)
+  // at every call, and kept current by the commits below
+  if ((int)ac->slot.size() != ac->n) build_slots(ac);
+#pragma omp parallel for schedule(static) if (ac->n >= 16384)
+  for (int i = 0; i < ac->n; ++i) put_rec(ac, i);
   std::map<ULL, std::vector<int>> levels;
   for (int i = 0; i < ac->n; ++i)
     if (ac->s[i].next_irr <= ac->next_reg_block) levels[ac->s[i].next_irr].push_back(i);
@@ -682,7 +618,7 @@ int irregular_levels(abyss_ac *ac) {
     {
 #pragma omp for schedule(dynamic, 8) reduction(+ : bad)
       for (int k = 0; k < (int)P.size(); ++k) {
-        irregular_one(ac, P[k], pend[k], mirror);
+        irregular_one(ac, P[k], pend[k]);
         // NewCurrentBlockIrr and the new irregular step use this particle's new
         // derivatives (WorkerRoutines.cpp:46-64), without touching its state.
         const Star &sp = ac->s[P[k]];
@@ -723,7 +659,7 @@ int irregular_levels(abyss_ac *ac) {
         }
         p.cur_irr = p.new_cur_irr;
         p.t_irr = p.cur_irr * ac->time_step;
-        if (mirror) put_rec(ac, P[k]);
+        put_rec(ac, P[k]);
       }
     }
     if (bad) {

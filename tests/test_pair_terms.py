@@ -1,5 +1,6 @@
-"""The host's vectorised irregular pair terms (abyss_b200/csrc/host/pair_terms.cpp)
-equal, bit for bit, the same formula evaluated one neighbour at a time.
+"""The host's vectorised irregular pair terms (abyss_b200/csrc/host/pair_terms.cpp),
+which gather each neighbour's record themselves, equal, bit for bit, the same
+formula evaluated one neighbour at a time.
 
 The file is compiled as the library's Makefile compiles it (g++ -O3
 -ffp-contract=off -fno-fast-math -fno-math-errno), once per instruction set its
@@ -22,21 +23,23 @@ FLAGS = ["-O3", "-std=c++17", "-ffp-contract=off", "-fno-fast-math", "-fno-math-
 
 SCALAR = r"""
 #include <cmath>
+#include "pair_terms.h"
 namespace scalar_terms {
-void irregular_terms(int nn, const double *X, const double *V, const double *A0, const double *A1, const double *T,
-                     const double *M, const double *pos, const double *vel, double new_time, double scale,
-                     double eps2, double *ta, double *tj) {
+using abyss_host::NbRec;
+void irregular_terms(int nn, const int *nb, const int *slot, const NbRec *rec, const double *pos, const double *vel,
+                     double new_time, double scale, double eps2, double *ta, double *tj) {
   for (int k = 0; k < nn; ++k) {
-    const double dt = (new_time - T[k]) * scale;
+    const NbRec &q = rec[slot[nb[k]]];
+    const double dt = (new_time - q.t) * scale;
     double x[3], v[3], r2 = 0.0, vx = 0.0;
     for (int d = 0; d < 3; ++d) {
       double pj, vj;
       if (dt == 0) {
-        pj = X[3 * k + d];
-        vj = V[3 * k + d];
+        pj = q.x[d];
+        vj = q.v[d];
       } else {
-        pj = ((A1[3 * k + d] * dt / 3 + A0[3 * k + d]) * dt / 2 + V[3 * k + d]) * dt + X[3 * k + d];
-        vj = (A1[3 * k + d] * dt / 2 + A0[3 * k + d]) * dt + V[3 * k + d];
+        pj = ((q.a1[d] * dt / 3 + q.a0[d]) * dt / 2 + q.v[d]) * dt + q.x[d];
+        vj = (q.a1[d] * dt / 2 + q.a0[d]) * dt + q.v[d];
       }
       x[d] = pj - pos[d];
       v[d] = vj - vel[d];
@@ -44,7 +47,7 @@ void irregular_terms(int nn, const double *X, const double *V, const double *A0,
       vx += v[d] * x[d];
     }
     const double r2s = r2 + eps2;
-    const double m_r3 = M[k] / (r2s * std::sqrt(r2s));
+    const double m_r3 = q.m / (r2s * std::sqrt(r2s));
     for (int d = 0; d < 3; ++d) {
       ta[3 * k + d] = m_r3 * x[d];
       tj[3 * k + d] = m_r3 * (v[d] - 3 * x[d] * vx / r2s);
@@ -55,12 +58,16 @@ void irregular_terms(int nn, const double *X, const double *V, const double *A0,
 """
 
 DRIVER = r"""
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <numeric>
 #include <random>
 #include <vector>
-#define SIG int, const double *, const double *, const double *, const double *, const double *, const double *, \
-            const double *, const double *, double, double, double, double *, double *
+#include "pair_terms.h"
+using abyss_host::NbRec;
+#define SIG int, const int *, const int *, const NbRec *, const double *, const double *, double, double, double, \
+            double *, double *
 namespace abyss_host { void irregular_terms(SIG); }
 namespace scalar_terms { void irregular_terms(SIG); }
 int main() {
@@ -68,30 +75,37 @@ int main() {
   std::normal_distribution<double> N(0, 1);
   std::uniform_real_distribution<double> U(0, 1);
   long bad = 0, total = 0;
+  const int n = 600;
   for (int trial = 0; trial < 4000; ++trial) {
-    const int nn = 1 + (int)(rng() % 130);
-    std::vector<double> X(3 * nn), V(3 * nn), A0(3 * nn), A1(3 * nn), T(nn), M(nn);
-    std::vector<double> ta1(3 * nn), tj1(3 * nn), ta2(3 * nn), tj2(3 * nn);
+    std::vector<NbRec> rec(n);
+    std::vector<int> slot(n);
+    std::iota(slot.begin(), slot.end(), 0);
+    std::shuffle(slot.begin(), slot.end(), rng);
     const double new_time = U(rng) * 2, scale = trial % 3 == 0 ? 1.0 : 0.0625 * (1 + U(rng));
-    for (int k = 0; k < nn; ++k) {
+    for (NbRec &q : rec) {
       for (int d = 0; d < 3; ++d) {
-        X[3 * k + d] = N(rng) * 0.1;
-        V[3 * k + d] = N(rng);
-        A0[3 * k + d] = N(rng) * 10;
-        A1[3 * k + d] = N(rng) * 100;
-        if (rng() % 17 == 0) X[3 * k + d] = V[3 * k + d] = -0.0;
-        if (rng() % 19 == 0) { A1[3 * k + d] = -0.0; A0[3 * k + d] = 0.0; }
+        q.x[d] = N(rng) * 0.1;
+        q.v[d] = N(rng);
+        q.a0[d] = N(rng) * 10;
+        q.a1[d] = N(rng) * 100;
+        if (rng() % 17 == 0) q.x[d] = q.v[d] = -0.0;
+        if (rng() % 19 == 0) { q.a1[d] = -0.0; q.a0[d] = 0.0; }
       }
-      T[k] = rng() % 4 == 0 ? new_time : new_time - U(rng) * 0.01;
-      M[k] = rng() % 23 == 0 ? 0.0 : U(rng) * 1e-3 + 1e-6;
+      q.t = rng() % 4 == 0 ? new_time : new_time - U(rng) * 0.01;
+      q.m = rng() % 23 == 0 ? 0.0 : U(rng) * 1e-3 + 1e-6;
     }
+    const int nn = 1 + (int)(rng() % 130);
+    std::vector<int> nb(nn);
+    for (int &j : nb) j = (int)(rng() % n);
+    std::sort(nb.begin(), nb.end());
+    std::vector<double> ta1(3 * nn), tj1(3 * nn), ta2(3 * nn), tj2(3 * nn);
     double pos[3], vel[3];
     for (int d = 0; d < 3; ++d) { pos[d] = N(rng) * 0.1; vel[d] = N(rng); }
     const double eps2 = trial % 5 == 0 ? 0.0 : 1e-8;
-    abyss_host::irregular_terms(nn, X.data(), V.data(), A0.data(), A1.data(), T.data(), M.data(), pos, vel,
-                                new_time, scale, eps2, ta1.data(), tj1.data());
-    scalar_terms::irregular_terms(nn, X.data(), V.data(), A0.data(), A1.data(), T.data(), M.data(), pos, vel,
-                                  new_time, scale, eps2, ta2.data(), tj2.data());
+    abyss_host::irregular_terms(nn, nb.data(), slot.data(), rec.data(), pos, vel, new_time, scale, eps2, ta1.data(),
+                                tj1.data());
+    scalar_terms::irregular_terms(nn, nb.data(), slot.data(), rec.data(), pos, vel, new_time, scale, eps2,
+                                  ta2.data(), tj2.data());
     for (int i = 0; i < 3 * nn; ++i) {
       ++total;
       if (std::memcmp(&ta1[i], &ta2[i], 8) || std::memcmp(&tj1[i], &tj2[i], 8)) ++bad;
@@ -127,10 +141,11 @@ def test_vectorised_terms_equal_scalar(tmp_path, isa):
     march = {"avx512f": ["-mavx512f", "-mavx2", "-mfma"], "avx2": ["-mavx2", "-mno-avx512f"],
              "x86-64": ["-mno-avx2", "-mno-avx512f"]}[isa]
     exe = tmp_path / "cmp"
-    subprocess.run(["g++", *FLAGS, *march, "-c", "terms.cpp", "-o", "terms.o"], cwd=tmp_path, check=True)
-    subprocess.run(["g++", "-O0", "-std=c++17", "-ffp-contract=off", "-c", "scalar.cpp", "-o", "scalar.o"],
+    inc = "-I" + os.path.dirname(SRC)
+    subprocess.run(["g++", *FLAGS, *march, inc, "-c", "terms.cpp", "-o", "terms.o"], cwd=tmp_path, check=True)
+    subprocess.run(["g++", "-O0", "-std=c++17", "-ffp-contract=off", inc, "-c", "scalar.cpp", "-o", "scalar.o"],
                    cwd=tmp_path, check=True)
-    subprocess.run(["g++", "-O1", "-std=c++17", "main.cpp", "terms.o", "scalar.o", "-o", str(exe)], cwd=tmp_path,
-                   check=True)
+    subprocess.run(["g++", "-O1", "-std=c++17", inc, "main.cpp", "terms.o", "scalar.o", "-o", str(exe)],
+                   cwd=tmp_path, check=True)
     total, bad = map(int, subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split())
     assert total > 100000 and bad == 0, f"{bad} of {total} terms differ"
