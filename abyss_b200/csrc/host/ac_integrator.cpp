@@ -804,11 +804,11 @@ void regular_correct_one(const abyss_ac *ac, int i, const double *acc, const dou
 }
 
 // The host half of a regular block once the force is known: corrector and
-// commit for every target (results in target order, lists [m][cap]).
-int finish_regular(abyss_ac *ac, const std::vector<int> &targets, const std::vector<double> &acc,
-                   const std::vector<double> &jerk, const std::vector<double> &airr,
-                   const std::vector<double> &jirr, const std::vector<int> &nnb, const std::vector<int> &lst,
-                   int cap);
+// commit for every target (results in target order, lists [m][cap]).  The
+// result vectors are kept, moved, as the last call's record.
+int finish_regular(abyss_ac *ac, const std::vector<int> &targets, std::vector<double> &&acc,
+                   std::vector<double> &&jerk, const std::vector<double> &airr, const std::vector<double> &jirr,
+                   std::vector<int> &&nnb, std::vector<int> &&lst, int cap);
 
 int regular_block(abyss_ac *ac, const std::vector<int> &targets) {
   const double new_time = ac->next_reg_block * ac->time_step;
@@ -821,22 +821,15 @@ int regular_block(abyss_ac *ac, const std::vector<int> &targets) {
     if (rc == ABYSS_OK) break;
     if (rc != 2 || attempt > 40) return rc < 0 ? rc : ABYSS_ERR_STATE;
   }
-  return finish_regular(ac, targets, acc, jerk, airr, jirr, nnb, lst, ac->p.nb_max);
+  return finish_regular(ac, targets, std::move(acc), std::move(jerk), airr, jirr, std::move(nnb), std::move(lst),
+                        ac->p.nb_max);
 }
 
-int finish_regular(abyss_ac *ac, const std::vector<int> &targets, const std::vector<double> &acc,
-                   const std::vector<double> &jerk, const std::vector<double> &airr,
-                   const std::vector<double> &jirr, const std::vector<int> &nnb, const std::vector<int> &lst,
-                   int cap) {
+int finish_regular(abyss_ac *ac, const std::vector<int> &targets, std::vector<double> &&acc,
+                   std::vector<double> &&jerk, const std::vector<double> &airr, const std::vector<double> &jirr,
+                   std::vector<int> &&nnb, std::vector<int> &&lst, int cap) {
   const int m = (int)targets.size();
   ac->st.pairs += (double)m * ac->n;
-  // keep the last call for parity checks
-  ac->last_targets = targets;
-  ac->last_acc = acc;
-  ac->last_jerk = jerk;
-  ac->last_nnb = nnb;
-  ac->last_list = lst;
-  ac->last_cap = cap;
   const double t0 = now_s();
   std::vector<Pending> pend(m);
 #pragma omp parallel for schedule(dynamic, 8)
@@ -875,6 +868,13 @@ int finish_regular(abyss_ac *ac, const std::vector<int> &targets, const std::vec
     update_radius(ac, p);
     p.next_irr = p.cur_irr + p.tb_irr;
   }
+  // the last call, for parity checks (abyss_ac_last_regular)
+  ac->last_targets = targets;
+  ac->last_acc = std::move(acc);
+  ac->last_jerk = std::move(jerk);
+  ac->last_nnb = std::move(nnb);
+  ac->last_list = std::move(lst);
+  ac->last_cap = cap;
   ac->st.sec_reg_host += now_s() - t0;
   if (bad) {
     ac->err = "regular time step out of range";
@@ -1316,7 +1316,8 @@ int abyss_ac_end_block(abyss_ac *ac, const double *acc, const double *jerk, cons
   std::vector<int> vn(nnb, nnb + m), vl(list, list + (size_t)m * list_cap);
   int rc;
   try {
-    rc = finish_regular(ac, ac->block_targets, va, vj, vai, vji, vn, vl, list_cap);
+    rc = finish_regular(ac, ac->block_targets, std::move(va), std::move(vj), vai, vji, std::move(vn), std::move(vl),
+                        list_cap);
   } catch (const std::exception &e) {
     ac->err = e.what();
     rc = ABYSS_ERR_STATE;
