@@ -592,16 +592,75 @@ void build_slots(abyss_ac *ac) {
   ac->jrec.assign(n, NbRec{});
 }
 
+// A thread's share of the particles filed under their next irregular level,
+// grouped by level.  A level's particles go to few next levels, so a linear
+// search over the groups is enough.
+struct Filing {
+  std::vector<std::pair<ULL, std::vector<int>>> groups;
+  void add(ULL key, int i) {
+    for (auto &g : groups)
+      if (g.first == key) {
+        g.second.push_back(i);
+        return;
+      }
+    groups.emplace_back(key, std::vector<int>{i});
+  }
+  void drain_into(std::map<ULL, std::vector<int>> &levels) {
+    for (auto &g : groups) {
+      std::vector<int> &dst = levels[g.first];
+      dst.insert(dst.end(), g.second.begin(), g.second.end());
+    }
+    groups.clear();
+  }
+};
+
 int irregular_levels(abyss_ac *ac) {
   const double t0 = now_s();
+#ifdef _OPENMP
+  const int nth = std::max(1, omp_get_max_threads());
+#else
+  const int nth = 1;
+#endif
   // the neighbour mirror is refreshed from the particles (the state of record)
   // at every call, and kept current by the commits below
   if ((int)ac->slot.size() != ac->n) build_slots(ac);
 #pragma omp parallel for schedule(static) if (ac->n >= 16384)
   for (int i = 0; i < ac->n; ++i) put_rec(ac, i);
+  // every particle due before the next regular block, filed under its next
+  // irregular level (the order within a level changes nothing, see below)
   std::map<ULL, std::vector<int>> levels;
-  for (int i = 0; i < ac->n; ++i)
-    if (ac->s[i].next_irr <= ac->next_reg_block) levels[ac->s[i].next_irr].push_back(i);
+  if (ac->n >= 16384 && nth > 1) {
+    std::vector<std::map<ULL, std::vector<int>>> part(nth);
+#pragma omp parallel num_threads(nth)
+    {
+#ifdef _OPENMP
+      std::map<ULL, std::vector<int>> &mine = part[omp_get_thread_num()];
+#else
+      std::map<ULL, std::vector<int>> &mine = part[0];
+#endif
+      ULL last = 0;
+      std::vector<int> *lv = nullptr;
+#pragma omp for schedule(static)
+      for (int i = 0; i < ac->n; ++i) {
+        const ULL key = ac->s[i].next_irr;
+        if (key > ac->next_reg_block) continue;
+        if (!lv || key != last) {
+          lv = &mine[key];
+          last = key;
+        }
+        lv->push_back(i);
+      }
+    }
+    for (auto &mine : part)
+      for (auto &kv : mine) {
+        std::vector<int> &dst = levels[kv.first];
+        dst.insert(dst.end(), kv.second.begin(), kv.second.end());
+      }
+  } else {
+    for (int i = 0; i < ac->n; ++i)
+      if (ac->s[i].next_irr <= ac->next_reg_block) levels[ac->s[i].next_irr].push_back(i);
+  }
+  std::vector<Filing> filing(nth);
   std::vector<Pending> pend;
   while (!levels.empty()) {
     auto it = levels.begin();
@@ -660,24 +719,21 @@ int irregular_levels(abyss_ac *ac) {
         p.cur_irr = p.new_cur_irr;
         p.t_irr = p.cur_irr * ac->time_step;
         put_rec(ac, P[k]);
+        // filed under its next level by the committing thread
+        if (p.next_irr <= ac->next_reg_block) {
+#ifdef _OPENMP
+          filing[omp_get_thread_num()].add(p.next_irr, P[k]);
+#else
+          filing[0].add(p.next_irr, P[k]);
+#endif
+        }
       }
     }
     if (bad) {
       ac->err = "irregular time step out of range";
       return ABYSS_ERR_STATE;
     }
-    // file each particle under its next irregular level (most share one)
-    ULL last_key = 0;
-    std::vector<int> *last = nullptr;
-    for (int i : P) {
-      const ULL key = ac->s[i].next_irr;
-      if (key > ac->next_reg_block) continue;
-      if (!last || key != last_key) {
-        last = &levels[key];
-        last_key = key;
-      }
-      last->push_back(i);
-    }
+    for (Filing &f : filing) f.drain_into(levels);
     ac->st.irr_levels++;
     ac->st.irr_steps += (long long)P.size();
   }
