@@ -3,7 +3,7 @@
  * The host keeps the reference's 4th-order Hermite predictor/corrector, block
  * timesteps and regular/irregular scheduling (src_mpi/RootRoutines.cpp:240-330,
  * 448-1075, 1310-1338; src_mpi/WorkerRoutines.cpp:46-143;
- * src_mpi/Particle/*.cpp) and calls the GPU regular force through abyss_reg.h
+ * the src_mpi/Particle/ sources) and calls the GPU regular force through abyss_reg.h
  * at every regular block, in place of calculateRegAccelerationOnGPU
  * (src_mpi/cuda/CalculateRegularAcceleration.cpp:27-324).
  *
