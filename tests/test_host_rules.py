@@ -5,7 +5,6 @@ import ctypes as C
 import numpy as np
 import pytest
 
-import oracle
 from abyss_b200 import _lib
 from abyss_b200._lib import ptr, _ip
 from tests.helpers import golden

@@ -8,7 +8,6 @@
 * GPU: abyss_init_derivs23 equals the oracle bit for bit, with and without
   softening (one target per thread, j ascending, round-to-nearest FP64).
 """
-import ctypes as C
 
 import numpy as np
 import pytest

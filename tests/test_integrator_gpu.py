@@ -13,7 +13,7 @@ import oracle
 from abyss_b200 import ic
 from abyss_b200.integrator import ACIntegrator
 from abyss_b200.regforce import RegularForce
-from tests.helpers import first_list_mismatch, row_rel_err
+from tests.helpers import first_list_mismatch
 
 pytestmark = pytest.mark.gpu
 

@@ -103,7 +103,6 @@ def test_timestep_rules_bit_exact():
 @pytest.mark.skipif(not oracle.ref_available(), reason="reference CPU library not built here")
 def test_restatement_matches_reference_eps0_fresh_case():
     """Beyond the stored vectors: a fresh seeded case through both codes."""
-    from abyss_b200 import ic
     import os
     import subprocess
     import sys
