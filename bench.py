@@ -39,7 +39,8 @@ N_DEFAULT = 1 << 20
 LIST_CAP = 256
 EPS2 = 1e-8
 K_NB = 100
-WORKLOAD = "king_w0=6_n=1048576_m=N_regular_block"
+def workload_name(n: int) -> str:
+    return f"king_w0=6_n={n}_m=N_regular_block"
 
 
 def parse():
@@ -259,7 +260,7 @@ def run_reference(args, world, rank, local, pg):
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * statistics.median(secs), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "n": n, "m": n, "list_cap": LIST_CAP, "eps2": EPS2,
+        "config": {"workload": workload_name(n), "n": n, "m": n, "list_cap": LIST_CAP, "eps2": EPS2,
                    "k_nb": K_NB, "sampled_targets_per_step": sample},
         "cpu_baseline": {"value": value, "unit": "Gpairs/s", "cores": threads, "kind": kind,
                          "sample": f"{sample} evenly spaced targets x all {n} j per step "
@@ -422,7 +423,7 @@ def run_ours(args, world, rank, local, pg):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.median(step_ms),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 pair arithmetic, f64 differencing/sums", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "n": n, "m": m, "list_cap": LIST_CAP, "eps2": EPS2,
+        "config": {"workload": workload_name(n), "n": n, "m": m, "list_cap": LIST_CAP, "eps2": EPS2,
                    "k_nb": K_NB, "parallelism": f"replicas{world}", "plan": plan,
                    "l2": "flushed between timed steps (256 MB write)"},
         "force_kernel": {"ms": f_ms, "gpairs_s": m * n / f_ms / 1e6,
