@@ -42,13 +42,15 @@ class ACIntegrator:
             raise _lib.AbyssError(rc, self._L.abyss_ac_last_error(self._h).decode())
 
     @classmethod
-    def load(cls, rf: RegularForce, path: str, threads: int = 0) -> "ACIntegrator":
-        """An integration restored from a checkpoint written by save() (include/abyss_io.h)."""
+    def load(cls, rf: RegularForce | None, path: str, threads: int = 0) -> "ACIntegrator":
+        """An integration restored from a checkpoint written by save() (include/abyss_io.h).
+        With rf None it serves host-side calls only (state, save, the split
+        form's begin_block/block_state/end_block); the others raise AbyssError."""
         self = cls.__new__(cls)
         self._L = _lib.lib()
         self.rf = rf
         h = C.c_void_p()
-        rc = self._L.abyss_ac_load(rf._h, str(path).encode(), int(threads), C.byref(h))
+        rc = self._L.abyss_ac_load(rf._h if rf is not None else None, str(path).encode(), int(threads), C.byref(h))
         if rc != 0:
             raise _lib.AbyssError(rc, f"abyss_ac_load failed for {path}")
         self._h = h
