@@ -127,6 +127,15 @@ def lib():
     L.abyss_host_regular_correct.argtypes = ([C.c_int, _dp, _dp, _dp, _dp, _dp, C.c_double, C.c_double,
                                               C.c_double, C.c_int, C.c_double, _dp, C.c_int, _ip, C.c_int,
                                               _ip] + [_dp] * 8)
+    L.abyss_host_irregular_steps.argtypes = ([C.c_int] + [_dp] * 9 + [_ip, _ip, C.c_int, C.c_double, C.c_double,
+                                                                      C.c_int, _ip] + [_dp] * 4)
+    L.abyss_host_time_level_irr.argtypes = [C.c_double, C.c_int, C.c_double, C.c_int, _dp, _dp, C.c_ulonglong,
+                                            C.c_ulonglong, C.c_ulonglong, C.c_int, _ip, _dp,
+                                            C.POINTER(C.c_ulonglong)]
+    L.abyss_host_time_level_reg.argtypes = [C.c_double, C.c_int, C.c_ulonglong, C.c_double, C.c_int, _dp,
+                                            C.c_double, C.c_ulonglong, _ip, _dp, C.POINTER(C.c_ulonglong), _ip]
+    L.abyss_host_update_radius.argtypes = [C.c_double, C.c_int, C.c_int, C.c_int]
+    L.abyss_host_update_radius.restype = C.c_double
     # host integrator (include/abyss_ac.h)
     L.abyss_ac_create.argtypes = [_vp, C.POINTER(ACParams), C.c_int, _dp, _dp, _dp, _dp, C.POINTER(_vp)]
     L.abyss_ac_destroy.argtypes = [_vp]

@@ -252,7 +252,7 @@ void time_step_reg(const abyss_ac *ac, Star &p) {
     p.dt_reg = 1 - p.t_reg;
     p.tb_reg = ac->block_max - p.cur_reg;
   }
-  if (p.dt_reg * ac->scale < 1e-13) throw std::runtime_error("regular time step is too small");
+  if (p.dt_reg * ac->scale * 1e4 < 1e-9) throw std::runtime_error("regular time step is too small");
   if (p.dt_reg > 1) throw std::runtime_error("regular time step exceeds the run");
 }
 
@@ -1546,6 +1546,126 @@ int abyss_host_regular_correct(int n, const double *x, const double *v, const do
   return ABYSS_OK;
 }
 
+int abyss_host_irregular_steps(int n, const double *x, const double *v, const double *mass,
+                               const double *a_tot, const double *a_reg, const double *a_irr,
+                               const double *t_reg, const double *t_irr, const double *dt_irr,
+                               const int *nnb, const int *nb, int nb_stride, double eps2, double scale,
+                               int count, const int *idx, double *new_pos, double *new_vel,
+                               double *a_irr_out, double *a_tot_out) {
+  if (n <= 0 || count < 0 || nb_stride < 0 || !x || !v || !mass || !a_tot || !a_reg || !a_irr || !t_reg ||
+      !t_irr || !dt_irr || !nnb || (count > 0 && (!idx || !new_pos || !new_vel || !a_irr_out || !a_tot_out)))
+    return ABYSS_ERR_ARG;
+  // the integrator's own state, so that the step runs through its own code
+  // (the neighbour mirror included)
+  abyss_ac tmp;
+  tmp.n = n;
+  tmp.scale = scale;
+  tmp.p.eps2 = eps2;
+  tmp.s.resize(n);
+  for (int i = 0; i < n; ++i) {
+    Star &p = tmp.s[i];
+    for (int d = 0; d < 3; ++d) {
+      p.x[d] = x[3 * (size_t)i + d];
+      p.v[d] = v[3 * (size_t)i + d];
+    }
+    std::memcpy(p.a_tot, a_tot + 12 * (size_t)i, sizeof(p.a_tot));
+    std::memcpy(p.a_reg, a_reg + 12 * (size_t)i, sizeof(p.a_reg));
+    std::memcpy(p.a_irr, a_irr + 12 * (size_t)i, sizeof(p.a_irr));
+    p.m = mass[i];
+    p.t_reg = t_reg[i];
+    p.t_irr = t_irr[i];
+    p.dt_irr = dt_irr[i];
+    if (nnb[i] < 0 || nnb[i] > nb_stride || (nnb[i] > 0 && !nb)) return ABYSS_ERR_ARG;
+    p.nb.assign(nb + (size_t)i * nb_stride, nb + (size_t)i * nb_stride + nnb[i]);
+    for (int j : p.nb)
+      if (j < 0 || j >= n || j == i) return ABYSS_ERR_ARG;
+  }
+  build_slots(&tmp);
+  for (int i = 0; i < n; ++i) put_rec(&tmp, i);
+  Pending out;
+  for (int k = 0; k < count; ++k) {
+    const int i = idx[k];
+    if (i < 0 || i >= n) return ABYSS_ERR_ARG;
+    irregular_one(&tmp, i, out);
+    const Star &p = tmp.s[i];
+    for (int d = 0; d < 3; ++d) {
+      new_pos[3 * (size_t)k + d] = out.move ? out.new_x[d] : p.x[d];
+      new_vel[3 * (size_t)k + d] = out.move ? out.new_v[d] : p.v[d];
+    }
+    std::memcpy(a_irr_out + 12 * (size_t)k, out.a_irr, sizeof(out.a_irr));
+    std::memcpy(a_tot_out + 12 * (size_t)k, out.a_tot, sizeof(out.a_tot));
+  }
+  return ABYSS_OK;
+}
+
+int abyss_host_time_level_irr(double scale, int time_block, double eta, int has_nb, const double *a_tot,
+                              const double *a_irr, unsigned long long new_cur_irr, unsigned long long cur_reg,
+                              unsigned long long tb_reg, int lv_reg, int *lv_irr, double *dt_irr,
+                              unsigned long long *tb_irr) {
+  if (!a_tot || !a_irr || !lv_irr || !dt_irr || !tb_irr) return ABYSS_ERR_ARG;
+  abyss_ac tmp;
+  tmp.scale = scale;
+  tmp.time_block = time_block;
+  tmp.p.eta_irr = eta;
+  double at[3][4], ai[3][4];
+  std::memcpy(at, a_tot, sizeof(at));
+  std::memcpy(ai, a_irr, sizeof(ai));
+  int lv = *lv_irr;
+  double dt = *dt_irr;
+  ULL tb = *tb_irr;
+  int rc = ABYSS_OK;
+  try {
+    time_step_irr_of(&tmp, has_nb != 0, at, ai, new_cur_irr, cur_reg, tb_reg, lv_reg, lv, dt, tb);
+  } catch (const std::exception &) {
+    rc = ABYSS_ERR_STATE;
+  }
+  *lv_irr = lv;
+  *dt_irr = dt;
+  *tb_irr = tb;
+  return rc;
+}
+
+int abyss_host_time_level_reg(double scale, int time_block, unsigned long long block_max, double eta,
+                              int has_nb, const double *a_reg, double t_reg, unsigned long long cur_reg,
+                              int *lv_reg, double *dt_reg, unsigned long long *tb_reg, int *lv_irr) {
+  if (!a_reg || !lv_reg || !dt_reg || !tb_reg || !lv_irr) return ABYSS_ERR_ARG;
+  abyss_ac tmp;
+  tmp.scale = scale;
+  tmp.time_block = time_block;
+  tmp.block_max = block_max;
+  tmp.p.eta_reg = eta;
+  Star p{};
+  std::memcpy(p.a_reg, a_reg, sizeof(p.a_reg));
+  if (has_nb) p.nb.assign(1, 0);
+  p.t_reg = t_reg;
+  p.cur_reg = cur_reg;
+  p.lv_reg = *lv_reg;
+  p.dt_reg = *dt_reg;
+  p.tb_reg = *tb_reg;
+  p.lv_irr = *lv_irr;
+  int rc = ABYSS_OK;
+  try {
+    time_step_reg(&tmp, p);
+  } catch (const std::exception &) {
+    rc = ABYSS_ERR_STATE;
+  }
+  *lv_reg = p.lv_reg;
+  *dt_reg = p.dt_reg;
+  *tb_reg = p.tb_reg;
+  *lv_irr = p.lv_irr;
+  return rc;
+}
+
+double abyss_host_update_radius(double r2nb, int nnb, int fix_nb, int nb_max) {
+  abyss_ac tmp;
+  tmp.p.fix_nb = fix_nb;
+  tmp.p.nb_max = nb_max;
+  Star p{};
+  p.nb.resize(nnb > 0 ? nnb : 0);
+  p.r2nb = r2nb;
+  update_radius(&tmp, p);
+  return p.r2nb;
+}
 
 }  // extern "C"
 

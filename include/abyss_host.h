@@ -30,6 +30,43 @@ int abyss_host_regular_correct(int n, const double *x, const double *v, const do
                                const double *jerk, const double *acc_irr, const double *jerk_irr,
                                double *new_pos, double *new_vel, double *a_reg_out,
                                double *a_tot_out);
+/* Particle::computeAccelerationIrr (src_mpi/Particle/ComputeAcceleration.cpp:14-190)
+ * for the `count` particles idx[k] of an n-particle state, each from the same
+ * pre-step state of all others (one irregular level of the integrator).
+ * Per particle: x, v [n][3]; mass, t_reg, t_irr, dt_irr [n] (CurrentTimeReg,
+ * CurrentTimeIrr, TimeStepIrr in code time); a_tot, a_reg, a_irr [n][3][4];
+ * nnb[n] neighbours in rows of nb_stride.  Writes, per listed particle k, the
+ * new position/velocity [count][3] and the new a_irr, a_tot [count][3][4].  A
+ * particle without neighbours keeps its position and derivatives, as in the
+ * reference.  The position correction uses dt^5 where the reference's line 162
+ * reads an uninitialised variable. */
+int abyss_host_irregular_steps(int n, const double *x, const double *v, const double *mass,
+                               const double *a_tot, const double *a_reg, const double *a_irr,
+                               const double *t_reg, const double *t_irr, const double *dt_irr,
+                               const int *nnb, const int *nb, int nb_stride, double eps2, double scale,
+                               int count, const int *idx, double *new_pos, double *new_vel,
+                               double *a_irr_out, double *a_tot_out);
+/* Particle::calculateTimeStepIrr (src_mpi/Particle/UpdateParticle.cpp:151-241):
+ * the new irregular level from the particle's new a_tot, a_irr [3][4] and its
+ * blocks (NewCurrentBlockIrr, CurrentBlockReg, TimeBlockReg, TimeLevelReg).
+ * lv_irr, dt_irr, tb_irr hold TimeLevelIrr, TimeStepIrr, TimeBlockIrr on entry
+ * and on return.  ABYSS_ERR_STATE where the reference throws (step > 1). */
+int abyss_host_time_level_irr(double scale, int time_block, double eta, int has_nb, const double *a_tot,
+                              const double *a_irr, unsigned long long new_cur_irr, unsigned long long cur_reg,
+                              unsigned long long tb_reg, int lv_reg, int *lv_irr, double *dt_irr,
+                              unsigned long long *tb_irr);
+/* Particle::calculateTimeStepReg (src_mpi/Particle/UpdateParticle.cpp:314-407):
+ * the new regular level from a_reg [3][4], CurrentTimeReg and CurrentBlockReg.
+ * lv_reg, dt_reg, tb_reg (TimeLevelReg, TimeStepReg, TimeBlockReg) and lv_irr
+ * (TimeLevelIrr, set to the regular level when has_nb is 0) are updated in
+ * place.  ABYSS_ERR_STATE where the reference throws. */
+int abyss_host_time_level_reg(double scale, int time_block, unsigned long long block_max, double eta,
+                              int has_nb, const double *a_reg, double t_reg, unsigned long long cur_reg,
+                              int *lv_reg, double *dt_reg, unsigned long long *tb_reg, int *lv_irr);
+/* Particle::updateRadius (src_mpi/Particle/UpdateParticle.cpp:108-139): the new
+ * squared neighbour radius after a regular step that found nnb neighbours,
+ * FixNumNeighbor and NumNeighborMax given as fix_nb and nb_max. */
+double abyss_host_update_radius(double r2nb, int nnb, int fix_nb, int nb_max);
 
 #ifdef __cplusplus
 }
