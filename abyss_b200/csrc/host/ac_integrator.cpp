@@ -117,6 +117,12 @@ struct abyss_ac {
 
 namespace {
 
+// 2^e and 2^e as a block count, exactly what the reference's
+// static_cast<double>(pow(2, e)) and static_cast<ULL>(pow(2, e)) give for every
+// int e (ldexp is exact; the libm pow call is not needed).
+inline double pow2(int e) { return std::ldexp(1.0, e); }
+inline ULL pow2_blocks(int e) { return static_cast<ULL>(std::ldexp(1.0, e)); }
+
 // UpdateParticle.cpp:37-59.
 inline void predict(const Star &p, double dt_code, double scale, double pos[3], double vel[3]) {
   const double dt = dt_code * scale;
@@ -155,8 +161,8 @@ double new_step_irr(const double f[3][4], const double df[3][4], double eta) {
 void block_step(const abyss_ac *ac, double dt, int &level, ULL &block, double &step) {
   level = static_cast<int>(std::floor(std::log(dt / ac->scale) / std::log(2.0)));
   if (level < ac->time_block) level = ac->time_block;
-  step = static_cast<double>(std::pow(2, level));
-  block = static_cast<ULL>(std::pow(2, level - ac->time_block));
+  step = pow2(level);
+  block = pow2_blocks(level - ac->time_block);
 }
 
 // UpdateParticle.cpp:151-241 (calculateTimeStepIrr).
@@ -181,8 +187,8 @@ void time_step_irr_of(const abyss_ac *ac, bool has_nb, const double (&a_tot)[3][
   } p{new_cur_irr, cur_reg, tb_reg, tb_irr, lv_reg, lv_irr, dt_irr};
   if (!has_nb) {
     lv_irr = p.lv_reg;
-    dt_irr = static_cast<double>(std::pow(2, p.lv_reg));
-    tb_irr = static_cast<ULL>(std::pow(2, p.lv_reg - ac->time_block));
+    dt_irr = pow2(p.lv_reg);
+    tb_irr = pow2_blocks(p.lv_reg - ac->time_block);
     return;
   }
   int lv;
@@ -215,8 +221,8 @@ void time_step_irr_of(const abyss_ac *ac, bool has_nb, const double (&a_tot)[3][
     tb = (ULL)(tb * 0.5);
   }
   lv_irr = std::max(ac->time_block, lv);
-  dt_irr = static_cast<double>(std::pow(2, lv_irr));
-  tb_irr = static_cast<ULL>(std::pow(2, lv_irr - ac->time_block));
+  dt_irr = pow2(lv_irr);
+  tb_irr = pow2_blocks(lv_irr - ac->time_block);
   if (dt_irr > 1) throw std::runtime_error("irregular time step exceeds the run");
 }
 
@@ -246,8 +252,8 @@ void time_step_reg(const abyss_ac *ac, Star &p) {
   }
   p.lv_reg = std::max(ac->time_block, lv);
   if (p.nb.empty()) p.lv_irr = p.lv_reg;
-  p.dt_reg = static_cast<double>(std::pow(2, p.lv_reg));
-  p.tb_reg = static_cast<ULL>(std::pow(2, p.lv_reg - ac->time_block));
+  p.dt_reg = pow2(p.lv_reg);
+  p.tb_reg = pow2_blocks(p.lv_reg - ac->time_block);
   if (p.t_reg + p.dt_reg > 1 && p.t_reg != 1.0) {
     p.dt_reg = 1 - p.t_reg;
     p.tb_reg = ac->block_max - p.cur_reg;
@@ -475,12 +481,12 @@ int initialise(abyss_ac *ac, const double *r2nb) {
     min_level = std::min(min_level, p.lv_irr);
   }
   ac->time_block = std::max(-60, min_level - 30);  // MIN_LEVEL_BUFFER, def.h:33
-  ac->block_max = static_cast<ULL>(std::pow(2, -ac->time_block));
-  ac->time_step = std::pow(2, ac->time_block);
+  ac->block_max = pow2_blocks(-ac->time_block);
+  ac->time_step = pow2(ac->time_block);
   for (int i = 0; i < n; ++i) {
     Star &p = ac->s[i];
-    p.tb_irr = static_cast<ULL>(std::pow(2, p.lv_irr - ac->time_block));
-    p.tb_reg = static_cast<ULL>(std::pow(2, p.lv_reg - ac->time_block));
+    p.tb_irr = pow2_blocks(p.lv_irr - ac->time_block);
+    p.tb_reg = pow2_blocks(p.lv_reg - ac->time_block);
     p.next_irr = p.cur_irr + p.tb_irr;
   }
   ac->next_reg_block = 0;
@@ -490,11 +496,12 @@ int initialise(abyss_ac *ac, const double *r2nb) {
 
 // ComputeAcceleration.cpp:14-190 for one particle, into `out` (phase one).
 void irregular_one(const abyss_ac *ac, int i, Pending &out) {
+  // an irregular step commits a_tot and a_irr (never a_reg); both are written
+  // in full below unless the particle has no neighbours
   const Star &p = ac->s[i];
-  std::memcpy(out.a_tot, p.a_tot, sizeof(out.a_tot));
-  std::memcpy(out.a_reg, p.a_reg, sizeof(out.a_reg));
-  std::memcpy(out.a_irr, p.a_irr, sizeof(out.a_irr));
   if (p.nb.empty()) {
+    std::memcpy(out.a_tot, p.a_tot, sizeof(out.a_tot));
+    std::memcpy(out.a_irr, p.a_irr, sizeof(out.a_irr));
     out.move = false;
     return;
   }
@@ -506,9 +513,6 @@ void irregular_one(const abyss_ac *ac, int i, Pending &out) {
   // the neighbours' state gathered, their terms computed independently (SIMD),
   // then added in neighbour order: the same sums as the one-pass loop
   const int nn = (int)p.nb.size();
-  thread_local std::vector<double> ta, tj;
-  ta.resize(3 * (size_t)nn);
-  tj.resize(3 * (size_t)nn);
   // the records are fetched ahead of the terms, which gather them themselves
   const NbRec *J = ac->jrec.data();
   const int *sl = ac->slot.data();
@@ -517,6 +521,9 @@ void irregular_one(const abyss_ac *ac, int i, Pending &out) {
     __builtin_prefetch(q);
     __builtin_prefetch(q + 64);
   }
+  thread_local std::vector<double> ta, tj;
+  ta.resize(3 * (size_t)nn);
+  tj.resize(3 * (size_t)nn);
   abyss_host::irregular_terms(nn, p.nb.data(), sl, J, pos, vel, new_time, ac->scale, ac->p.eps2, ta.data(),
                               tj.data());
   for (int k = 0; k < nn; ++k)
@@ -614,6 +621,72 @@ struct Filing {
   }
 };
 
+// One irregular level: every particle's step from the pre-level state, then
+// (after the loop's barrier) every commit.  The loops are work-shared among the
+// threads of the enclosing parallel region, or run by the caller alone outside
+// one.  *bad is set when a step fails; nothing is committed then.
+void run_level(abyss_ac *ac, const std::vector<int> &P, std::vector<Pending> &pend, std::vector<Filing> &filing,
+               int *bad) {
+  const int np = (int)P.size();
+#pragma omp for schedule(dynamic, 8)
+  for (int k = 0; k < np; ++k) {
+    irregular_one(ac, P[k], pend[k]);
+    // NewCurrentBlockIrr and the new irregular step use this particle's new
+    // derivatives (WorkerRoutines.cpp:46-64), without touching its state.
+    const Star &sp = ac->s[P[k]];
+    int lv_irr = sp.lv_irr;
+    double dt_irr = sp.dt_irr;
+    ULL tb_irr = sp.tb_irr;
+    const ULL new_cur = sp.cur_irr + sp.tb_irr;
+    try {
+      time_step_irr_of(ac, !sp.nb.empty(), pend[k].a_tot, pend[k].a_irr, new_cur, sp.cur_reg, sp.tb_reg, sp.lv_reg,
+                       lv_irr, dt_irr, tb_irr);
+    } catch (const std::exception &) {
+#pragma omp atomic write
+      *bad = 1;
+    }
+    pend[k].lv_irr = lv_irr;
+    pend[k].dt_irr = dt_irr;
+    pend[k].tb_irr = tb_irr;
+    pend[k].new_cur_irr = new_cur;
+  }
+  // the loop's barrier: every step is done and *bad final
+  int failed;
+#pragma omp atomic read
+  failed = *bad;
+  if (failed) return;
+  // phase two: commit (IrrForce results + IrrUpdate, WorkerRoutines.cpp:76-87)
+#pragma omp for schedule(static)
+  for (int k = 0; k < np; ++k) {
+    Star &p = ac->s[P[k]];
+    const Pending &q = pend[k];
+    p.lv_irr = q.lv_irr;
+    p.dt_irr = q.dt_irr;
+    p.tb_irr = q.tb_irr;
+    p.new_cur_irr = q.new_cur_irr;
+    std::memcpy(p.a_tot, q.a_tot, sizeof(p.a_tot));
+    std::memcpy(p.a_irr, q.a_irr, sizeof(p.a_irr));
+    p.next_irr = p.new_cur_irr + p.tb_irr;
+    if (!p.nb.empty() && q.move) {
+      for (int d = 0; d < 3; ++d) {
+        p.x[d] = q.new_x[d];
+        p.v[d] = q.new_v[d];
+      }
+    }
+    p.cur_irr = p.new_cur_irr;
+    p.t_irr = p.cur_irr * ac->time_step;
+    put_rec(ac, P[k]);
+    // filed under its next level by the committing thread
+    if (p.next_irr <= ac->next_reg_block) {
+#ifdef _OPENMP
+      filing[omp_get_thread_num()].add(p.next_irr, P[k]);
+#else
+      filing[0].add(p.next_irr, P[k]);
+#endif
+    }
+  }
+}
+
 int irregular_levels(abyss_ac *ac) {
   const double t0 = now_s();
 #ifdef _OPENMP
@@ -670,64 +743,13 @@ int irregular_levels(abyss_ac *ac) {
     levels.erase(it);
     pend.resize(P.size());
     int bad = 0;
-    const bool par = P.size() >= 32;  // small levels: a thread team costs more than it saves
-    // one thread team per level: every particle's step from the pre-level state,
-    // then (after the loop's barrier) every commit
-#pragma omp parallel if (par)
-    {
-#pragma omp for schedule(dynamic, 8) reduction(+ : bad)
-      for (int k = 0; k < (int)P.size(); ++k) {
-        irregular_one(ac, P[k], pend[k]);
-        // NewCurrentBlockIrr and the new irregular step use this particle's new
-        // derivatives (WorkerRoutines.cpp:46-64), without touching its state.
-        const Star &sp = ac->s[P[k]];
-        int lv_irr = sp.lv_irr;
-        double dt_irr = sp.dt_irr;
-        ULL tb_irr = sp.tb_irr;
-        const ULL new_cur = sp.cur_irr + sp.tb_irr;
-        try {
-          time_step_irr_of(ac, !sp.nb.empty(), pend[k].a_tot, pend[k].a_irr, new_cur, sp.cur_reg, sp.tb_reg,
-                           sp.lv_reg, lv_irr, dt_irr, tb_irr);
-        } catch (const std::exception &) {
-          bad++;
-        }
-        pend[k].lv_irr = lv_irr;
-        pend[k].dt_irr = dt_irr;
-        pend[k].tb_irr = tb_irr;
-        pend[k].new_cur_irr = new_cur;
-      }
-      // phase two: commit (IrrForce results + IrrUpdate, WorkerRoutines.cpp:76-87);
-      // on a failed step nothing is committed
-#pragma omp for schedule(static)
-      for (int k = 0; k < (int)P.size(); ++k) {
-        if (bad) continue;
-        Star &p = ac->s[P[k]];
-        const Pending &q = pend[k];
-        p.lv_irr = q.lv_irr;
-        p.dt_irr = q.dt_irr;
-        p.tb_irr = q.tb_irr;
-        p.new_cur_irr = q.new_cur_irr;
-        std::memcpy(p.a_tot, q.a_tot, sizeof(p.a_tot));
-        std::memcpy(p.a_irr, q.a_irr, sizeof(p.a_irr));
-        p.next_irr = p.new_cur_irr + p.tb_irr;
-        if (!p.nb.empty() && q.move) {
-          for (int d = 0; d < 3; ++d) {
-            p.x[d] = q.new_x[d];
-            p.v[d] = q.new_v[d];
-          }
-        }
-        p.cur_irr = p.new_cur_irr;
-        p.t_irr = p.cur_irr * ac->time_step;
-        put_rec(ac, P[k]);
-        // filed under its next level by the committing thread
-        if (p.next_irr <= ac->next_reg_block) {
-#ifdef _OPENMP
-          filing[omp_get_thread_num()].add(p.next_irr, P[k]);
-#else
-          filing[0].add(p.next_irr, P[k]);
-#endif
-        }
-      }
+    // small levels, or one thread: no thread team (its set-up costs more than
+    // the level)
+    if (nth > 1 && P.size() >= 32) {
+#pragma omp parallel
+      run_level(ac, P, pend, filing, &bad);
+    } else {
+      run_level(ac, P, pend, filing, &bad);
     }
     if (bad) {
       ac->err = "irregular time step out of range";
