@@ -13,7 +13,9 @@ block_state, end_block).  The resulting positions and velocities:
   * match the digests recorded when the fixture was made, which pin the host's
     step (prediction, the vectorised neighbour terms, the correctors, neighbour
     changes, the time-step rules, radius updates, the level order) against any
-    change of its results.
+    change of its results;
+  * are the same again for four integrations advanced at once on four host
+    threads, one thread each (how the serving loop runs them).
 Calls that need the GPU raise instead of touching a device.
 """
 import hashlib
@@ -91,3 +93,33 @@ def test_regular_blocks_with_the_oracle_force_on_cpu():
         finally:
             ac.close()
     assert digests == [BLOCKS30_DIGEST, BLOCKS30_DIGEST]
+
+
+def test_concurrent_integrations_on_host_threads():
+    """The serving pattern: several integrations, one host thread each (no
+    thread team inside), advanced at the same time.  Each reaches the digest
+    of the lone run."""
+    import threading
+
+    acs = [_load(1) for _ in range(4)]
+    digests = [None] * len(acs)
+    errors = []
+
+    def work(k):
+        try:
+            assert run_blocks_with_oracle(acs[k], 30) == 30
+            digests[k] = _digest(acs[k])
+        except Exception as exc:  # reported below, on the main thread
+            errors.append(exc)
+
+    threads = [threading.Thread(target=work, args=(k,)) for k in range(len(acs))]
+    try:
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+    finally:
+        for ac in acs:
+            ac.close()
+    assert not errors, errors
+    assert digests == [BLOCKS30_DIGEST] * len(acs)
