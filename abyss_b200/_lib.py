@@ -134,6 +134,10 @@ def lib():
                                             C.POINTER(C.c_ulonglong)]
     L.abyss_host_time_level_reg.argtypes = [C.c_double, C.c_int, C.c_ulonglong, C.c_double, C.c_int, _dp,
                                             C.c_double, C.c_ulonglong, _ip, _dp, C.POINTER(C.c_ulonglong), _ip]
+    L.abyss_host_initial_time_steps.argtypes = [C.c_double, C.c_int, C.c_ulonglong, C.c_double, C.c_double, C.c_int,
+                                                _dp, _dp, _dp, _ip, _dp, C.POINTER(C.c_ulonglong), _ip, _dp,
+                                                C.POINTER(C.c_ulonglong)]
+    L.abyss_host_initial_time_steps.restype = None
     L.abyss_host_update_radius.argtypes = [C.c_double, C.c_int, C.c_int, C.c_int]
     L.abyss_host_update_radius.restype = C.c_double
     # host integrator (include/abyss_ac.h)

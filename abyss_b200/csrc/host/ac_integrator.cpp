@@ -1678,6 +1678,30 @@ int abyss_host_time_level_reg(double scale, int time_block, unsigned long long b
   return rc;
 }
 
+void abyss_host_initial_time_steps(double scale, int time_block, unsigned long long block_max, double eta_reg,
+                                   double eta_irr, int has_nb, const double *a_tot, const double *a_reg,
+                                   const double *a_irr, int *lv_reg, double *dt_reg, unsigned long long *tb_reg,
+                                   int *lv_irr, double *dt_irr, unsigned long long *tb_irr) {
+  abyss_ac tmp;
+  tmp.scale = scale;
+  tmp.time_block = time_block;
+  tmp.block_max = block_max;
+  tmp.p.eta_reg = eta_reg;
+  tmp.p.eta_irr = eta_irr;
+  Star p{};
+  std::memcpy(p.a_tot, a_tot, sizeof(p.a_tot));
+  std::memcpy(p.a_reg, a_reg, sizeof(p.a_reg));
+  std::memcpy(p.a_irr, a_irr, sizeof(p.a_irr));
+  if (has_nb) p.nb.assign(1, 0);
+  init_time_step(&tmp, p);
+  *lv_reg = p.lv_reg;
+  *dt_reg = p.dt_reg;
+  *tb_reg = p.tb_reg;
+  *lv_irr = p.lv_irr;
+  *dt_irr = p.dt_irr;
+  *tb_irr = p.tb_irr;
+}
+
 double abyss_host_update_radius(double r2nb, int nnb, int fix_nb, int nb_max) {
   abyss_ac tmp;
   tmp.p.fix_nb = fix_nb;

@@ -63,6 +63,13 @@ int abyss_host_time_level_irr(double scale, int time_block, double eta, int has_
 int abyss_host_time_level_reg(double scale, int time_block, unsigned long long block_max, double eta,
                               int has_nb, const double *a_reg, double t_reg, unsigned long long cur_reg,
                               int *lv_reg, double *dt_reg, unsigned long long *tb_reg, int *lv_irr);
+/* Particle::initializeTimeStep (src_mpi/Particle/Initialize.cpp:199-230): the
+ * first regular and irregular levels, steps and blocks from the initial
+ * a_tot, a_reg, a_irr [3][4] (eta_reg and eta_irr both the reference's eta). */
+void abyss_host_initial_time_steps(double scale, int time_block, unsigned long long block_max, double eta_reg,
+                                   double eta_irr, int has_nb, const double *a_tot, const double *a_reg,
+                                   const double *a_irr, int *lv_reg, double *dt_reg, unsigned long long *tb_reg,
+                                   int *lv_irr, double *dt_irr, unsigned long long *tb_irr);
 /* Particle::updateRadius (src_mpi/Particle/UpdateParticle.cpp:108-139): the new
  * squared neighbour radius after a regular step that found nnb neighbours,
  * FixNumNeighbor and NumNeighborMax given as fix_nb and nb_max. */

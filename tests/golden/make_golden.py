@@ -13,7 +13,8 @@ synthetic clusters and stores inputs and outputs as compressed .npz files:
 * irregular step and its new level (*_irr.npz)   computeAccelerationIrr (ComputeAcceleration.cpp:14-190),
                                                 calculateTimeStepIrr (UpdateParticle.cpp:151-241)
 * level rules and radius update (ref_levels)    calculateTimeStepIrr, calculateTimeStepReg
-                                                (UpdateParticle.cpp:314-407), updateRadius (:108-139)
+                                                (UpdateParticle.cpp:314-407), updateRadius (:108-139),
+                                                initializeTimeStep (Initialize.cpp:199-230)
 
 Run from the repository root with the reference tree present:
     make -C oracle && python tests/golden/make_golden.py
@@ -316,6 +317,29 @@ def make_levels(seed: int, tblock: int = -30):
     for c, val in cols.items():
         dt = np.uint64 if c in ("cur_reg", "tb_reg", "out_tb_reg") else None
         res["reg_" + c] = np.array(val, dtype=dt)
+    # initializeTimeStep (Initialize.cpp:199-230) at the start of a run
+    cols = {c: [] for c in ("scale", "has_nb", "a_tot", "a_reg", "a_irr", "out_lv_reg", "out_tb_reg", "out_dt_reg",
+                            "out_lv_irr", "out_tb_irr", "out_dt_irr")}
+    for _ in range(k):
+        scale = float(rng.choice(scales))
+        L.ref_set_globals(scale, tblock, bmax)
+        has_nb = int(rng.uniform() < 0.85)
+        lv = rng.uniform(-16, 2)  # some steps above 1, which the rule caps
+        ar = _derivs(rng, 2.0 ** lv * scale, eta)
+        ai = _derivs(rng, 2.0 ** (lv - rng.uniform(0, 6)) * scale, eta)
+        at = ar + ai
+        L.ref_set_particle(0, _p(zx), _p(zx), 1.0, 0.0, _p(np.ascontiguousarray(at.reshape(12))),
+                           _p(np.ascontiguousarray(ar.reshape(12))), _p(np.ascontiguousarray(ai.reshape(12))),
+                           0.0, 0.0, 0.0, 0.0, has_nb, _p(nb, _ip))
+        L.ref_initialize_time_step(0)
+        ull, lvl, dts = _blocks(L, 0)
+        for c, val in (("scale", scale), ("has_nb", has_nb), ("a_tot", at), ("a_reg", ar), ("a_irr", ai),
+                       ("out_lv_reg", lvl[0]), ("out_tb_reg", ull[2]), ("out_dt_reg", dts[0]),
+                       ("out_lv_irr", lvl[1]), ("out_tb_irr", ull[3]), ("out_dt_irr", dts[1])):
+            cols[c].append(val)
+    for c, val in cols.items():
+        dt = np.uint64 if c in ("out_tb_reg", "out_tb_irr") else None
+        res["init_" + c] = np.array(val, dtype=dt)
     # updateRadius over every count from 0 to 2 NumNeighborMax
     fix, nbmax = int(L.ref_fix_num_neighbor()), int(L.ref_num_neighbor_max())
     counts = np.arange(0, min(2 * nbmax, CAP) + 1, dtype=np.int32)

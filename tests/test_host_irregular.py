@@ -9,8 +9,9 @@ Golden vectors from the reference's CPU code (tests/golden/make_golden.py):
   corrector's a3 dt^5/120 term: the reference reads an uninitialised dt5
   (ComputeAcceleration.cpp:162), which the compiled reference treats as zero,
   and the integrator uses dt^4 * dt.
-* calculateTimeStepIrr, calculateTimeStepReg and updateRadius on seeded block
-  states that reach each branch: bit-exact levels, blocks and steps.  (The
+* calculateTimeStepIrr, calculateTimeStepReg, initializeTimeStep and
+  updateRadius on seeded block states that reach each branch: bit-exact
+  levels, blocks and steps.  (The
   regular rule's clamp at the end of the run is not reached from states on the
   block grid: a level only rises where the current block is aligned to it.)
 With the reference tree built (oracle/_ref), a fresh seeded state is checked
@@ -220,3 +221,23 @@ def test_irregular_step_against_the_reference_library():
                            _p(_c(st["a_tot"][i])), _p(_c(st["a_reg"][i])), _p(_c(st["a_irr"][i])),
                            float(st["t_reg"][i]), float(st["t_irr"][i]), float(st["dt_reg"][i]),
                            float(st["dt_irr"][i]), int(st["nnb"][i]), _p(nb[i], _ip))
+
+
+def test_initial_time_steps_bit_exact():
+    L = _lib.lib()
+    g = golden("ref_levels.npz")
+    tblock, eta, bmax = int(g["time_block"]), float(g["eta"]), int(g["block_max"])
+    capped = 0
+    for q in range(g["init_scale"].shape[0]):
+        lv_reg, lv_irr = C.c_int(), C.c_int()
+        dt_reg, dt_irr = C.c_double(), C.c_double()
+        tb_reg, tb_irr = C.c_ulonglong(), C.c_ulonglong()
+        L.abyss_host_initial_time_steps(float(g["init_scale"][q]), tblock, bmax, eta, eta, int(g["init_has_nb"][q]),
+                                        ptr(_c(g["init_a_tot"][q])), ptr(_c(g["init_a_reg"][q])),
+                                        ptr(_c(g["init_a_irr"][q])), C.byref(lv_reg), C.byref(dt_reg),
+                                        C.byref(tb_reg), C.byref(lv_irr), C.byref(dt_irr), C.byref(tb_irr))
+        got = (lv_reg.value, dt_reg.value, tb_reg.value, lv_irr.value, dt_irr.value, tb_irr.value)
+        want = tuple(g["init_out_" + c][q] for c in ("lv_reg", "dt_reg", "tb_reg", "lv_irr", "dt_irr", "tb_irr"))
+        assert got == want, (q, got, want)
+        capped += dt_reg.value == 1.0
+    assert capped > 0  # steps above the run's length are capped at 1
