@@ -55,3 +55,46 @@ def test_context_creation_without_gpu_reports_error():
     h = C.c_void_p()
     rc = L.abyss_create(0, C.byref(h))
     assert rc == _lib.ABYSS_ERR_NODEVICE
+
+
+def _zero_args(argtypes):
+    args = []
+    for t in argtypes:
+        if t in (C.c_int, C.c_uint, C.c_longlong, C.c_ulonglong):
+            args.append(0)
+        elif t in (C.c_double, C.c_float):
+            args.append(0.0)
+        else:
+            args.append(None)
+    return args
+
+
+def test_null_handles_return_errors():
+    """Every call that takes a context, ensemble or integrator handle, given a
+    null handle and null or zero arguments, answers with an error code (or its
+    documented null result) and touches nothing: the boundary never traps."""
+    from abyss_b200 import ensemble, serve
+
+    L = _lib.lib()
+    ensemble._bind(L)
+    serve._bind(L)
+    called = 0
+    for name in declared_functions():
+        if not name.startswith("abyss_") or name.startswith(("abyss_host_", "abyss_compat_")):
+            continue
+        f = getattr(L, name)
+        if not f.argtypes:
+            continue
+        r = f(*_zero_args(f.argtypes))
+        called += 1
+        if name in ("abyss_ac_destroy", "abyss_ens_destroy"):
+            assert r in (0, _lib.ABYSS_ERR_ARG), name  # deleting nothing is allowed
+        elif name in ("abyss_last_error", "abyss_ac_last_error"):
+            assert r and r.startswith(b"null"), name
+        elif name in ("abyss_stream",):
+            assert r is None
+        elif name in ("abyss_ac_time", "abyss_ens_device_bytes", "abyss_ens_list_cap"):
+            assert r == 0, name
+        else:
+            assert r == _lib.ABYSS_ERR_ARG, (name, r)
+    assert called > 50
