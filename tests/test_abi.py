@@ -98,3 +98,25 @@ def test_null_handles_return_errors():
         else:
             assert r == _lib.ABYSS_ERR_ARG, (name, r)
     assert called > 50
+
+
+def test_reference_entry_points_with_null_arguments():
+    """The reference's six entry points (void in its ABI) report bad calls
+    through abyss_compat_status() instead of trapping."""
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    L = _lib.lib()
+    expect = {"InitializeDevice": _lib.ABYSS_ERR_NODEVICE, "OpenDevice": _lib.ABYSS_ERR_NODEVICE,
+              "SendToDevice": _lib.ABYSS_ERR_ARG, "SendToDevice_f64": _lib.ABYSS_ERR_ARG,
+              "CalculateAccelerationOnDevice": _lib.ABYSS_ERR_STATE,
+              "CalculateAccelerationOnDevice_f64": _lib.ABYSS_ERR_STATE}
+    for name, status in expect.items():
+        f = getattr(L, name)
+        f(*([None] * len(f.argtypes or [])))
+        assert L.abyss_compat_status() == status, name
+    # with no device open these two do nothing
+    for name in ("ProfileDevice", "CloseDevice"):
+        f = getattr(L, name)
+        f(*([None] * len(f.argtypes or [])))
