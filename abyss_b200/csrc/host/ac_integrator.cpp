@@ -36,6 +36,7 @@
 #include <thread>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <stdexcept>
 #include <string>
 #include <unordered_set>
@@ -1742,6 +1743,10 @@ bool get(std::ifstream &f, T &v) {
 
 }  // namespace
 
+namespace {
+int load_body(std::ifstream &f, abyss_ctx *ctx, int n, int threads, abyss_ac **out);
+}  // namespace
+
 extern "C" {
 
 int abyss_ac_save(const abyss_ac *ac, const char *path) {
@@ -1794,7 +1799,28 @@ int abyss_ac_load(abyss_ctx *ctx, const char *path, int threads, abyss_ac **out)
   if (!f.read(magic, 8) || std::memcmp(magic, kCkptMagic, 8) != 0) return ABYSS_ERR_STATE;
   if (!get(f, version) || version != kCkptVersion || !get(f, dsz) || dsz != sizeof(Star::a_tot)) return ABYSS_ERR_STATE;
   if (!get(f, n) || n < 2) return ABYSS_ERR_STATE;
-  abyss_ac *ac = new abyss_ac;
+  // the bytes left bound the particle count that the file may claim, so that
+  // a damaged count is refused before anything is allocated for it
+  constexpr long long kMinRecord = sizeof(Star::x) + sizeof(Star::v) + sizeof(Star::m) + 3 * sizeof(Star::a_tot) +
+                                   5 * sizeof(double) + 6 * sizeof(ULL) + 3 * sizeof(int);
+  const std::streampos here = f.tellg();
+  f.seekg(0, std::ios::end);
+  const long long left = (long long)(f.tellg() - here);
+  f.seekg(here);
+  if (!f || (long long)n > left / kMinRecord) return ABYSS_ERR_STATE;
+  return load_body(f, ctx, n, threads, out);
+}
+
+}  // extern "C"
+
+namespace {
+
+// The checkpoint after its header (n particles, within the file's size): the
+// integrator, or an error; host allocation failure is ABYSS_ERR_OOM.
+int load_body(std::ifstream &f, abyss_ctx *ctx, int n, int threads, abyss_ac **out) try {
+  char magic[8];
+  std::unique_ptr<abyss_ac> owner(new abyss_ac);
+  abyss_ac *ac = owner.get();
   ac->ctx = ctx;
   ac->n = n;
   int done = 0;
@@ -1823,13 +1849,16 @@ int abyss_ac_load(abyss_ctx *ctx, const char *path, int threads, abyss_ac **out)
       if (j < 0 || j >= n) ok = false;
   }
   if (ok) ok = f.read(magic, 8) && std::memcmp(magic, kCkptMagic, 8) == 0;
-  if (!ok) {
-    delete ac;
-    return ABYSS_ERR_STATE;
-  }
-  *out = ac;
+  if (!ok) return ABYSS_ERR_STATE;
+  *out = owner.release();
   return ABYSS_OK;
+} catch (const std::bad_alloc &) {
+  return ABYSS_ERR_OOM;
 }
+
+}  // namespace
+
+extern "C" {
 
 int abyss_ac_write_snapshot(const abyss_ac *ac, const char *path, double output_time, double output_time_step) {
   if (!ac || !path) return ABYSS_ERR_ARG;

@@ -123,3 +123,46 @@ def test_concurrent_integrations_on_host_threads():
             ac.close()
     assert not errors, errors
     assert digests == [BLOCKS30_DIGEST] * len(acs)
+
+
+def test_save_load_round_trip_on_cpu(tmp_path):
+    """A checkpoint saved after host-only blocks loads back to the same state,
+    continues to the same digest, and saves to the same bytes."""
+    ac = _load(2)
+    try:
+        assert run_blocks_with_oracle(ac, 10) == 10
+        path = tmp_path / "mid.ckpt"
+        ac.save(str(path))
+        assert run_blocks_with_oracle(ac, 20) == 20
+        want = _digest(ac)
+    finally:
+        ac.close()
+    b = ACIntegrator.load(None, str(path), threads=2)
+    try:
+        again = tmp_path / "again.ckpt"
+        b.save(str(again))
+        assert again.read_bytes() == path.read_bytes()
+        assert run_blocks_with_oracle(b, 20) == 20
+        assert _digest(b) == want == BLOCKS30_DIGEST
+    finally:
+        b.close()
+
+
+def test_damaged_checkpoints_are_refused(tmp_path):
+    """Truncated files, a wrong magic and damaged particle counts are refused
+    with an error: never read past their end, never allocated for."""
+    data = open(CKPT, "rb").read()
+    cases = {f"cut{k}": data[:k] for k in (0, 7, 8, 64, len(data) // 2, len(data) - 8, len(data) - 1)}
+    cases["magic"] = b"NOTABYSS" + data[8:]
+    cases["tail"] = data[:-8] + b"NOTABYSS"
+    # the particle count (after the magic, version and record size): a huge one
+    # is refused before any allocation, one more than stored runs out of records
+    n = int.from_bytes(data[16:20], "little")
+    assert n == 1024
+    for name, bad_n in (("n_huge", 2**31 - 1), ("n_plus", n + 1), ("n_one", 1)):
+        cases[name] = data[:16] + bad_n.to_bytes(4, "little") + data[20:]
+    for name, blob in cases.items():
+        p = tmp_path / (name + ".ckpt")
+        p.write_bytes(blob)
+        with pytest.raises(_lib.AbyssError):
+            ACIntegrator.load(None, str(p))
