@@ -36,7 +36,9 @@ int abyss_ac_write_snapshot(const struct abyss_ac *ac, const char *path, double 
  * abyss_ac_load rebuilds the integration on ctx without recomputing anything,
  * so that continuing it gives the same results, bit for bit, as never having
  * stopped; threads replaces the saved host thread count.  A file that is not a
- * complete checkpoint of this version is refused with ABYSS_ERR_STATE.  ctx may
+ * complete checkpoint of this version is refused with ABYSS_ERR_STATE, before
+ * any allocation where its particle count exceeds what its size can hold; a
+ * failed host allocation returns ABYSS_ERR_OOM.  ctx may
  * be NULL: the integration then serves host-side calls only (state queries, the
  * irregular steps of abyss_ac_begin_block, abyss_ac_save); calls that need the
  * GPU return ABYSS_ERR_ARG. */
