@@ -1390,13 +1390,16 @@ int abyss_ac_end_block(abyss_ac *ac, const double *acc, const double *jerk, cons
     ac->st.radius_retries++;
     return ABYSS_WARN_OVERFLOW;
   }
-  std::vector<double> va(acc, acc + 3 * (size_t)m), vj(jerk, jerk + 3 * (size_t)m),
-      vai(acc_irr, acc_irr + 3 * (size_t)m), vji(jerk_irr, jerk_irr + 3 * (size_t)m);
-  std::vector<int> vn(nnb, nnb + m), vl(list, list + (size_t)m * list_cap);
   int rc;
   try {
+    std::vector<double> va(acc, acc + 3 * (size_t)m), vj(jerk, jerk + 3 * (size_t)m),
+        vai(acc_irr, acc_irr + 3 * (size_t)m), vji(jerk_irr, jerk_irr + 3 * (size_t)m);
+    std::vector<int> vn(nnb, nnb + m), vl(list, list + (size_t)m * list_cap);
     rc = finish_regular(ac, ac->block_targets, std::move(va), std::move(vj), vai, vji, std::move(vn), std::move(vl),
                         list_cap);
+  } catch (const std::bad_alloc &) {
+    ac->err = "end_block: host allocation failed";
+    rc = ABYSS_ERR_OOM;
   } catch (const std::exception &e) {
     ac->err = e.what();
     rc = ABYSS_ERR_STATE;
