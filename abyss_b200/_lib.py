@@ -93,6 +93,7 @@ def lib():
     L.abyss_regular_force.argtypes = [_vp, C.c_int, _ip, C.c_double, C.c_int, C.POINTER(Tuning),
                                       _dp, _dp, _dp, _dp, _ip, _ip, _ip]
     L.abyss_last_plan.argtypes = [_vp, C.POINTER(Tuning), _ip]
+    L.abyss_last_order.argtypes = [_vp, _ip]
     L.abyss_set_profiling.argtypes = [_vp, C.c_int]
     L.abyss_last_timing.argtypes = [_vp, _fp]
     L.abyss_set_tuning_table.argtypes = [_vp, C.c_int, _ip, C.POINTER(Tuning)]

@@ -803,6 +803,18 @@ int abyss_last_plan(const abyss_ctx *c, abyss_tuning *plan, int *n_chunks) {
   return ABYSS_OK;
 }
 
+int abyss_last_order(abyss_ctx *c, int *rows) {
+  if (!c || !rows) return ABYSS_ERR_ARG;
+  if (!c->launched) return fail(c, ABYSS_ERR_STATE, "last_order: nothing launched");
+  cudaSetDevice(c->device);
+  const bool ordered = (c->plan.kernel == 1 || c->plan.kernel == 3) && c->plan.mode == 1;
+  D2H out;
+  CK(out.queue(c, {{rows, ordered ? c->order_o.p : c->iota.p, (size_t)c->launched_m * 4}}), "D2H order");
+  CK(ctx_wait(c), "synchronize");
+  out.finish();
+  return ABYSS_OK;
+}
+
 int abyss_set_profiling(abyss_ctx *c, int on) {
   if (!c) return ABYSS_ERR_ARG;
   c->profiling = on != 0;

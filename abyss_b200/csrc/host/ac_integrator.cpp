@@ -908,13 +908,28 @@ int finish_regular(abyss_ac *ac, const std::vector<int> &targets, std::vector<do
                    std::vector<double> &&jerk, const std::vector<double> &airr, const std::vector<double> &jirr,
                    std::vector<int> &&nnb, std::vector<int> &&lst, int cap) {
   const int m = (int)targets.size();
-  ac->st.pairs += (double)m * ac->n;
   const double t0 = now_s();
   std::vector<Pending> pend(m);
-#pragma omp parallel for schedule(dynamic, 8)
-  for (int k = 0; k < m; ++k)
-    regular_correct_one(ac, targets[k], &acc[3 * (size_t)k], &jerk[3 * (size_t)k], &airr[3 * (size_t)k],
-                        &jirr[3 * (size_t)k], &lst[(size_t)k * cap], nnb[k], pend[k]);
+  // an exception cannot leave an OpenMP loop: a failed allocation is counted
+  // and reported after it, before anything is committed
+  int failed = 0;
+#pragma omp parallel for schedule(dynamic, 8) reduction(+ : failed)
+  for (int k = 0; k < m; ++k) {
+    try {
+      regular_correct_one(ac, targets[k], &acc[3 * (size_t)k], &jerk[3 * (size_t)k], &airr[3 * (size_t)k],
+                          &jirr[3 * (size_t)k], &lst[(size_t)k * cap], nnb[k], pend[k]);
+    } catch (const std::bad_alloc &) {
+      failed++;
+    }
+  }
+  if (failed) {
+    ac->err = "regular block: host allocation failed";
+    return ABYSS_ERR_OOM;
+  }
+  // the last call's record (abyss_ac_last_regular) is copied before the commit,
+  // so that nothing after the first committed particle allocates
+  ac->last_targets = targets;
+  ac->st.pairs += (double)m * ac->n;
   // RegCudaUpdate (WorkerRoutines.cpp:124-143), committed after every corrector ran
   int bad = 0;
   for (int k = 0; k < m; ++k) {
@@ -948,7 +963,6 @@ int finish_regular(abyss_ac *ac, const std::vector<int> &targets, std::vector<do
     p.next_irr = p.cur_irr + p.tb_irr;
   }
   // the last call, for parity checks (abyss_ac_last_regular)
-  ac->last_targets = targets;
   ac->last_acc = std::move(acc);
   ac->last_jerk = std::move(jerk);
   ac->last_nnb = std::move(nnb);
@@ -1379,6 +1393,22 @@ int abyss_ac_end_block(abyss_ac *ac, const double *acc, const double *jerk, cons
   }
   set_threads(ac);
   const int m = (int)ac->block_targets.size();
+  // results from the caller are checked before anything is used: a negative
+  // count or a neighbour index outside the cluster is refused, block left open
+  for (int k = 0; k < m; ++k) {
+    if (nnb[k] < 0) {
+      ac->err = "end_block: negative neighbour count in row " + std::to_string(k);
+      return ABYSS_ERR_ARG;
+    }
+    const int q = nnb[k] < list_cap ? nnb[k] : list_cap;
+    const int *row = list + (size_t)k * list_cap;
+    for (int i = 0; i < q; ++i)
+      if (row[i] < 0 || row[i] >= ac->n) {
+        ac->err = "end_block: neighbour index " + std::to_string(row[i]) + " outside the cluster in row " +
+                  std::to_string(k);
+        return ABYSS_ERR_ARG;
+      }
+  }
   // a list that did not fit: shrink those radii, commit nothing, ask for a redo
   bool over = false;
   for (int k = 0; k < m; ++k)
@@ -1404,7 +1434,9 @@ int abyss_ac_end_block(abyss_ac *ac, const double *acc, const double *jerk, cons
     ac->err = e.what();
     rc = ABYSS_ERR_STATE;
   }
-  ac->in_block = false;
+  // an allocation failure happens before the commit: the block stays open and
+  // end_block may be called again
+  if (rc != ABYSS_ERR_OOM) ac->in_block = false;
   if (rc != ABYSS_OK) return rc;
   if (ac->next_reg_block * ac->time_step >= 1) ac->done = true;
   if (done) *done = ac->done ? 1 : 0;
@@ -1793,7 +1825,7 @@ int abyss_ac_save(const abyss_ac *ac, const char *path) {
 }
 
 int abyss_ac_load(abyss_ctx *ctx, const char *path, int threads, abyss_ac **out) {
-  if (!path || !out) return ABYSS_ERR_ARG;  // a null ctx: host-side calls only
+  if (!path || !out || threads < 0) return ABYSS_ERR_ARG;  // a null ctx: host-side calls only
   std::ifstream f(path, std::ios::binary);
   if (!f) return ABYSS_ERR_ARG;
   char magic[8];
@@ -1831,6 +1863,17 @@ int load_body(std::ifstream &f, abyss_ctx *ctx, int n, int threads, abyss_ac **o
             get(f, ac->time_step) && get(f, ac->next_reg_block) && get(f, done) && get(f, ac->st);
   ac->done = done != 0;
   ac->p.threads = threads;
+  // header fields in the range the integrator produces (abyss_ac_create's
+  // parameter rule; block times of 2^time_block with time_block in [-62, -1]),
+  // so that a damaged file cannot size buffers or shift block counts out of range
+  const abyss_ac_params &q = ac->p;
+  if (ok)
+    ok = q.nb_max > 0 && q.nb_max <= (1 << 20) && q.fix_nb > 0 && q.fix_nb < q.nb_max && q.t_end > 0 &&
+         std::isfinite(q.t_end) && q.eta_reg > 0 && q.eta_irr > 0 && q.eps2 >= 0 && std::isfinite(q.eps2) &&
+         ac->scale > 0 && std::isfinite(ac->scale) && ac->time_block >= -62 && ac->time_block <= -1 &&
+         ac->block_max == pow2_blocks(-ac->time_block) && ac->time_step == pow2(ac->time_block) &&
+         ac->next_reg_block <= ac->block_max;
+  const int lv_lo = ac->time_block, lv_hi = ac->time_block + 62;
   if (ok) ac->s.resize(n);
   for (int i = 0; ok && i < n; ++i) {
     Star &p = ac->s[i];
@@ -1839,6 +1882,9 @@ int load_body(std::ifstream &f, abyss_ctx *ctx, int n, int threads, abyss_ac **o
     ok = get(f, p.x) && get(f, p.v) && get(f, p.m) && get(f, p.a_tot) && get(f, p.a_reg) && get(f, p.a_irr) &&
          get(f, p.r2nb) && get(f, p.t_reg) && get(f, p.t_irr) && get(f, p.dt_reg) && get(f, p.dt_irr) &&
          get(f, u) && get(f, p.lv_reg) && get(f, p.lv_irr) && get(f, nn) && nn >= 0 && nn <= n;
+    if (ok)
+      ok = p.lv_reg >= lv_lo && p.lv_reg <= lv_hi && p.lv_irr >= lv_lo && p.lv_irr <= lv_hi && p.r2nb >= 0 &&
+           std::isfinite(p.r2nb) && std::isfinite(p.m);
     if (!ok) break;
     p.cur_reg = u[0];
     p.cur_irr = u[1];

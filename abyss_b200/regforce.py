@@ -165,6 +165,14 @@ class RegularForce:
         d["n_chunks"] = int(s.value)
         return d
 
+    def last_order(self) -> np.ndarray:
+        """Target rows in the order the last launch processed them; consecutive
+        runs of threads x ipt rows share an i-block (and, in anchor mode, the
+        anchor position of the run's first row)."""
+        rows = np.zeros(self.m, np.int32)
+        self._check(self._L.abyss_last_order(self._h, ptr(rows, _ip)))
+        return rows
+
     def set_profiling(self, on: bool):
         self._check(self._L.abyss_set_profiling(self._h, 1 if on else 0))
 

@@ -9,7 +9,7 @@ Each run reports |dE/E| between t = 0 and the end (all particles synchronised
 there), the step counts and where the time went.  ``on_block`` is called after
 every regular block with (integration, initial conditions, block count); the
 test suite uses it to re-check blocks against the FP64 oracle
-(tests/check_runs.py).
+(tests/test_runs_gpu.py).
 
     python -m abyss_b200.runs c1
 """

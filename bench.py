@@ -54,6 +54,14 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched-ensemble, serving and energy measurements after the timed region")
+    ap.add_argument("--case", type=int, nargs=2, metavar=("N", "M"),
+                    help="profiling case instead of the benchmark: one regular-force call (repeated "
+                         "--repeat times) of M evenly spaced targets of an N-particle cluster, 100 "
+                         "neighbours each, list capacity 256, eps2 = 1e-8; prints the plan")
+    ap.add_argument("--case-model", default="king", choices=["king", "plummer"],
+                    help="cluster of --case: King W0 = 6 or Plummer, seed 3")
+    ap.add_argument("--tuning", default="{}", help="--case launch shape as a JSON abyss_tuning object")
+    ap.add_argument("--repeat", type=int, default=1, help="--case calls")
     return ap.parse_args()
 
 
@@ -214,6 +222,49 @@ def cpu_reference_baseline(c, sample_targets: int, nthreads: int):
     return sample_targets * n / el / 1e9, el
 
 
+def sampled_parity(st, outs, rows: int, nthreads: int) -> dict:
+    """The timed workload's own outputs (the last e2e step, host copies) against
+    the FP64 oracle on `rows` sampled targets: lists and counts bit-exact, and
+    the force bar of the GPU tests (|da| <= 1e-6 |a| + 1e-7 A per row, jerk
+    1e-5 / 1e-6, A the sum of the regular terms' magnitudes)."""
+    import oracle
+
+    c = st.cluster
+    n = c.n
+    acc, jerk, nnb, lst = outs
+    rng = np.random.default_rng(11)
+    sel = np.unique(np.concatenate([np.linspace(0, n - 1, rows // 2).astype(np.int64),
+                                    rng.choice(n, rows - rows // 2, replace=False)]))
+    t = sel.astype(np.int32)  # m = N with targets 0..N-1: row r is target r
+    px, pv = oracle.predict(c.x, c.v, st.a0, st.a1, st.t0, st.new_time, st.time_scale)
+    t_start = time.perf_counter()
+    ref = oracle.reg_force(px, pv, c.m, c.r2nb, EPS2, t, LIST_CAP, nthreads=nthreads, with_irr=False)
+    sa, sj = oracle.reg_scale(px, pv, c.m, c.r2nb, EPS2, t, nthreads=nthreads)
+    el = time.perf_counter() - t_start
+    exact = bool(np.array_equal(nnb[sel], ref["nnb"]))
+    if exact:
+        for k, r in enumerate(sel):
+            q = min(int(ref["nnb"][k]), LIST_CAP)
+            if not np.array_equal(lst[r, :q], ref["list"][k, :q]):
+                exact = False
+                break
+    da = np.linalg.norm(acc[sel] - ref["acc_reg"], axis=1)
+    dj = np.linalg.norm(jerk[sel] - ref["jerk_reg"], axis=1)
+    na = np.linalg.norm(ref["acc_reg"], axis=1)
+    nj = np.linalg.norm(ref["jerk_reg"], axis=1)
+    use_a = float((da / (1e-6 * na + 1e-7 * sa)).max())
+    use_j = float((dj / (1e-5 * nj + 1e-6 * sj)).max())
+    return {"rows": int(len(sel)), "lists_and_counts_exact": exact,
+            "acc_rel_max": float((da / na).max()), "acc_rel_median": float(np.median(da / na)),
+            "jerk_rel_max": float((dj / nj).max()), "jerk_rel_median": float(np.median(dj / nj)),
+            "bound_use_acc": use_a, "bound_use_jerk": use_j,
+            "rows_needing_floor_acc": int(np.count_nonzero(da > 1e-6 * na)),
+            "rows_needing_floor_jerk": int(np.count_nonzero(dj > 1e-5 * nj)),
+            "pass": exact and use_a <= 1.0 and use_j <= 1.0,
+            "checker": f"FP64 oracle (oracle/liboracle.so), {el:.1f} s on {nthreads} threads",
+            "sample": f"{len(sel)} targets: evenly spaced and seeded random rows of the last e2e step"}
+
+
 def host_threads() -> int:
     try:
         return len(os.sched_getaffinity(0))
@@ -289,16 +340,15 @@ def run_reference_gpu(args, world, rank, local, pg):
 def run_ours(args, world, rank, local, pg):
     import torch
 
+    from abyss_b200 import workloads
     from abyss_b200.regforce import RegularForce
 
     n = args.n
     m = n
-    c = workload(n)
-    a0 = np.zeros((n, 3))
-    a1 = np.zeros((n, 3))
-    t0 = np.zeros(n)
-    new_time = 0.0
-    time_scale = 1.0
+    st = workloads.kernel_sweep_state(n)
+    c = st.cluster
+    a0, a1, t0 = st.a0, st.a1, st.t0
+    new_time, time_scale = st.new_time, st.time_scale
     targets = np.arange(m, dtype=np.int32)
     rf = RegularForce(local)
     stream = torch.cuda.ExternalStream(rf.stream, device=torch.device("cuda", local))
@@ -386,9 +436,7 @@ def run_ours(args, world, rank, local, pg):
     # sweep of active-block sizes (same j-set), device-resident, kernel only
     sweep = {}
     if not args.no_sweep:
-        rng = np.random.default_rng(0)
-        for mm in (1, 32, 1024, 32768):
-            t = np.sort(rng.choice(n, mm, replace=False)).astype(np.int32)
+        for mm, t in workloads.sweep_targets(n).items():
             rf.set_targets(t)
             rf.predict(new_time, time_scale)
             for _ in range(3):
@@ -450,6 +498,8 @@ def run_ours(args, world, rank, local, pg):
             kind, what = "port", "FP64 restatement of ComputeAcceleration.cpp:235-299"
         line["cpu_baseline"] = {"value": v, "unit": "Gpairs/s", "cores": threads, "kind": kind,
                                 "sample": f"{sample} evenly spaced targets x all {n} j ({el:.1f} s, {what})"}
+        # the same CPU leg checks the timed step's outputs on sampled rows
+        line["parity"] = sampled_parity(st, (out_acc, out_jerk, out_nnb, out_list), 512, threads)
     if rank == 0 and world == 1 and not args.no_extras:
         line["extras"] = extras(local)
     if rank == 0:
@@ -499,8 +549,32 @@ def extras(device: int) -> dict:
     return out
 
 
+def run_case(args):
+    """One regular-force call shape for a profiler capture: the plan it ran and
+    the mean neighbour count, so that a capture can be tied to its shape."""
+    from abyss_b200 import ic
+    from abyss_b200.regforce import RegularForce
+
+    n, m = args.case
+    c = ic.king(n, 3, 6.0, k_nb=K_NB) if args.case_model == "king" else ic.plummer(n, 3, k_nb=K_NB)
+    rf = RegularForce(0)
+    try:
+        rf.send_to_device(c.m, c.x, c.v, c.r2nb)
+        t = np.arange(0, n, max(1, n // m), dtype=np.int32)[:m]
+        tu = json.loads(args.tuning)
+        for _ in range(args.repeat):
+            res = rf.calculate_acceleration(t, eps2=EPS2, list_cap=LIST_CAP, tuning=tu)
+        print(json.dumps({"case": f"{args.case_model} n={n} m={len(t)}", "plan": res.plan,
+                          "mean_nnb": float(res.nnb.mean())}), flush=True)
+    finally:
+        rf.close()
+
+
 def main():
     args = parse()
+    if args.case:
+        run_case(args)
+        return
     world, rank, local, pg = dist_setup(args)
     try:
         if args.impl == "reference":

@@ -120,6 +120,13 @@ int abyss_regular_force(abyss_ctx *ctx, int m, const int *targets, double eps2, 
 
 /* The shape the last abyss_launch used (after auto selection) and its j-chunk count. */
 int abyss_last_plan(const abyss_ctx *ctx, abyss_tuning *plan, int *n_chunks);
+/* The order in which the last launch processed its targets: rows[s] is the
+ * target row (index into the targets of abyss_set_targets) in processing slot
+ * s, m entries.  Consecutive slots share an i-block of threads x ipt targets;
+ * in anchor mode the slots follow the targets' Morton order and each i-block's
+ * offsets are taken from its first slot's position.  Identity otherwise.
+ * Synchronizes the stream.  No reference counterpart (diagnostics). */
+int abyss_last_order(abyss_ctx *ctx, int *rows);
 /* Time each phase of subsequent launches with CUDA events on the context stream. */
 int abyss_set_profiling(abyss_ctx *ctx, int on);
 /* Milliseconds of the last profiled launch: [0] target ordering, [1] force

@@ -21,6 +21,7 @@ Calls that need the GPU raise instead of touching a device.
 import hashlib
 import os
 
+import numpy as np
 import pytest
 
 from abyss_b200 import _lib
@@ -161,8 +162,63 @@ def test_damaged_checkpoints_are_refused(tmp_path):
     assert n == 1024
     for name, bad_n in (("n_huge", 2**31 - 1), ("n_plus", n + 1), ("n_one", 1)):
         cases[name] = data[:16] + bad_n.to_bytes(4, "little") + data[20:]
+    # header and particle fields outside the range the integrator produces:
+    # params at byte 20 (nb_max at 48), time_block at 76, particle 0's record
+    # at 188 with its regular level at 188 + 432
+    import struct
+
+    assert struct.unpack_from("<i", data, 48)[0] == 320 and struct.unpack_from("<i", data, 76)[0] == -45
+    assert struct.unpack_from("<ii", data, 620) == (-7, -9)
+
+    def patch(off, fmt, val):
+        b = bytearray(data)
+        struct.pack_into(fmt, b, off, val)
+        return bytes(b)
+
+    cases["nb_max_zero"] = patch(48, "<i", 0)
+    cases["nb_max_huge"] = patch(48, "<i", 2**30)
+    cases["time_block_positive"] = patch(76, "<i", 5)
+    cases["time_block_low"] = patch(76, "<i", -4000)
+    cases["level_huge"] = patch(620, "<i", 10**6)
+    cases["level_below_block"] = patch(624, "<i", -46)
     for name, blob in cases.items():
         p = tmp_path / (name + ".ckpt")
         p.write_bytes(blob)
         with pytest.raises(_lib.AbyssError):
             ACIntegrator.load(None, str(p))
+
+
+def test_end_block_refuses_bad_results_and_stays_open():
+    """A negative neighbour count or a neighbour index outside the cluster is
+    refused (ABYSS_ERR_ARG) before anything is used; the block stays open, and
+    the correct results then commit to the state of an undisturbed run."""
+    import oracle
+
+    want = None
+    ac = _load(2)
+    try:
+        assert run_blocks_with_oracle(ac, 1) == 1
+        want = _digest(ac)
+    finally:
+        ac.close()
+    ac = _load(2)
+    try:
+        targets, new_time, scale = ac.begin_block()
+        st = ac.block_state()
+        px, pv = oracle.predict(st["x"], st["v"], st["a0"], st["a1"], st["t0"], new_time, scale)
+        ref = oracle.reg_force(px, pv, st["mass"], st["r2nb"], ac.params.eps2, targets, ac.nb_max)
+        args = [ref[k] for k in ("acc_reg", "jerk_reg", "acc_irr", "jerk_irr")]
+        bad_nnb = ref["nnb"].copy()
+        bad_nnb[len(bad_nnb) // 2] = -3
+        with pytest.raises(_lib.AbyssError):
+            ac.end_block(*args, bad_nnb, ref["list"])
+        r = int(np.argmax(ref["nnb"]))
+        for bad in (-1, ac.n, 2**31 - 1):
+            lst = ref["list"].copy()
+            lst[r, ref["nnb"][r] - 1] = bad
+            with pytest.raises(_lib.AbyssError):
+                ac.end_block(*args, ref["nnb"], lst)
+        assert ac.end_block(*args, ref["nnb"], ref["list"]) in ("ok", "done")
+        assert _digest(ac) == want
+    finally:
+        ac.close()

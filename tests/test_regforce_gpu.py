@@ -19,13 +19,9 @@ import pytest
 import oracle
 from abyss_b200 import ic
 from abyss_b200.regforce import RegularForce
-from tests.helpers import first_list_mismatch, golden, lists_equal, row_rel_err
+from tests.helpers import ACC_TOL, IRR_TOL, JERK_TOL, check_force, golden, lists_equal, row_rel_err
 
 pytestmark = pytest.mark.gpu
-
-ACC_TOL = 1e-6
-JERK_TOL = 1e-5
-IRR_TOL = 1e-12
 
 TILE_DS = dict(kernel=1, mode=2)
 TILE_ANCHOR = dict(kernel=1, mode=1)
@@ -59,30 +55,7 @@ def rf():
 def check(res, ref, tag, scale, acc_tol=ACC_TOL, jerk_tol=JERK_TOL):
     """Lists exact; forces within the bar in the module docstring.  `scale` is
     (A, J): per-target sums of the magnitudes of the regular acc / jerk terms."""
-    mm = first_list_mismatch(res.nnb, res.list, ref["nnb"], ref["list"])
-    assert mm is None, f"{tag}: list mismatch at row {mm}"
-    da = np.linalg.norm(res.acc_reg - ref["acc_reg"], axis=1)
-    dj = np.linalg.norm(res.jerk_reg - ref["jerk_reg"], axis=1)
-    na = np.linalg.norm(ref["acc_reg"], axis=1)
-    nj = np.linalg.norm(ref["jerk_reg"], axis=1)
-    ea = da / np.maximum(acc_tol * na + 0.1 * acc_tol * scale[0], 1e-300)
-    ej = dj / np.maximum(jerk_tol * nj + 0.1 * jerk_tol * scale[1], 1e-300)
-    rel_a = row_rel_err(res.acc_reg, ref["acc_reg"])
-    rel_j = row_rel_err(res.jerk_reg, ref["jerk_reg"])
-    norm_a = np.linalg.norm(da) / max(np.linalg.norm(na), 1e-300)
-    norm_j = np.linalg.norm(dj) / max(np.linalg.norm(nj), 1e-300)
-    print(f"{tag}: rel acc max {rel_a.max():.2e} med {np.median(rel_a):.2e} norm {norm_a:.2e} | "
-          f"jerk max {rel_j.max():.2e} med {np.median(rel_j):.2e} norm {norm_j:.2e} | "
-          f"bound use acc {ea.max():.2f} jerk {ej.max():.2f} | plan {res.plan}")
-    assert ea.max() <= 1.0, f"{tag}: acc error {ea.max():.2f} x the bound"
-    assert ej.max() <= 1.0, f"{tag}: jerk error {ej.max():.2f} x the bound"
-    if na.size > 16:
-        assert norm_a <= acc_tol and norm_j <= jerk_tol, f"{tag}: norm-wise {norm_a:.2e} {norm_j:.2e}"
-    has = ref["nnb"] > 0
-    if has.any():
-        ei = row_rel_err(res.acc_irr[has], ref["acc_irr"][has])
-        eij = row_rel_err(res.jerk_irr[has], ref["jerk_irr"][has])
-        assert ei.max() <= IRR_TOL and eij.max() <= IRR_TOL, f"{tag}: irregular {ei.max()} {eij.max()}"
+    return check_force(res, ref, tag, scale, acc_tol, jerk_tol)
 
 
 @pytest.mark.parametrize("name", ["ref_plummer1024_s1.npz", "ref_king2048_s3.npz"])

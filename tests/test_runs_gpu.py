@@ -1,33 +1,27 @@
-"""The single-cluster integrations of abyss_b200.runs with their regular blocks
-re-checked against the FP64 oracle (needs a CUDA GPU).
+"""Configuration 1 integrated to its end on the GPU, with regular blocks
+re-checked against the FP64 oracle.
 
-    python tests/check_runs.py c1 --check-every 5
-
-Every k-th regular block is recomputed by the oracle on the same predicted
-j-set: the lists must be identical, and the worst per-target force error is
-reported in units of the test bound (|da| <= 1e-6 |a| + 1e-7 A for the
-acceleration, 1e-5 and 1e-6 for the jerk, A the sum of the term magnitudes).
+Plummer N = 1024 (seed 1, equal masses), eps = 1e-4, ~32 neighbours, eta_reg =
+0.02, eta_irr = 0.01, to t = 10 (abyss_b200.runs "c1").  Every 5th regular
+block is recomputed by the oracle on the same predicted j-set: lists and
+counts identical, and per-target force errors within the bound of
+tests/test_regforce_gpu.py (|da| <= 1e-6 |a| + 1e-7 A; jerk 1e-5 and 1e-6;
+A the sum of the term magnitudes).  The run's |dE/E| is printed.
 """
-import argparse
-import json
-import os
-import sys
-
 import numpy as np
+import pytest
 
-ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-if ROOT not in sys.path:
-    sys.path.insert(0, ROOT)
+import oracle
+from abyss_b200 import runs
 
-import oracle  # noqa: E402
-from abyss_b200 import runs  # noqa: E402
+pytestmark = pytest.mark.gpu
 
 
 def block_checker(every: int, sample_targets: int = 256):
     checks = dict(blocks_checked=0, list_mismatches=0, worst_acc=0.0, worst_jerk=0.0)
 
     def on_block(ac, c, blocks):
-        if every <= 0 or blocks % every:
+        if blocks % every:
             return
         last = ac.last_regular()
         t = last["targets"]
@@ -52,18 +46,11 @@ def block_checker(every: int, sample_targets: int = 256):
     return on_block, checks
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("config", choices=sorted(runs.CONFIGS))
-    ap.add_argument("--check-every", type=int, default=5)
-    ap.add_argument("--threads", type=int, default=0)
-    ap.add_argument("--t-stop", type=float, default=1.0)
-    args = ap.parse_args()
-    on_block, checks = block_checker(args.check_every)
-    out = runs.run(args.config, threads=args.threads, t_stop=args.t_stop, on_block=on_block)
-    out["oracle_checks"] = checks
-    print(json.dumps(out))
-
-
-if __name__ == "__main__":
-    main()
+def test_configuration1_to_the_end_every_5th_block_against_oracle():
+    on_block, checks = block_checker(5)
+    out = runs.run("c1", on_block=on_block)
+    print(f"c1: {out['stats']['blocks']} blocks, |dE/E| = {out['dE_over_E']:.3e}, oracle checks {checks}")
+    assert out["code_time"] >= 1.0
+    assert checks["blocks_checked"] >= 100
+    assert checks["list_mismatches"] == 0
+    assert checks["worst_acc"] <= 1.0 and checks["worst_jerk"] <= 1.0
