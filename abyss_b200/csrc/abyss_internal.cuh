@@ -70,6 +70,9 @@ struct Work {
   const int *row_nchunks;    // chunks per row (else n_chunks)
   const int *row_joff;       // first particle of the row's cluster (lists are cluster-local)
   const int *row_jlen;       // particles of the row's cluster (else js.n)
+  // anchor mode of a single cluster: per i-block anchor (x, y, z); null = the
+  // block's first target
+  const double *anchor = nullptr;
 };
 
 struct Outputs {

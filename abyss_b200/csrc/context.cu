@@ -108,6 +108,7 @@ struct abyss_ctx {
   int m = 0;
   DevBuf<int> targets, order_t, order_o, iota, rows, rows_alt, bbox;
   DevBuf<uint32_t> keys, keys_alt;
+  DevBuf<double> anchor;  // anchor mode: [i-blocks][3] bounding-box centres
   DevBuf<char> cub_tmp;
   size_t cub_bytes = 0;
   // per-launch work and outputs
@@ -365,7 +366,7 @@ int abyss_destroy(abyss_ctx *c) {
   if (!c) return ABYSS_ERR_ARG;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
-  DevBuf<double> *dbl[] = {&c->x, &c->v, &c->a0, &c->a1, &c->t0, &c->mass, &c->r2nb, &c->px, &c->py,
+  DevBuf<double> *dbl[] = {&c->anchor, &c->x, &c->v, &c->a0, &c->a1, &c->t0, &c->mass, &c->r2nb, &c->px, &c->py,
                            &c->pz, &c->pvx, &c->pvy, &c->pvz, &c->part, &c->acc_reg, &c->jerk_reg,
                            &c->acc_irr, &c->jerk_irr, &c->e_x, &c->e_v, &c->e_m, &c->e_row,
                            &c->i_a0, &c->i_a1, &c->i_r2, &c->i_out};
@@ -566,7 +567,7 @@ static abyss_tuning plan_for(abyss_ctx *c, int m, const abyss_tuning *user) {
   // Built-in rule (measured on B200, King W0=6, N = 2^20): lanes over j for
   // tiny active sets; one target per thread on the scalar tile kernel, in
   // blocks of 32, 64 or 128 threads, up to 128 targets; otherwise the packed
-  // tile kernel, with anchor offsets on Morton-ordered targets once the active
+  // tile kernel, with anchor offsets on Hilbert-ordered targets once the active
   // set is dense enough for them to be accurate, double-single offsets below
   // that.
   if (t.kernel == 0) {
@@ -704,14 +705,17 @@ int abyss_launch(abyss_ctx *c, double eps2, int list_cap, const abyss_tuning *tu
       CK(c->rows.ensure(m), "alloc rows");
       CK(c->rows_alt.ensure(m), "alloc rows");
       CK(c->bbox.ensure(6), "alloc bbox");
-      c->cub_bytes = morton_temp_bytes((int)c->keys.cap);
+      c->cub_bytes = sort_temp_bytes((int)c->keys.cap);
       CK(c->cub_tmp.ensure(c->cub_bytes), "alloc sort scratch");
     }
-    launch_morton_order(c->stream, m, c->targets.p, js, c->bbox.p, c->keys.p, c->keys_alt.p,
-                        c->rows.p, c->rows_alt.p, c->cub_tmp.p, c->cub_bytes, c->order_t.p,
-                        c->order_o.p, c->sm_count);
+    const int per_block = t.threads * t.ipt;
+    CK(c->anchor.ensure((size_t)3 * n_iblocks), "alloc anchors");
+    launch_spatial_order(c->stream, m, c->targets.p, js, c->bbox.p, c->keys.p, c->keys_alt.p, c->rows.p,
+                         c->rows_alt.p, c->cub_tmp.p, c->cub_bytes, c->order_t.p, c->order_o.p, per_block,
+                         c->anchor.p, c->sm_count);
     w.order_t = c->order_t.p;
     w.order_o = c->order_o.p;
+    w.anchor = c->anchor.p;
   } else {
     w.order_t = c->targets.p;
     w.order_o = c->iota.p;

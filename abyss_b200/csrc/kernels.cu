@@ -1,7 +1,8 @@
 // sm_100a kernels of the Ahmad-Cohen regular-force path.
 //
 //   predict_jset      device-side j prediction (UpdateParticle.cpp:37-59), FP64
-//   target_bbox/morton  spatial ordering of targets for the anchor mode
+//   target_bbox/curve_key/block_anchor  spatial ordering of targets and the
+//                       i-block anchors of the anchor mode
 //   reg_force_tile    i in registers, j-tiles through shared memory by TMA bulk
 //                     copies, FP32 pair arithmetic with Kahan-folded tile sums,
 //                     guarded FP32 neighbour test re-decided in FP64
@@ -23,6 +24,7 @@
 
 #include "abyss_internal.cuh"
 #include "kernels.cuh"
+#include "curve.cuh"
 
 namespace abyss {
 
@@ -185,19 +187,11 @@ __global__ void target_bbox(int m, const int *__restrict__ targets, const double
   }
 }
 
-__device__ __forceinline__ uint32_t spread10(uint32_t v) {
-  v &= 0x3ffu;
-  v = (v | (v << 16)) & 0x030000ffu;
-  v = (v | (v << 8)) & 0x0300f00fu;
-  v = (v | (v << 4)) & 0x030c30c3u;
-  v = (v | (v << 2)) & 0x09249249u;
-  return v;
-}
-
-__global__ void target_morton(int m, const int *__restrict__ targets, const double *__restrict__ px,
-                              const double *__restrict__ py, const double *__restrict__ pz,
-                              const int *__restrict__ bbox, uint32_t *__restrict__ keys,
-                              int *__restrict__ rows) {
+// Hilbert key of each target on a 1024^3 grid over the targets' FP32 bounding box.
+__global__ void target_curve_key(int m, const int *__restrict__ targets, const double *__restrict__ px,
+                                 const double *__restrict__ py, const double *__restrict__ pz,
+                                 const int *__restrict__ bbox, uint32_t *__restrict__ keys,
+                                 int *__restrict__ rows) {
   const float lo[3] = {from_ordered(bbox[0]), from_ordered(bbox[1]), from_ordered(bbox[2])};
   const float hi[3] = {from_ordered(bbox[3]), from_ordered(bbox[4]), from_ordered(bbox[5])};
   float sc[3];
@@ -213,8 +207,44 @@ __global__ void target_morton(int m, const int *__restrict__ targets, const doub
       f = fminf(fmaxf(f, 0.0f), 1023.0f);
       q[d] = (uint32_t)f;
     }
-    keys[s] = (spread10(q[0]) << 2) | (spread10(q[1]) << 1) | spread10(q[2]);
+    keys[s] = hilbert_key10(q[0], q[1], q[2]);
     rows[s] = s;
+  }
+}
+
+// Anchor of each i-block of `per_block` consecutive slots of the processing
+// order: the centre of the block's FP64 bounding box, so that no target of the
+// block is further from it than half the block's extent per axis.  One warp
+// per block; min/max are exact, so the anchor does not depend on the order of
+// the reduction.
+__global__ void block_anchor(int m, int per_block, const int *__restrict__ order_t,
+                             const double *__restrict__ px, const double *__restrict__ py,
+                             const double *__restrict__ pz, double *__restrict__ anchor) {
+  const int lane = threadIdx.x & 31;
+  const int nblk = (m + per_block - 1) / per_block;
+  for (int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < nblk; b += (gridDim.x * blockDim.x) >> 5) {
+    const int s0 = b * per_block, s1 = min(m, s0 + per_block);
+    double lo[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, hi[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+    for (int s = s0 + lane; s < s1; s += 32) {
+      const int t = order_t[s];
+      const double c[3] = {px[t], py[t], pz[t]};
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        lo[d] = fmin(lo[d], c[d]);
+        hi[d] = fmax(hi[d], c[d]);
+      }
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+      for (int o = 16; o > 0; o >>= 1) {
+        lo[d] = fmin(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
+        hi[d] = fmax(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
+      }
+    if (lane < 3) {
+      const double l = lane == 0 ? lo[0] : lane == 1 ? lo[1] : lo[2];
+      const double h = lane == 0 ? hi[0] : lane == 1 ? hi[1] : hi[2];
+      anchor[3 * (size_t)b + lane] = __dadd_rn(l, __dmul_rn(0.5, __dsub_rn(h, l)));
+    }
   }
 }
 
@@ -505,10 +535,17 @@ __global__ void __launch_bounds__(NT, MINB) reg_force_tile(JSet js, Work w, int 
     // ---- targets of this block into registers (coordinates) and shared memory (indices)
     double ax = 0.0, ay = 0.0, az = 0.0;
     if (ANCHOR) {
-      const int t0 = w.order_t[base];
-      ax = js.px[t0];
-      ay = js.py[t0];
-      az = js.pz[t0];
+      if (w.anchor && !w.items) {  // the i-block's bounding-box centre
+        const double *a = w.anchor + 3 * (size_t)(base / (NT * IPT));
+        ax = a[0];
+        ay = a[1];
+        az = a[2];
+      } else {  // the block's first target
+        const int t0 = w.order_t[base];
+        ax = js.px[t0];
+        ay = js.py[t0];
+        az = js.pz[t0];
+      }
     }
     // scalar layout: [k]; packed layout: [k/2].{x,y}; coordinates held negated
     float hx[IPT], hy[IPT], hz[IPT], lx[IPT], ly[IPT], lz[IPT], vx[IPT], vy[IPT], vz[IPT], r2g[IPT];
@@ -1297,25 +1334,30 @@ void launch_iota(cudaStream_t s, int m, int *out, int sm_count) {
   iota_kernel<<<max(1, min((m + 255) / 256, sm_count * 8)), 256, 0, s>>>(m, out);
 }
 
-size_t morton_temp_bytes(int m_cap) {
+size_t sort_temp_bytes(int m_cap) {
   size_t bytes = 0;
   cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const uint32_t *)nullptr, (uint32_t *)nullptr,
                                   (const int *)nullptr, (int *)nullptr, m_cap, 0, 30);
   return bytes;
 }
 
-void launch_morton_order(cudaStream_t s, int m, const int *targets, const JSet &js, int *bbox,
-                         uint32_t *keys, uint32_t *keys_alt, int *rows, int *rows_alt,
-                         void *cub_tmp, size_t cub_bytes, int *order_t, int *order_o,
-                         int sm_count) {
+void launch_spatial_order(cudaStream_t s, int m, const int *targets, const JSet &js, int *bbox,
+                          uint32_t *keys, uint32_t *keys_alt, int *rows, int *rows_alt, void *cub_tmp,
+                          size_t cub_bytes, int *order_t, int *order_o, int per_block, double *anchor,
+                          int sm_count) {
   const int init[6] = {INT_MAX, INT_MAX, INT_MAX, INT_MIN, INT_MIN, INT_MIN};
   cudaMemcpyAsync(bbox, init, sizeof(init), cudaMemcpyHostToDevice, s);
   const int blocks = max(1, min((m + 255) / 256, sm_count * 4));
   target_bbox<<<blocks, 256, 0, s>>>(m, targets, js.px, js.py, js.pz, bbox);
-  target_morton<<<blocks, 256, 0, s>>>(m, targets, js.px, js.py, js.pz, bbox, keys, rows);
+  target_curve_key<<<blocks, 256, 0, s>>>(m, targets, js.px, js.py, js.pz, bbox, keys, rows);
   size_t bytes = cub_bytes;
   cub::DeviceRadixSort::SortPairs(cub_tmp, bytes, keys, keys_alt, rows, rows_alt, m, 0, 30, s);
   gather_order<<<blocks, 256, 0, s>>>(m, targets, rows_alt, order_t, order_o);
+  if (anchor) {
+    const int nblk = (m + per_block - 1) / per_block;
+    const int ablocks = max(1, min((nblk + 7) / 8, sm_count * 4));
+    block_anchor<<<ablocks, 256, 0, s>>>(m, per_block, order_t, js.px, js.py, js.pz, anchor);
+  }
 }
 
 // ------------------------------------------------------------------ tile variants

@@ -18,10 +18,14 @@ void launch_unpack_predicted(cudaStream_t s, int n, const double *pos, const dou
                              const double *mass, double *px, double *py, double *pz, double *pvx,
                              double *pvy, double *pvz, float4 *vm, int sm_count);
 void launch_iota(cudaStream_t s, int m, int *out, int sm_count);
-size_t morton_temp_bytes(int m_cap);
-void launch_morton_order(cudaStream_t s, int m, const int *targets, const JSet &js, int *bbox,
-                         uint32_t *keys, uint32_t *keys_alt, int *rows, int *rows_alt,
-                         void *cub_tmp, size_t cub_bytes, int *order_t, int *order_o, int sm_count);
+size_t sort_temp_bytes(int m_cap);
+// Spatial order of the targets (Hilbert key of their positions, stable radix
+// sort) into order_t/order_o; with `anchor`, also the bounding-box centre of
+// every i-block of per_block consecutive slots ([nblk][3] doubles).
+void launch_spatial_order(cudaStream_t s, int m, const int *targets, const JSet &js, int *bbox,
+                          uint32_t *keys, uint32_t *keys_alt, int *rows, int *rows_alt, void *cub_tmp,
+                          size_t cub_bytes, int *order_t, int *order_o, int per_block, double *anchor,
+                          int sm_count);
 int tile_occupancy(int nt, int ipt, bool anchor, bool pack, int unr, int minb);
 int launch_tile(cudaStream_t s, int nt, int ipt, bool anchor, bool pack, int unr, int minb, int grid,
                 const JSet &js, const Work &w, int n_iblocks);

@@ -167,10 +167,11 @@ def captured_traffic(n, m, plan):
 
 def launches_per_step(plan) -> int:
     """Kernels one device step launches (all compiled into libabyss_reg.so):
-    predict_jset; for anchor offsets the Morton ordering (target_bbox,
-    target_morton, CUB radix sort: histogram, exclusive sum, 4 onesweep passes,
-    gather_order); the force kernel; finalize_rows and relist_rows."""
-    order = 9 if plan.get("mode") == 1 and plan.get("kernel") in (1, 3) else 0
+    predict_jset; for anchor offsets the spatial ordering (target_bbox,
+    target_curve_key, CUB radix sort: histogram, exclusive sum, 4 onesweep
+    passes, gather_order, block_anchor); the force kernel; finalize_rows and
+    relist_rows."""
+    order = 10 if plan.get("mode") == 1 and plan.get("kernel") in (1, 3) else 0
     return 1 + order + 1 + 2
 
 

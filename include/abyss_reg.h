@@ -123,8 +123,9 @@ int abyss_last_plan(const abyss_ctx *ctx, abyss_tuning *plan, int *n_chunks);
 /* The order in which the last launch processed its targets: rows[s] is the
  * target row (index into the targets of abyss_set_targets) in processing slot
  * s, m entries.  Consecutive slots share an i-block of threads x ipt targets;
- * in anchor mode the slots follow the targets' Morton order and each i-block's
- * offsets are taken from its first slot's position.  Identity otherwise.
+ * in anchor mode the slots follow the targets' Hilbert-curve order and each
+ * i-block's offsets are taken from the centre of its targets' bounding box.
+ * Identity otherwise.
  * Synchronizes the stream.  No reference counterpart (diagnostics). */
 int abyss_last_order(abyss_ctx *ctx, int *rows);
 /* Time each phase of subsequent launches with CUDA events on the context stream. */

@@ -12,11 +12,12 @@ the CPU (bit-identical to the device predictor) and checks:
   * m <= 1024: every row;
   * m = 32768 and m = N: 512 random rows plus every row of the i-blocks whose
     anchor offsets are least accurate.  In anchor mode (the default for
-    m >= 16384) a block's FP32 offsets are taken relative to its first target,
-    so their error grows with the block's spread -- the largest distance of a
-    block's target from that anchor -- relative to the targets' neighbour
-    radius; the blocks with the largest spread / R_nb and the largest spread
-    are checked whole.
+    m >= 16384) targets are ordered along a Hilbert curve and a block's FP32
+    offsets are taken relative to the centre of its bounding box, so their
+    error grows with the block's spread -- the largest distance of a block's
+    target from that anchor -- relative to the targets' neighbour radius; the
+    blocks with the largest spread / R_nb and the largest spread are checked
+    whole.
 
 Bar: the one of tests/test_regforce_gpu.py (lists and counts bit-exact; per
 row |da| <= 1e-6 |a| + 1e-7 A, jerk 1e-5 / 1e-6; norm-wise 1e-6 / 1e-5;
@@ -59,7 +60,8 @@ def widest_blocks(order_rows, targets, px, r2nb, per_block, k):
     spread = np.zeros(nb)
     for b in range(nb):
         s = slots[b * per_block:(b + 1) * per_block]
-        d = np.abs(px[s] - px[s[0]]).max(axis=1)
+        lo, hi = px[s].min(axis=0), px[s].max(axis=0)
+        d = np.abs(px[s] - (lo + 0.5 * (hi - lo))).max(axis=1)
         spread[b] = d.max()
         rel[b] = (d.max() / np.sqrt(r2nb[s])).max()
     pick = list(np.argsort(rel)[-k:]) + [int(np.argmax(spread))]
@@ -109,3 +111,23 @@ def test_full_block_default_plan(sweep):
     plan, stats = run_case(rf, c, px, pv, np.arange(N, dtype=np.int32), sample_all=False)
     assert plan["kernel"] == 3 and plan["mode"] == 1, plan
     assert stats["rows"] >= 512
+
+
+def test_anchor_order_is_the_hilbert_order(sweep):
+    """The device's processing order for anchor offsets is the stable sort of
+    the targets' Hilbert keys on a 1024^3 grid over their FP32 bounding box,
+    restated here on the CPU with the kernel's FP32 quantisation."""
+    from tests.test_curve_key import numpy_hilbert
+
+    rf, c, px, pv = sweep
+    targets = workloads.sweep_targets(N)[32768]
+    rf.set_targets(targets)
+    rf.launch(EPS2, LIST_CAP)
+    rf.fetch(LIST_CAP)
+    order = rf.last_order()
+    p = px[targets].astype(np.float32)
+    lo, hi = p.min(axis=0), p.max(axis=0)
+    sc = np.float32(1023.0) / (hi - lo)
+    q = np.clip((p - lo) * sc, np.float32(0.0), np.float32(1023.0)).astype(np.int64)
+    want = np.argsort(numpy_hilbert(q), kind="stable")
+    assert np.array_equal(order, want)

@@ -141,7 +141,7 @@ def test_no_neighbours_and_all_neighbours(rf):
     # (anchor offsets are left out: with R_nb = 0 the closest pairs enter the
     # regular sum, and anchor offsets of a spread-out block of targets are only
     # accurate for pairs wider than the block; the library picks anchor mode only
-    # for large, Morton-ordered active sets)
+    # for large active sets ordered along a Hilbert curve)
     for tu in (TILE_DS, JMAJOR, PACKED):
         res = rf.calculate_acceleration(t, 1e-8, 64, tu)
         assert res.nnb.sum() == 0
@@ -216,7 +216,8 @@ def test_bad_arguments_are_reported_not_trapped(rf):
                                                 (3, 128, 6), (3, 128, 8)])
 def test_anchor_mode_on_dense_active_set(rf, kernel, threads, ipt):
     """Anchor offsets are accurate when a block's targets are spatially compact,
-    which the library arranges by Morton-ordering large active sets."""
+    which the library arranges by ordering large active sets along a Hilbert
+    curve (blocks anchored at the centre of their bounding box)."""
     c = ic.king(65536, 17, 6.0, k_nb=80)
     t = np.arange(c.n, dtype=np.int32)
     rf.send_to_device(c.m, c.x, c.v, c.r2nb)
