@@ -158,6 +158,14 @@ def lib():
     L.abyss_ac_end_block.argtypes = [_vp, _dp, _dp, _dp, _dp, _ip, _ip, C.c_int, _ip]
     L.abyss_ac_last_error.argtypes = [_vp]
     L.abyss_ac_last_error.restype = C.c_char_p
+    L.abyss_ac_host_timers.argtypes = [_vp, _dp]
+    # irregular steps on the device (include/abyss_irr.h)
+    _ull = C.POINTER(C.c_ulonglong)
+    L.abyss_ac_set_device_irregular.argtypes = [_vp, C.c_int]
+    L.abyss_ac_device_irregular_info.argtypes = [_vp, _ip, C.POINTER(C.c_longlong), _dp, C.POINTER(C.c_longlong)]
+    L.abyss_device_irregular_steps.argtypes = ([C.c_int, C.c_int] + [_dp] * 9 + [_ip, _ip, C.c_int, C.c_double,
+                                               C.c_double, C.c_int, C.c_double, _ip, _ull, _ull, C.c_int, _ip] +
+                                               [_dp] * 4 + [_ip, _dp, _ull])
     _LIB = L
     return L
 

@@ -41,6 +41,8 @@
 #include <string>
 #include <unordered_set>
 #include <vector>
+
+#include <cuda_runtime.h>
 #ifdef _OPENMP
 #include <omp.h>
 #endif
@@ -48,8 +50,15 @@
 #include "../../../include/abyss_ac.h"
 #include "../../../include/abyss_ens.h"
 #include "../../../include/abyss_io.h"
+#include "../../../include/abyss_irr.h"
 #include "../../../include/abyss_reg.h"
+#include "../irregular.h"
 #include "pair_terms.h"
+
+struct abyss_ctx;
+namespace abyss {
+int ctx_device(abyss_ctx *c);  // context.cu
+}
 
 namespace {
 
@@ -114,6 +123,27 @@ struct abyss_ac {
   // are near it in space, are near in memory too
   std::vector<NbRec> jrec;
   std::vector<int> slot;
+  // irregular levels on the device (abyss_ac_set_device_irregular): the
+  // engine's copy of the state is current when eng_synced, except for the
+  // particles in eng_dirty (committed by the host since the last download)
+  bool dev_irr = false;
+  abyss_irr::Engine *eng = nullptr;
+  bool eng_synced = false;
+  std::vector<int> eng_dirty;
+  long long dev_borderline = 0;
+  long long dev_cycles[6] = {0, 0, 0, 0, 0, 0};
+  double dev_sec_copy = 0.0;
+  // pinned staging of the j-set uploaded for each regular block: x, v, a0, a1
+  // ([n][3] each), t0, m, r2nb ([n] each)
+  double *jstage = nullptr;
+  size_t jstage_n = 0;
+  // wall seconds outside the stats' timers: j-set fill, upload and prediction;
+  // the next-block scan
+  double sec_jset = 0.0, sec_sched = 0.0;
+  ~abyss_ac() {
+    if (eng) abyss_irr::engine_destroy(eng);
+    if (jstage) cudaFreeHost(jstage);
+  }
 };
 
 namespace {
@@ -348,9 +378,25 @@ int regular_gpu(abyss_ac *ac, const std::vector<int> &targets, bool upload_r2,
 }
 
 int upload_and_predict(abyss_ac *ac, double new_time) {
+  const double tstart = now_s();
   const int n = ac->n;
-  std::vector<double> x(3 * (size_t)n), v(3 * (size_t)n), a0(3 * (size_t)n), a1(3 * (size_t)n), t0(n),
-      m(n), r2(n);
+  const size_t N = n;
+  // the staging is pinned (plain DMA, no driver staging) and kept across blocks
+  if (ac->jstage_n != N) {
+    if (ac->jstage) cudaFreeHost(ac->jstage);
+    ac->jstage = nullptr;
+    ac->jstage_n = 0;
+    if (cudaHostAlloc((void **)&ac->jstage, sizeof(double) * 15 * N, cudaHostAllocDefault) != cudaSuccess) {
+      cudaGetLastError();
+      ac->jstage = nullptr;
+      ac->err = "upload/predict: pinned staging allocation failed";
+      return ABYSS_ERR_OOM;
+    }
+    ac->jstage_n = N;
+  }
+  double *x = ac->jstage, *v = x + 3 * N, *a0 = v + 3 * N, *a1 = a0 + 3 * N, *t0 = a1 + 3 * N, *m = t0 + N,
+         *r2 = m + N;
+#pragma omp parallel for schedule(static) if (n >= 8192)
   for (int j = 0; j < n; ++j) {
     const Star &p = ac->s[j];
     for (int d = 0; d < 3; ++d) {
@@ -364,12 +410,12 @@ int upload_and_predict(abyss_ac *ac, double new_time) {
     m[j] = p.m;
     r2[j] = p.r2nb;
   }
-  int rc = abyss_upload_state(ac->ctx, n, x.data(), v.data(), a0.data(), a1.data(), t0.data(), m.data(),
-                              r2.data());
-  ac->last_r2 = r2;
+  int rc = abyss_upload_state(ac->ctx, n, x, v, a0, a1, t0, m, r2);
+  ac->last_r2.assign(r2, r2 + N);
   if (rc == ABYSS_OK) rc = abyss_predict(ac->ctx, new_time, ac->scale);
   if (rc == ABYSS_OK) rc = abyss_synchronize(ac->ctx);
   if (rc != ABYSS_OK) ac->err = std::string("upload/predict: ") + abyss_last_error(ac->ctx);
+  ac->sec_jset += now_s() - tstart;
   return rc;
 }
 
@@ -688,7 +734,143 @@ void run_level(abyss_ac *ac, const std::vector<int> &P, std::vector<Pending> &pe
   }
 }
 
+// The integrator's fields of a particle as the device irregular phase takes
+// them; its list goes to lists[list_off ..].
+void pack_image(const abyss_ac *ac, int i, abyss_irr::Image &g, int *lists, long long list_off) {
+  const Star &p = ac->s[i];
+  for (int d = 0; d < 3; ++d) {
+    g.x[d] = p.x[d];
+    g.v[d] = p.v[d];
+  }
+  g.m = p.m;
+  g.t_irr = p.t_irr;
+  g.t_reg = p.t_reg;
+  g.dt_irr = p.dt_irr;
+  std::memcpy(g.a_tot, p.a_tot, sizeof(g.a_tot));
+  std::memcpy(g.a_reg, p.a_reg, sizeof(g.a_reg));
+  std::memcpy(g.a_irr, p.a_irr, sizeof(g.a_irr));
+  g.cur_irr = p.cur_irr;
+  g.tb_irr = p.tb_irr;
+  g.next_irr = p.next_irr;
+  g.new_cur_irr = p.new_cur_irr;
+  g.cur_reg = p.cur_reg;
+  g.tb_reg = p.tb_reg;
+  g.lv_irr = p.lv_irr;
+  g.lv_reg = p.lv_reg;
+  g.nnb = (int)p.nb.size();
+  g.index = i;
+  g.list_off = list_off;
+  if (!p.nb.empty()) std::memcpy(lists + list_off, p.nb.data(), sizeof(int) * p.nb.size());
+}
+
+// What an irregular phase changed, back into particle i's fields.
+void unpack_changed(abyss_ac *ac, int i, const abyss_irr::Changed &g) {
+  Star &p = ac->s[i];
+  for (int d = 0; d < 3; ++d) {
+    p.x[d] = g.x[d];
+    p.v[d] = g.v[d];
+  }
+  p.t_irr = g.t_irr;
+  p.dt_irr = g.dt_irr;
+  std::memcpy(p.a_tot, g.a_tot, sizeof(p.a_tot));
+  std::memcpy(p.a_irr, g.a_irr, sizeof(p.a_irr));
+  p.cur_irr = g.cur_irr;
+  p.tb_irr = g.tb_irr;
+  p.next_irr = g.next_irr;
+  p.new_cur_irr = g.new_cur_irr;
+  p.lv_irr = g.lv_irr;
+}
+
+// The irregular levels up to the next regular block on the device
+// (irregular.cu): the particles the host changed since the last call go up,
+// the level loop runs on the GPU, every particle's irregular fields come back.
+int irregular_levels_device(abyss_ac *ac) {
+  const double t0 = now_s();
+  using namespace abyss_irr;
+  int rc = ABYSS_OK;
+  if (!ac->eng) {
+    rc = engine_create(abyss::ctx_device(ac->ctx), &ac->eng);
+    if (rc != ABYSS_OK) {
+      ac->err = "device irregular steps: no engine on the context's device";
+      return rc;
+    }
+    ac->eng_synced = false;
+  }
+  const int n = ac->n, cap = ac->p.nb_max;
+  for (int i = 0; i < n; ++i)
+    if ((int)ac->s[i].nb.size() > cap) {
+      ac->err = "device irregular steps: a neighbour list longer than nb_max";
+      return ABYSS_ERR_STATE;
+    }
+  rc = engine_reserve(ac->eng, n, cap);
+  if (rc != ABYSS_OK) {
+    ac->err = engine_error(ac->eng);
+    ac->eng_synced = false;
+    return rc;
+  }
+  Image *img = engine_images(ac->eng);
+  int *lists = engine_lists(ac->eng);
+  // the particles to send: all of them, or those the host committed since
+  std::vector<int> &dirty = ac->eng_dirty;
+  if (!ac->eng_synced) {
+    dirty.resize(n);
+    for (int i = 0; i < n; ++i) dirty[i] = i;
+  } else {
+    std::sort(dirty.begin(), dirty.end());
+    dirty.erase(std::unique(dirty.begin(), dirty.end()), dirty.end());
+  }
+  const int count = (int)dirty.size();
+  std::vector<long long> off(count + 1, 0);
+  for (int k = 0; k < count; ++k) off[k + 1] = off[k] + (long long)ac->s[dirty[k]].nb.size();
+#pragma omp parallel for schedule(static) if (count >= 16384)
+  for (int k = 0; k < count; ++k) pack_image(ac, dirty[k], img[k], lists, off[k]);
+  rc = engine_upload(ac->eng, count, off[count]);
+  if (rc != ABYSS_OK) {
+    ac->err = engine_error(ac->eng);
+    ac->eng_synced = false;
+    return rc;
+  }
+  ac->eng_dirty.clear();
+  const double t1 = now_s();
+  Params P;
+  P.scale = ac->scale;
+  P.time_step = ac->time_step;
+  P.eps2 = ac->p.eps2;
+  P.eta_irr = ac->p.eta_irr;
+  P.ln2 = std::log(2.0);
+  P.time_block = ac->time_block;
+  P.next_reg_block = ac->next_reg_block;
+  RunStats rs;
+  const int run = engine_run_levels(ac->eng, P, &rs);
+  const double t2 = now_s();
+  // the levels committed before a failure are kept, as on the host
+  rc = engine_download(ac->eng);
+  if (rc != ABYSS_OK) {
+    ac->err = engine_error(ac->eng);
+    ac->eng_synced = false;
+    return rc;
+  }
+  const Changed *chg = engine_changed(ac->eng);
+#pragma omp parallel for schedule(static) if (n >= 16384)
+  for (int i = 0; i < n; ++i)
+    if (chg[i].touched) unpack_changed(ac, i, chg[i]);
+  ac->eng_synced = true;
+  ac->st.irr_levels += rs.levels;
+  ac->st.irr_steps += rs.steps;
+  ac->dev_borderline += rs.borderline;
+  for (int q = 0; q < 6; ++q) ac->dev_cycles[q] += rs.cycles[q];
+  const double t3 = now_s();
+  ac->dev_sec_copy += (t1 - t0) + (t3 - t2);
+  ac->st.sec_irr += t3 - t0;
+  if (run != ABYSS_OK) {
+    ac->err = engine_error(ac->eng);
+    return run;
+  }
+  return ABYSS_OK;
+}
+
 int irregular_levels(abyss_ac *ac) {
+  if (ac->dev_irr) return irregular_levels_device(ac);
   const double t0 = now_s();
 #ifdef _OPENMP
   const int nth = std::max(1, omp_get_max_threads());
@@ -927,8 +1109,10 @@ int finish_regular(abyss_ac *ac, const std::vector<int> &targets, std::vector<do
     return ABYSS_ERR_OOM;
   }
   // the last call's record (abyss_ac_last_regular) is copied before the commit,
-  // so that nothing after the first committed particle allocates
+  // so that nothing after the first committed particle allocates; so is the
+  // device irregular phase's list of particles to send up again
   ac->last_targets = targets;
+  if (ac->dev_irr) ac->eng_dirty.insert(ac->eng_dirty.end(), targets.begin(), targets.end());
   ac->st.pairs += (double)m * ac->n;
   // RegCudaUpdate (WorkerRoutines.cpp:124-143), committed after every corrector ran
   int bad = 0;
@@ -1282,10 +1466,119 @@ int abyss_ac_destroy(abyss_ac *ac) {
   return ABYSS_OK;
 }
 
+int abyss_ac_host_timers(const abyss_ac *ac, double *sec2) {
+  if (!ac || !sec2) return ABYSS_ERR_ARG;
+  sec2[0] = ac->sec_jset;
+  sec2[1] = ac->sec_sched;
+  return ABYSS_OK;
+}
+
+int abyss_ac_set_device_irregular(abyss_ac *ac, int on) {
+  if (!ac) return ABYSS_ERR_ARG;
+  if (ac->in_block) {
+    ac->err = "set_device_irregular: a split block is open";
+    return ABYSS_ERR_STATE;
+  }
+  if (on && !ac->ctx) {
+    ac->err = "set_device_irregular: the integration has no GPU context";
+    return ABYSS_ERR_STATE;
+  }
+  ac->dev_irr = on != 0;
+  ac->eng_synced = false;  // the host may have stepped particles meanwhile
+  ac->eng_dirty.clear();
+  return ABYSS_OK;
+}
+
+int abyss_ac_device_irregular_info(const abyss_ac *ac, int *on, long long *borderline, double *sec_copy,
+                                   long long *cycles6) {
+  if (!ac) return ABYSS_ERR_ARG;
+  if (on) *on = ac->dev_irr ? 1 : 0;
+  if (cycles6)
+    for (int q = 0; q < 6; ++q) cycles6[q] = ac->dev_cycles[q];
+  if (borderline) *borderline = ac->dev_borderline;
+  if (sec_copy) *sec_copy = ac->dev_sec_copy;
+  return ABYSS_OK;
+}
+
+int abyss_device_irregular_steps(int device, int n, const double *x, const double *v, const double *mass,
+                                 const double *a_tot, const double *a_reg, const double *a_irr,
+                                 const double *t_reg, const double *t_irr, const double *dt_irr,
+                                 const int *nnb, const int *nb, int nb_stride, double eps2, double scale,
+                                 int time_block, double eta_irr, const int *lv_reg,
+                                 const unsigned long long *cur_reg, const unsigned long long *tb_reg, int count,
+                                 const int *idx, double *new_pos, double *new_vel, double *a_irr_out,
+                                 double *a_tot_out, int *lv_irr_out, double *dt_irr_out,
+                                 unsigned long long *tb_irr_out) {
+  if (n <= 0 || count < 0 || nb_stride <= 0 || !x || !v || !mass || !a_tot || !a_reg || !a_irr || !t_reg ||
+      !t_irr || !dt_irr || !nnb || !lv_reg || !cur_reg || !tb_reg || time_block < -62 || time_block > -1 ||
+      (count > 0 && (!idx || !new_pos || !new_vel || !a_irr_out || !a_tot_out)))
+    return ABYSS_ERR_ARG;
+  for (int i = 0; i < n; ++i) {
+    if (nnb[i] < 0 || nnb[i] > nb_stride || (nnb[i] > 0 && !nb)) return ABYSS_ERR_ARG;
+    for (int k = 0; k < nnb[i]; ++k) {
+      const int j = nb[(size_t)i * nb_stride + k];
+      if (j < 0 || j >= n || j == i) return ABYSS_ERR_ARG;
+    }
+  }
+  for (int k = 0; k < count; ++k)
+    if (idx[k] < 0 || idx[k] >= n) return ABYSS_ERR_ARG;
+  using namespace abyss_irr;
+  Engine *e = nullptr;
+  int rc = engine_create(device, &e);
+  if (rc != ABYSS_OK) return rc;
+  std::unique_ptr<Engine, void (*)(Engine *)> hold(e, engine_destroy);
+  if ((rc = engine_reserve(e, n, nb_stride)) != ABYSS_OK) return rc;
+  Image *img = engine_images(e);
+  int *lists = engine_lists(e);
+  const double step = pow2(time_block);
+  for (int i = 0; i < n; ++i) {
+    Image &g = img[i];
+    for (int d = 0; d < 3; ++d) {
+      g.x[d] = x[3 * (size_t)i + d];
+      g.v[d] = v[3 * (size_t)i + d];
+    }
+    g.m = mass[i];
+    g.t_irr = t_irr[i];
+    g.t_reg = t_reg[i];
+    g.dt_irr = dt_irr[i];
+    std::memcpy(g.a_tot, a_tot + 12 * (size_t)i, sizeof(g.a_tot));
+    std::memcpy(g.a_reg, a_reg + 12 * (size_t)i, sizeof(g.a_reg));
+    std::memcpy(g.a_irr, a_irr + 12 * (size_t)i, sizeof(g.a_irr));
+    // block counts of times on the 2^time_block grid, the level of the step
+    g.cur_irr = (ULL)(t_irr[i] / step);
+    g.tb_irr = (ULL)(dt_irr[i] / step);
+    g.next_irr = g.cur_irr + g.tb_irr;
+    g.new_cur_irr = 0;
+    g.cur_reg = cur_reg[i];
+    g.tb_reg = tb_reg[i];
+    g.lv_irr = dt_irr[i] > 0 ? std::ilogb(dt_irr[i]) : time_block;
+    g.lv_reg = lv_reg[i];
+    g.nnb = nnb[i];
+    g.index = i;
+    g.list_off = (long long)i * nb_stride;
+    if (nnb[i] > 0) std::memcpy(lists + (size_t)i * nb_stride, nb + (size_t)i * nb_stride, sizeof(int) * nnb[i]);
+  }
+  if ((rc = engine_upload(e, n, (long long)n * nb_stride)) != ABYSS_OK) return rc;
+  Params P;
+  P.scale = scale;
+  P.time_step = step;
+  P.eps2 = eps2;
+  P.eta_irr = eta_irr;
+  P.ln2 = std::log(2.0);
+  P.time_block = time_block;
+  P.next_reg_block = 0;
+  return engine_steps(e, P, count, idx, new_pos, new_vel, a_irr_out, a_tot_out, lv_irr_out, dt_irr_out, tb_irr_out);
+}
+
 namespace {
 // updateNextRegTime (RootRoutines.cpp:1310-1338): the next regular block time
 // and its particles, in ascending index.
 std::vector<int> next_regular_block(abyss_ac *ac) {
+  struct Clock {
+    abyss_ac *ac;
+    double t0 = now_s();
+    ~Clock() { ac->sec_sched += now_s() - t0; }
+  } clock{ac};
   ULL tmin = ac->block_max;
   std::vector<int> targets;
   for (int i = 0; i < ac->n; ++i) {

@@ -127,6 +127,26 @@ class ACIntegrator:
         self._check(rc)
         return "done" if done.value else "ok"
 
+    def host_timers(self) -> dict:
+        t = np.zeros(2)
+        self._check(self._L.abyss_ac_host_timers(self._h, ptr(t)))
+        return {"sec_jset": float(t[0]), "sec_sched": float(t[1])}
+
+    def set_device_irregular(self, on: bool = True):
+        """Run the irregular levels on the GPU (include/abyss_irr.h); the
+        results are the same as on the host threads."""
+        self._check(self._L.abyss_ac_set_device_irregular(self._h, 1 if on else 0))
+
+    def device_irregular_info(self) -> dict:
+        on = C.c_int(0)
+        border = C.c_longlong(0)
+        sec = C.c_double(0.0)
+        cyc = (C.c_longlong * 6)()
+        self._check(self._L.abyss_ac_device_irregular_info(self._h, C.byref(on), C.byref(border), C.byref(sec), cyc))
+        parts = ("member_list", "unused", "steps", "barrier_after_steps", "commit", "barrier_after_commit")
+        return {"on": bool(on.value), "borderline": int(border.value), "sec_copy": float(sec.value),
+                "cycles": dict(zip(parts, [int(c) for c in cyc]))}
+
     def run(self, t_code: float = 1.0):
         self._check(self._L.abyss_ac_run(self._h, float(t_code)))
 

@@ -6,7 +6,8 @@
       mass 1, eps = 1e-4, ~64 neighbours, integrated to t = 2.
 
 Each run reports |dE/E| between t = 0 and the end (all particles synchronised
-there), the step counts and where the time went.  ``on_block`` is called after
+there), the step counts and where the time went.  The irregular levels run on
+the host threads, or with ``device_irregular`` on the GPU (the same results).  ``on_block`` is called after
 every regular block with (integration, initial conditions, block count); the
 test suite uses it to re-check blocks against the FP64 oracle
 (tests/test_runs_gpu.py).
@@ -30,13 +31,15 @@ CONFIGS = {
 EPS = 1e-4
 
 
-def run(name: str, threads: int = 0, t_stop: float = 1.0, on_block=None):
+def run(name: str, threads: int = 0, t_stop: float = 1.0, on_block=None, device_irregular: bool = False):
     cfg = CONFIGS[name]
     c = ic.plummer(cfg["n"], cfg["seed"], masses=cfg["masses"], k_nb=cfg["k_nb"])
     rf = RegularForce(0)
     t0 = time.perf_counter()
     ac = ACIntegrator(rf, c.x, c.v, c.m, c.r2nb, eps2=EPS * EPS, eta_reg=0.02, eta_irr=0.01,
                       fix_nb=cfg["k_nb"], t_end=cfg["t_end"], threads=threads)
+    if device_irregular:
+        ac.set_device_irregular(True)
     e0 = ac.energy()
     blocks = 0
     done = False
@@ -48,7 +51,10 @@ def run(name: str, threads: int = 0, t_stop: float = 1.0, on_block=None):
     wall = time.perf_counter() - t0
     e1 = ac.energy()
     out = dict(config=name, n=c.n, t_end=cfg["t_end"], code_time=ac.time, e0=e0, e1=e1,
-               dE_over_E=abs((e1 - e0) / e0), wall_s=wall, stats=ac.stats())
+               dE_over_E=abs((e1 - e0) / e0), wall_s=wall, stats=ac.stats(),
+               irregular="device" if device_irregular else "host", host_timers=ac.host_timers())
+    if device_irregular:
+        out["device_irregular"] = ac.device_irregular_info()
     ac.close()
     rf.close()
     return out
@@ -59,8 +65,10 @@ def main():
     ap.add_argument("config", choices=sorted(CONFIGS))
     ap.add_argument("--threads", type=int, default=0)
     ap.add_argument("--t-stop", type=float, default=1.0, help="stop at this code time (1 = t_end)")
+    ap.add_argument("--device-irregular", action="store_true", help="irregular levels on the GPU")
     args = ap.parse_args()
-    print(json.dumps(run(args.config, threads=args.threads, t_stop=args.t_stop)))
+    print(json.dumps(run(args.config, threads=args.threads, t_stop=args.t_stop,
+                         device_irregular=args.device_irregular)))
 
 
 if __name__ == "__main__":

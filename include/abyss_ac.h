@@ -124,6 +124,10 @@ int abyss_ac_last_regular(const abyss_ac *ac, int *m, int *targets, double *px, 
                           double *r2nb, double *acc_reg, double *jerk_reg, int *nnb, int *list,
                           int list_cap);
 const char *abyss_ac_last_error(const abyss_ac *ac);
+/* Wall seconds outside the stats' timers, summed over the run: [0] filling,
+ * uploading and predicting the j-set of each regular block, [1] finding each
+ * next regular block (updateNextRegTime, RootRoutines.cpp:1310-1338). */
+int abyss_ac_host_timers(const abyss_ac *ac, double *sec2);
 /* Particle count and parameters of an integration (either may be NULL). */
 int abyss_ac_info(const abyss_ac *ac, int *n, abyss_ac_params *p);
 
