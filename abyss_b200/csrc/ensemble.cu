@@ -83,6 +83,9 @@ struct abyss_ens {
   // (15 doubles per particle: x, v, a0, a1 [3] each, t0, mass, r2nb)
   double *stage = nullptr;
   int chunk_j = 2048;  // j per chunk of a cluster (>= 128): its chunk count is ceil(n_k / chunk_j), <= kSMax
+  // tuned chunk lengths by cluster size: the first entry with n_k <= chunk_nmax
+  // applies, else chunk_j
+  std::vector<int> chunk_nmax, chunk_len;
   // pinned host staging of a wave's description (set_wave) and of its results
   // (fetch_view), so that neither goes through pageable copies
   unsigned char *wstage = nullptr;
@@ -474,6 +477,42 @@ int abyss_ens_set_chunk(abyss_ens *e, int j_per_chunk) {
   return ABYSS_OK;
 }
 
+int abyss_ens_set_tuning(abyss_ens *e, const abyss_tuning *shape, int k, const int *n_max,
+                         const int *j_per_chunk) {
+  if (!e || k < 0 || (k > 0 && (!n_max || !j_per_chunk))) return ABYSS_ERR_ARG;
+  for (int q = 0; q < k; ++q)
+    if (j_per_chunk[q] < kTJ || n_max[q] <= 0 || (q > 0 && n_max[q] <= n_max[q - 1]))
+      return efail(e, ABYSS_ERR_ARG, "set_tuning: chunk table must rise in n_max, chunks >= 128 j");
+  if (e->busy[0] || e->busy[1]) return efail(e, ABYSS_ERR_STATE, "set_tuning: a submitted wave is not collected yet");
+  if (shape) {
+    abyss_tuning t = *shape;
+    if (t.kernel != 1 && t.kernel != 3) return efail(e, ABYSS_ERR_ARG, "set_tuning: ensemble needs a tile kernel");
+    if (t.mode == 0) t.mode = 2;
+    // a wave's clusters are not spatially ordered: anchor offsets would be inaccurate
+    if (t.mode != 2) return efail(e, ABYSS_ERR_ARG, "set_tuning: ensemble needs double-single offsets");
+    if (t.threads == 0) t.threads = 128;
+    if (t.ipt == 0) t.ipt = t.kernel == 3 ? 2 : 1;
+    // the work-list capacity assumes at least 128 targets per block
+    if (t.threads * t.ipt < 128) return efail(e, ABYSS_ERR_ARG, "set_tuning: fewer than 128 targets per block");
+    const int occ = tile_occupancy(t.threads, t.ipt, false, t.kernel == 3, t.unroll, t.min_blocks);
+    if (occ <= 0) return efail(e, ABYSS_ERR_ARG, "set_tuning: not a compiled tile shape");
+    t.j_split = 0;
+    t.grid = 0;
+    e->shape = t;
+    e->grid = occ * e->sm_count;
+  }
+  e->chunk_nmax.assign(n_max, n_max + k);
+  e->chunk_len.assign(j_per_chunk, j_per_chunk + k);
+  e->rows = 0;  // the next wave is laid out with the new shape
+  return ABYSS_OK;
+}
+
+int abyss_ens_get_shape(const abyss_ens *e, abyss_tuning *shape) {
+  if (!e || !shape) return ABYSS_ERR_ARG;
+  *shape = e->shape;
+  return ABYSS_OK;
+}
+
 int abyss_ens_stage(abyss_ens *e, int k, double **x, double **v, double **a0, double **a1, double **t0,
                     double **mass, double **r2nb) {
   if (!e || k < 0 || k >= e->nc || e->n_k[k] == 0 || !x || !v || !a0 || !a1 || !t0 || !mass || !r2nb)
@@ -603,7 +642,13 @@ int abyss_ens_set_wave(abyss_ens *e, int nk, const int *clusters, const double *
     e->h_active[k] = 1;
     e->h_time[k] = new_time[i];
     e->h_scale[k] = time_scale[i];
-    int S = std::max(1, std::min(kSMax, (nkp + e->chunk_j - 1) / e->chunk_j));
+    int cj = e->chunk_j;
+    for (size_t q = 0; q < e->chunk_nmax.size(); ++q)
+      if (nkp <= e->chunk_nmax[q]) {
+        cj = e->chunk_len[q];
+        break;
+      }
+    int S = std::max(1, std::min(kSMax, (nkp + cj - 1) / cj));
     int chunk = ((nkp + S - 1) / S + kTJ - 1) / kTJ * kTJ;
     S = (nkp + chunk - 1) / chunk;
     e->wave_rows_begin[i] = row;

@@ -115,6 +115,7 @@ struct abyss_ac {
   std::vector<int> last_targets, last_nnb, last_list;
   std::vector<double> last_px, last_pv, last_r2, last_acc, last_jerk;
   int last_cap = 0;
+  std::vector<double> reg_airr, reg_jirr;  // buffers of the regular call's FP64 irregular part
   // split form: the regular block begun and not yet ended
   bool in_block = false;
   std::vector<int> block_targets;
@@ -349,12 +350,14 @@ int regular_gpu(abyss_ac *ac, const std::vector<int> &targets, bool upload_r2,
                 std::vector<double> &jirr, std::vector<int> &nnb, std::vector<int> &lst) {
   const int m = (int)targets.size();
   const int cap = ac->p.nb_max;
-  acc.assign(3 * (size_t)m, 0);
-  jerk.assign(3 * (size_t)m, 0);
-  airr.assign(3 * (size_t)m, 0);
-  jirr.assign(3 * (size_t)m, 0);
-  nnb.assign(m, 0);
-  lst.assign((size_t)m * cap, 0);
+  // every element is written by the call below: sized, not cleared (the list
+  // alone is m x cap ints, tens of MB per block at N = 65 536)
+  acc.resize(3 * (size_t)m);
+  jerk.resize(3 * (size_t)m);
+  airr.resize(3 * (size_t)m);
+  jirr.resize(3 * (size_t)m);
+  nnb.resize(m);
+  lst.resize((size_t)m * cap);
   (void)upload_r2;
   for (int attempt = 0; attempt < 40; ++attempt) {
     int ovf = 0;
@@ -1073,8 +1076,21 @@ int finish_regular(abyss_ac *ac, const std::vector<int> &targets, std::vector<do
 
 int regular_block(abyss_ac *ac, const std::vector<int> &targets) {
   const double new_time = ac->next_reg_block * ac->time_step;
-  std::vector<double> acc, jerk, airr, jirr;
-  std::vector<int> nnb, lst;
+  // the last block's result buffers are reused (finish_regular moves this
+  // block's back into the record), so that no block allocates or clears them
+  std::vector<double> acc = std::move(ac->last_acc), jerk = std::move(ac->last_jerk), airr, jirr;
+  std::vector<int> nnb = std::move(ac->last_nnb), lst = std::move(ac->last_list);
+  ac->last_targets.clear();  // no record until this block's is complete
+  airr.swap(ac->reg_airr);
+  jirr.swap(ac->reg_jirr);
+  struct Back {  // the FP64 irregular parts' buffers go back too
+    abyss_ac *ac;
+    std::vector<double> &a, &j;
+    ~Back() {
+      ac->reg_airr.swap(a);
+      ac->reg_jirr.swap(j);
+    }
+  } back{ac, airr, jirr};
   for (int attempt = 0;; ++attempt) {
     int rc = upload_and_predict(ac, new_time);
     if (rc != ABYSS_OK) return rc;
@@ -1783,6 +1799,12 @@ int abyss_ac_last_regular(const abyss_ac *ac, int *m, int *targets, double *px, 
                           int list_cap) {
   if (!ac || !m) return ABYSS_ERR_ARG;
   const int mm = (int)ac->last_targets.size();
+  const size_t M = mm;
+  if (ac->last_acc.size() < 3 * M || ac->last_jerk.size() < 3 * M || ac->last_nnb.size() < M ||
+      ac->last_list.size() < M * (size_t)ac->last_cap) {
+    *m = 0;
+    return ABYSS_ERR_STATE;  // a block failed after taking the record's buffers
+  }
   *m = mm;
   if (px || pv) {
     int rc = abyss_read_predicted(ac->ctx, px, pv, nullptr);

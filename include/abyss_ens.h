@@ -53,6 +53,21 @@ int abyss_ens_free_particles(const abyss_ens *e);
 int abyss_ens_set_chunk(abyss_ens *e, int j_per_chunk);
 /* Neighbour-list capacity per target (the row stride of fetched lists). */
 int abyss_ens_list_cap(const abyss_ens *e);
+/* Launch shape of the ensemble's force kernel and its j-chunk length by
+ * cluster size, as an autotuner picked them (abyss_b200/autotune.py
+ * tune_ensemble).  shape: a compiled tile shape with double-single offsets
+ * (kernel 1 or 3, mode 2, at least 128 targets per block), NULL to keep the
+ * shape; k entries (n_max, j_per_chunk) in rising n_max: the first entry with
+ * n_k <= n_max sets the chunk length of a cluster of n_k particles, larger
+ * clusters take abyss_ens_set_chunk's.  Applies from the next wave.  A
+ * cluster's chunking depends on its own size only, so its results stay the
+ * same alone and in any mix.  No reference counterpart: the reference fixes
+ * BatchSize 64, GridDimY 64 and NNB_per_block 128 at compile time
+ * (src_mpi/def.h:77-79). */
+int abyss_ens_set_tuning(abyss_ens *e, const struct abyss_tuning *shape, int k, const int *n_max,
+                         const int *j_per_chunk);
+/* The launch shape in use. */
+int abyss_ens_get_shape(const abyss_ens *e, struct abyss_tuning *shape);
 /* Device bytes the ensemble holds (for admission control). */
 long long abyss_ens_device_bytes(const abyss_ens *e);
 /* Un-predicted FP64 state of cluster k, as abyss_upload_state. */
