@@ -1,6 +1,6 @@
 """Autotuner of the regular-force launch shape.
 
-For each active-set size bucket it times every compiled tile-kernel shape
+Single cluster (``tune``): for each active-set size bucket it times every compiled tile-kernel shape
 (abyss_tile_variants: threads, targets per thread, anchor or double-single
 offsets, packed FP32x2 or scalar arithmetic, j unroll, register cap) and the
 j-major kernel, over a few j-split choices, on the caller's own j-set, and keeps
@@ -8,6 +8,13 @@ the fastest shape whose offsets are accurate at that size (anchor offsets only
 from `anchor_min` targets up).  The result is a table of (m_max, shape) entries;
 ``install`` hands it to the library (abyss_set_tuning_table), ``save``/``load``
 keep it as JSON.
+
+Batched ensemble (``tune_ensemble``): on the ensemble's own waves (its
+clusters and their uneven active sets, in the CUDA-graph form) it times every
+compiled double-single tile shape with at least 128 targets per block, keeps
+the fastest, then picks the j-chunk length of each cluster-size bucket in turn
+(``Ensemble.set_tuning``).  The chunk length trades work-list parallelism
+against the FP64 chunk partials that the finalize pass sums.
 
     python -m abyss_b200.autotune --n 1048576 --out tuning.json
 """
@@ -83,6 +90,68 @@ def tune(rf: RegularForce, n: int, buckets=BUCKETS, anchor_min: int = 16384, see
         if best is not None:
             table.append((int(m), best[0], best[1]))
     return table
+
+
+ENS_CHUNKS = (512, 1024, 2048, 4096, 8192)
+ENS_BUCKETS = (1024, 4096, 16384)
+
+
+def _ensemble_ms(ens, waves, eps2: float = 1e-8, reps: int = 1) -> float:
+    """GPU milliseconds of all waves in the graph form (after one warm launch each)."""
+    from .ensemble import GRAPH
+
+    total = 0.0
+    for ks, ts in waves:
+        ens.set_wave(ks, np.zeros(len(ks)), np.ones(len(ks)), ts)
+        ens.launch(eps2, GRAPH)
+        ens.last_ms()  # waits for the wave; its rows are not needed here
+        best = float("inf")
+        for _ in range(reps):
+            ens.launch(eps2, GRAPH)
+            best = min(best, ens.last_ms())
+        total += best
+    return total
+
+
+def tune_ensemble(ens, waves, chunks=ENS_CHUNKS, buckets=ENS_BUCKETS, verbose=False):
+    """Launch shape and per-size chunk table for an Ensemble whose clusters
+    are uploaded, timed on `waves` [(clusters, targets)].  Installs the winner
+    and returns {"shape", "chunks", "ms", "default_ms", "trials"}."""
+    default_shape = ens.shape()
+    ens.set_tuning(None, ())
+    default_ms = _ensemble_ms(ens, waves)
+    trials = []
+    shapes = [sh for sh in variants() if sh["mode"] == 2 and sh["threads"] * sh["ipt"] >= 128]
+    best_shape, best_ms = default_shape, default_ms
+    for sh in shapes:
+        try:
+            ens.set_tuning(sh, ())
+            ms = _ensemble_ms(ens, waves)
+        except _lib.AbyssError:
+            continue
+        trials.append(("shape", sh, ms))
+        if verbose:
+            print("shape", sh, round(ms, 3))
+        if ms < best_ms:
+            best_shape, best_ms = sh, ms
+    # chunk length per cluster-size bucket, one bucket at a time
+    table = [[b, 2048] for b in buckets]
+    for q in range(len(table)):
+        keep = table[q][1]
+        for cj in chunks:
+            table[q][1] = cj
+            ens.set_tuning(best_shape, [tuple(e) for e in table])
+            ms = _ensemble_ms(ens, waves)
+            trials.append(("chunk", (table[q][0], cj), ms))
+            if verbose:
+                print("chunk", table[q][0], cj, round(ms, 3))
+            if ms < best_ms:
+                best_ms, keep = ms, cj
+        table[q][1] = keep
+    chunks_out = [tuple(e) for e in table]
+    ens.set_tuning(best_shape, chunks_out)
+    return {"shape": {k: best_shape[k] for k in ("kernel", "mode", "threads", "ipt", "unroll", "min_blocks")},
+            "chunks": chunks_out, "ms": best_ms, "default_ms": default_ms, "trials": len(trials)}
 
 
 def install(rf: RegularForce, table):

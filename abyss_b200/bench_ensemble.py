@@ -7,7 +7,8 @@ Regular blocks of K clusters of uneven N with uneven active sets, run as
   plain    the same kernels, one cluster per launch
 on the same GPU, same inputs.  Reported: cluster blocks per second (a cluster
 block is one regular-force evaluation of one cluster's active set), pairs per
-second and the ratio of each form to plain.
+second and the ratio of each form to plain; with ``tune``, the graph form again
+with the shape and chunk table that autotune.tune_ensemble picks on these waves.
 
     python -m abyss_b200.bench_ensemble [--clusters 512] [--waves 6]
 """
@@ -27,7 +28,7 @@ EPS2 = 1e-8
 LIST_CAP = 128
 
 
-def measure(rf: RegularForce, clusters, waves, warmup: int = 1):
+def measure(rf: RegularForce, clusters, waves, warmup: int = 1, tune: bool = False):
     sizes = [c.n for c in clusters]
     ens = Ensemble(rf, sizes, list_cap=LIST_CAP)
     for i, c in enumerate(clusters):
@@ -58,6 +59,27 @@ def measure(rf: RegularForce, clusters, waves, warmup: int = 1):
                      "gpairs_s": pairs / (gpu_ms / 1e3) / 1e9, "kernel_launches": launches}
     out["graph_vs_plain"] = out["graph"]["cluster_blocks_per_s"] / out["plain"]["cluster_blocks_per_s"]
     out["batched_vs_plain"] = out["batched"]["cluster_blocks_per_s"] / out["plain"]["cluster_blocks_per_s"]
+    if tune:
+        # the autotuner's shape and chunk table, picked on these waves (its own
+        # timing runs are not counted), then the graph form measured again
+        from . import autotune
+
+        t0 = time.perf_counter()
+        res = autotune.tune_ensemble(ens, waves)
+        out["tuning"] = {"shape": res["shape"], "chunks": res["chunks"], "trials": res["trials"],
+                         "tuning_s": time.perf_counter() - t0}
+        gpu_ms = 0.0
+        for wi, (ks, ts) in enumerate(waves):
+            ens.set_wave(ks, np.zeros(len(ks)), np.ones(len(ks)), ts)
+            for _ in range(warmup if wi == 0 else 0):
+                ens.launch(EPS2, GRAPH)
+                ens.fetch()
+            ens.launch(EPS2, GRAPH)
+            ens.fetch()
+            gpu_ms += ens.last_ms()
+        out["graph_tuned"] = {"gpu_ms": gpu_ms, "cluster_blocks_per_s": blocks / (gpu_ms / 1e3),
+                              "gpairs_s": pairs / (gpu_ms / 1e3) / 1e9}
+        out["graph_tuned_vs_plain"] = out["graph_tuned"]["cluster_blocks_per_s"] / out["plain"]["cluster_blocks_per_s"]
     ens.close()
     return out
 
@@ -67,11 +89,12 @@ def main():
     ap.add_argument("--clusters", type=int, default=512)
     ap.add_argument("--waves", type=int, default=6)
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--tune", action="store_true")
     args = ap.parse_args()
     clusters = workloads.ensemble(k=args.clusters)
     waves = workloads.ensemble_waves(clusters, args.waves)
     rf = RegularForce(args.device)
-    res = measure(rf, clusters, waves)
+    res = measure(rf, clusters, waves, tune=args.tune)
     print(json.dumps(res))
     rf.close()
 

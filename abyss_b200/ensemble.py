@@ -34,6 +34,8 @@ def _bind(L):
     L.abyss_ens_upload_staged.argtypes = [_vp, C.c_int, _ip]
     L.abyss_ens_list_cap.argtypes = [_vp]
     L.abyss_ens_set_chunk.argtypes = [_vp, C.c_int]
+    L.abyss_ens_set_tuning.argtypes = [_vp, C.POINTER(Tuning), C.c_int, _ip, _ip]
+    L.abyss_ens_get_shape.argtypes = [_vp, C.POINTER(Tuning)]
     L.abyss_ens_submit.argtypes = [_vp, C.c_int, _ip, _dp, _dp, _ip, _ip, C.c_double, C.c_int, _ip]
     L.abyss_ens_ready.argtypes = [_vp, C.c_int]
     L.abyss_ens_collect.argtypes = [_vp, C.c_int] + [C.POINTER(_dp)] * 4 + [C.POINTER(_ip)] * 2 + [_ip, _fp]
@@ -151,6 +153,23 @@ class Ensemble:
     def set_chunk(self, j_per_chunk: int):
         """j per chunk of a cluster's work items (its chunk count depends on its size only)."""
         self._check(self._L.abyss_ens_set_chunk(self._h, int(j_per_chunk)))
+
+    def set_tuning(self, shape: dict | None = None, chunks=()):
+        """Launch shape of the force kernel (a tile shape with double-single
+        offsets, as autotune.tune_ensemble picks it; None keeps it) and the
+        j-chunk length by cluster size: `chunks` is [(n_max, j_per_chunk)] in
+        rising n_max, the first entry with n_k <= n_max applies (include/abyss_ens.h
+        abyss_ens_set_tuning).  Applies from the next wave."""
+        tu = Tuning(**shape) if shape else None
+        nm = np.array([c[0] for c in chunks], np.int32)
+        jc = np.array([c[1] for c in chunks], np.int32)
+        self._check(self._L.abyss_ens_set_tuning(self._h, C.byref(tu) if tu is not None else None, len(chunks),
+                                                 ptr(nm, _ip), ptr(jc, _ip)))
+
+    def shape(self) -> dict:
+        t = Tuning()
+        self._check(self._L.abyss_ens_get_shape(self._h, C.byref(t)))
+        return t.as_dict()
 
     def upload_staged(self, clusters):
         cl = np.ascontiguousarray(clusters, np.int32)

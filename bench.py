@@ -519,13 +519,16 @@ def extras(device: int) -> dict:
     rf = RegularForce(device)
     clusters = workloads.ensemble(k=512)
     waves = workloads.ensemble_waves(clusters, 6)
-    ens = bench_ensemble.measure(rf, clusters, waves)
+    ens = bench_ensemble.measure(rf, clusters, waves, tune=True)
     rf.close()
     out["batched_ensemble"] = {
         "workload": "512 Plummer clusters, N log-uniform in [256, 16384], 6 waves of regular blocks",
         "cluster_blocks_per_s_graph": ens["graph"]["cluster_blocks_per_s"],
         "cluster_blocks_per_s_plain": ens["plain"]["cluster_blocks_per_s"],
-        "gpairs_s_graph": ens["graph"]["gpairs_s"], "graph_vs_plain": ens["graph_vs_plain"]}
+        "gpairs_s_graph": ens["graph"]["gpairs_s"], "graph_vs_plain": ens["graph_vs_plain"],
+        "cluster_blocks_per_s_graph_tuned": ens["graph_tuned"]["cluster_blocks_per_s"],
+        "gpairs_s_graph_tuned": ens["graph_tuned"]["gpairs_s"],
+        "graph_tuned_vs_plain": ens["graph_tuned_vs_plain"], "tuning": ens["tuning"]}
     kw = dict(rate=2000.0, duration=0.5, nmin=256, nmax=2048, t_end=0.0625)
     res = {}
     for serial in (False, True):

@@ -168,3 +168,95 @@ def test_two_waves_in_flight_match_blocking_waves(rf):
             for f in ("acc_reg", "jerk_reg", "acc_irr", "jerk_irr", "nnb", "list"):
                 assert np.array_equal(getattr(g, f), getattr(w, f)), (rep, f)
     e.close()
+
+
+TUNED_SHAPE = dict(kernel=3, mode=2, threads=128, ipt=4, unroll=2, min_blocks=4)
+TUNED_CHUNKS = [(1024, 512), (4096, 1024)]
+
+
+def test_tuned_shape_and_chunks_change_the_plan_not_the_parity(rf):
+    """A tuning (launch shape + chunk table by cluster size) changes the work
+    list; every cluster's rows still match the oracle, the batched, graph and
+    plain forms agree bit for bit, and a cluster alone gives the same rows as
+    in the mix (its chunking depends on its own size only)."""
+    e, clusters = make_ensemble(rf, k=12, seed=13)
+    rng = np.random.default_rng(21)
+    chosen, targets = random_wave(rng, clusters)
+    e.set_wave(chosen, np.zeros(len(chosen)), np.ones(len(chosen)), targets)
+    e.launch(EPS2, GRAPH)
+    e.fetch()
+    default_shape, default_items = e.shape(), e.last_stats()["items"]
+    e.set_tuning(TUNED_SHAPE, TUNED_CHUNKS)
+    sh = e.shape()
+    assert (sh["threads"], sh["ipt"], sh["unroll"], sh["min_blocks"]) == (128, 4, 2, 4) != (
+        default_shape["threads"], default_shape["ipt"], default_shape["unroll"], default_shape["min_blocks"])
+    e.set_wave(chosen, np.zeros(len(chosen)), np.ones(len(chosen)), targets)
+    res = {}
+    for mode in (GRAPH, BATCHED, PLAIN):
+        e.launch(EPS2, mode)
+        res[mode] = e.fetch()
+    assert e.last_stats()["items"] != default_items
+    mix = res[GRAPH]
+    for f in ("acc_reg", "jerk_reg", "acc_irr", "jerk_irr", "nnb", "list"):
+        assert np.array_equal(getattr(res[BATCHED], f), getattr(mix, f)), f
+        assert np.array_equal(getattr(res[PLAIN], f), getattr(mix, f)), f
+    for idx, ci in enumerate(chosen):
+        c = clusters[ci]
+        lo, hi = e.row_splits[idx], e.row_splits[idx + 1]
+        t = targets[idx]
+        ref = oracle.reg_force(c.x, c.v, c.m, c.r2nb, EPS2, t, 128)
+        sub = type(mix)(mix.acc_reg[lo:hi], mix.jerk_reg[lo:hi], mix.acc_irr[lo:hi], mix.jerk_irr[lo:hi],
+                        mix.nnb[lo:hi], mix.list[lo:hi])
+        check(sub, ref, f"tuned/cluster{ci}", oracle.reg_scale(c.x, c.v, c.m, c.r2nb, EPS2, t))
+    for idx, ci in enumerate(chosen):
+        e.set_wave([ci], [0.0], [1.0], [targets[idx]])
+        e.launch(EPS2, GRAPH)
+        alone = e.fetch()
+        lo, hi = e.row_splits[0], e.row_splits[1]
+        lo2 = sum(len(t) for t in targets[:idx])
+        for f in ("acc_reg", "jerk_reg", "acc_irr", "jerk_irr", "nnb", "list"):
+            assert np.array_equal(getattr(alone, f)[lo:hi], getattr(mix, f)[lo2:lo2 + len(targets[idx])]), (ci, f)
+    e.close()
+
+
+def test_bad_tunings_are_refused(rf):
+    from abyss_b200._lib import AbyssError
+
+    e, clusters = make_ensemble(rf, k=4, seed=14)
+    for shape, chunks in ((dict(kernel=3, mode=1, threads=128, ipt=2), ()),      # anchor offsets
+                          (dict(kernel=2, ipt=4), ()),                           # not a tile kernel
+                          (dict(kernel=1, mode=2, threads=32, ipt=1), ()),       # < 128 targets per block
+                          (dict(kernel=3, mode=2, threads=96, ipt=2), ()),       # not compiled
+                          (None, [(1024, 64)]),                                  # chunk < 128 j
+                          (None, [(4096, 512), (1024, 512)])):                   # n_max not rising
+        with pytest.raises(AbyssError):
+            e.set_tuning(shape, chunks)
+    e.set_wave([1], [0.0], [1.0], [np.arange(5, dtype=np.int32)])
+    e.launch(EPS2, GRAPH)
+    assert e.fetch().acc_reg.shape == (5, 3)
+    e.close()
+
+
+def test_autotuner_picks_a_shape_on_the_ensembles_waves(rf):
+    """tune_ensemble times the compiled double-single shapes and chunk lengths
+    on the ensemble's own waves, installs the fastest, and the installed shape
+    still gives the oracle's lists."""
+    from abyss_b200 import autotune
+
+    e, clusters = make_ensemble(rf, k=16, seed=15)
+    rng = np.random.default_rng(8)
+    waves = [random_wave(rng, clusters) for _ in range(2)]
+    res = autotune.tune_ensemble(e, waves, chunks=(512, 2048))
+    print("tuned ensemble:", res)
+    assert res["ms"] <= res["default_ms"] and res["trials"] > 4
+    assert e.shape()["threads"] == res["shape"]["threads"] and e.shape()["ipt"] == res["shape"]["ipt"]
+    chosen, targets = waves[0]
+    e.set_wave(chosen, np.zeros(len(chosen)), np.ones(len(chosen)), targets)
+    e.launch(EPS2, GRAPH)
+    got = e.fetch()
+    for idx, ci in enumerate(chosen):
+        c = clusters[ci]
+        lo, hi = e.row_splits[idx], e.row_splits[idx + 1]
+        ref = oracle.reg_force(c.x, c.v, c.m, c.r2nb, EPS2, targets[idx], 128)
+        assert np.array_equal(got.nnb[lo:hi], ref["nnb"])
+    e.close()
