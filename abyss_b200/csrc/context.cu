@@ -546,6 +546,10 @@ int abyss_set_targets(abyss_ctx *c, int m, const int *targets) {
 }
 
 // ------------------------------------------------------------------ planning
+// Launches of at most this many rows on the j-major kernel finalize in the force
+// kernel's last block instead of a second launch.
+constexpr int kFuseRows = 2;
+
 static abyss_tuning plan_for(abyss_ctx *c, int m, const abyss_tuning *user) {
   abyss_tuning t{};
   if (user) t = *user;
@@ -721,17 +725,6 @@ int abyss_launch(abyss_ctx *c, double eps2, int list_cap, const abyss_tuning *tu
     w.order_o = c->iota.p;
   }
   if (c->profiling) CK(cudaEventRecord(c->ev[1], c->stream), "event");
-  if (t.kernel == 1 || t.kernel == 3) {
-    if (launch_tile(c->stream, t.threads, t.ipt, t.mode == 1, t.kernel == 3, t.unroll, t.min_blocks, grid, js,
-                    w, n_iblocks) != 0)
-      return fail(c, ABYSS_ERR_ARG, "launch: unsupported tile shape");
-    t.grid = grid;
-  } else {
-    if (launch_jmajor(c->stream, t.ipt, js, w, L) != 0)
-      return fail(c, ABYSS_ERR_ARG, "launch: unsupported j-major shape");
-  }
-  CK(cudaGetLastError(), "force kernel launch");
-  if (c->profiling) CK(cudaEventRecord(c->ev[2], c->stream), "event");
   Outputs o;
   o.targets = c->targets.p;
   o.acc_reg = c->acc_reg.p;
@@ -742,8 +735,22 @@ int abyss_launch(abyss_ctx *c, double eps2, int list_cap, const abyss_tuning *tu
   o.list = c->list.p;
   o.overflow_rows = c->ovf.p;
   o.ovf_list = c->ovf_list.p;
-  launch_finalize(c->stream, js, w, o, c->sm_count);
-  CK(cudaGetLastError(), "finalize launch");
+  if (t.kernel == 1 || t.kernel == 3) {
+    if (launch_tile(c->stream, t.threads, t.ipt, t.mode == 1, t.kernel == 3, t.unroll, t.min_blocks, grid, js,
+                    w, n_iblocks) != 0)
+      return fail(c, ABYSS_ERR_ARG, "launch: unsupported tile shape");
+    t.grid = grid;
+  } else {
+    // a launch of at most kFuseRows rows finalizes in its force kernel's last block
+    if (launch_jmajor(c->stream, t.ipt, js, w, L, m <= kFuseRows ? &o : nullptr) != 0)
+      return fail(c, ABYSS_ERR_ARG, "launch: unsupported j-major shape");
+  }
+  CK(cudaGetLastError(), "force kernel launch");
+  if (c->profiling) CK(cudaEventRecord(c->ev[2], c->stream), "event");
+  if (!(t.kernel == 2 && m <= kFuseRows)) {
+    launch_finalize(c->stream, js, w, o, c->sm_count);
+    CK(cudaGetLastError(), "finalize launch");
+  }
   if (c->profiling) CK(cudaEventRecord(c->ev[3], c->stream), "event");
   t.j_split = S;
   c->plan = t;

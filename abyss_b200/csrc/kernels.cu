@@ -793,8 +793,13 @@ __global__ void __launch_bounds__(NT, MINB) reg_force_tile(JSet js, Work w, int 
 // warps in a fixed order, so a launch is deterministic.
 constexpr int kJmWarps = 4;
 
+template <int NT>
+__device__ void finalize_row_block(const JSet &js, const Work &w, const Outputs &o, int sort_cap, int r,
+                                   int *fin_smem, double (*red)[6], int *s_nl_total);
+
 template <int MI>
-__global__ void __launch_bounds__(32 * kJmWarps) reg_force_jmajor(JSet js, Work w, int Lw) {
+__global__ void __launch_bounds__(32 * kJmWarps, MI <= 2 ? 5 : 1) reg_force_jmajor(JSet js, Work w, Outputs o, int Lw,
+                                                                  int fuse_sort_cap) {
   __shared__ double s_red[kJmWarps][MI][6];
   const unsigned FULL = 0xffffffffu;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -835,23 +840,44 @@ __global__ void __launch_bounds__(32 * kJmWarps) reg_force_jmajor(JSet js, Work 
 #pragma unroll
       for (int c = 0; c < 6; ++c) p[k][c] = make_float2(0.0f, 0.0f);
 
+    // j records, two per lane a step; a pad is massless and far away: never a
+    // candidate, adds 0.  The next step's records are loaded before this
+    // step's arithmetic, so that a warp keeps two steps of loads in flight.
+    double nX0 = 1e30, nY0 = 1e30, nZ0 = 1e30, nX1 = 1e30, nY1 = 1e30, nZ1 = 1e30;
+    float4 nV0 = make_float4(0.f, 0.f, 0.f, 0.f), nV1 = nV0;
+    if (jw0 + lane < jw1) {
+      nX0 = js.px[jw0 + lane];
+      nY0 = js.py[jw0 + lane];
+      nZ0 = js.pz[jw0 + lane];
+      nV0 = js.vm[jw0 + lane];
+    }
+    if (jw0 + 32 + lane < jw1) {
+      nX1 = js.px[jw0 + 32 + lane];
+      nY1 = js.py[jw0 + 32 + lane];
+      nZ1 = js.pz[jw0 + 32 + lane];
+      nV1 = js.vm[jw0 + 32 + lane];
+    }
     for (int jb = jw0; jb < jw1; jb += 64) {
       const int ja = jb + lane, jc = jb + 32 + lane;
       const bool ina = ja < jw1, inc = jc < jw1;
-      // j records; a pad is massless and far away: never a candidate, adds 0
-      double X0 = 1e30, Y0 = 1e30, Z0 = 1e30, X1 = 1e30, Y1 = 1e30, Z1 = 1e30;
-      float4 V0 = make_float4(0.f, 0.f, 0.f, 0.f), V1 = V0;
-      if (ina) {
-        X0 = js.px[ja];
-        Y0 = js.py[ja];
-        Z0 = js.pz[ja];
-        V0 = js.vm[ja];
-      }
-      if (inc) {
-        X1 = js.px[jc];
-        Y1 = js.py[jc];
-        Z1 = js.pz[jc];
-        V1 = js.vm[jc];
+      const double X0 = nX0, Y0 = nY0, Z0 = nZ0, X1 = nX1, Y1 = nY1, Z1 = nZ1;
+      const float4 V0 = nV0, V1 = nV1;
+      {
+        const int qa = jb + 64 + lane, qc = jb + 96 + lane;
+        nX0 = nY0 = nZ0 = nX1 = nY1 = nZ1 = 1e30;
+        nV0 = nV1 = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (qa < jw1) {
+          nX0 = js.px[qa];
+          nY0 = js.py[qa];
+          nZ0 = js.pz[qa];
+          nV0 = js.vm[qa];
+        }
+        if (qc < jw1) {
+          nX1 = js.px[qc];
+          nY1 = js.py[qc];
+          nZ1 = js.pz[qc];
+          nV1 = js.vm[qc];
+        }
       }
       const float2 xh = make_float2((float)X0, (float)X1);
       const float2 yh = make_float2((float)Y0, (float)Y1);
@@ -928,6 +954,24 @@ __global__ void __launch_bounds__(32 * kJmWarps) reg_force_jmajor(JSet js, Work 
     }
     __syncthreads();
   }
+  if (fuse_sort_cap > 0) {
+    // the block that finishes last finalizes the rows in place (few rows): no
+    // second launch.  Every block's partials and list entries are made visible
+    // before it counts itself done; no block waits on another.
+    extern __shared__ int fin_smem[];
+    __shared__ double red[kJmWarps][6];
+    __shared__ int s_nl_total[2];
+    __shared__ int s_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = atomicAdd(w.item_counter, 1) == (int)gridDim.x - 1;
+    __syncthreads();
+    if (s_last) {
+      __threadfence();
+      for (int r = 0; r < w.m; ++r) finalize_row_block<32 * kJmWarps>(js, w, o, fuse_sort_cap, r, fin_smem, red,
+                                                                       s_nl_total);
+    }
+  }
 }
 
 // ============================================================ list sort
@@ -938,7 +982,8 @@ __global__ void __launch_bounds__(32 * kJmWarps) reg_force_jmajor(JSet js, Work 
 template <class Sync>
 __device__ __forceinline__ void rank_sort(const int *lrow, int nl, int *buf, int P, int tid, int nthr, Sync sync) {
   int *stage = buf + P / 2;
-  for (int k = tid; k < nl; k += nthr) stage[k] = lrow[k];
+  // L2-coherent: the entries may come from other blocks of the same launch
+  for (int k = tid; k < nl; k += nthr) stage[k] = __ldcg(&lrow[k]);
   sync();
   for (int k = tid; k < nl; k += nthr) {
     const int e = stage[k];
@@ -1087,112 +1132,121 @@ __device__ __forceinline__ void block_sum6(double (&v)[6], double (*red)[6]) {
   __syncthreads();
 }
 
+// One row's finalize by a block of NT threads (called by every thread of the
+// block): FP64 sum of the chunk partials, the sorted list, the FP64 irregular
+// part, and the re-list of an overflowed row.  Reads that may see other
+// blocks' writes of the same launch are L2-coherent, so the force kernel's last
+// block can finalize in place (reg_force_jmajor with fused rows).
+template <int NT>
+__device__ void finalize_row_block(const JSet &js, const Work &w, const Outputs &o, int sort_cap, int r,
+                                   int *fin_smem, double (*red)[6], int *s_nl_total) {
+  const int nch = w.row_nchunks ? w.row_nchunks[r] : w.n_chunks;
+  const int joff = w.row_joff ? w.row_joff[r] : 0;
+  double s[6] = {0, 0, 0, 0, 0, 0};
+  for (int c = threadIdx.x; c < nch; c += NT) {
+    const double *src = w.part + ((size_t)r * w.s_stride + c) * 6;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) s[q] += __ldcg(&src[q]);
+  }
+  block_sum6<NT>(s, red);
+
+  {
+    const int total = __ldcg(&w.lcnt[r]);
+    const int nl = min(total, w.cap);
+    if (threadIdx.x == 0) {
+      s_nl_total[0] = nl;
+      s_nl_total[1] = total;
+    }
+    if (2 * nl <= sort_cap)
+      rank_sort(w.lst + (size_t)r * w.cap, nl, fin_smem, sort_cap, threadIdx.x, NT, []() { __syncthreads(); });
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  if (threadIdx.x < 32 && 2 * s_nl_total[0] > sort_cap) {
+    const int nl = s_nl_total[0];
+    const int *lrow = w.lst + (size_t)r * w.cap;
+    int P = 32;
+    while (P < nl) P <<= 1;
+    int *buf = fin_smem;
+    for (int k = lane; k < P; k += 32) buf[k] = k < nl ? __ldcg(&lrow[k]) : INT_MAX;
+    __syncwarp();
+    for (int kk = 2; kk <= P; kk <<= 1) {
+      for (int jj = kk >> 1; jj > 0; jj >>= 1) {
+        for (int i = lane; i < P; i += 32) {
+          const int l = i ^ jj;
+          if (l > i) {
+            const int a = buf[i], b = buf[l];
+            const bool up = (i & kk) == 0;
+            if ((a > b) == up) {
+              buf[i] = b;
+              buf[l] = a;
+            }
+          }
+        }
+        __syncwarp();
+      }
+    }
+  }
+  __syncthreads();
+  const int nl = s_nl_total[0], total = s_nl_total[1];
+  const int *buf = fin_smem;
+  int *out = o.list + (size_t)r * w.cap;
+  for (int k = threadIdx.x; k < nl; k += NT) out[k] = buf[k] - joff;
+
+  const int t = o.targets[r];
+  const double xi = js.px[t], yi = js.py[t], zi = js.pz[t];
+  const double vxi = js.pvx[t], vyi = js.pvy[t], vzi = js.pvz[t];
+  double a[6] = {0, 0, 0, 0, 0, 0};
+  for (int k = threadIdx.x; k < nl; k += NT) {
+    const int j = buf[k];
+    const double x[3] = {__dsub_rn(js.px[j], xi), __dsub_rn(js.py[j], yi), __dsub_rn(js.pz[j], zi)};
+    const double v[3] = {__dsub_rn(js.pvx[j], vxi), __dsub_rn(js.pvy[j], vyi), __dsub_rn(js.pvz[j], vzi)};
+    double r2 = 0.0, vx = 0.0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      r2 = __dadd_rn(r2, __dmul_rn(x[d], x[d]));
+      vx = __dadd_rn(vx, __dmul_rn(v[d], x[d]));
+    }
+    const double r2s = __dadd_rn(r2, w.eps2);
+    const double m_r3 = __ddiv_rn(__ddiv_rn(js.mass[j], r2s), __dsqrt_rn(r2s));
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      a[d] = __dadd_rn(a[d], __dmul_rn(m_r3, x[d]));
+      const double corr = __ddiv_rn(__dmul_rn(__dmul_rn(3.0, x[d]), vx), r2s);
+      a[3 + d] = __dadd_rn(a[3 + d], __dmul_rn(m_r3, __dsub_rn(v[d], corr)));
+    }
+  }
+  block_sum6<NT>(a, red);
+
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      o.acc_reg[3 * r + d] = s[d];
+      o.jerk_reg[3 * r + d] = s[3 + d];
+      o.acc_irr[3 * r + d] = a[d];
+      o.jerk_irr[3 * r + d] = a[3 + d];
+    }
+    o.nnb[r] = total;
+    if (total > w.cap) {
+      const int q = atomicAdd(o.overflow_rows, 1);
+      o.ovf_list[q] = r;
+      atomicOr(w.status, kErrOverflow);
+    }
+  }
+  __syncthreads();
+  // an overflowed row is re-listed here, by warp 0, instead of by relist_rows
+  if (total > w.cap && threadIdx.x < 32) relist_row(js, w, o, r);
+  __syncthreads();
+}
+
 template <int NT>
 __global__ void __launch_bounds__(NT) finalize_rows_block(JSet js, Work w, Outputs o, int sort_cap) {
   extern __shared__ int fin_smem[];  // the row's sort buffer
   __shared__ double red[NT / 32][6];
-  __shared__ int s_nl, s_total;
-  const int lane = threadIdx.x & 31;
+  __shared__ int s_nl_total[2];
   const int m_rows = w.m_dev ? *w.m_dev : w.m;
-  for (int r = blockIdx.x; r < m_rows; r += gridDim.x) {
-    const int nch = w.row_nchunks ? w.row_nchunks[r] : w.n_chunks;
-    const int joff = w.row_joff ? w.row_joff[r] : 0;
-    double s[6] = {0, 0, 0, 0, 0, 0};
-    for (int c = threadIdx.x; c < nch; c += NT) {
-      const double *src = w.part + ((size_t)r * w.s_stride + c) * 6;
-#pragma unroll
-      for (int q = 0; q < 6; ++q) s[q] += src[q];
-    }
-    block_sum6<NT>(s, red);
-
-    {
-      const int total = w.lcnt[r];
-      const int nl = min(total, w.cap);
-      if (threadIdx.x == 0) {
-        s_nl = nl;
-        s_total = total;
-      }
-      if (2 * nl <= sort_cap)
-        rank_sort(w.lst + (size_t)r * w.cap, nl, fin_smem, sort_cap, threadIdx.x, NT,
-                  []() { __syncthreads(); });
-    }
-    __syncthreads();
-    if (threadIdx.x < 32 && 2 * s_nl > sort_cap) {
-      const int nl = s_nl;
-      const int *lrow = w.lst + (size_t)r * w.cap;
-      int P = 32;
-      while (P < nl) P <<= 1;
-      int *buf = fin_smem;
-      for (int k = lane; k < P; k += 32) buf[k] = k < nl ? lrow[k] : INT_MAX;
-      __syncwarp();
-      for (int kk = 2; kk <= P; kk <<= 1) {
-        for (int jj = kk >> 1; jj > 0; jj >>= 1) {
-          for (int i = lane; i < P; i += 32) {
-            const int l = i ^ jj;
-            if (l > i) {
-              const int a = buf[i], b = buf[l];
-              const bool up = (i & kk) == 0;
-              if ((a > b) == up) {
-                buf[i] = b;
-                buf[l] = a;
-              }
-            }
-          }
-          __syncwarp();
-        }
-      }
-    }
-    __syncthreads();
-    const int nl = s_nl, total = s_total;
-    const int *buf = fin_smem;
-    int *out = o.list + (size_t)r * w.cap;
-    for (int k = threadIdx.x; k < nl; k += NT) out[k] = buf[k] - joff;
-
-    const int t = o.targets[r];
-    const double xi = js.px[t], yi = js.py[t], zi = js.pz[t];
-    const double vxi = js.pvx[t], vyi = js.pvy[t], vzi = js.pvz[t];
-    double a[6] = {0, 0, 0, 0, 0, 0};
-    for (int k = threadIdx.x; k < nl; k += NT) {
-      const int j = buf[k];
-      const double x[3] = {__dsub_rn(js.px[j], xi), __dsub_rn(js.py[j], yi), __dsub_rn(js.pz[j], zi)};
-      const double v[3] = {__dsub_rn(js.pvx[j], vxi), __dsub_rn(js.pvy[j], vyi), __dsub_rn(js.pvz[j], vzi)};
-      double r2 = 0.0, vx = 0.0;
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        r2 = __dadd_rn(r2, __dmul_rn(x[d], x[d]));
-        vx = __dadd_rn(vx, __dmul_rn(v[d], x[d]));
-      }
-      const double r2s = __dadd_rn(r2, w.eps2);
-      const double m_r3 = __ddiv_rn(__ddiv_rn(js.mass[j], r2s), __dsqrt_rn(r2s));
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        a[d] = __dadd_rn(a[d], __dmul_rn(m_r3, x[d]));
-        const double corr = __ddiv_rn(__dmul_rn(__dmul_rn(3.0, x[d]), vx), r2s);
-        a[3 + d] = __dadd_rn(a[3 + d], __dmul_rn(m_r3, __dsub_rn(v[d], corr)));
-      }
-    }
-    block_sum6<NT>(a, red);
-
-    if (threadIdx.x == 0) {
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        o.acc_reg[3 * r + d] = s[d];
-        o.jerk_reg[3 * r + d] = s[3 + d];
-        o.acc_irr[3 * r + d] = a[d];
-        o.jerk_irr[3 * r + d] = a[3 + d];
-      }
-      o.nnb[r] = total;
-      if (total > w.cap) {
-        const int q = atomicAdd(o.overflow_rows, 1);
-        o.ovf_list[q] = r;
-        atomicOr(w.status, kErrOverflow);
-      }
-    }
-    __syncthreads();
-    // an overflowed row is re-listed here, by warp 0, instead of by relist_rows
-    if (total > w.cap && threadIdx.x < 32) relist_row(js, w, o, r);
-    __syncthreads();
-  }
+  for (int r = blockIdx.x; r < m_rows; r += gridDim.x)
+    finalize_row_block<NT>(js, w, o, sort_cap, r, fin_smem, red, s_nl_total);
 }
 
 // ============================================================ re-list
@@ -1460,14 +1514,29 @@ int jmajor_occupancy(int mi) {
   return e == cudaSuccess ? std::max(occ, 1) : 1;
 }
 
-int launch_jmajor(cudaStream_t s, int mi, const JSet &js, const Work &w, int Lw) {
-  // one block per j-chunk (w.n_chunks of them), kJmWarps sub-chunks of Lw each
+int launch_jmajor(cudaStream_t s, int mi, const JSet &js, const Work &w, int Lw, const Outputs *fuse) {
+  // one block per j-chunk (w.n_chunks of them), kJmWarps sub-chunks of Lw each;
+  // with `fuse`, the last block to finish finalizes the rows (w.item_counter
+  // must be zero)
   const int blocks = w.n_chunks;
+  int P = 0;
+  size_t smem = 0;
+  Outputs o{};
+  if (fuse) {
+    o = *fuse;
+    P = 32;
+    while (P < w.cap) P <<= 1;
+    smem = (size_t)P * sizeof(int);
+  }
+  auto go = [&](auto kern) {
+    if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    kern<<<blocks, 32 * kJmWarps, smem, s>>>(js, w, o, Lw, P);
+  };
   switch (mi) {
-    case 1: reg_force_jmajor<1><<<blocks, 32 * kJmWarps, 0, s>>>(js, w, Lw); break;
-    case 2: reg_force_jmajor<2><<<blocks, 32 * kJmWarps, 0, s>>>(js, w, Lw); break;
-    case 4: reg_force_jmajor<4><<<blocks, 32 * kJmWarps, 0, s>>>(js, w, Lw); break;
-    case 8: reg_force_jmajor<8><<<blocks, 32 * kJmWarps, 0, s>>>(js, w, Lw); break;
+    case 1: go(reg_force_jmajor<1>); break;
+    case 2: go(reg_force_jmajor<2>); break;
+    case 4: go(reg_force_jmajor<4>); break;
+    case 8: go(reg_force_jmajor<8>); break;
     default: return -1;
   }
   return 0;

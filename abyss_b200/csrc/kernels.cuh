@@ -35,7 +35,9 @@ int tile_variant_shape(int i, int *shape6);
 // sub-chunk of Lw particles (a multiple of 64).
 int jmajor_warps();
 int jmajor_occupancy(int mi);  // resident blocks per SM
-int launch_jmajor(cudaStream_t s, int mi, const JSet &js, const Work &w, int Lw);
+// With `fuse` (few rows), the last block to finish also finalizes the rows into
+// *fuse, in place of launch_finalize; w.item_counter must be zero.
+int launch_jmajor(cudaStream_t s, int mi, const JSet &js, const Work &w, int Lw, const Outputs *fuse = nullptr);
 void launch_finalize(cudaStream_t s, const JSet &js, const Work &w, const Outputs &o, int sm_count);
 void launch_predict_multi(cudaStream_t s, int n, const int *cid, const int *active,
                           const double *new_time, const double *time_scale, const double *x,

@@ -99,7 +99,14 @@ class Request:
 class Server:
     def __init__(self, device: int = 0, capacity: int = 1 << 21, max_clusters: int = 512, list_cap: int = 128,
                  eps2: float = 1e-8, eta_reg: float = 0.02, eta_irr: float = 0.01, host_threads: int = 16,
-                 slice_ms: float = 20.0, max_n: int = 16384, chunk_j: int = 256):
+                 slice_ms: float = 20.0, max_n: int = 16384, chunk_j: int = 256, device_irregular_min_n: int = 0,
+                 team_min_n: int = 16384):
+        """device_irregular_min_n > 0: integrations of at least that many
+        particles run their irregular levels on the GPU (include/abyss_irr.h)
+        instead of on their worker thread; the results are the same.
+        team_min_n: integrations of at least that many particles get a team of
+        1 + n / team_min_n host threads (at most host_threads) for their host
+        work; smaller ones run on their worker thread alone."""
         self.rf = RegularForce(device)
         self.ens = Ensemble(self.rf, None, list_cap=list_cap, capacity=capacity, max_clusters=max_clusters)
         # short j-chunks: a serving wave is small and latency-bound, so its work
@@ -107,6 +114,8 @@ class Server:
         self.ens.set_chunk(chunk_j)
         self.eps2 = eps2
         self.eta_reg, self.eta_irr = eta_reg, eta_irr
+        self.device_irregular_min_n = int(device_irregular_min_n)
+        self.team_min_n = max(1, int(team_min_n))
         self.list_cap = list_cap
         nthreads = max(1, host_threads)
         self.host_threads = nthreads
@@ -174,9 +183,15 @@ class Server:
             rf, lock = ctx
             with lock:
                 t2 = time.perf_counter()
+                # one host thread per integration, except for large clusters,
+                # whose per-block host work (j-set fill, corrector) would set
+                # the stream's tail on one thread
+                threads = 1 if r.n < self.team_min_n else min(self.host_threads, r.n // self.team_min_n + 1)
                 r.ac = ACIntegrator(rf, c.x, c.v, c.m, c.r2nb, eps2=self.eps2, eta_reg=self.eta_reg,
                                     eta_irr=self.eta_irr, fix_nb=r.k_nb, nb_max=self.list_cap, t_end=r.t_end,
-                                    threads=1)
+                                    threads=threads)
+                if self.device_irregular_min_n > 0 and r.n >= self.device_irregular_min_n:
+                    r.ac.set_device_irregular(True)
                 t3 = time.perf_counter()
                 r.e0 = r.ac.energy()
                 t4 = time.perf_counter()
@@ -286,7 +301,8 @@ class Server:
             r.e1 = r.ac.energy()
         r.finished = self.now()
         r.result = dict(rid=r.rid, n=r.n, model=r.model, dE_over_E=abs((r.e1 - r.e0) / r.e0), blocks=r.blocks,
-                        latency_s=r.finished - r.arrival, queue_s=r.admitted - r.arrival)
+                        latency_s=r.finished - r.arrival, queue_s=r.admitted - r.arrival,
+                        device_irregular=r.ac.device_irregular_info()["on"])
         r.result["x_final"] = r.ac.state()["x"]
         r.ac.close()
         r.ac = None
@@ -317,10 +333,12 @@ def poisson_requests(rate: float, duration: float, nmin: int, nmax: int, seed: i
 
 def serve(rate: float = 200.0, duration: float = 2.0, nmin: int = 256, nmax: int = 2048, t_end: float = 0.0625,
           capacity: int = 1 << 21, seed: int = 5, host_threads: int = 16, serial: bool = False,
-          chunk_j: int = 256, slice_ms: float = 20.0):
+          chunk_j: int = 256, slice_ms: float = 20.0, device_irregular_min_n: int = 0, reqs=None):
     """Run a Poisson stream through the server (or, with serial=True, one request at
-    a time through the same code) and report latency percentiles and throughput."""
-    reqs = poisson_requests(rate, duration, nmin, nmax, seed=seed, t_end=t_end)
+    a time through the same code) and report latency percentiles and throughput.
+    `reqs` replaces the generated stream (requests with prebuilt clusters)."""
+    if reqs is None:
+        reqs = poisson_requests(rate, duration, nmin, nmax, seed=seed, t_end=t_end)
     # a request arrives with its particles: build the payloads before the clock starts
     for r in reqs:
         r.cluster = r.make_cluster()
@@ -329,7 +347,8 @@ def serve(rate: float = 200.0, duration: float = 2.0, nmin: int = 256, nmax: int
         rounds, wave_ms, peak = 0, 0.0, 1
         srv = None
     else:
-        srv = Server(capacity=capacity, host_threads=host_threads, max_n=nmax, chunk_j=chunk_j, slice_ms=slice_ms)
+        srv = Server(capacity=capacity, host_threads=host_threads, max_n=max(nmax, max(r.n for r in reqs)),
+                     chunk_j=chunk_j, slice_ms=slice_ms, device_irregular_min_n=device_irregular_min_n)
         for r in reqs:
             srv.submit(r)
         srv.run_until_idle()
@@ -339,7 +358,11 @@ def serve(rate: float = 200.0, duration: float = 2.0, nmin: int = 256, nmax: int
     wall = max(r.finished for r in done) if done else 0.0
     lat = np.array([r.result["latency_s"] for r in done])
     de = np.array([r.result["dE_over_E"] for r in done])
-    res = dict(requests=len(reqs), completed=len(done), wall_s=wall,
+    blocks = int(sum(r.blocks for r in done))
+    res = dict(requests=len(reqs), completed=len(done), wall_s=wall, cluster_blocks=blocks,
+               cluster_blocks_per_s=blocks / wall if wall > 0 else None,
+               frac_dE_below_1e6=float(np.mean(de <= 1e-6)) if len(de) else None,
+               device_irregular_requests=int(sum(bool(r.result.get("device_irregular")) for r in done)),
                clusters_per_s=len(done) / wall if wall > 0 else None,
                p50_latency_s=float(np.percentile(lat, 50)) if len(lat) else None,
                p99_latency_s=float(np.percentile(lat, 99)) if len(lat) else None,
@@ -347,7 +370,7 @@ def serve(rate: float = 200.0, duration: float = 2.0, nmin: int = 256, nmax: int
                median_dE_over_E=float(np.median(de)) if len(de) else None,
                rounds=rounds, gpu_wave_ms=wave_ms, peak_active=peak, phase_s=phases,
                config=dict(rate=rate, duration=duration, nmin=nmin, nmax=nmax, t_end=t_end, capacity=capacity,
-                           seed=seed, serial=serial))
+                           seed=seed, serial=serial, device_irregular_min_n=device_irregular_min_n))
     return res, done
 
 
@@ -375,6 +398,7 @@ def serve_serial(reqs, host_threads: int = 16):
         t = time.perf_counter()
         ac.run(1.0)
         phases["run"] += time.perf_counter() - t
+        r.blocks = int(ac.stats()["blocks"])
         r.e1 = ac.energy()
         r.finished = time.perf_counter() - t0
         r.result = dict(rid=r.rid, n=r.n, model=r.model, dE_over_E=abs((r.e1 - r.e0) / r.e0),
@@ -385,12 +409,69 @@ def serve_serial(reqs, host_threads: int = 16):
     return done, phases
 
 
+def c4_requests(k: int = 512, t_end: float = 5.0):
+    """The batched-ensemble configuration as one serving job: the k equal-mass
+    Plummer clusters of workloads.ensemble (N log-uniform in [256, 16384],
+    seed 4, cluster i seeded 4000 + i, 24 neighbours), all arriving at once,
+    each integrated to t = t_end."""
+    from . import workloads
+
+    clusters = workloads.ensemble(k=k)
+    return [Request(i, 0.0, "plummer", c.n, 4000 + i, t_end=t_end, k_nb=24, cluster=c)
+            for i, c in enumerate(clusters)]
+
+
+def run_config(name: str, duration: float = 1.0, sample: int = 16, device_irregular_min_n: int = 4096,
+               host_threads: int = 16, capacity: int = 1 << 22):
+    """A stated configuration through the continuous server, and the serial
+    plain form on an evenly spaced sample of the same requests (the whole
+    stream one at a time would take hours): its clusters/s is the sample's
+    count over the sample's back-to-back run time.
+      c4: the 512 ensemble clusters to t = 5, all arriving at once;
+      c5: Poisson 200 requests/s for `duration` s (seed 5), Plummer or King W0
+          3/6/9, Kroupa IMF, N log-uniform in [1024, 131072], to t = 1."""
+    if name == "c4":
+        reqs = c4_requests()
+        nmax = 16384
+    else:
+        reqs = poisson_requests(200.0, duration, 1024, 131072, seed=5, t_end=1.0)
+        nmax = 131072
+    for r in reqs:
+        r.cluster = r.make_cluster()
+    res, done = serve(reqs=reqs, nmax=nmax, capacity=capacity, host_threads=host_threads,
+                      device_irregular_min_n=device_irregular_min_n)
+    res.pop("phase_s", None)
+    de = {r.rid: r.result["dE_over_E"] for r in done}
+    res["dE_over_E_by_request"] = [de[k] for k in sorted(de)]
+    # serial plain on a sample (fresh requests: the served ones hold their results)
+    step = max(1, len(reqs) // max(1, sample))
+    pick = [r.rid for r in reqs][::step][:sample]
+    if name == "c4":
+        fresh = {r.rid: r for r in c4_requests()}
+    else:
+        fresh = {r.rid: r for r in poisson_requests(200.0, duration, 1024, 131072, seed=5, t_end=1.0)}
+    sub = [fresh[k] for k in pick]
+    for r in sub:
+        r.arrival = 0.0
+        r.cluster = r.make_cluster()
+    sdone, phases = serve_serial(sub, host_threads)
+    run_s = phases["init"] + phases["run"]
+    res["serial_plain_sample"] = dict(requests=len(sub), run_s=run_s, clusters_per_s=len(sub) / run_s,
+                                      dE_over_E=[r.result["dE_over_E"] for r in sdone])
+    res["vs_serial_plain"] = res["clusters_per_s"] / res["serial_plain_sample"]["clusters_per_s"]
+    return res
+
+
 def main():
     """Serving benchmark: a seeded Poisson stream through the continuous server and
     through serial plain integrations.  The defaults (2000 requests/s for 0.5 s,
     N log-uniform in [256, 2048], t_end = 1/16) arrive faster than either can
-    serve them, so clusters/s measures throughput at saturation."""
+    serve them, so clusters/s measures throughput at saturation.  With
+    --config c4 or c5, the stated configuration (run_config)."""
     ap = argparse.ArgumentParser()
+    ap.add_argument("--config", choices=["c4", "c5"], default=None)
+    ap.add_argument("--sample", type=int, default=16)
+    ap.add_argument("--device-irregular-min-n", type=int, default=4096)
     ap.add_argument("--rate", type=float, default=2000.0)
     ap.add_argument("--duration", type=float, default=0.5)
     ap.add_argument("--nmin", type=int, default=256)
@@ -399,6 +480,10 @@ def main():
     ap.add_argument("--capacity", type=int, default=1 << 21)
     ap.add_argument("--threads", type=int, default=16)
     args = ap.parse_args()
+    if args.config:
+        print(json.dumps(run_config(args.config, duration=args.duration, sample=args.sample,
+                                    device_irregular_min_n=args.device_irregular_min_n, host_threads=args.threads)))
+        return
     out = {}
     for serial in (False, True):
         res, _ = serve(args.rate, args.duration, args.nmin, args.nmax, args.t_end, args.capacity,

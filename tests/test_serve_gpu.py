@@ -44,3 +44,29 @@ def test_request_same_alone_and_in_mix():
     assert alone["blocks"] == in_mix["blocks"]
     assert np.array_equal(alone["x_final"], in_mix["x_final"])
     assert alone["dE_over_E"] == in_mix["dE_over_E"]
+
+
+def test_device_irregular_levels_in_serving_give_the_same_results():
+    """A stream served with the larger integrations' irregular levels on the GPU
+    (several worker threads launching them at once) ends in the same state, bit
+    for bit, as the same stream with every integration's levels on its worker
+    thread."""
+    def run(min_n):
+        reqs = poisson_requests(rate=400.0, duration=0.04, nmin=256, nmax=2048, seed=13, t_end=0.03125, k_nb=16)
+        srv = Server(capacity=1 << 17, max_clusters=32, list_cap=64, host_threads=8, max_n=2048,
+                     device_irregular_min_n=min_n)
+        for r in reqs:
+            srv.submit(r)
+        srv.run_until_idle(max_seconds=300)
+        done = {r.rid: r.result for r in srv.done}
+        srv.close()
+        return done
+
+    host = run(0)
+    dev = run(512)
+    assert sum(1 for r in dev.values() if r["device_irregular"]) >= 2
+    assert sorted(host) == sorted(dev)
+    for k in host:
+        assert host[k]["blocks"] == dev[k]["blocks"], k
+        assert np.array_equal(host[k]["x_final"], dev[k]["x_final"]), k
+        assert host[k]["dE_over_E"] == dev[k]["dE_over_E"], k
