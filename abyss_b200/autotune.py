@@ -70,6 +70,8 @@ def tune(rf: RegularForce, n: int, buckets=BUCKETS, anchor_min: int = 16384, see
         cands = []
         if m <= 64:
             cands += [dict(kernel=2, ipt=i) for i in (1, 2, 4, 8) if i <= max(1, m)]
+        if 16 <= m <= 256:  # warps sharing targets
+            cands += [dict(kernel=4, ipt=i, j_split=s) for i in (1, 2) for s in (0, 1024, 2048)]
         for sh in shapes:
             if sh["mode"] == 1 and m < anchor_min:
                 continue

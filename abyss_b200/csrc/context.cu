@@ -569,14 +569,22 @@ static abyss_tuning plan_for(abyss_ctx *c, int m, const abyss_tuning *user) {
       }
   }
   // Built-in rule (measured on B200, King W0=6, N = 2^20): lanes over j for
-  // tiny active sets; one target per thread on the scalar tile kernel, in
-  // blocks of 32, 64 or 128 threads, up to 128 targets; otherwise the packed
+  // tiny active sets; warps sharing targets up to 96; one target per thread on
+  // the scalar tile kernel in 128-thread blocks up to 128 targets (or 32/64-thread
+  // blocks when a tuning asks for them); otherwise the packed
   // tile kernel, with anchor offsets on Hilbert-ordered targets once the active
   // set is dense enough for them to be accurate, double-single offsets below
   // that.
   if (t.kernel == 0) {
     if (m <= 24) {
       t.kernel = 2;
+    } else if (m <= 96 && t.threads == 0 && t.ipt == 0 && (t.mode == 0 || t.mode == 2)) {
+      // 25-96 targets: the block's 4 warps share 32 (up to 48 targets) or 64
+      // targets and split each j-tile (measured 374 against 347 Gpairs/s at
+      // m = 32 and 495 against 467 at m = 64 for one target per thread)
+      t.kernel = 4;
+      t.ipt = m <= 48 ? 1 : 2;
+      if (t.j_split == 0) t.j_split = m <= 48 ? 2048 : 1024;
     } else if (m <= 128 && (t.threads == 0 || t.threads == (m <= 48 ? 32 : m <= 96 ? 64 : 128)) &&
                (t.ipt == 0 || t.ipt == 1) && (t.mode == 0 || t.mode == 2)) {
       t.kernel = 1;
@@ -615,6 +623,13 @@ static abyss_tuning plan_for(abyss_ctx *c, int m, const abyss_tuning *user) {
         if (t.j_split == 0 && m <= 256) t.j_split = 2048;
       }
     }
+  } else if (t.kernel == 4) {
+    // warps sharing targets: 4 warps, double-single offsets, 32 x ipt targets per block
+    t.mode = 2;
+    t.threads = 128;
+    if (t.ipt == 0) t.ipt = 1;
+    t.unroll = 1;
+    t.min_blocks = 1;
   } else {
     if (t.mode == 0) t.mode = (m >= 4096) ? 1 : 2;
     if (t.threads == 0) t.threads = 128;
@@ -644,10 +659,11 @@ int abyss_launch(abyss_ctx *c, double eps2, int list_cap, const abyss_tuning *tu
     L = (n + want * nw - 1) / (want * nw);
     L = std::max(64, (L + 63) / 64 * 64);
     S = (n + L * nw - 1) / (L * nw);
-  } else if (t.kernel == 1 || t.kernel == 3) {
-    const int per_block = t.threads * t.ipt;
+  } else if (t.kernel == 1 || t.kernel == 3 || t.kernel == 4) {
+    const int per_block = t.kernel == 4 ? 32 * t.ipt : t.threads * t.ipt;
     n_iblocks = (m + per_block - 1) / per_block;
-    const int occ = tile_occupancy(t.threads, t.ipt, t.mode == 1, t.kernel == 3, t.unroll, t.min_blocks);
+    const int occ = t.kernel == 4 ? tile_split_occupancy(t.ipt)
+                                  : tile_occupancy(t.threads, t.ipt, t.mode == 1, t.kernel == 3, t.unroll, t.min_blocks);
     if (occ <= 0) return fail(c, ABYSS_ERR_ARG, "launch: unsupported tile shape");
     // persistent grid: every SM holds the same number of CTAs, which take
     // (i-block, j-chunk) items from a device counter
@@ -735,7 +751,11 @@ int abyss_launch(abyss_ctx *c, double eps2, int list_cap, const abyss_tuning *tu
   o.list = c->list.p;
   o.overflow_rows = c->ovf.p;
   o.ovf_list = c->ovf_list.p;
-  if (t.kernel == 1 || t.kernel == 3) {
+  if (t.kernel == 4) {
+    if (launch_tile_split(c->stream, t.ipt, grid, js, w, n_iblocks) != 0)
+      return fail(c, ABYSS_ERR_ARG, "launch: unsupported tile shape");
+    t.grid = grid;
+  } else if (t.kernel == 1 || t.kernel == 3) {
     if (launch_tile(c->stream, t.threads, t.ipt, t.mode == 1, t.kernel == 3, t.unroll, t.min_blocks, grid, js,
                     w, n_iblocks) != 0)
       return fail(c, ABYSS_ERR_ARG, "launch: unsupported tile shape");

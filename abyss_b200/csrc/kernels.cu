@@ -473,9 +473,16 @@ struct TileLayout {
 // test in a warp-uniform slow path (list entry, or regular contribution).
 // Tile partials are FP32; they are folded into Kahan-compensated FP32 sums kept
 // in shared memory, and written per (chunk, target) for the FP64 finalize.
-template <int NT, int IPT, int TJ, int NST, bool ANCHOR, bool PACK, int UNR, int MINB>
+//
+// JW > 1 (warps sharing targets): the block's JW warps hold the same 32 x IPT
+// targets and each takes every JW-th group of 32 j of a tile, so that a small
+// active set still fills the SMs with warps; at the end of an item warp 0 adds
+// the warps' sums in FP64 in warp order.
+template <int NT, int IPT, int TJ, int NST, bool ANCHOR, bool PACK, int UNR, int MINB, int JW = 1>
 __global__ void __launch_bounds__(NT, MINB) reg_force_tile(JSet js, Work w, int n_iblocks) {
+  static_assert(JW == 1 || NT == 32 * JW, "warps sharing targets: one target slot per lane");
   using LY = TileLayout<NT, IPT, TJ, NST, ANCHOR, PACK>;
+  constexpr int TS = JW > 1 ? 32 : NT;  // target slots per k (per lane, or per thread)
   constexpr int TJP = LY::TJP;
   constexpr int CW = LY::CW;
   // With PACK, targets 0 .. NPK-1 run in pairs on FP32x2 instructions and an odd
@@ -492,6 +499,8 @@ __global__ void __launch_bounds__(NT, MINB) reg_force_tile(JSet js, Work w, int 
   uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + LY::bar);
   int *s_item = reinterpret_cast<int *>(smem_raw + LY::item);
   const int tid = threadIdx.x;
+  const int sl = JW > 1 ? (tid & 31) : tid;  // this thread's target slot
+  const int wid = tid >> 5;
   const unsigned FULL = 0xffffffffu;
 
   if (tid == 0) {
@@ -519,8 +528,8 @@ __global__ void __launch_bounds__(NT, MINB) reg_force_tile(JSet js, Work w, int 
     } else {
       const int ib = item / w.n_chunks;
       ch = item - ib * w.n_chunks;
-      base = ib * NT * IPT;
-      count = min(NT * IPT, m_rows - base);
+      base = ib * TS * IPT;
+      count = min(TS * IPT, m_rows - base);
       j0 = ch * w.chunk_len;
       j1 = min(js.n, j0 + w.chunk_len);
     }
@@ -536,7 +545,7 @@ __global__ void __launch_bounds__(NT, MINB) reg_force_tile(JSet js, Work w, int 
     double ax = 0.0, ay = 0.0, az = 0.0;
     if (ANCHOR) {
       if (w.anchor && !w.items) {  // the i-block's bounding-box centre
-        const double *a = w.anchor + 3 * (size_t)(base / (NT * IPT));
+        const double *a = w.anchor + 3 * (size_t)(base / (TS * IPT));
         ax = a[0];
         ay = a[1];
         az = a[2];
@@ -551,12 +560,14 @@ __global__ void __launch_bounds__(NT, MINB) reg_force_tile(JSet js, Work w, int 
     float hx[IPT], hy[IPT], hz[IPT], lx[IPT], ly[IPT], lz[IPT], vx[IPT], vy[IPT], vz[IPT], r2g[IPT];
 #pragma unroll
     for (int k = 0; k < IPT; ++k) {
-      const int s = base + k * NT + tid;
-      const bool valid = k * NT + tid < count;
+      const int s = base + k * TS + sl;
+      const bool valid = k * TS + sl < count;
       const int si = valid ? s : base;
       const int t = w.order_t[si];
-      s_ti[k * NT + tid] = t;
-      s_row[k * NT + tid] = valid ? w.order_o[si] : -1;
+      if (JW == 1 || wid == 0) {
+        s_ti[k * TS + sl] = t;
+        s_row[k * TS + sl] = valid ? w.order_o[si] : -1;
+      }
       const double X = js.px[t], Y = js.py[t], Z = js.pz[t];
       double spread = 0.0;
       if (ANCHOR) {
@@ -660,7 +671,7 @@ __global__ void __launch_bounds__(NT, MINB) reg_force_tile(JSet js, Work w, int 
       // the data, so the j iterations schedule freely.  Up to UNR - 1 pad entries
       // past cnt may be visited: they are far away and massless, never
       // candidates, and contribute exactly 0.
-      for (int g0 = 0; g0 < cnt; g0 += 32) {
+      for (int g0 = JW > 1 ? 32 * wid : 0; g0 < cnt; g0 += 32 * JW) {
         const int gl = min(32, cnt - g0);
         unsigned cbits = 0u;
         for (int l = 0; l < gl; l += UNR) {
@@ -731,11 +742,11 @@ __global__ void __launch_bounds__(NT, MINB) reg_force_tile(JSet js, Work w, int 
               r2k = gg.r2;
             }
             if (!(r2k < r2g[k])) continue;
-            const int ti = s_ti[k * NT + tid];
+            const int ti = s_ti[k * TS + sl];
             if (jg == ti) continue;
             const double r2e = exact_r2(js.px[ti], js.py[ti], js.pz[ti], js.px[jg], js.py[jg], js.pz[jg]);
             if (r2e < js.r2nb[ti]) {
-              const int row = s_row[k * NT + tid];
+              const int row = s_row[k * TS + sl];
               const int pos = atomicAdd(&w.lcnt[row], 1);
               if (pos < w.cap) w.lst[(size_t)row * w.cap + pos] = jg;
             } else {
@@ -768,14 +779,36 @@ __global__ void __launch_bounds__(NT, MINB) reg_force_tile(JSet js, Work w, int 
         }
     }
 
+    if constexpr (JW == 1) {
 #pragma unroll
-    for (int k = 0; k < IPT; ++k) {
-      const int row = s_row[k * NT + tid];
-      if (row < 0) continue;
-      double *dst = w.part + ((size_t)row * w.s_stride + ch) * 6;
+      for (int k = 0; k < IPT; ++k) {
+        const int row = s_row[k * NT + tid];
+        if (row < 0) continue;
+        double *dst = w.part + ((size_t)row * w.s_stride + ch) * 6;
 #pragma unroll
-      for (int c = 0; c < 6; ++c)
-        dst[c] = (double)ksm[(k * 12 + c) * NT + tid] - (double)ksm[(k * 12 + 6 + c) * NT + tid];
+        for (int c = 0; c < 6; ++c)
+          dst[c] = (double)ksm[(k * 12 + c) * NT + tid] - (double)ksm[(k * 12 + 6 + c) * NT + tid];
+      }
+    } else {
+      // the warps' compensated sums of each target, in FP64 in warp order
+      __syncthreads();
+      if (wid == 0) {
+#pragma unroll
+        for (int k = 0; k < IPT; ++k) {
+          const int row = s_row[k * TS + sl];
+          if (row < 0) continue;
+          double *dst = w.part + ((size_t)row * w.s_stride + ch) * 6;
+#pragma unroll
+          for (int c = 0; c < 6; ++c) {
+            double v = 0.0;
+#pragma unroll
+            for (int q = 0; q < JW; ++q)
+              v += (double)ksm[(k * 12 + c) * NT + 32 * q + sl] - (double)ksm[(k * 12 + 6 + c) * NT + 32 * q + sl];
+            dst[c] = v;
+          }
+        }
+      }
+      __syncthreads();  // the next item's set-up rewrites the sums and the target slots
     }
   }
 }
@@ -1482,6 +1515,42 @@ int launch_tile(cudaStream_t s, int nt, int ipt, bool anchor, bool pack, int unr
   const TileVariant *v = find_variant(nt, ipt, anchor, pack, unr, minb);
   if (!v) return -1;
   v->launch(s, grid, js, w, n_iblocks);
+  return 0;
+}
+
+// Warps sharing targets (kernel 4): 4 warps, scalar pair arithmetic,
+// double-single offsets; 32 x ipt targets per block.
+template <int IPT>
+static int split_occ() {
+  constexpr int TJ = 128, NST = 3, NT = 128;
+  auto k = reg_force_tile<NT, IPT, TJ, NST, false, false, 1, 1, 4>;
+  const size_t sm = TileLayout<NT, IPT, TJ, NST, false, false>::bytes;
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  int blocks = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k, NT, sm);
+  return blocks;
+}
+
+template <int IPT>
+static void split_run(cudaStream_t s, int grid, const JSet &js, const Work &w, int n_iblocks) {
+  constexpr int TJ = 128, NST = 3, NT = 128;
+  auto k = reg_force_tile<NT, IPT, TJ, NST, false, false, 1, 1, 4>;
+  const size_t sm = TileLayout<NT, IPT, TJ, NST, false, false>::bytes;
+  k<<<grid, NT, sm, s>>>(js, w, n_iblocks);
+}
+
+int tile_split_occupancy(int ipt) {
+  const int occ = ipt == 1 ? split_occ<1>() : ipt == 2 ? split_occ<2>() : -1;
+  return cudaGetLastError() == cudaSuccess ? occ : -1;
+}
+
+int launch_tile_split(cudaStream_t s, int ipt, int grid, const JSet &js, const Work &w, int n_iblocks) {
+  if (ipt == 1)
+    split_run<1>(s, grid, js, w, n_iblocks);
+  else if (ipt == 2)
+    split_run<2>(s, grid, js, w, n_iblocks);
+  else
+    return -1;
   return 0;
 }
 

@@ -441,6 +441,13 @@ def run_config(name: str, duration: float = 1.0, sample: int = 16, device_irregu
     res, done = serve(reqs=reqs, nmax=nmax, capacity=capacity, host_threads=host_threads,
                       device_irregular_min_n=device_irregular_min_n)
     res.pop("phase_s", None)
+    res["config"] = dict(
+        name=name, requests=len(reqs), device_irregular_min_n=device_irregular_min_n, host_threads=host_threads,
+        capacity=capacity,
+        workload=("512 equal-mass Plummer clusters, N log-uniform in [256, 16384] (seed 4, cluster k seeded "
+                  "4000 + k), eps = 1e-4, all arriving at t = 0, each to t = 5" if name == "c4" else
+                  f"Poisson 200 requests/s for {duration} s (seed 5), Plummer or King W0 3/6/9, Kroupa IMF, "
+                  "N log-uniform in [1024, 131072], eps = 1e-4, each to t = 1"))
     de = {r.rid: r.result["dE_over_E"] for r in done}
     res["dE_over_E_by_request"] = [de[k] for k in sorted(de)]
     # serial plain on a sample (fresh requests: the served ones hold their results)

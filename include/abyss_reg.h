@@ -44,7 +44,9 @@ typedef struct abyss_ctx abyss_ctx;
  * installed with abyss_set_tuning_table). */
 typedef struct abyss_tuning {
   int kernel;  /* 1 = tile kernel (i in registers, j-tiles by TMA), 2 = j-major kernel,
-                  3 = tile kernel with packed FP32x2 pair arithmetic */
+                  3 = tile kernel with packed FP32x2 pair arithmetic,
+                  4 = tile kernel whose 4 warps share 32 x ipt targets (ipt 1 or 2) and
+                      split each j-tile, for small active sets (double-single) */
   int mode;    /* tile kernel: 1 = anchor offsets on spatially ordered targets, 2 = double-single */
   int threads; /* tile kernel: 128 or 256 */
   int ipt;     /* tile: targets per thread 1, 2, 4;  j-major: targets per pass 1, 2, 4, 8 */
