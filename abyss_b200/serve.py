@@ -100,13 +100,19 @@ class Server:
     def __init__(self, device: int = 0, capacity: int = 1 << 21, max_clusters: int = 512, list_cap: int = 128,
                  eps2: float = 1e-8, eta_reg: float = 0.02, eta_irr: float = 0.01, host_threads: int = 16,
                  slice_ms: float = 20.0, max_n: int = 16384, chunk_j: int = 256, device_irregular_min_n: int = 0,
-                 team_min_n: int = 16384):
+                 team_min_n: int = 16384, lane_min_n: int = 0, lane_threads: int = 2, lane_team: int = 4):
         """device_irregular_min_n > 0: integrations of at least that many
         particles run their irregular levels on the GPU (include/abyss_irr.h)
         instead of on their worker thread; the results are the same.
         team_min_n: integrations of at least that many particles get a team of
         1 + n / team_min_n host threads (at most host_threads) for their host
-        work; smaller ones run on their worker thread alone."""
+        work; smaller ones run on their worker thread alone.
+        lane_min_n > 0: requests of at least that many particles skip the waves:
+        one of their regular blocks fills the GPU alone, so batching gains them
+        nothing and its round trips would set their latency.  Each runs whole on
+        one of lane_threads host threads, through a context of its own, with a
+        team of lane_team threads and (above device_irregular_min_n) its
+        irregular levels on the GPU."""
         self.rf = RegularForce(device)
         self.ens = Ensemble(self.rf, None, list_cap=list_cap, capacity=capacity, max_clusters=max_clusters)
         # short j-chunks: a serving wave is small and latency-bound, so its work
@@ -116,6 +122,14 @@ class Server:
         self.eta_reg, self.eta_irr = eta_reg, eta_irr
         self.device_irregular_min_n = int(device_irregular_min_n)
         self.team_min_n = max(1, int(team_min_n))
+        self.lane_min_n = int(lane_min_n)
+        self.lane_team = max(1, int(lane_team))
+        self.lane_jobs: list = []  # (request, future) of large requests run whole
+        self.lane_pool = ThreadPoolExecutor(max_workers=max(1, lane_threads)) if self.lane_min_n > 0 else None
+        self.lane_ctx: queue.Queue = queue.Queue()
+        if self.lane_min_n > 0:
+            for _ in range(max(1, lane_threads)):
+                self.lane_ctx.put(RegularForce(device))
         self.list_cap = list_cap
         nthreads = max(1, host_threads)
         self.host_threads = nthreads
@@ -159,6 +173,10 @@ class Server:
     def close(self):
         self._reap(wait=True)
         self.pool.shutdown()
+        if self.lane_pool is not None:
+            self.lane_pool.shutdown()
+            while not self.lane_ctx.empty():
+                self.lane_ctx.get().close()
         for r, _ in self.building:
             if r.ac is not None:
                 r.ac.close()
@@ -214,6 +232,10 @@ class Server:
         for r in self.waiting:
             if r.arrival > self.now():
                 still.append(r)
+                continue
+            if self.lane_min_n > 0 and r.n >= self.lane_min_n:
+                r.admitted = self.now()
+                self.lane_jobs.append((r, self.lane_pool.submit(self._run_lane, r)))
                 continue
             slot = self.ens.attach(r.n)
             if slot is None:
@@ -285,6 +307,41 @@ class Server:
         ph["retire"] += time.perf_counter() - t
         self.rounds += 1
 
+    def _run_lane(self, r: Request):
+        """A large request run whole, outside the waves (the plain single-cluster
+        path on a context of this lane)."""
+        c = r.make_cluster()
+        rf = self.lane_ctx.get()
+        try:
+            ac = ACIntegrator(rf, c.x, c.v, c.m, c.r2nb, eps2=self.eps2, eta_reg=self.eta_reg,
+                              eta_irr=self.eta_irr, fix_nb=r.k_nb, nb_max=self.list_cap, t_end=r.t_end,
+                              threads=self.lane_team)
+            if self.device_irregular_min_n > 0 and r.n >= self.device_irregular_min_n:
+                ac.set_device_irregular(True)
+            r.e0 = ac.energy()
+            ac.run(1.0)
+            r.e1 = ac.energy()
+            r.blocks = int(ac.stats()["blocks"])
+            r.finished = self.now()
+            r.result = dict(rid=r.rid, n=r.n, model=r.model, dE_over_E=abs((r.e1 - r.e0) / r.e0), blocks=r.blocks,
+                            latency_s=r.finished - r.arrival, queue_s=r.admitted - r.arrival,
+                            device_irregular=ac.device_irregular_info()["on"], lane=True,
+                            x_final=ac.state()["x"])
+            ac.close()
+        finally:
+            self.lane_ctx.put(rf)
+        r.cluster = None
+
+    def _reap_lane(self, wait: bool = False):
+        still = []
+        for r, fut in self.lane_jobs:
+            if wait or fut.done():
+                fut.result()
+                self.done.append(r)
+            else:
+                still.append((r, fut))
+        self.lane_jobs = still
+
     def _reap(self, wait: bool = False):
         still = []
         for r, fut in self.retiring:
@@ -308,11 +365,16 @@ class Server:
         r.ac = None
 
     def run_until_idle(self, max_seconds: float = 1e9):
-        while (self.waiting or self.building or self.active) and self.now() < max_seconds:
-            if not self.active and self.waiting and all(r.arrival > self.now() for r in self.waiting):
-                time.sleep(max(0.0, min(r.arrival for r in self.waiting) - self.now()))
+        while (self.waiting or self.building or self.active or self.lane_jobs) and self.now() < max_seconds:
+            self._reap_lane()
+            if not self.active and not self.building and self.waiting and \
+                    all(r.arrival > self.now() for r in self.waiting):
+                time.sleep(max(0.0, min(0.05, min(r.arrival for r in self.waiting) - self.now())))
+            if not self.active and not self.building and not self.waiting and self.lane_jobs:
+                time.sleep(0.01)  # only large requests left: they run on their own threads
             self.round()
         self._reap(wait=True)
+        self._reap_lane(wait=True)
 
 
 def poisson_requests(rate: float, duration: float, nmin: int, nmax: int, seed: int = 5, t_end: float = 1.0,
@@ -333,7 +395,8 @@ def poisson_requests(rate: float, duration: float, nmin: int, nmax: int, seed: i
 
 def serve(rate: float = 200.0, duration: float = 2.0, nmin: int = 256, nmax: int = 2048, t_end: float = 0.0625,
           capacity: int = 1 << 21, seed: int = 5, host_threads: int = 16, serial: bool = False,
-          chunk_j: int = 256, slice_ms: float = 20.0, device_irregular_min_n: int = 0, reqs=None):
+          chunk_j: int = 256, slice_ms: float = 20.0, device_irregular_min_n: int = 0, reqs=None,
+          lane_min_n: int = 0):
     """Run a Poisson stream through the server (or, with serial=True, one request at
     a time through the same code) and report latency percentiles and throughput.
     `reqs` replaces the generated stream (requests with prebuilt clusters)."""
@@ -348,7 +411,8 @@ def serve(rate: float = 200.0, duration: float = 2.0, nmin: int = 256, nmax: int
         srv = None
     else:
         srv = Server(capacity=capacity, host_threads=host_threads, max_n=max(nmax, max(r.n for r in reqs)),
-                     chunk_j=chunk_j, slice_ms=slice_ms, device_irregular_min_n=device_irregular_min_n)
+                     chunk_j=chunk_j, slice_ms=slice_ms, device_irregular_min_n=device_irregular_min_n,
+                     lane_min_n=lane_min_n)
         for r in reqs:
             srv.submit(r)
         srv.run_until_idle()
@@ -422,7 +486,7 @@ def c4_requests(k: int = 512, t_end: float = 5.0):
 
 
 def run_config(name: str, duration: float = 1.0, sample: int = 16, device_irregular_min_n: int = 4096,
-               host_threads: int = 16, capacity: int = 1 << 22):
+               host_threads: int = 16, capacity: int = 1 << 22, lane_min_n: int = 32768):
     """A stated configuration through the continuous server, and the serial
     plain form on an evenly spaced sample of the same requests (the whole
     stream one at a time would take hours): its clusters/s is the sample's
@@ -439,11 +503,11 @@ def run_config(name: str, duration: float = 1.0, sample: int = 16, device_irregu
     for r in reqs:
         r.cluster = r.make_cluster()
     res, done = serve(reqs=reqs, nmax=nmax, capacity=capacity, host_threads=host_threads,
-                      device_irregular_min_n=device_irregular_min_n)
+                      device_irregular_min_n=device_irregular_min_n, lane_min_n=lane_min_n)
     res.pop("phase_s", None)
     res["config"] = dict(
         name=name, requests=len(reqs), device_irregular_min_n=device_irregular_min_n, host_threads=host_threads,
-        capacity=capacity,
+        capacity=capacity, lane_min_n=lane_min_n,
         workload=("512 equal-mass Plummer clusters, N log-uniform in [256, 16384] (seed 4, cluster k seeded "
                   "4000 + k), eps = 1e-4, all arriving at t = 0, each to t = 5" if name == "c4" else
                   f"Poisson 200 requests/s for {duration} s (seed 5), Plummer or King W0 3/6/9, Kroupa IMF, "
@@ -479,6 +543,7 @@ def main():
     ap.add_argument("--config", choices=["c4", "c5"], default=None)
     ap.add_argument("--sample", type=int, default=16)
     ap.add_argument("--device-irregular-min-n", type=int, default=4096)
+    ap.add_argument("--lane-min-n", type=int, default=32768)
     ap.add_argument("--rate", type=float, default=2000.0)
     ap.add_argument("--duration", type=float, default=0.5)
     ap.add_argument("--nmin", type=int, default=256)
@@ -489,7 +554,8 @@ def main():
     args = ap.parse_args()
     if args.config:
         print(json.dumps(run_config(args.config, duration=args.duration, sample=args.sample,
-                                    device_irregular_min_n=args.device_irregular_min_n, host_threads=args.threads)))
+                                    device_irregular_min_n=args.device_irregular_min_n, host_threads=args.threads,
+                                    lane_min_n=args.lane_min_n)))
         return
     out = {}
     for serial in (False, True):

@@ -70,3 +70,34 @@ def test_device_irregular_levels_in_serving_give_the_same_results():
         assert host[k]["blocks"] == dev[k]["blocks"], k
         assert np.array_equal(host[k]["x_final"], dev[k]["x_final"]), k
         assert host[k]["dE_over_E"] == dev[k]["dE_over_E"], k
+
+
+def test_large_requests_run_whole_on_the_lane():
+    """Requests above the lane size run whole outside the waves (the plain
+    single-cluster path on a lane context, device irregular levels) while the
+    others are served; a lane result equals the same integration run directly."""
+    from abyss_b200.integrator import ACIntegrator
+    from abyss_b200.regforce import RegularForce
+
+    reqs = poisson_requests(rate=400.0, duration=0.04, nmin=256, nmax=3000, seed=14, t_end=0.03125, k_nb=16)
+    srv = Server(capacity=1 << 17, max_clusters=32, list_cap=64, host_threads=8, max_n=3000,
+                 device_irregular_min_n=1024, lane_min_n=1500)
+    for r in reqs:
+        srv.submit(r)
+    srv.run_until_idle(max_seconds=300)
+    done = {r.rid: r for r in srv.done}
+    srv.close()
+    assert len(done) == len(reqs)
+    lane = [r for r in done.values() if r.result.get("lane")]
+    assert lane and len(lane) < len(reqs)
+    probe = lane[0]
+    c = Request(probe.rid, 0.0, probe.model, probe.n, probe.seed, t_end=probe.t_end, k_nb=probe.k_nb).make_cluster()
+    rf = RegularForce(0)
+    try:
+        ac = ACIntegrator(rf, c.x, c.v, c.m, c.r2nb, eps2=1e-8, eta_reg=0.02, eta_irr=0.01, fix_nb=probe.k_nb,
+                          nb_max=64, t_end=probe.t_end, threads=1)
+        ac.run(1.0)
+        assert np.array_equal(ac.state()["x"], probe.result["x_final"])
+        ac.close()
+    finally:
+        rf.close()
