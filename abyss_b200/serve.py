@@ -486,7 +486,7 @@ def c4_requests(k: int = 512, t_end: float = 5.0):
 
 
 def run_config(name: str, duration: float = 1.0, sample: int = 16, device_irregular_min_n: int = 4096,
-               host_threads: int = 16, capacity: int = 1 << 22, lane_min_n: int = 32768):
+               host_threads: int = 16, capacity: int = 1 << 22, lane_min_n: int = 0):
     """A stated configuration through the continuous server, and the serial
     plain form on an evenly spaced sample of the same requests (the whole
     stream one at a time would take hours): its clusters/s is the sample's
@@ -543,7 +543,8 @@ def main():
     ap.add_argument("--config", choices=["c4", "c5"], default=None)
     ap.add_argument("--sample", type=int, default=16)
     ap.add_argument("--device-irregular-min-n", type=int, default=4096)
-    ap.add_argument("--lane-min-n", type=int, default=32768)
+    ap.add_argument("--lane-min-n", type=int, default=0,
+                    help="requests of at least this many particles run whole outside the waves (0: none)")
     ap.add_argument("--rate", type=float, default=2000.0)
     ap.add_argument("--duration", type=float, default=0.5)
     ap.add_argument("--nmin", type=int, default=256)
