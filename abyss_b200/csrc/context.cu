@@ -628,7 +628,7 @@ static abyss_tuning plan_for(abyss_ctx *c, int m, const abyss_tuning *user) {
     t.mode = 2;
     t.threads = 128;
     if (t.ipt == 0) t.ipt = 1;
-    t.unroll = 1;
+    if (t.unroll == 0) t.unroll = 1;
     t.min_blocks = 1;
   } else {
     if (t.mode == 0) t.mode = (m >= 4096) ? 1 : 2;
@@ -662,7 +662,7 @@ int abyss_launch(abyss_ctx *c, double eps2, int list_cap, const abyss_tuning *tu
   } else if (t.kernel == 1 || t.kernel == 3 || t.kernel == 4) {
     const int per_block = t.kernel == 4 ? 32 * t.ipt : t.threads * t.ipt;
     n_iblocks = (m + per_block - 1) / per_block;
-    const int occ = t.kernel == 4 ? tile_split_occupancy(t.ipt)
+    const int occ = t.kernel == 4 ? tile_split_occupancy(t.ipt, t.unroll)
                                   : tile_occupancy(t.threads, t.ipt, t.mode == 1, t.kernel == 3, t.unroll, t.min_blocks);
     if (occ <= 0) return fail(c, ABYSS_ERR_ARG, "launch: unsupported tile shape");
     // persistent grid: every SM holds the same number of CTAs, which take
@@ -752,7 +752,7 @@ int abyss_launch(abyss_ctx *c, double eps2, int list_cap, const abyss_tuning *tu
   o.overflow_rows = c->ovf.p;
   o.ovf_list = c->ovf_list.p;
   if (t.kernel == 4) {
-    if (launch_tile_split(c->stream, t.ipt, grid, js, w, n_iblocks) != 0)
+    if (launch_tile_split(c->stream, t.ipt, t.unroll, grid, js, w, n_iblocks) != 0)
       return fail(c, ABYSS_ERR_ARG, "launch: unsupported tile shape");
     t.grid = grid;
   } else if (t.kernel == 1 || t.kernel == 3) {

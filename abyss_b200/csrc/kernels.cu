@@ -1519,11 +1519,11 @@ int launch_tile(cudaStream_t s, int nt, int ipt, bool anchor, bool pack, int unr
 }
 
 // Warps sharing targets (kernel 4): 4 warps, scalar pair arithmetic,
-// double-single offsets; 32 x ipt targets per block.
-template <int IPT>
+// double-single offsets; 32 x ipt targets per block; 1 or 2 j per step.
+template <int IPT, int UNR>
 static int split_occ() {
   constexpr int TJ = 128, NST = 3, NT = 128;
-  auto k = reg_force_tile<NT, IPT, TJ, NST, false, false, 1, 1, 4>;
+  auto k = reg_force_tile<NT, IPT, TJ, NST, false, false, UNR, 1, 4>;
   const size_t sm = TileLayout<NT, IPT, TJ, NST, false, false>::bytes;
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   int blocks = 0;
@@ -1531,24 +1531,30 @@ static int split_occ() {
   return blocks;
 }
 
-template <int IPT>
+template <int IPT, int UNR>
 static void split_run(cudaStream_t s, int grid, const JSet &js, const Work &w, int n_iblocks) {
   constexpr int TJ = 128, NST = 3, NT = 128;
-  auto k = reg_force_tile<NT, IPT, TJ, NST, false, false, 1, 1, 4>;
+  auto k = reg_force_tile<NT, IPT, TJ, NST, false, false, UNR, 1, 4>;
   const size_t sm = TileLayout<NT, IPT, TJ, NST, false, false>::bytes;
   k<<<grid, NT, sm, s>>>(js, w, n_iblocks);
 }
 
-int tile_split_occupancy(int ipt) {
-  const int occ = ipt == 1 ? split_occ<1>() : ipt == 2 ? split_occ<2>() : -1;
+int tile_split_occupancy(int ipt, int unr) {
+  int occ = -1;
+  if (ipt == 1) occ = unr == 2 ? split_occ<1, 2>() : split_occ<1, 1>();
+  if (ipt == 2) occ = unr == 2 ? split_occ<2, 2>() : split_occ<2, 1>();
   return cudaGetLastError() == cudaSuccess ? occ : -1;
 }
 
-int launch_tile_split(cudaStream_t s, int ipt, int grid, const JSet &js, const Work &w, int n_iblocks) {
-  if (ipt == 1)
-    split_run<1>(s, grid, js, w, n_iblocks);
-  else if (ipt == 2)
-    split_run<2>(s, grid, js, w, n_iblocks);
+int launch_tile_split(cudaStream_t s, int ipt, int unr, int grid, const JSet &js, const Work &w, int n_iblocks) {
+  if (ipt == 1 && unr == 2)
+    split_run<1, 2>(s, grid, js, w, n_iblocks);
+  else if (ipt == 1 && unr == 1)
+    split_run<1, 1>(s, grid, js, w, n_iblocks);
+  else if (ipt == 2 && unr == 2)
+    split_run<2, 2>(s, grid, js, w, n_iblocks);
+  else if (ipt == 2 && unr == 1)
+    split_run<2, 1>(s, grid, js, w, n_iblocks);
   else
     return -1;
   return 0;

@@ -45,6 +45,8 @@ SHAPES = [
     ("jmajor-8", dict(kernel=2, ipt=8)),
     ("split-ds-128x1", dict(kernel=4, ipt=1)),
     ("split-ds-128x2", dict(kernel=4, ipt=2)),
+    ("split-ds-128x1-u2", dict(kernel=4, ipt=1, unroll=2)),
+    ("split-ds-128x2-u2", dict(kernel=4, ipt=2, unroll=2)),
 ]
 
 
