@@ -579,11 +579,13 @@ static abyss_tuning plan_for(abyss_ctx *c, int m, const abyss_tuning *user) {
     if (m <= 24) {
       t.kernel = 2;
     } else if (m <= 96 && t.threads == 0 && t.ipt == 0 && (t.mode == 0 || t.mode == 2)) {
-      // 25-96 targets: the block's 4 warps share 32 (up to 48 targets) or 64
-      // targets and split each j-tile (measured 374 against 347 Gpairs/s at
-      // m = 32 and 495 against 467 at m = 64 for one target per thread)
+      // 25-96 targets: the block's 4 warps share 32 targets (64 for 49-64
+      // targets) and split each j-tile, two j per step (measured 384 against
+      // 347 Gpairs/s at m = 32, 502 against 467 at m = 64, 518 at m = 96, for
+      // one target per thread in 32/64/128-thread blocks)
       t.kernel = 4;
-      t.ipt = m <= 48 ? 1 : 2;
+      t.ipt = (m > 48 && m <= 64) ? 2 : 1;
+      t.unroll = 2;
       if (t.j_split == 0) t.j_split = m <= 48 ? 2048 : 1024;
     } else if (m <= 128 && (t.threads == 0 || t.threads == (m <= 48 ? 32 : m <= 96 ? 64 : 128)) &&
                (t.ipt == 0 || t.ipt == 1) && (t.mode == 0 || t.mode == 2)) {

@@ -337,33 +337,52 @@ __device__ void store_pend(Pend *dst, const Pend &pd) {
 }
 
 // IrrUpdate: commit particle i's pending step; returns its next block time.
+// Every pending field is loaded before the first store: with loads and stores
+// interleaved the compiler cannot tell them apart (possible aliasing) and would
+// run some thirty L2 round trips one after another.
 __device__ ULL commit(const State &S, const Params &P, int i) {
   const Pend *q = &S.pend[i];
   const int lv = __ldcg(&q->lv_irr);
+  const int move = __ldcg(&q->move);
   const double dtv = __ldcg(&q->dt_irr);
   const ULL tb = __ldcg(&q->tb_irr), nc = __ldcg(&q->new_cur);
+  double at[12], ai[12], nx[3], nv[3];
+#pragma unroll
+  for (int k = 0; k < 12; ++k) {
+    at[k] = __ldcg(&q->a_tot[k]);
+    ai[k] = __ldcg(&q->a_irr[k]);
+  }
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    nx[d] = __ldcg(&q->nx[d]);
+    nv[d] = __ldcg(&q->nv[d]);
+  }
+  const int nn = S.nnb[i];
   S.lv_irr[i] = lv;
   S.dt_irr[i] = dtv;
   S.tb_irr[i] = tb;
   S.new_cur_irr[i] = nc;
   Rec *r = &S.rec[i];
+#pragma unroll
   for (int k = 0; k < 12; ++k) {
-    S.a_tot[12 * (size_t)i + k] = __ldcg(&q->a_tot[k]);
-    S.a_irr[12 * (size_t)i + k] = __ldcg(&q->a_irr[k]);
+    S.a_tot[12 * (size_t)i + k] = at[k];
+    S.a_irr[12 * (size_t)i + k] = ai[k];
   }
   const ULL next = nc + tb;
   S.next_irr[i] = next;
-  if (S.nnb[i] > 0 && __ldcg(&q->move)) {
+  if (nn > 0 && move) {
+#pragma unroll
     for (int d = 0; d < 3; ++d) {
-      r->x[d] = __ldcg(&q->nx[d]);
-      r->v[d] = __ldcg(&q->nv[d]);
+      r->x[d] = nx[d];
+      r->v[d] = nv[d];
     }
   }
   S.cur_irr[i] = nc;
   r->t = (double)nc * P.time_step;
+#pragma unroll
   for (int d = 0; d < 3; ++d) {
-    r->a0[d] = __ldcg(&q->a_tot[4 * d + 0]);
-    r->a1[d] = __ldcg(&q->a_tot[4 * d + 1]);
+    r->a0[d] = at[4 * d + 0];
+    r->a1[d] = at[4 * d + 1];
   }
   S.touched[i] = 1;
   return next;
