@@ -163,6 +163,8 @@ def lib():
     _ull = C.POINTER(C.c_ulonglong)
     L.abyss_ac_set_device_irregular.argtypes = [_vp, C.c_int]
     L.abyss_ac_device_irregular_info.argtypes = [_vp, _ip, C.POINTER(C.c_longlong), _dp, C.POINTER(C.c_longlong)]
+    L.abyss_ac_set_device_resident.argtypes = [_vp, C.c_int]
+    L.abyss_ac_device_resident_info.argtypes = [_vp, _ip, C.POINTER(C.c_longlong), _dp]
     L.abyss_device_irregular_steps.argtypes = ([C.c_int, C.c_int] + [_dp] * 9 + [_ip, _ip, C.c_int, C.c_double,
                                                C.c_double, C.c_int, C.c_double, _ip, _ull, _ull, C.c_int, _ip] +
                                                [_dp] * 4 + [_ip, _dp, _ull])

@@ -19,6 +19,7 @@
 
 #include "../../include/abyss_reg.h"
 #include "abyss_internal.cuh"
+#include "ctx_internal.h"
 #include "kernels.cuh"
 
 using namespace abyss;
@@ -336,6 +337,83 @@ namespace abyss {
 cudaStream_t ctx_stream(abyss_ctx *c) { return c->stream; }
 int ctx_device(abyss_ctx *c) { return c->device; }
 int ctx_sm_count(abyss_ctx *c) { return c->sm_count; }
+
+// ---- used by whole regular blocks on the device (host/ac_integrator.cpp):
+// the state the host would upload is written into the context by a kernel on
+// its stream, the targets come from device memory, and the results stay there.
+
+// Device arrays of the j-set state for n particles, to be written on the
+// context stream before abyss_predict (as abyss_upload_state would).
+int ctx_state_buffers(abyss_ctx *c, int n, abyss_irr::JsetDst *d) {
+  if (!c || n <= 0 || !d) return ABYSS_ERR_ARG;
+  cudaSetDevice(c->device);
+  int rc = ensure_jset(c, n);
+  if (rc != ABYSS_OK) return rc;
+  const size_t v3 = (size_t)3 * n;
+  CK(c->x.ensure(v3), "alloc x");
+  CK(c->v.ensure(v3), "alloc v");
+  CK(c->a0.ensure(v3), "alloc a0");
+  CK(c->a1.ensure(v3), "alloc a1");
+  CK(c->t0.ensure(n), "alloc t0");
+  *d = abyss_irr::JsetDst{c->x.p, c->v.p, c->a0.p, c->a1.p, c->t0.p, c->mass.p, c->r2nb.p};
+  c->n = n;
+  c->have_state = true;
+  c->have_jset = false;
+  return ABYSS_OK;
+}
+
+// m targets copied on the context stream from device memory (indices already
+// inside the j-set: they come from the integrator's own scheduling kernel).
+int ctx_targets_from_device(abyss_ctx *c, int m, const int *d_targets) {
+  if (!c || m <= 0 || !d_targets) return ABYSS_ERR_ARG;
+  if (c->n <= 0 || m > c->n) return fail(c, ABYSS_ERR_STATE, "targets: no j-set of that size");
+  cudaSetDevice(c->device);
+  int rc = ensure_targets(c, m);
+  if (rc != ABYSS_OK) return rc;
+  CK(cudaMemcpyAsync(c->targets.p, d_targets, sizeof(int) * (size_t)m, cudaMemcpyDeviceToDevice, c->stream),
+     "D2D targets");
+  c->m = m;
+  return ABYSS_OK;
+}
+
+// The last launch's status word and overflowed-row count (waits for it).
+int ctx_launch_status(abyss_ctx *c, int *status, int *ovf) {
+  if (!c || !status || !ovf) return ABYSS_ERR_ARG;
+  if (!c->launched) return fail(c, ABYSS_ERR_STATE, "status: nothing launched");
+  cudaSetDevice(c->device);
+  int v[2] = {0, 0};
+  CK(cudaMemcpyAsync(&v[0], c->status.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "D2H status");
+  CK(cudaMemcpyAsync(&v[1], c->ovf.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "D2H overflow");
+  CK(ctx_wait(c), "synchronize");
+  *status = v[0] & kErrTimeout ? ABYSS_ERR_TIMEOUT : ABYSS_OK;
+  *ovf = v[1];
+  return ABYSS_OK;
+}
+
+// Device pointers of the last launch's results.
+int ctx_results(abyss_ctx *c, abyss_irr::RegResults *r) {
+  if (!c || !r) return ABYSS_ERR_ARG;
+  if (!c->launched) return fail(c, ABYSS_ERR_STATE, "results: nothing launched");
+  *r = abyss_irr::RegResults{c->acc_reg.p, c->jerk_reg.p, c->acc_irr.p, c->jerk_irr.p, c->nnb.p, c->list.p,
+                             c->launched_cap};
+  return ABYSS_OK;
+}
+
+// The last launch's targets (m) and the j-set radii (n), into host memory.
+int ctx_read_targets(abyss_ctx *c, int *targets, double *r2nb) {
+  if (!c) return ABYSS_ERR_ARG;
+  if (!c->launched) return fail(c, ABYSS_ERR_STATE, "read targets: nothing launched");
+  cudaSetDevice(c->device);
+  if (targets)
+    CK(cudaMemcpyAsync(targets, c->targets.p, sizeof(int) * (size_t)c->launched_m, cudaMemcpyDeviceToHost,
+                       c->stream),
+       "D2H targets");
+  if (r2nb)
+    CK(cudaMemcpyAsync(r2nb, c->r2nb.p, sizeof(double) * (size_t)c->n, cudaMemcpyDeviceToHost, c->stream),
+       "D2H radii");
+  CK(ctx_wait(c), "synchronize");
+  return ABYSS_OK;
+}
 }  // namespace abyss
 
 extern "C" {

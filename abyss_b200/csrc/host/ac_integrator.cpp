@@ -53,12 +53,8 @@
 #include "../../../include/abyss_irr.h"
 #include "../../../include/abyss_reg.h"
 #include "../irregular.h"
+#include "../ctx_internal.h"
 #include "pair_terms.h"
-
-struct abyss_ctx;
-namespace abyss {
-int ctx_device(abyss_ctx *c);  // context.cu
-}
 
 namespace {
 
@@ -134,6 +130,13 @@ struct abyss_ac {
   long long dev_borderline = 0;
   long long dev_cycles[6] = {0, 0, 0, 0, 0, 0};
   double dev_sec_copy = 0.0;
+  // whole blocks on the device (abyss_ac_set_device_resident): the engine's
+  // state is the state of record while dev_res; the particles here are a copy,
+  // refreshed from the device when host_stale and something reads them
+  bool dev_res = false, host_stale = false;
+  long long res_borderline = 0;
+  double res_sec_sync = 0.0;
+  int res_last_m = 0;  // the last device block's size (its record is the context's)
   // pinned staging of the j-set uploaded for each regular block: x, v, a0, a1
   // ([n][3] each), t0, m, r2nb ([n] each)
   double *jstage = nullptr;
@@ -763,6 +766,8 @@ void pack_image(const abyss_ac *ac, int i, abyss_irr::Image &g, int *lists, long
   g.nnb = (int)p.nb.size();
   g.index = i;
   g.list_off = list_off;
+  g.r2nb = p.r2nb;
+  g.dt_reg = p.dt_reg;
   if (!p.nb.empty()) std::memcpy(lists + list_off, p.nb.data(), sizeof(int) * p.nb.size());
 }
 
@@ -868,6 +873,255 @@ int irregular_levels_device(abyss_ac *ac) {
   if (run != ABYSS_OK) {
     ac->err = engine_error(ac->eng);
     return run;
+  }
+  return ABYSS_OK;
+}
+
+// ------------------------------------------------------------ whole blocks on the device
+// With abyss_ac_set_device_resident the state of record lives in the engine's
+// device arrays and a block never leaves the GPU: the next block's particles
+// (updateNextRegTime), the irregular levels, the j-set handed to the context,
+// the regular force and the corrector, commit, time steps and radii
+// (irregular.cu blk_*).  The host learns the block time and size and reads
+// the particles back only when something asks for them.
+
+// Every field of particle i from a device image (and its list).
+void unpack_image(abyss_ac *ac, int i, const abyss_irr::Image &g, const int *list) {
+  Star &p = ac->s[i];
+  for (int d = 0; d < 3; ++d) {
+    p.x[d] = g.x[d];
+    p.v[d] = g.v[d];
+  }
+  p.m = g.m;
+  p.t_irr = g.t_irr;
+  p.t_reg = g.t_reg;
+  p.dt_irr = g.dt_irr;
+  p.dt_reg = g.dt_reg;
+  p.r2nb = g.r2nb;
+  std::memcpy(p.a_tot, g.a_tot, sizeof(p.a_tot));
+  std::memcpy(p.a_reg, g.a_reg, sizeof(p.a_reg));
+  std::memcpy(p.a_irr, g.a_irr, sizeof(p.a_irr));
+  p.cur_irr = g.cur_irr;
+  p.tb_irr = g.tb_irr;
+  p.next_irr = g.next_irr;
+  p.new_cur_irr = g.new_cur_irr;
+  p.cur_reg = g.cur_reg;
+  p.tb_reg = g.tb_reg;
+  p.lv_irr = g.lv_irr;
+  p.lv_reg = g.lv_reg;
+  p.nb.assign(list, list + g.nnb);
+}
+
+// The particles here from the device, if a device block changed them since
+// they were last read.  Logically const: the copy is a cache of the device's.
+int resident_sync_host(const abyss_ac *cac) {
+  abyss_ac *ac = const_cast<abyss_ac *>(cac);
+  if (!ac->dev_res || !ac->host_stale) return ABYSS_OK;
+  const double t0 = now_s();
+  int rc = abyss_irr::engine_download_all(ac->eng);
+  if (rc != ABYSS_OK) {
+    ac->err = std::string("device state: ") + abyss_irr::engine_error(ac->eng);
+    return rc;
+  }
+  const abyss_irr::Image *img = abyss_irr::engine_images(ac->eng);
+  const int *lists = abyss_irr::engine_lists(ac->eng);
+  const size_t cap = ac->p.nb_max;
+  int failed = 0;
+#pragma omp parallel for schedule(static) reduction(+ : failed) if (ac->n >= 16384)
+  for (int i = 0; i < ac->n; ++i) {
+    try {
+      unpack_image(ac, i, img[i], lists + (size_t)i * cap);
+    } catch (const std::bad_alloc &) {
+      failed++;
+    }
+  }
+  if (failed) {
+    ac->err = "device state: host allocation failed";
+    return ABYSS_ERR_OOM;
+  }
+  ac->host_stale = false;
+  ac->res_sec_sync += now_s() - t0;
+  return ABYSS_OK;
+}
+
+// The engine holds every particle (after the mode was switched on).
+int resident_ensure(abyss_ac *ac) {
+  using namespace abyss_irr;
+  if (!ac->eng) {
+    int rc = engine_create(abyss::ctx_device(ac->ctx), &ac->eng);
+    if (rc != ABYSS_OK) {
+      ac->err = "device blocks: no engine on the context's device";
+      return rc;
+    }
+    ac->eng_synced = false;
+  }
+  if (ac->eng_synced) return ABYSS_OK;
+  const double t0 = now_s();
+  const int n = ac->n, cap = ac->p.nb_max;
+  for (int i = 0; i < n; ++i)
+    if ((int)ac->s[i].nb.size() > cap) {
+      ac->err = "device blocks: a neighbour list longer than nb_max";
+      return ABYSS_ERR_STATE;
+    }
+  int rc = engine_reserve(ac->eng, n, cap);
+  if (rc != ABYSS_OK) {
+    ac->err = engine_error(ac->eng);
+    return rc;
+  }
+  Image *img = engine_images(ac->eng);
+  int *lists = engine_lists(ac->eng);
+  std::vector<long long> off(n + 1, 0);
+  for (int i = 0; i < n; ++i) off[i + 1] = off[i] + (long long)ac->s[i].nb.size();
+#pragma omp parallel for schedule(static) if (n >= 16384)
+  for (int i = 0; i < n; ++i) pack_image(ac, i, img[i], lists, off[i]);
+  rc = engine_upload(ac->eng, n, off[n]);
+  if (rc != ABYSS_OK) {
+    ac->err = engine_error(ac->eng);
+    return rc;
+  }
+  ac->eng_synced = true;
+  ac->eng_dirty.clear();
+  ac->res_sec_sync += now_s() - t0;
+  return ABYSS_OK;
+}
+
+abyss_irr::Params irr_params(const abyss_ac *ac) {
+  abyss_irr::Params P;
+  P.scale = ac->scale;
+  P.time_step = ac->time_step;
+  P.eps2 = ac->p.eps2;
+  P.eta_irr = ac->p.eta_irr;
+  P.ln2 = std::log(2.0);
+  P.time_block = ac->time_block;
+  P.next_reg_block = ac->next_reg_block;
+  return P;
+}
+
+// One block with the state on the device: the same steps, in the same order,
+// as next_regular_block + irregular_levels + regular_block.
+int resident_block(abyss_ac *ac) {
+  using namespace abyss_irr;
+  int rc = resident_ensure(ac);
+  if (rc != ABYSS_OK) return rc;
+  Engine *e = ac->eng;
+  void *stream = abyss_stream(ac->ctx);
+  const int n = ac->n, cap = ac->p.nb_max;
+  double t0 = now_s();
+  ULL tmin = 0;
+  int m = 0;
+  rc = engine_next_block(e, stream, ac->block_max, &tmin, &m);
+  ac->sec_sched += now_s() - t0;
+  if (rc != ABYSS_OK) {
+    ac->err = std::string("device blocks: ") + engine_error(e);
+    return rc;
+  }
+  ac->next_reg_block = tmin;
+  if (m <= 0) {
+    ac->err = "device blocks: no particle due before the end of the run";
+    return ABYSS_ERR_STATE;
+  }
+  // the irregular levels up to the block
+  t0 = now_s();
+  Params P = irr_params(ac);
+  RunStats rs;
+  ac->host_stale = true;
+  const int run = engine_run_levels(e, P, &rs);
+  ac->st.irr_levels += rs.levels;
+  ac->st.irr_steps += rs.steps;
+  ac->dev_borderline += rs.borderline;
+  for (int q = 0; q < 6; ++q) ac->dev_cycles[q] += rs.cycles[q];
+  ac->st.sec_irr += now_s() - t0;
+  if (run != ABYSS_OK) {
+    ac->err = engine_error(e);
+    return run;
+  }
+  // the regular force; a target whose list overflowed has its radius shrunk
+  // and the call is repeated (regular_gpu)
+  const double new_time = ac->next_reg_block * ac->time_step;
+  for (int attempt = 0;; ++attempt) {
+    t0 = now_s();
+    JsetDst d{};
+    rc = abyss::ctx_state_buffers(ac->ctx, n, &d);
+    if (rc == ABYSS_OK) rc = engine_fill_jset(e, stream, d);
+    if (rc == ABYSS_OK) rc = abyss_predict(ac->ctx, new_time, ac->scale);
+    ac->sec_jset += now_s() - t0;
+    t0 = now_s();
+    if (rc == ABYSS_OK) rc = abyss::ctx_targets_from_device(ac->ctx, m, engine_block_targets(e));
+    if (rc == ABYSS_OK) rc = abyss_launch(ac->ctx, ac->p.eps2, cap, nullptr);
+    int st = ABYSS_OK, ovf = 0;
+    if (rc == ABYSS_OK) rc = abyss::ctx_launch_status(ac->ctx, &st, &ovf);
+    ac->st.sec_reg_gpu += now_s() - t0;
+    if (rc == ABYSS_OK) rc = st;
+    if (rc != ABYSS_OK) {
+      ac->err = std::string("regular force: ") + abyss_last_error(ac->ctx);
+      return rc;
+    }
+    if (ovf == 0) break;
+    if (attempt > 40) {
+      ac->err = "regular force: neighbour lists kept overflowing";
+      return ABYSS_ERR_STATE;
+    }
+    ac->st.radius_retries++;
+    RegResults r{};
+    rc = abyss::ctx_results(ac->ctx, &r);
+    if (rc == ABYSS_OK) rc = engine_shrink_radii(e, stream, m, r.nnb, cap);
+    if (rc != ABYSS_OK) {
+      ac->err = std::string("device blocks: ") + engine_error(e);
+      return rc;
+    }
+  }
+  // corrector, commit, time steps and radii
+  t0 = now_s();
+  BlockParams bp;
+  bp.irr = P;
+  bp.eta_reg = ac->p.eta_reg;
+  bp.block_max = ac->block_max;
+  bp.fix_nb = ac->p.fix_nb;
+  bp.nb_max = cap;
+  RegResults r{};
+  rc = abyss::ctx_results(ac->ctx, &r);
+  ac->res_last_m = 0;
+  ac->st.pairs += (double)m * n;
+  if (rc == ABYSS_OK) rc = engine_correct_block(e, stream, bp, m, r, &ac->res_borderline);
+  ac->st.sec_reg_host += now_s() - t0;
+  if (rc != ABYSS_OK) {
+    ac->err = engine_error(e);
+    return rc;
+  }
+  ac->res_last_m = m;
+  ac->st.reg_steps += m;
+  ac->st.blocks++;
+  return ABYSS_OK;
+}
+
+// abyss_ac_last_regular of a device block: the record is the context's last
+// launch (targets, radii and predicted j-set as the force saw them).
+int resident_last_regular(const abyss_ac *ac, int *m, int *targets, double *px, double *pv, double *r2nb,
+                          double *acc_reg, double *jerk_reg, int *nnb, int *list, int list_cap) {
+  const int mm = ac->res_last_m;
+  *m = 0;
+  if (mm <= 0) return ABYSS_ERR_STATE;
+  if (!targets && !px && !pv && !r2nb && !acc_reg && !jerk_reg && !nnb && !list) {
+    *m = mm;  // the size alone
+    return ABYSS_OK;
+  }
+  const size_t M = mm, cap = ac->p.nb_max;
+  std::vector<double> acc(3 * M), jerk(3 * M);
+  std::vector<int> nn(M), lst(M * cap);
+  int ovf = 0;
+  int rc = abyss_fetch(ac->ctx, acc.data(), jerk.data(), nullptr, nullptr, nn.data(), lst.data(), &ovf);
+  if (rc == ABYSS_OK) rc = abyss::ctx_read_targets(ac->ctx, targets, r2nb);
+  if (rc == ABYSS_OK && (px || pv)) rc = abyss_read_predicted(ac->ctx, px, pv, nullptr);
+  if (rc != ABYSS_OK) return rc;
+  *m = mm;
+  for (size_t k = 0; k < M; ++k) {
+    for (int d = 0; d < 3; ++d) {
+      if (acc_reg) acc_reg[3 * k + d] = acc[3 * k + d];
+      if (jerk_reg) jerk_reg[3 * k + d] = jerk[3 * k + d];
+    }
+    if (nnb) nnb[k] = nn[k];
+    if (list)
+      for (size_t q = 0; q < std::min((size_t)list_cap, cap); ++q) list[k * list_cap + q] = lst[k * cap + q];
   }
   return ABYSS_OK;
 }
@@ -1499,9 +1753,49 @@ int abyss_ac_set_device_irregular(abyss_ac *ac, int on) {
     ac->err = "set_device_irregular: the integration has no GPU context";
     return ABYSS_ERR_STATE;
   }
+  if (ac->dev_res) {  // the device's copy stays the state of record
+    ac->dev_irr = on != 0;
+    return ABYSS_OK;
+  }
   ac->dev_irr = on != 0;
   ac->eng_synced = false;  // the host may have stepped particles meanwhile
   ac->eng_dirty.clear();
+  return ABYSS_OK;
+}
+
+int abyss_ac_set_device_resident(abyss_ac *ac, int on) {
+  if (!ac) return ABYSS_ERR_ARG;
+  if (ac->in_block) {
+    ac->err = "set_device_resident: a split block is open";
+    return ABYSS_ERR_STATE;
+  }
+  if (on && !ac->ctx) {
+    ac->err = "set_device_resident: the integration has no GPU context";
+    return ABYSS_ERR_STATE;
+  }
+  if ((on != 0) == ac->dev_res) return ABYSS_OK;
+  if (on) {
+    ac->eng_synced = false;  // the first device block sends every particle up
+    ac->host_stale = false;
+    ac->res_last_m = 0;
+    ac->dev_res = true;
+    return ABYSS_OK;
+  }
+  const int rc = resident_sync_host(ac);
+  if (rc != ABYSS_OK) return rc;
+  ac->dev_res = false;
+  ac->eng_synced = false;  // a later device irregular phase sends every particle up
+  ac->eng_dirty.clear();
+  // the host's last-call record is of a block before the switch
+  ac->last_targets.clear();
+  return ABYSS_OK;
+}
+
+int abyss_ac_device_resident_info(const abyss_ac *ac, int *on, long long *borderline, double *sec_sync) {
+  if (!ac) return ABYSS_ERR_ARG;
+  if (on) *on = ac->dev_res ? 1 : 0;
+  if (borderline) *borderline = ac->res_borderline;
+  if (sec_sync) *sec_sync = ac->res_sec_sync;
   return ABYSS_OK;
 }
 
@@ -1624,6 +1918,13 @@ int abyss_ac_advance_block(abyss_ac *ac, int *done) {
     if (done) *done = 1;
     return ABYSS_OK;
   }
+  if (ac->dev_res) {
+    const int rc = resident_block(ac);
+    if (rc != ABYSS_OK) return rc;
+    if (ac->next_reg_block * ac->time_step >= 1) ac->done = true;
+    if (done) *done = ac->done ? 1 : 0;
+    return ABYSS_OK;
+  }
   std::vector<int> targets = next_regular_block(ac);
   int rc = irregular_levels(ac);
   if (rc != ABYSS_OK) return rc;
@@ -1643,6 +1944,10 @@ int abyss_ac_begin_block(abyss_ac *ac, int *m, double *new_time, double *time_sc
   if (!ac || !m) return ABYSS_ERR_ARG;
   if (ac->in_block) {
     ac->err = "begin_block: a block is already open";
+    return ABYSS_ERR_STATE;
+  }
+  if (ac->dev_res) {
+    ac->err = "begin_block: the state is resident on the device (abyss_ac_set_device_resident)";
     return ABYSS_ERR_STATE;
   }
   set_threads(ac);
@@ -1766,6 +2071,8 @@ double abyss_ac_time(const abyss_ac *ac) { return ac ? ac->next_reg_block * ac->
 
 int abyss_ac_get_state(const abyss_ac *ac, double *x, double *v, int *nnb, double *r2nb) {
   if (!ac) return ABYSS_ERR_ARG;
+  const int rc = resident_sync_host(ac);
+  if (rc != ABYSS_OK) return rc;
   for (int i = 0; i < ac->n; ++i) {
     const Star &s = ac->s[i];
     for (int d = 0; d < 3; ++d) {
@@ -1781,9 +2088,10 @@ int abyss_ac_get_state(const abyss_ac *ac, double *x, double *v, int *nnb, doubl
 int abyss_ac_energy(abyss_ac *ac, double *energy) {
   if (!ac || !energy) return ABYSS_ERR_ARG;
   std::vector<double> x(3 * (size_t)ac->n), v(3 * (size_t)ac->n), m(ac->n);
-  abyss_ac_get_state(ac, x.data(), v.data(), nullptr, nullptr);
+  int rc = abyss_ac_get_state(ac, x.data(), v.data(), nullptr, nullptr);
+  if (rc != ABYSS_OK) return rc;
   for (int i = 0; i < ac->n; ++i) m[i] = ac->s[i].m;
-  int rc = abyss_energy(ac->ctx, ac->n, x.data(), v.data(), m.data(), ac->p.eps2, energy);
+  rc = abyss_energy(ac->ctx, ac->n, x.data(), v.data(), m.data(), ac->p.eps2, energy);
   if (rc != ABYSS_OK) ac->err = abyss_last_error(ac->ctx);
   return rc;
 }
@@ -1798,6 +2106,7 @@ int abyss_ac_last_regular(const abyss_ac *ac, int *m, int *targets, double *px, 
                           double *r2nb, double *acc_reg, double *jerk_reg, int *nnb, int *list,
                           int list_cap) {
   if (!ac || !m) return ABYSS_ERR_ARG;
+  if (ac->dev_res) return resident_last_regular(ac, m, targets, px, pv, r2nb, acc_reg, jerk_reg, nnb, list, list_cap);
   const int mm = (int)ac->last_targets.size();
   const size_t M = mm;
   if (ac->last_acc.size() < 3 * M || ac->last_jerk.size() < 3 * M || ac->last_nnb.size() < M ||
@@ -2102,6 +2411,8 @@ extern "C" {
 int abyss_ac_save(const abyss_ac *ac, const char *path) {
   if (!ac || !path) return ABYSS_ERR_ARG;
   if (ac->in_block) return ABYSS_ERR_STATE;  // only between regular blocks
+  const int rs = resident_sync_host(ac);
+  if (rs != ABYSS_OK) return rs;
   std::ofstream f(path, std::ios::binary | std::ios::trunc);
   if (!f) return ABYSS_ERR_ARG;
   f.write(kCkptMagic, sizeof(kCkptMagic));
@@ -2226,6 +2537,8 @@ extern "C" {
 
 int abyss_ac_write_snapshot(const abyss_ac *ac, const char *path, double output_time, double output_time_step) {
   if (!ac || !path) return ABYSS_ERR_ARG;
+  const int rs = resident_sync_host(ac);
+  if (rs != ABYSS_OK) return rs;
   std::ofstream f(path, std::ios::trunc);
   if (!f) return ABYSS_ERR_ARG;
   const double now = ac->next_reg_block * ac->time_step;  // code time of the state

@@ -1,5 +1,8 @@
 // Irregular steps on the device (irregular.h): the level loop of the
-// Ahmad-Cohen irregular force in one persistent cooperative kernel.
+// Ahmad-Cohen irregular force in one persistent cooperative kernel; and the
+// rest of a block -- the next block's particles, the regular corrector, commit,
+// time steps and radii -- for integrations whose state stays on the device
+// (the blk_* kernels below).
 //
 // The host integrator runs, between two regular blocks, every particle whose
 // next irregular time is due, level by level in increasing block time
@@ -51,6 +54,8 @@ constexpr int kMaxSlice = 4096;  // particles per block of the level loop
 constexpr int kBad = 1;       // a time step out of range
 constexpr int kTimeout = 2;   // a grid-barrier wait ran out
 constexpr int kBadIndex = 4;  // an uploaded image named a particle outside the cluster
+constexpr int kRegBad = 8;    // a regular block's time step out of range
+constexpr int kSchedChunk = 2048;  // particles per block of the block-scheduling kernels (256 x 8)
 constexpr long long kBarrierSpins = 5000000;  // x up to 256 ns sleep: about a second
 
 // A particle as its neighbours' steps read it (one 128-byte line).
@@ -68,7 +73,16 @@ struct Pend {
   int lv_irr, move;
 };
 
+// A regular block's corrector results for one target, committed once every
+// target's corrector has run (the host integrator's Pending).
+struct RPend {
+  double nx[3], nv[3];
+  double a_reg[12], a_irr[12], a_tot[12];
+};
+
 struct Ctl {
+  ULL tmin;  // the next regular block's time (engine_next_block)
+  int m, pad2;  // and its number of particles
   ULL lmin[2];
   unsigned bar_count, bar_unused;
   int status, pad;
@@ -87,6 +101,10 @@ struct State {
   ULL *cur_irr, *tb_irr, *next_irr, *new_cur_irr, *cur_reg, *tb_reg;
   int *lv_irr, *lv_reg, *nnb, *nb, *touched;
   int *members;   // the level's particles, in any order
+  double *r2nb, *dt_reg;  // read and written by whole regular blocks only
+  int *tg;        // the regular block's particles, ascending
+  int *bcnt;      // per scheduling block: its particles due
+  RPend *rpend;   // [m] regular corrector results
   Pend *pend;
   Ctl *ctl;
   Image *img;     // device staging of images
@@ -601,6 +619,8 @@ __global__ void irr_scatter(State S, int count) {
     }
     S.t_reg[i] = g.t_reg;
     S.dt_irr[i] = g.dt_irr;
+    S.r2nb[i] = g.r2nb;
+    S.dt_reg[i] = g.dt_reg;
     S.cur_irr[i] = g.cur_irr;
     S.tb_irr[i] = g.tb_irr;
     S.next_irr[i] = g.next_irr;
@@ -648,6 +668,421 @@ __global__ void irr_gather(State S) {
   }
 }
 
+// ------------------------------------------------------------ whole regular blocks
+// The regular half of a block with the state resident here: the next block's
+// particles, the j-set handed to the regular-force context, and the corrector
+// and commit of every target once the context has its forces.  Each step keeps
+// the host integrator's operation order (host/ac_integrator.cpp
+// next_regular_block, upload_and_predict, regular_correct_one, finish_regular),
+// so that a block equals the host's bit for bit.
+
+// Sum and exclusive scan of one int per thread over a block of 256 threads.
+__device__ int block_sum_int(int v) {
+  __shared__ int s_part[8];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = v;
+  __syncthreads();
+  int r = 0;
+  for (int k = 0; k < 8; ++k) r += s_part[k];
+  __syncthreads();
+  return r;
+}
+
+__device__ int block_exscan_int(int v) {
+  __shared__ int s_warp[8];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int inc = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int u = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += u;
+  }
+  if (lane == 31) s_warp[w] = inc;
+  __syncthreads();
+  int before = 0;
+  for (int k = 0; k < w; ++k) before += s_warp[k];
+  __syncthreads();
+  return before + inc - v;
+}
+
+__device__ __forceinline__ ULL reg_due(const State &S, int i) { return S.cur_reg[i] + S.tb_reg[i]; }
+
+// next_regular_block: the smallest cur_reg + tb_reg not above block_max.
+__global__ void __launch_bounds__(kThreads) blk_min(State S, ULL block_max) {
+  ULL mn = ULLONG_MAX;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < S.n; i += gridDim.x * blockDim.x) {
+    const ULL t = reg_due(S, i);
+    if (t <= block_max && t < mn) mn = t;
+  }
+  mn = block_min(mn);
+  if (threadIdx.x == 0 && mn != ULLONG_MAX) atomicMin(&S.ctl->tmin, mn);
+}
+
+// Particles due at tmin per chunk of kSchedChunk.
+__global__ void __launch_bounds__(kThreads) blk_count(State S) {
+  const ULL t = S.ctl->tmin;
+  const int b0 = blockIdx.x * kSchedChunk, b1 = min(S.n, b0 + kSchedChunk);
+  int c = 0;
+  for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) c += reg_due(S, i) == t;
+  c = block_sum_int(c);
+  if (threadIdx.x == 0) S.bcnt[blockIdx.x] = c;
+}
+
+// The particles due at tmin in ascending index: chunk b starts after the
+// counts of the chunks before it, thread k of a chunk takes its 8 particles
+// [8k, 8k + 8).  The last thread of the last chunk writes the total.
+__global__ void __launch_bounds__(kThreads) blk_collect(State S) {
+  const ULL t = S.ctl->tmin;
+  int off = 0;
+  for (int b = threadIdx.x; b < (int)blockIdx.x; b += blockDim.x) off += S.bcnt[b];
+  off = block_sum_int(off);
+  const int i0 = blockIdx.x * kSchedChunk + 8 * threadIdx.x;
+  unsigned due = 0;
+#pragma unroll
+  for (int q = 0; q < 8; ++q)
+    if (i0 + q < S.n && reg_due(S, i0 + q) == t) due |= 1u << q;
+  const int c = __popc(due);
+  const int ex = block_exscan_int(c);
+  int pos = off + ex;
+#pragma unroll
+  for (int q = 0; q < 8; ++q)
+    if ((due >> q) & 1u) S.tg[pos++] = i0 + q;
+  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == blockDim.x - 1) S.ctl->m = off + ex + c;
+}
+
+// upload_and_predict's state: a0, a1 = a_tot[.][0], a_tot[.][1]; t0 = t_reg
+// without neighbours, else t_irr (CalculateRegularAcceleration.cpp:371-374).
+__global__ void blk_fill(State S, JsetDst d) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < S.n; i += gridDim.x * blockDim.x) {
+    const Rec &r = S.rec[i];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      d.x[3 * (size_t)i + k] = r.x[k];
+      d.v[3 * (size_t)i + k] = r.v[k];
+      d.a0[3 * (size_t)i + k] = S.a_tot[12 * (size_t)i + 4 * k + 0];
+      d.a1[3 * (size_t)i + k] = S.a_tot[12 * (size_t)i + 4 * k + 1];
+    }
+    d.t0[i] = S.nnb[i] == 0 ? S.t_reg[i] : r.t;
+    d.mass[i] = r.m;
+    d.r2nb[i] = S.r2nb[i];
+  }
+}
+
+// regular_gpu's overflow rule: r2nb *= 0.8 for every target whose list overflowed.
+__global__ void blk_shrink(State S, int m, const int *nnb, int cap) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x)
+    if (nnb[k] > cap) {
+      const int i = S.tg[k];
+      S.r2nb[i] = S.r2nb[i] * 0.8;
+    }
+}
+
+__device__ __forceinline__ bool listed(const int *list, int n, int j) {
+  for (int q = 0; q < n; ++q)
+    if (list[q] == j) return true;
+  return false;
+}
+
+// The host's pair_force of a changed neighbour j with sign s: j predicted to
+// new_time from its own last time (t_reg without neighbours, else t_irr).
+__device__ void change_terms(const State &S, int j, double new_time, double scale, double eps2,
+                             const double (&pi)[3], const double (&vi)[3], double sign, double (&ta)[3],
+                             double (&tj)[3]) {
+  const Rec &q = S.rec[j];
+  const double t0 = S.nnb[j] == 0 ? S.t_reg[j] : q.t;
+  const double dt = (new_time - t0) * scale;
+  double x[3], v[3], r2 = 0.0, vx = 0.0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double a0 = S.a_tot[12 * (size_t)j + 4 * d + 0], a1 = S.a_tot[12 * (size_t)j + 4 * d + 1];
+    double pj, vj;
+    if (dt == 0) {
+      pj = q.x[d];
+      vj = q.v[d];
+    } else {
+      pj = ((a1 * dt / 3 + a0) * dt / 2 + q.v[d]) * dt + q.x[d];
+      vj = (a1 * dt / 2 + a0) * dt + q.v[d];
+    }
+    x[d] = pj - pi[d];
+    v[d] = vj - vi[d];
+    r2 += x[d] * x[d];
+    vx += x[d] * v[d];
+  }
+  const double r2s = r2 + eps2;
+  const double m_r3 = q.m / r2s / sqrt(r2s);
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    ta[d] = sign * m_r3 * x[d];
+    tj[d] = sign * m_r3 * (v[d] - 3 * x[d] * vx / r2s);
+  }
+}
+
+// updateRegularParticleCuda (ComputeAcceleration.cpp:405-661) for the block's
+// targets, one warp each, from the pre-block state: the target predicted to
+// the block time (only a particle without neighbours moves), the force of
+// every lost (old, not new) and gained (new, not old) neighbour in the
+// interleaved order of the host's neighbour_change, the fourth-order Hermite
+// corrector and the new derivatives.  Lanes compute the changed neighbours'
+// terms, 32 list positions (64 slots) a round; lane c < 6 then adds component
+// c in slot order: the host's sequential sums.
+__global__ void __launch_bounds__(kThreads) blk_correct(State S, BlockParams B, int m, RegResults R) {
+  __shared__ double s_terms[kThreads / 32][6 * 64];
+  __shared__ unsigned char s_has[kThreads / 32][64];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  double *terms = s_terms[wib];
+  unsigned char *has = s_has[wib];
+  const double scale = B.irr.scale;
+  for (int k = warp; k < m; k += nwarps) {
+    const int i = S.tg[k];
+    // the force call is repeated until no list overflows; the clamp keeps a
+    // row read inside its capacity regardless
+    const int n_old = S.nnb[i], n_new = min(R.nnb[k], R.cap);
+    const int *old_nb = S.nb + (size_t)i * S.cap;
+    const int *new_nb = R.list + (size_t)k * R.cap;
+    const Rec &r = S.rec[i];
+    double at[12], ar[12], ai[12];
+#pragma unroll
+    for (int q = 0; q < 12; ++q) {
+      at[q] = S.a_tot[12 * (size_t)i + q];
+      ar[q] = S.a_reg[12 * (size_t)i + q];
+      ai[q] = S.a_irr[12 * (size_t)i + q];
+    }
+    const double t_reg = S.t_reg[i], dt_reg = S.dt_reg[i];
+    const double new_time = t_reg + dt_reg;
+    const double dtp = (n_old == 0 ? dt_reg : 0.0) * scale;
+    double pos[3], vel[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      if (dtp == 0) {
+        pos[d] = r.x[d];
+        vel[d] = r.v[d];
+      } else {
+        pos[d] = ((at[4 * d + 1] * dtp / 3 + at[4 * d + 0]) * dtp / 2 + r.v[d]) * dtp + r.x[d];
+        vel[d] = (at[4 * d + 1] * dtp / 2 + at[4 * d + 0]) * dtp + r.v[d];
+      }
+    }
+    double sum = 0.0;
+    const int size = max(n_old, n_new);
+    for (int base = 0; base < size; base += 32) {
+      const int kk = base + lane;
+      double ta[3] = {0.0, 0.0, 0.0}, tj[3] = {0.0, 0.0, 0.0};
+      double ua[3] = {0.0, 0.0, 0.0}, uj[3] = {0.0, 0.0, 0.0};
+      bool lost = false, gained = false;
+      if (kk < n_old) {
+        const int j = old_nb[kk];
+        lost = !listed(new_nb, n_new, j);
+        if (lost) change_terms(S, j, new_time, scale, B.irr.eps2, pos, vel, -1.0, ta, tj);
+      }
+      if (kk < n_new) {
+        const int j = new_nb[kk];
+        gained = !listed(old_nb, n_old, j);
+        if (gained) change_terms(S, j, new_time, scale, B.irr.eps2, pos, vel, +1.0, ua, uj);
+      }
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        terms[d * 64 + 2 * lane] = ta[d];
+        terms[(3 + d) * 64 + 2 * lane] = tj[d];
+        terms[d * 64 + 2 * lane + 1] = ua[d];
+        terms[(3 + d) * 64 + 2 * lane + 1] = uj[d];
+      }
+      has[2 * lane] = lost;
+      has[2 * lane + 1] = gained;
+      __syncwarp();
+      if (lane < 6)
+        for (int l = 0; l < 64; ++l)
+          if (has[l]) sum += terms[lane * 64 + l];
+      __syncwarp();
+    }
+    double a_tmp[3], adot_tmp[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      a_tmp[d] = __shfl_sync(0xffffffffu, sum, d);
+      adot_tmp[d] = __shfl_sync(0xffffffffu, sum, 3 + d);
+    }
+    if (lane != 0) continue;
+    // hermite_regular and commit_derivatives (ComputeAcceleration.cpp:592-660)
+    const double dt = dt_reg * scale;
+    const double dt2 = dt * dt, dt3 = dt2 * dt, dt4 = dt3 * dt, dt5 = dt4 * dt;
+    RPend *o = &S.rpend[k];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double acc = R.acc_reg[3 * (size_t)k + d], jerk = R.jerk_reg[3 * (size_t)k + d];
+      const double da_dt2 = (ar[4 * d + 0] - acc - a_tmp[d]) / dt2;
+      const double adot_dt = (ar[4 * d + 1] + jerk + adot_tmp[d]) / dt;
+      const double a2 = -6 * da_dt2 - 2 * adot_dt - 2 * ar[4 * d + 1] / dt;
+      const double a3 = (12 * da_dt2 + 6 * adot_dt) / dt;
+      o->nx[d] = pos[d] + a2 * dt4 / 24 + a3 * dt5 / 120;
+      o->nv[d] = vel[d] + a2 * dt3 / 6 + a3 * dt4 / 24;
+      double nr[4] = {acc, jerk, a2, a3};
+      double ni[4] = {R.acc_irr[3 * (size_t)k + d], R.jerk_irr[3 * (size_t)k + d], ai[4 * d + 2], ai[4 * d + 3]};
+      double nt[4] = {nr[0] + ni[0], nr[1] + ni[1], n_new == 0 ? a2 : at[4 * d + 2], n_new == 0 ? a3 : at[4 * d + 3]};
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        o->a_reg[4 * d + q] = nr[q];
+        o->a_irr[4 * d + q] = ni[q];
+        o->a_tot[4 * d + q] = nt[q];
+      }
+    }
+  }
+}
+
+// calculateTimeStepReg (UpdateParticle.cpp:314-407, host/ac_integrator.cpp
+// time_step_reg) with cur_reg and t_reg already advanced; lv_reg, tb_reg,
+// dt_reg (and lv_irr of a particle without neighbours) updated in place.
+// Returns false for a step out of range.
+__device__ bool level_reg(const BlockParams &B, const double *a_reg, bool has_nb, ULL cur_reg, double t_reg,
+                          int &lv_reg, ULL &tb_reg, double &dt_reg, int &lv_irr, long long &border) {
+  const Params &P = B.irr;
+  int lv = block_level(P, new_step_irr(a_reg, a_reg, B.eta_reg), border);
+  const int lv0 = lv;
+  if (lv >= lv_reg + 1) {
+    if (fmod((double)cur_reg, 2.0 * (double)tb_reg) == 0 && t_reg != 0) {
+      lv = lv_reg + 1;
+      ULL tb = tb_reg * 2;
+      // ends within lv0 - lv rounds
+      while ((lv0 > lv) && (fmod((double)cur_reg, 2.0 * (double)tb) == 0)) {
+        tb = 2 * tb;
+        lv = lv + 1;
+      }
+    } else {
+      lv = lv_reg;
+    }
+  } else if (lv < lv_reg) {
+    lv = lv_reg - 1;
+    if (lv0 < lv) lv--;
+  } else {
+    lv = lv_reg;
+  }
+  lv_reg = max(P.time_block, lv);
+  if (!has_nb) lv_irr = lv_reg;
+  dt_reg = pow2d(lv_reg);
+  tb_reg = pow2_blocks(lv_reg - P.time_block);
+  if (t_reg + dt_reg > 1 && t_reg != 1.0) {
+    dt_reg = 1 - t_reg;
+    tb_reg = B.block_max - cur_reg;
+  }
+  if (dt_reg * P.scale * 1e4 < 1e-9) return false;
+  return !(dt_reg > 1);
+}
+
+// updateRadius (UpdateParticle.cpp:108-139, host/ac_integrator.cpp
+// update_radius): the powers there are of small integers, exact in FP64, and
+// are written as products.
+__device__ double new_radius(double r2nb, int nnb, int fix, int nbmax) {
+  if (nnb > fix) {
+    const double c = (nbmax - fix);
+    const double b = 0.9 / (c * c);
+    const double x = nnb - fix;
+    const double a = b * fabs(x) * x;
+    return r2nb * (1. - a);
+  }
+  if (nnb < fix) {
+    const double c = (nbmax - fix);
+    const double b = 0.5 / (c * c * c);
+    const double x = nnb - fix;
+    const double a = b * (x * x * x);
+    return r2nb * (1. - a);
+  }
+  return r2nb;
+}
+
+// RegCudaUpdate (WorkerRoutines.cpp:124-143) and finish_regular's commit, one
+// warp per target: the new list, derivatives, position and velocity, then the
+// regular and irregular steps, the radius and the next irregular time.
+__global__ void __launch_bounds__(kThreads) blk_commit(State S, BlockParams B, int m, RegResults R) {
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const Params &P = B.irr;
+  long long border = 0;
+  for (int k = warp; k < m; k += nwarps) {
+    const int i = S.tg[k];
+    const int n_new = min(R.nnb[k], R.cap);
+    for (int q = lane; q < n_new; q += 32) S.nb[(size_t)i * S.cap + q] = R.list[(size_t)k * R.cap + q];
+    if (lane != 0) continue;
+    const RPend &o = S.rpend[k];
+    Rec &r = S.rec[i];
+    S.nnb[i] = n_new;
+#pragma unroll
+    for (int q = 0; q < 12; ++q) {
+      S.a_reg[12 * (size_t)i + q] = o.a_reg[q];
+      S.a_irr[12 * (size_t)i + q] = o.a_irr[q];
+      S.a_tot[12 * (size_t)i + q] = o.a_tot[q];
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      r.x[d] = o.nx[d];
+      r.v[d] = o.nv[d];
+      r.a0[d] = o.a_tot[4 * d + 0];
+      r.a1[d] = o.a_tot[4 * d + 1];
+    }
+    const ULL cur_reg = S.cur_reg[i] + S.tb_reg[i];
+    const double t_reg = (double)cur_reg * P.time_step;
+    int lv_reg = S.lv_reg[i], lv_irr = S.lv_irr[i];
+    ULL tb_reg = S.tb_reg[i], tb_irr = S.tb_irr[i];
+    double dt_reg = S.dt_reg[i], dt_irr = S.dt_irr[i];
+    bool ok = level_reg(B, o.a_reg, n_new > 0, cur_reg, t_reg, lv_reg, tb_reg, dt_reg, lv_irr, border);
+    // the host's time_step_irr is skipped when time_step_reg failed
+    if (ok)
+      ok = level_irr(P, n_new > 0, o.a_tot, o.a_irr, S.new_cur_irr[i], cur_reg, tb_reg, lv_reg, lv_irr, dt_irr,
+                     tb_irr, border);
+    ULL cur_irr = S.cur_irr[i];
+    if (n_new == 0) {
+      cur_irr = cur_reg;
+      r.t = (double)cur_reg * P.time_step;
+    }
+    S.cur_reg[i] = cur_reg;
+    S.t_reg[i] = t_reg;
+    S.lv_reg[i] = lv_reg;
+    S.tb_reg[i] = tb_reg;
+    S.dt_reg[i] = dt_reg;
+    S.lv_irr[i] = lv_irr;
+    S.tb_irr[i] = tb_irr;
+    S.dt_irr[i] = dt_irr;
+    S.cur_irr[i] = cur_irr;
+    S.r2nb[i] = new_radius(S.r2nb[i], n_new, B.fix_nb, B.nb_max);
+    S.next_irr[i] = cur_irr + tb_irr;
+    if (!ok) atomicOr(&S.ctl->status, kRegBad);
+  }
+  if (lane == 0 && border) atomicAdd((unsigned long long *)&S.ctl->borderline, (unsigned long long)border);
+}
+
+// Every particle's fields as an image (list_off = i * cap; the lists are
+// copied as they lie).
+__global__ void blk_gather_all(State S) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < S.n; i += gridDim.x * blockDim.x) {
+    Image &g = S.img[i];
+    const Rec &r = S.rec[i];
+    for (int d = 0; d < 3; ++d) {
+      g.x[d] = r.x[d];
+      g.v[d] = r.v[d];
+    }
+    g.m = r.m;
+    g.t_irr = r.t;
+    g.t_reg = S.t_reg[i];
+    g.dt_irr = S.dt_irr[i];
+    for (int q = 0; q < 12; ++q) {
+      g.a_tot[q] = S.a_tot[12 * (size_t)i + q];
+      g.a_reg[q] = S.a_reg[12 * (size_t)i + q];
+      g.a_irr[q] = S.a_irr[12 * (size_t)i + q];
+    }
+    g.cur_irr = S.cur_irr[i];
+    g.tb_irr = S.tb_irr[i];
+    g.next_irr = S.next_irr[i];
+    g.new_cur_irr = S.new_cur_irr[i];
+    g.cur_reg = S.cur_reg[i];
+    g.tb_reg = S.tb_reg[i];
+    g.r2nb = S.r2nb[i];
+    g.dt_reg = S.dt_reg[i];
+    g.lv_irr = S.lv_irr[i];
+    g.lv_reg = S.lv_reg[i];
+    g.nnb = S.nnb[i];
+    g.index = i;
+    g.list_off = (long long)i * S.cap;
+  }
+}
+
 template <class T>
 cudaError_t dalloc(T **p, size_t count) {
   if (*p) cudaFree(*p);
@@ -688,7 +1123,7 @@ int fail(Engine *e, int code, const std::string &msg) {
 void free_state(State &S) {
   void *ps[] = {S.rec, S.a_tot, S.a_reg, S.a_irr, S.t_reg, S.dt_irr, S.cur_irr, S.tb_irr, S.next_irr,
                 S.new_cur_irr, S.cur_reg, S.tb_reg, S.lv_irr, S.lv_reg, S.nnb, S.nb, S.touched, S.members, S.pend,
-                S.img, S.lists, S.chg};
+                S.img, S.lists, S.chg, S.r2nb, S.dt_reg, S.tg, S.bcnt, S.rpend};
   for (void *p : ps)
     if (p) cudaFree(p);
   Ctl *c = S.ctl;
@@ -793,6 +1228,11 @@ int engine_reserve(Engine *e, int n, int cap) {
   ECK(dalloc(&S.img, N), "alloc");
   ECK(dalloc(&S.lists, N * cap), "alloc");
   ECK(dalloc(&S.chg, N), "alloc");
+  ECK(dalloc(&S.r2nb, N), "alloc");
+  ECK(dalloc(&S.dt_reg, N), "alloc");
+  ECK(dalloc(&S.tg, N), "alloc");
+  ECK(dalloc(&S.bcnt, N / kSchedChunk + 1), "alloc");
+  ECK(dalloc(&S.rpend, N), "alloc");
   ECK(cudaMemsetAsync(S.touched, 0, sizeof(int) * N, e->stream), "clear");
   ECK(cudaMemsetAsync(S.nnb, 0, sizeof(int) * N, e->stream), "clear");
   ECK(cudaHostAlloc((void **)&e->h_img, sizeof(Image) * N, cudaHostAllocDefault), "pinned images");
@@ -926,5 +1366,91 @@ int engine_steps(Engine *e, const Params &p, int count, const int *idx, double *
   if (c.status & kBad) return fail(e, ABYSS_ERR_STATE, "irregular time step out of range");
   return ABYSS_OK;
 }
+
+// ------------------------------------------------------------ whole regular blocks
+
+const int *engine_block_targets(const Engine *e) { return e ? e->S.tg : nullptr; }
+
+int engine_next_block(Engine *e, void *stream, ULL block_max, ULL *tmin, int *m) {
+  if (!e || e->n <= 0 || !tmin || !m) return ABYSS_ERR_ARG;
+  cudaSetDevice(e->device);
+  cudaStream_t s = (cudaStream_t)stream;
+  Ctl c{};
+  c.tmin = ULLONG_MAX;
+  c.lmin[0] = c.lmin[1] = ULLONG_MAX;
+  ECK(cudaMemcpyAsync(e->S.ctl, &c, sizeof(c), cudaMemcpyHostToDevice, s), "reset control words");
+  const int chunks = (e->n + kSchedChunk - 1) / kSchedChunk;
+  const int blocks = std::max(1, std::min((e->n + kThreads - 1) / kThreads, 4 * e->sm_count));
+  blk_min<<<blocks, kThreads, 0, s>>>(e->S, block_max);
+  blk_count<<<chunks, kThreads, 0, s>>>(e->S);
+  blk_collect<<<chunks, kThreads, 0, s>>>(e->S);
+  ECK(cudaGetLastError(), "next block launch");
+  ECK(cudaMemcpyAsync(&c, e->S.ctl, sizeof(c), cudaMemcpyDeviceToHost, s), "read control words");
+  ECK(cudaStreamSynchronize(s), "synchronize");
+  if (c.tmin == ULLONG_MAX) {
+    *tmin = block_max;
+    *m = 0;
+  } else {
+    *tmin = c.tmin;
+    *m = c.m;
+  }
+  return ABYSS_OK;
+}
+
+int engine_fill_jset(Engine *e, void *stream, const JsetDst &d) {
+  if (!e || e->n <= 0 || !d.x || !d.v || !d.a0 || !d.a1 || !d.t0 || !d.mass || !d.r2nb) return ABYSS_ERR_ARG;
+  cudaSetDevice(e->device);
+  const int blocks = std::max(1, std::min((e->n + 255) / 256, 4 * e->sm_count));
+  blk_fill<<<blocks, 256, 0, (cudaStream_t)stream>>>(e->S, d);
+  ECK(cudaGetLastError(), "j-set fill launch");
+  return ABYSS_OK;
+}
+
+int engine_shrink_radii(Engine *e, void *stream, int m, const int *nnb, int cap) {
+  if (!e || m < 0 || m > e->n || (m > 0 && !nnb)) return ABYSS_ERR_ARG;
+  if (m == 0) return ABYSS_OK;
+  cudaSetDevice(e->device);
+  const int blocks = std::max(1, std::min((m + 255) / 256, 4 * e->sm_count));
+  blk_shrink<<<blocks, 256, 0, (cudaStream_t)stream>>>(e->S, m, nnb, cap);
+  ECK(cudaGetLastError(), "radius launch");
+  return ABYSS_OK;
+}
+
+int engine_correct_block(Engine *e, void *stream, const BlockParams &bp, int m, const RegResults &r,
+                         long long *borderline) {
+  if (!e || m <= 0 || m > e->n || !r.acc_reg || !r.jerk_reg || !r.acc_irr || !r.jerk_irr || !r.nnb || !r.list)
+    return ABYSS_ERR_ARG;
+  if (r.cap > e->cap || bp.nb_max != e->cap)
+    return fail(e, ABYSS_ERR_ARG, "regular block: list capacity differs from the engine's");
+  cudaSetDevice(e->device);
+  cudaStream_t s = (cudaStream_t)stream;
+  Ctl c{};
+  c.lmin[0] = c.lmin[1] = ULLONG_MAX;
+  ECK(cudaMemcpyAsync(e->S.ctl, &c, sizeof(c), cudaMemcpyHostToDevice, s), "reset control words");
+  const int blocks = std::max(1, std::min((int)(((size_t)m * 32 + kThreads - 1) / kThreads), 8 * e->sm_count));
+  blk_correct<<<blocks, kThreads, 0, s>>>(e->S, bp, m, r);
+  blk_commit<<<blocks, kThreads, 0, s>>>(e->S, bp, m, r);
+  ECK(cudaGetLastError(), "corrector launch");
+  ECK(cudaMemcpyAsync(&c, e->S.ctl, sizeof(c), cudaMemcpyDeviceToHost, s), "read control words");
+  ECK(cudaStreamSynchronize(s), "synchronize");
+  if (borderline) *borderline += c.borderline;
+  if (c.status & kRegBad) return fail(e, ABYSS_ERR_STATE, "regular time step out of range");
+  return ABYSS_OK;
+}
+
+int engine_download_all(Engine *e) {
+  if (!e || e->n <= 0) return ABYSS_ERR_ARG;
+  cudaSetDevice(e->device);
+  const int blocks = std::max(1, std::min((e->n + 255) / 256, 4 * e->sm_count));
+  blk_gather_all<<<blocks, 256, 0, e->stream>>>(e->S);
+  ECK(cudaGetLastError(), "gather launch");
+  ECK(cudaMemcpyAsync(e->h_img, e->S.img, sizeof(Image) * (size_t)e->n, cudaMemcpyDeviceToHost, e->stream),
+      "D2H images");
+  ECK(cudaMemcpyAsync(e->h_lists, e->S.nb, sizeof(int) * (size_t)e->n * e->cap, cudaMemcpyDeviceToHost, e->stream),
+      "D2H lists");
+  ECK(cudaStreamSynchronize(e->stream), "synchronize");
+  return ABYSS_OK;
+}
+
 
 }  // namespace abyss_irr

@@ -22,6 +22,7 @@ struct Image {
   double x[3], v[3], m, t_irr, t_reg, dt_irr;
   double a_tot[12], a_reg[12], a_irr[12];  // [d][k] row-major, 3 x 4
   ULL cur_irr, tb_irr, next_irr, new_cur_irr, cur_reg, tb_reg;
+  double r2nb, dt_reg;  // read by whole regular blocks on the device only
   int lv_irr, lv_reg, nnb, index;
   long long list_off;  // first of its nnb neighbours in the staged lists
 };
@@ -57,6 +58,31 @@ struct RunStats {
   long long cycles[6] = {0, 0, 0, 0, 0, 0};
 };
 
+// Constants of whole regular blocks on the device (engine_next_block ..
+// engine_correct_block): the irregular phase's plus the regular step's rules.
+struct BlockParams {
+  Params irr;        // next_reg_block: the block being corrected
+  double eta_reg;    // Aarseth accuracy parameter of regular steps
+  ULL block_max;     // block count of code time 1
+  int fix_nb;        // FixNumNeighbor of updateRadius
+  int nb_max;        // NumNeighborMax of updateRadius (also the list capacity)
+};
+
+// Device arrays of a regular-force context's j-set state (context.cu), which
+// engine_fill_jset writes: x, v, a0, a1 [n][3], t0, mass, r2nb [n].
+struct JsetDst {
+  double *x, *v, *a0, *a1, *t0, *mass, *r2nb;
+};
+
+// Device results of the context's last regular-force launch, row k being the
+// block's k-th target: acc/jerk regular and irregular [m][3], nnb [m], list
+// [m][cap] ascending.
+struct RegResults {
+  const double *acc_reg, *jerk_reg, *acc_irr, *jerk_irr;
+  const int *nnb, *list;
+  int cap;
+};
+
 struct Engine;
 
 // Engine on `device` (the context's device); ABYSS_* codes.
@@ -87,5 +113,34 @@ Changed *engine_changed(Engine *e);
 // and block count of calculateTimeStepIrr.
 int engine_steps(Engine *e, const Params &p, int count, const int *idx, double *new_pos, double *new_vel,
                  double *a_irr, double *a_tot, int *lv_irr, double *dt_irr, ULL *tb_irr);
+
+// ---- whole regular blocks with the state resident on the device
+// (src_mpi/RootRoutines.cpp:1310-1338 updateNextRegTime and the regular half
+// of the block loop; UpdateParticle.cpp:108-139, 314-407;
+// ComputeAcceleration.cpp:405-661).  All of them run on `stream` (the
+// regular-force context's), after the engine holds the whole state
+// (engine_upload of every particle).
+//
+// The next regular block: tmin = the smallest cur_reg + tb_reg not above
+// block_max (block_max when there is none) and its m particles, in ascending
+// index (engine_block_targets, device memory).  Synchronizes.
+int engine_next_block(Engine *e, void *stream, ULL block_max, ULL *tmin, int *m);
+const int *engine_block_targets(const Engine *e);
+// The context's j-set state from the engine's: t0 is t_reg for a particle
+// without neighbours, else t_irr (CalculateRegularAcceleration.cpp:371-374).
+int engine_fill_jset(Engine *e, void *stream, const JsetDst &d);
+// r2nb *= 0.8 for every target k whose list overflowed (nnb[k] > cap).
+int engine_shrink_radii(Engine *e, void *stream, int m, const int *nnb, int cap);
+// Corrector and commit of the block's m targets from the context's results
+// (updateRegularParticleCuda, RegCudaUpdate, calculateTimeStepReg/Irr,
+// updateRadius), every target from the pre-block state.  Synchronizes.
+// Returns ABYSS_OK, ABYSS_ERR_STATE (a time step out of range; the block is
+// committed, as on the host) or ABYSS_ERR_CUDA; borderline level decisions
+// are added to *borderline.
+int engine_correct_block(Engine *e, void *stream, const BlockParams &bp, int m, const RegResults &r,
+                         long long *borderline);
+// Every particle's fields into the pinned staging: engine_images()[i] is
+// particle i (list_off = i * cap), its list at engine_lists() + i * cap.
+int engine_download_all(Engine *e);
 
 }  // namespace abyss_irr

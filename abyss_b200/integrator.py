@@ -147,6 +147,18 @@ class ACIntegrator:
         return {"on": bool(on.value), "borderline": int(border.value), "sec_copy": float(sec.value),
                 "cycles": dict(zip(parts, [int(c) for c in cyc]))}
 
+    def set_device_resident(self, on: bool = True):
+        """Run whole blocks on the GPU with the state kept there
+        (include/abyss_irr.h); the results are the same as on the host."""
+        self._check(self._L.abyss_ac_set_device_resident(self._h, 1 if on else 0))
+
+    def device_resident_info(self) -> dict:
+        on = C.c_int(0)
+        border = C.c_longlong(0)
+        sec = C.c_double(0.0)
+        self._check(self._L.abyss_ac_device_resident_info(self._h, C.byref(on), C.byref(border), C.byref(sec)))
+        return {"on": bool(on.value), "borderline": int(border.value), "sec_sync": float(sec.value)}
+
     def run(self, t_code: float = 1.0):
         self._check(self._L.abyss_ac_run(self._h, float(t_code)))
 

@@ -7,7 +7,8 @@
 
 Each run reports |dE/E| between t = 0 and the end (all particles synchronised
 there), the step counts and where the time went.  The irregular levels run on
-the host threads, or with ``device_irregular`` on the GPU (the same results).  ``on_block`` is called after
+the host threads, or with ``device_irregular`` on the GPU; with ``device_blocks`` whole blocks run on the GPU
+with the state kept there (the same results either way).  ``on_block`` is called after
 every regular block with (integration, initial conditions, block count); the
 test suite uses it to re-check blocks against the FP64 oracle
 (tests/test_runs_gpu.py).
@@ -31,7 +32,8 @@ CONFIGS = {
 EPS = 1e-4
 
 
-def run(name: str, threads: int = 0, t_stop: float = 1.0, on_block=None, device_irregular: bool = False):
+def run(name: str, threads: int = 0, t_stop: float = 1.0, on_block=None, device_irregular: bool = False,
+        device_blocks: bool = False):
     cfg = CONFIGS[name]
     c = ic.plummer(cfg["n"], cfg["seed"], masses=cfg["masses"], k_nb=cfg["k_nb"])
     rf = RegularForce(0)
@@ -40,6 +42,8 @@ def run(name: str, threads: int = 0, t_stop: float = 1.0, on_block=None, device_
                       fix_nb=cfg["k_nb"], t_end=cfg["t_end"], threads=threads)
     if device_irregular:
         ac.set_device_irregular(True)
+    if device_blocks:
+        ac.set_device_resident(True)
     e0 = ac.energy()
     blocks = 0
     done = False
@@ -52,9 +56,12 @@ def run(name: str, threads: int = 0, t_stop: float = 1.0, on_block=None, device_
     e1 = ac.energy()
     out = dict(config=name, n=c.n, t_end=cfg["t_end"], code_time=ac.time, e0=e0, e1=e1,
                dE_over_E=abs((e1 - e0) / e0), wall_s=wall, stats=ac.stats(),
-               irregular="device" if device_irregular else "host", host_timers=ac.host_timers())
-    if device_irregular:
+               irregular="device" if device_irregular or device_blocks else "host",
+               blocks_on="device" if device_blocks else "host", host_timers=ac.host_timers())
+    if device_irregular or device_blocks:
         out["device_irregular"] = ac.device_irregular_info()
+    if device_blocks:
+        out["device_blocks"] = ac.device_resident_info()
     ac.close()
     rf.close()
     return out
@@ -66,9 +73,10 @@ def main():
     ap.add_argument("--threads", type=int, default=0)
     ap.add_argument("--t-stop", type=float, default=1.0, help="stop at this code time (1 = t_end)")
     ap.add_argument("--device-irregular", action="store_true", help="irregular levels on the GPU")
+    ap.add_argument("--device-blocks", action="store_true", help="whole blocks on the GPU, state kept there")
     args = ap.parse_args()
     print(json.dumps(run(args.config, threads=args.threads, t_stop=args.t_stop,
-                         device_irregular=args.device_irregular)))
+                         device_irregular=args.device_irregular, device_blocks=args.device_blocks)))
 
 
 if __name__ == "__main__":

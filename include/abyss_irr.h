@@ -34,6 +34,26 @@ int abyss_ac_set_device_irregular(struct abyss_ac *ac, int on);
 int abyss_ac_device_irregular_info(const struct abyss_ac *ac, int *on, long long *borderline,
                                    double *sec_copy, long long *cycles6);
 
+/* Whole blocks on the GPU (on != 0): the state of record moves to the device
+ * and a block never leaves it -- the next block's particles
+ * (updateNextRegTime, src_mpi/RootRoutines.cpp:1310-1338), the irregular
+ * levels above, the regular force, the corrector and commit
+ * (updateRegularParticleCuda and RegCudaUpdate, ComputeAcceleration.cpp:
+ * 405-661, WorkerRoutines.cpp:124-143), the regular and irregular time steps
+ * and the neighbour radius (UpdateParticle.cpp:108-139, 151-241, 314-407).
+ * The host learns each block's time and size only.  Results equal the host
+ * integrator's bit for bit, as above; level decisions within 1e-12 of a
+ * power-of-two boundary are counted.  The particles are read back when the
+ * state is asked for (abyss_ac_get_state, abyss_ac_energy, abyss_ac_save,
+ * abyss_ac_write_snapshot, and on == 0); abyss_ac_last_regular gives the last
+ * device block.  The split form (abyss_ac_begin_block) is refused while on.
+ * Not while a split block is open. */
+int abyss_ac_set_device_resident(struct abyss_ac *ac, int on);
+/* Whether whole blocks run on the device, the borderline level decisions of
+ * their regular steps, and the wall seconds spent copying the whole state
+ * between host and device. */
+int abyss_ac_device_resident_info(const struct abyss_ac *ac, int *on, long long *borderline, double *sec_sync);
+
 /* One irregular step of each of `count` particles idx[k] of an n-particle
  * state, on GPU `device`, nothing committed: the arguments of
  * abyss_host_irregular_steps (include/abyss_host.h) plus the level inputs of
