@@ -550,6 +550,11 @@ def extras(device: int) -> dict:
     c1 = runs.run("c1")
     out["energy_c1"] = {"workload": "Plummer N = 1024, eps = 1e-4, to t = 10", "dE_over_E": c1["dE_over_E"],
                         "regular_blocks": c1["stats"]["blocks"], "wall_s": c1["wall_s"]}
+    c2 = runs.run("c2", device_blocks=True)
+    out["energy_c2"] = {"workload": "Plummer N = 65536, Kroupa IMF, eps = 1e-4, to t = 2, whole blocks on the GPU",
+                        "dE_over_E": c2["dE_over_E"], "regular_blocks": c2["stats"]["blocks"],
+                        "wall_s": c2["wall_s"], "irregular_s": c2["stats"]["sec_irr"],
+                        "borderline": c2["device_blocks"]["borderline"] + c2["device_irregular"]["borderline"]}
     return out
 
 
