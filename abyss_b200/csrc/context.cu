@@ -381,12 +381,13 @@ int ctx_launch_status(abyss_ctx *c, int *status, int *ovf) {
   if (!c || !status || !ovf) return ABYSS_ERR_ARG;
   if (!c->launched) return fail(c, ABYSS_ERR_STATE, "status: nothing launched");
   cudaSetDevice(c->device);
-  int v[2] = {0, 0};
-  CK(cudaMemcpyAsync(&v[0], c->status.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "D2H status");
-  CK(cudaMemcpyAsync(&v[1], c->ovf.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "D2H overflow");
+  int st = 0, ov = 0;
+  D2H out;  // through the pinned staging: many host threads wait on one GPU
+  CK(out.queue(c, {{&st, c->status.p, sizeof(int)}, {&ov, c->ovf.p, sizeof(int)}}), "D2H status");
   CK(ctx_wait(c), "synchronize");
-  *status = v[0] & kErrTimeout ? ABYSS_ERR_TIMEOUT : ABYSS_OK;
-  *ovf = v[1];
+  out.finish();
+  *status = st & kErrTimeout ? ABYSS_ERR_TIMEOUT : ABYSS_OK;
+  *ovf = ov;
   return ABYSS_OK;
 }
 
@@ -404,14 +405,12 @@ int ctx_read_targets(abyss_ctx *c, int *targets, double *r2nb) {
   if (!c) return ABYSS_ERR_ARG;
   if (!c->launched) return fail(c, ABYSS_ERR_STATE, "read targets: nothing launched");
   cudaSetDevice(c->device);
-  if (targets)
-    CK(cudaMemcpyAsync(targets, c->targets.p, sizeof(int) * (size_t)c->launched_m, cudaMemcpyDeviceToHost,
-                       c->stream),
-       "D2H targets");
-  if (r2nb)
-    CK(cudaMemcpyAsync(r2nb, c->r2nb.p, sizeof(double) * (size_t)c->n, cudaMemcpyDeviceToHost, c->stream),
-       "D2H radii");
+  D2H out;
+  CK(out.queue(c, {{targets, c->targets.p, targets ? sizeof(int) * (size_t)c->launched_m : 0},
+                   {r2nb, c->r2nb.p, r2nb ? sizeof(double) * (size_t)c->n : 0}}),
+     "D2H targets and radii");
   CK(ctx_wait(c), "synchronize");
+  out.finish();
   return ABYSS_OK;
 }
 }  // namespace abyss

@@ -145,7 +145,7 @@ struct abyss_ac {
   // the next-block scan
   double sec_jset = 0.0, sec_sched = 0.0;
   ~abyss_ac() {
-    if (eng) abyss_irr::engine_destroy(eng);
+    if (eng) abyss_irr::engine_give(eng);
     if (jstage) cudaFreeHost(jstage);
   }
 };
@@ -797,7 +797,7 @@ int irregular_levels_device(abyss_ac *ac) {
   using namespace abyss_irr;
   int rc = ABYSS_OK;
   if (!ac->eng) {
-    rc = engine_create(abyss::ctx_device(ac->ctx), &ac->eng);
+    rc = engine_take(abyss::ctx_device(ac->ctx), &ac->eng);
     if (rc != ABYSS_OK) {
       ac->err = "device irregular steps: no engine on the context's device";
       return rc;
@@ -948,7 +948,7 @@ int resident_sync_host(const abyss_ac *cac) {
 int resident_ensure(abyss_ac *ac) {
   using namespace abyss_irr;
   if (!ac->eng) {
-    int rc = engine_create(abyss::ctx_device(ac->ctx), &ac->eng);
+    int rc = engine_take(abyss::ctx_device(ac->ctx), &ac->eng);
     if (rc != ABYSS_OK) {
       ac->err = "device blocks: no engine on the context's device";
       return rc;

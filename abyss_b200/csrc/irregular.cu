@@ -38,7 +38,9 @@
 #include <climits>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
+#include <vector>
 
 #include <cuda_runtime.h>
 
@@ -1099,10 +1101,14 @@ struct Engine {
   cudaStream_t stream = nullptr;
   std::string err;
   int n = 0, cap = 0;
+  int alloc_n = 0;  // particles the arrays and the pinned staging hold
   State S{};
   Image *h_img = nullptr;  // pinned
   int *h_lists = nullptr;  // pinned
   Changed *h_chg = nullptr;  // pinned
+  // pinned control words, one way each: a copy from pageable memory waits in
+  // the driver's staging path, which the host threads of many engines share
+  Ctl *h_ctl_in = nullptr, *h_ctl_out = nullptr;
 };
 
 namespace {
@@ -1131,18 +1137,26 @@ void free_state(State &S) {
   S.ctl = c;
 }
 
-int reset_ctl(Engine *e) {
+// The control words reset on `s` (tmin to its largest value).  The previous
+// copy out of the pinned word has finished: every engine call waits for its
+// stream before it returns.
+int reset_ctl(Engine *e, cudaStream_t s) {
   Ctl c{};
+  c.tmin = ULLONG_MAX;
   c.lmin[0] = c.lmin[1] = ULLONG_MAX;
-  ECK(cudaMemcpyAsync(e->S.ctl, &c, sizeof(c), cudaMemcpyHostToDevice, e->stream), "reset control words");
+  *e->h_ctl_in = c;
+  ECK(cudaMemcpyAsync(e->S.ctl, e->h_ctl_in, sizeof(Ctl), cudaMemcpyHostToDevice, s), "reset control words");
   return ABYSS_OK;
 }
+int reset_ctl(Engine *e) { return reset_ctl(e, e->stream); }
 
-int read_ctl(Engine *e, Ctl *c) {
-  ECK(cudaMemcpyAsync(c, e->S.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, e->stream), "read control words");
-  ECK(cudaStreamSynchronize(e->stream), "synchronize");
+int read_ctl(Engine *e, Ctl *c, cudaStream_t s) {
+  ECK(cudaMemcpyAsync(e->h_ctl_out, e->S.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s), "read control words");
+  ECK(cudaStreamSynchronize(s), "synchronize");
+  *c = *e->h_ctl_out;
   return ABYSS_OK;
 }
+int read_ctl(Engine *e, Ctl *c) { return read_ctl(e, c, e->stream); }
 
 }  // namespace
 
@@ -1166,7 +1180,9 @@ int engine_create(int device, Engine **out) {
   int per_sm = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, irr_levels, kThreads, 0) != cudaSuccess || per_sm < 1 ||
       cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaMalloc((void **)&e->S.ctl, sizeof(Ctl)) != cudaSuccess) {
+      cudaMalloc((void **)&e->S.ctl, sizeof(Ctl)) != cudaSuccess ||
+      cudaHostAlloc((void **)&e->h_ctl_in, sizeof(Ctl), cudaHostAllocDefault) != cudaSuccess ||
+      cudaHostAlloc((void **)&e->h_ctl_out, sizeof(Ctl), cudaHostAllocDefault) != cudaSuccess) {
     cudaGetLastError();
     engine_destroy(e);
     return ABYSS_ERR_CUDA;
@@ -1185,17 +1201,68 @@ void engine_destroy(Engine *e) {
   if (e->h_img) cudaFreeHost(e->h_img);
   if (e->h_lists) cudaFreeHost(e->h_lists);
   if (e->h_chg) cudaFreeHost(e->h_chg);
+  if (e->h_ctl_in) cudaFreeHost(e->h_ctl_in);
+  if (e->h_ctl_out) cudaFreeHost(e->h_ctl_out);
   if (e->stream) cudaStreamDestroy(e->stream);
   delete e;
 }
 
 const char *engine_error(const Engine *e) { return e ? e->err.c_str() : "null engine"; }
 
+namespace {
+constexpr size_t kPoolMax = 16;  // engines kept per process
+std::mutex g_pool_mu;
+std::vector<Engine *> g_pool;
+}  // namespace
+
+int engine_take(int device, Engine **out) {
+  if (!out) return ABYSS_ERR_ARG;
+  {
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    for (size_t k = g_pool.size(); k-- > 0;)
+      if (g_pool[k]->device == device) {
+        *out = g_pool[k];
+        g_pool.erase(g_pool.begin() + (long)k);
+        (*out)->err.clear();
+        return ABYSS_OK;
+      }
+  }
+  return engine_create(device, out);
+}
+
+void engine_give(Engine *e) {
+  if (!e) return;
+  cudaSetDevice(e->device);
+  if (cudaStreamSynchronize(e->stream) == cudaSuccess) {
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    if (g_pool.size() < kPoolMax) {
+      g_pool.push_back(e);
+      return;
+    }
+  }
+  cudaGetLastError();
+  engine_destroy(e);
+}
+
 int engine_reserve(Engine *e, int n, int cap) {
   if (!e || n <= 0 || cap <= 0) return ABYSS_ERR_ARG;
   if (n == e->n && cap == e->cap) return ABYSS_OK;
   cudaSetDevice(e->device);
   ECK(cudaStreamSynchronize(e->stream), "synchronize");
+  if (cap == e->cap && n <= e->alloc_n) {
+    // a smaller (or regrown) cluster in the arrays already held: no
+    // allocation, which would synchronize the device for every other stream
+    ECK(cudaMemsetAsync(e->S.touched, 0, sizeof(int) * (size_t)n, e->stream), "clear");
+    ECK(cudaMemsetAsync(e->S.nnb, 0, sizeof(int) * (size_t)n, e->stream), "clear");
+    ECK(cudaStreamSynchronize(e->stream), "synchronize");
+    e->S.n = n;
+    e->n = n;
+    return ABYSS_OK;
+  }
+  // growth by at least half again, so that an engine reused for clusters of
+  // rising sizes reallocates only a few times
+  const int grow = cap == e->cap ? e->alloc_n + e->alloc_n / 2 : 0;
+  const int n_alloc = std::max(n, grow);
   free_state(e->S);
   if (e->h_img) cudaFreeHost(e->h_img);
   if (e->h_lists) cudaFreeHost(e->h_lists);
@@ -1203,9 +1270,9 @@ int engine_reserve(Engine *e, int n, int cap) {
   e->h_img = nullptr;
   e->h_lists = nullptr;
   e->h_chg = nullptr;
-  e->n = e->cap = 0;
+  e->n = e->cap = e->alloc_n = 0;
   State &S = e->S;
-  const size_t N = n;
+  const size_t N = n_alloc;
   ECK(dalloc(&S.rec, N), "alloc");
   ECK(dalloc(&S.a_tot, 12 * N), "alloc");
   ECK(dalloc(&S.a_reg, 12 * N), "alloc");
@@ -1242,6 +1309,7 @@ int engine_reserve(Engine *e, int n, int cap) {
   S.cap = cap;
   e->n = n;
   e->cap = cap;
+  e->alloc_n = n_alloc;
   return ABYSS_OK;
 }
 
@@ -1375,18 +1443,17 @@ int engine_next_block(Engine *e, void *stream, ULL block_max, ULL *tmin, int *m)
   if (!e || e->n <= 0 || !tmin || !m) return ABYSS_ERR_ARG;
   cudaSetDevice(e->device);
   cudaStream_t s = (cudaStream_t)stream;
-  Ctl c{};
-  c.tmin = ULLONG_MAX;
-  c.lmin[0] = c.lmin[1] = ULLONG_MAX;
-  ECK(cudaMemcpyAsync(e->S.ctl, &c, sizeof(c), cudaMemcpyHostToDevice, s), "reset control words");
+  int rc = reset_ctl(e, s);
+  if (rc != ABYSS_OK) return rc;
   const int chunks = (e->n + kSchedChunk - 1) / kSchedChunk;
   const int blocks = std::max(1, std::min((e->n + kThreads - 1) / kThreads, 4 * e->sm_count));
   blk_min<<<blocks, kThreads, 0, s>>>(e->S, block_max);
   blk_count<<<chunks, kThreads, 0, s>>>(e->S);
   blk_collect<<<chunks, kThreads, 0, s>>>(e->S);
   ECK(cudaGetLastError(), "next block launch");
-  ECK(cudaMemcpyAsync(&c, e->S.ctl, sizeof(c), cudaMemcpyDeviceToHost, s), "read control words");
-  ECK(cudaStreamSynchronize(s), "synchronize");
+  Ctl c;
+  rc = read_ctl(e, &c, s);
+  if (rc != ABYSS_OK) return rc;
   if (c.tmin == ULLONG_MAX) {
     *tmin = block_max;
     *m = 0;
@@ -1424,15 +1491,15 @@ int engine_correct_block(Engine *e, void *stream, const BlockParams &bp, int m, 
     return fail(e, ABYSS_ERR_ARG, "regular block: list capacity differs from the engine's");
   cudaSetDevice(e->device);
   cudaStream_t s = (cudaStream_t)stream;
-  Ctl c{};
-  c.lmin[0] = c.lmin[1] = ULLONG_MAX;
-  ECK(cudaMemcpyAsync(e->S.ctl, &c, sizeof(c), cudaMemcpyHostToDevice, s), "reset control words");
+  int rc = reset_ctl(e, s);
+  if (rc != ABYSS_OK) return rc;
   const int blocks = std::max(1, std::min((int)(((size_t)m * 32 + kThreads - 1) / kThreads), 8 * e->sm_count));
   blk_correct<<<blocks, kThreads, 0, s>>>(e->S, bp, m, r);
   blk_commit<<<blocks, kThreads, 0, s>>>(e->S, bp, m, r);
   ECK(cudaGetLastError(), "corrector launch");
-  ECK(cudaMemcpyAsync(&c, e->S.ctl, sizeof(c), cudaMemcpyDeviceToHost, s), "read control words");
-  ECK(cudaStreamSynchronize(s), "synchronize");
+  Ctl c;
+  rc = read_ctl(e, &c, s);
+  if (rc != ABYSS_OK) return rc;
   if (borderline) *borderline += c.borderline;
   if (c.status & kRegBad) return fail(e, ABYSS_ERR_STATE, "regular time step out of range");
   return ABYSS_OK;

@@ -90,8 +90,16 @@ int engine_create(int device, Engine **out);
 void engine_destroy(Engine *e);
 const char *engine_error(const Engine *e);
 // Size the device state for n particles with lists of capacity cap (keeps
-// the state when the sizes are unchanged).
+// the state when the sizes are unchanged; a smaller n with the same capacity
+// reuses the arrays, cleared).
 int engine_reserve(Engine *e, int n, int cap);
+// Engines kept for reuse between integrations (an engine's arrays and pinned
+// staging are allocated once for the largest cluster it held; allocating them
+// per integration would synchronize the device under every other stream).
+// engine_take gives a pooled engine of `device` or a new one; engine_give
+// returns one to the pool (or frees it when the pool is full).
+int engine_take(int device, Engine **out);
+void engine_give(Engine *e);
 // Pinned staging: n images and n x cap list entries (packed: image k's list
 // starts at its list_off).
 Image *engine_images(Engine *e);

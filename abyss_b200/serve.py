@@ -100,7 +100,8 @@ class Server:
     def __init__(self, device: int = 0, capacity: int = 1 << 21, max_clusters: int = 512, list_cap: int = 128,
                  eps2: float = 1e-8, eta_reg: float = 0.02, eta_irr: float = 0.01, host_threads: int = 16,
                  slice_ms: float = 20.0, max_n: int = 16384, chunk_j: int = 256, device_irregular_min_n: int = 0,
-                 team_min_n: int = 16384, lane_min_n: int = 0, lane_threads: int = 2, lane_team: int = 4):
+                 team_min_n: int = 16384, lane_min_n: int = 0, lane_threads: int = 2, lane_team: int = 4,
+                 device_blocks_min_n: int = 0):
         """device_irregular_min_n > 0: integrations of at least that many
         particles run their irregular levels on the GPU (include/abyss_irr.h)
         instead of on their worker thread; the results are the same.
@@ -112,7 +113,11 @@ class Server:
         nothing and its round trips would set their latency.  Each runs whole on
         one of lane_threads host threads, through a context of its own, with a
         team of lane_team threads and (above device_irregular_min_n) its
-        irregular levels on the GPU."""
+        irregular levels on the GPU.
+        device_blocks_min_n > 0: a lane's request of at least that many
+        particles runs with whole blocks on the GPU and its state kept there
+        (abyss_ac_set_device_resident): the host only waits, so many lanes can
+        share the GPU; the results are the same."""
         self.rf = RegularForce(device)
         self.ens = Ensemble(self.rf, None, list_cap=list_cap, capacity=capacity, max_clusters=max_clusters)
         # short j-chunks: a serving wave is small and latency-bound, so its work
@@ -121,6 +126,7 @@ class Server:
         self.eps2 = eps2
         self.eta_reg, self.eta_irr = eta_reg, eta_irr
         self.device_irregular_min_n = int(device_irregular_min_n)
+        self.device_blocks_min_n = int(device_blocks_min_n)
         self.team_min_n = max(1, int(team_min_n))
         self.lane_min_n = int(lane_min_n)
         self.lane_team = max(1, int(lane_team))
@@ -316,7 +322,10 @@ class Server:
             ac = ACIntegrator(rf, c.x, c.v, c.m, c.r2nb, eps2=self.eps2, eta_reg=self.eta_reg,
                               eta_irr=self.eta_irr, fix_nb=r.k_nb, nb_max=self.list_cap, t_end=r.t_end,
                               threads=self.lane_team)
-            if self.device_irregular_min_n > 0 and r.n >= self.device_irregular_min_n:
+            on_device = self.device_blocks_min_n > 0 and r.n >= self.device_blocks_min_n
+            if on_device:
+                ac.set_device_resident(True)
+            elif self.device_irregular_min_n > 0 and r.n >= self.device_irregular_min_n:
                 ac.set_device_irregular(True)
             r.e0 = ac.energy()
             ac.run(1.0)
@@ -325,7 +334,8 @@ class Server:
             r.finished = self.now()
             r.result = dict(rid=r.rid, n=r.n, model=r.model, dE_over_E=abs((r.e1 - r.e0) / r.e0), blocks=r.blocks,
                             latency_s=r.finished - r.arrival, queue_s=r.admitted - r.arrival,
-                            device_irregular=ac.device_irregular_info()["on"], lane=True,
+                            device_irregular=on_device or ac.device_irregular_info()["on"], lane=True,
+                            device_blocks=on_device,
                             x_final=ac.state()["x"])
             ac.close()
         finally:
@@ -396,7 +406,7 @@ def poisson_requests(rate: float, duration: float, nmin: int, nmax: int, seed: i
 def serve(rate: float = 200.0, duration: float = 2.0, nmin: int = 256, nmax: int = 2048, t_end: float = 0.0625,
           capacity: int = 1 << 21, seed: int = 5, host_threads: int = 16, serial: bool = False,
           chunk_j: int = 256, slice_ms: float = 20.0, device_irregular_min_n: int = 0, reqs=None,
-          lane_min_n: int = 0):
+          lane_min_n: int = 0, lane_threads: int = 2, device_blocks_min_n: int = 0):
     """Run a Poisson stream through the server (or, with serial=True, one request at
     a time through the same code) and report latency percentiles and throughput.
     `reqs` replaces the generated stream (requests with prebuilt clusters)."""
@@ -412,7 +422,7 @@ def serve(rate: float = 200.0, duration: float = 2.0, nmin: int = 256, nmax: int
     else:
         srv = Server(capacity=capacity, host_threads=host_threads, max_n=max(nmax, max(r.n for r in reqs)),
                      chunk_j=chunk_j, slice_ms=slice_ms, device_irregular_min_n=device_irregular_min_n,
-                     lane_min_n=lane_min_n)
+                     lane_min_n=lane_min_n, lane_threads=lane_threads, device_blocks_min_n=device_blocks_min_n)
         for r in reqs:
             srv.submit(r)
         srv.run_until_idle()
@@ -427,6 +437,7 @@ def serve(rate: float = 200.0, duration: float = 2.0, nmin: int = 256, nmax: int
                cluster_blocks_per_s=blocks / wall if wall > 0 else None,
                frac_dE_below_1e6=float(np.mean(de <= 1e-6)) if len(de) else None,
                device_irregular_requests=int(sum(bool(r.result.get("device_irregular")) for r in done)),
+               device_blocks_requests=int(sum(bool(r.result.get("device_blocks")) for r in done)),
                clusters_per_s=len(done) / wall if wall > 0 else None,
                p50_latency_s=float(np.percentile(lat, 50)) if len(lat) else None,
                p99_latency_s=float(np.percentile(lat, 99)) if len(lat) else None,
@@ -434,7 +445,9 @@ def serve(rate: float = 200.0, duration: float = 2.0, nmin: int = 256, nmax: int
                median_dE_over_E=float(np.median(de)) if len(de) else None,
                rounds=rounds, gpu_wave_ms=wave_ms, peak_active=peak, phase_s=phases,
                config=dict(rate=rate, duration=duration, nmin=nmin, nmax=nmax, t_end=t_end, capacity=capacity,
-                           seed=seed, serial=serial, device_irregular_min_n=device_irregular_min_n))
+                           seed=seed, serial=serial, device_irregular_min_n=device_irregular_min_n,
+                           lane_min_n=lane_min_n, lane_threads=lane_threads,
+                           device_blocks_min_n=device_blocks_min_n))
     return res, done
 
 
@@ -486,7 +499,8 @@ def c4_requests(k: int = 512, t_end: float = 5.0):
 
 
 def run_config(name: str, duration: float = 1.0, sample: int = 16, device_irregular_min_n: int = 4096,
-               host_threads: int = 16, capacity: int = 1 << 22, lane_min_n: int = 0):
+               host_threads: int = 16, capacity: int = 1 << 22, lane_min_n: int = 0, lane_threads: int = 2,
+               device_blocks_min_n: int = 0):
     """A stated configuration through the continuous server, and the serial
     plain form on an evenly spaced sample of the same requests (the whole
     stream one at a time would take hours): its clusters/s is the sample's
@@ -503,11 +517,12 @@ def run_config(name: str, duration: float = 1.0, sample: int = 16, device_irregu
     for r in reqs:
         r.cluster = r.make_cluster()
     res, done = serve(reqs=reqs, nmax=nmax, capacity=capacity, host_threads=host_threads,
-                      device_irregular_min_n=device_irregular_min_n, lane_min_n=lane_min_n)
+                      device_irregular_min_n=device_irregular_min_n, lane_min_n=lane_min_n,
+                      lane_threads=lane_threads, device_blocks_min_n=device_blocks_min_n)
     res.pop("phase_s", None)
     res["config"] = dict(
         name=name, requests=len(reqs), device_irregular_min_n=device_irregular_min_n, host_threads=host_threads,
-        capacity=capacity, lane_min_n=lane_min_n,
+        capacity=capacity, lane_min_n=lane_min_n, lane_threads=lane_threads, device_blocks_min_n=device_blocks_min_n,
         workload=("512 equal-mass Plummer clusters, N log-uniform in [256, 16384] (seed 4, cluster k seeded "
                   "4000 + k), eps = 1e-4, all arriving at t = 0, each to t = 5" if name == "c4" else
                   f"Poisson 200 requests/s for {duration} s (seed 5), Plummer or King W0 3/6/9, Kroupa IMF, "
@@ -545,6 +560,9 @@ def main():
     ap.add_argument("--device-irregular-min-n", type=int, default=4096)
     ap.add_argument("--lane-min-n", type=int, default=0,
                     help="requests of at least this many particles run whole outside the waves (0: none)")
+    ap.add_argument("--lane-threads", type=int, default=2, help="host threads (and contexts) of the lane")
+    ap.add_argument("--device-blocks-min-n", type=int, default=0,
+                    help="lane requests of at least this many particles run whole blocks on the GPU (0: none)")
     ap.add_argument("--rate", type=float, default=2000.0)
     ap.add_argument("--duration", type=float, default=0.5)
     ap.add_argument("--nmin", type=int, default=256)
@@ -556,7 +574,8 @@ def main():
     if args.config:
         print(json.dumps(run_config(args.config, duration=args.duration, sample=args.sample,
                                     device_irregular_min_n=args.device_irregular_min_n, host_threads=args.threads,
-                                    lane_min_n=args.lane_min_n)))
+                                    lane_min_n=args.lane_min_n, lane_threads=args.lane_threads,
+                                    device_blocks_min_n=args.device_blocks_min_n)))
         return
     out = {}
     for serial in (False, True):
