@@ -337,6 +337,7 @@ namespace abyss {
 cudaStream_t ctx_stream(abyss_ctx *c) { return c->stream; }
 int ctx_device(abyss_ctx *c) { return c->device; }
 int ctx_sm_count(abyss_ctx *c) { return c->sm_count; }
+int ctx_wait_spin(abyss_ctx *c) { return c->wait_spin_us; }
 
 // ---- used by whole regular blocks on the device (host/ac_integrator.cpp):
 // the state the host would upload is written into the context by a kernel on

@@ -11,6 +11,7 @@ struct abyss_ctx;
 namespace abyss {
 cudaStream_t ctx_stream(abyss_ctx *c);
 int ctx_device(abyss_ctx *c);
+int ctx_wait_spin(abyss_ctx *c);  // the wait policy of abyss_set_wait (< 0: stream synchronisation)
 int ctx_state_buffers(abyss_ctx *c, int n, abyss_irr::JsetDst *d);
 int ctx_targets_from_device(abyss_ctx *c, int m, const int *d_targets);
 int ctx_launch_status(abyss_ctx *c, int *status, int *ovf);

@@ -804,6 +804,7 @@ int irregular_levels_device(abyss_ac *ac) {
     }
     ac->eng_synced = false;
   }
+  engine_set_wait(ac->eng, abyss::ctx_wait_spin(ac->ctx));  // the context's wait policy
   const int n = ac->n, cap = ac->p.nb_max;
   for (int i = 0; i < n; ++i)
     if ((int)ac->s[i].nb.size() > cap) {
@@ -955,6 +956,7 @@ int resident_ensure(abyss_ac *ac) {
     }
     ac->eng_synced = false;
   }
+  engine_set_wait(ac->eng, abyss::ctx_wait_spin(ac->ctx));  // the context's wait policy
   if (ac->eng_synced) return ABYSS_OK;
   const double t0 = now_s();
   const int n = ac->n, cap = ac->p.nb_max;
@@ -1025,7 +1027,7 @@ int resident_block(abyss_ac *ac) {
   Params P = irr_params(ac);
   RunStats rs;
   ac->host_stale = true;
-  const int run = engine_run_levels(e, P, &rs);
+  const int run = engine_run_levels(e, P, &rs, stream);  // the context's stream: one stream per integration
   ac->st.irr_levels += rs.levels;
   ac->st.irr_steps += rs.steps;
   ac->dev_borderline += rs.borderline;

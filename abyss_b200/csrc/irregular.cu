@@ -35,6 +35,7 @@
 // L2-coherent loads (__ldcg): an SM's L1 does not see other SMs' stores.
 #include <algorithm>
 #include <cfloat>
+#include <chrono>
 #include <climits>
 #include <cstdio>
 #include <cstring>
@@ -1109,6 +1110,11 @@ struct Engine {
   // pinned control words, one way each: a copy from pageable memory waits in
   // the driver's staging path, which the host threads of many engines share
   Ctl *h_ctl_in = nullptr, *h_ctl_out = nullptr;
+  // how a call waits for its stream: < 0 the stream synchronisation (the
+  // thread keeps its core), else poll for spin_us then sleep in a blocking
+  // event wait (many engines driven from more host threads than cores)
+  int spin_us = -1;
+  cudaEvent_t ev_wait = nullptr;
 };
 
 namespace {
@@ -1150,9 +1156,24 @@ int reset_ctl(Engine *e, cudaStream_t s) {
 }
 int reset_ctl(Engine *e) { return reset_ctl(e, e->stream); }
 
+// Wait on the host for everything queued on `s`, by the engine's policy.
+cudaError_t sync_stream(Engine *e, cudaStream_t s) {
+  if (e->spin_us < 0 || !e->ev_wait) return cudaStreamSynchronize(s);
+  cudaError_t err = cudaEventRecord(e->ev_wait, s);
+  if (err != cudaSuccess) return err;
+  const auto t0 = std::chrono::steady_clock::now();
+  const auto spin = std::chrono::microseconds(e->spin_us);
+  for (;;) {
+    err = cudaEventQuery(e->ev_wait);
+    if (err != cudaErrorNotReady) return err;
+    if (std::chrono::steady_clock::now() - t0 >= spin) break;
+  }
+  return cudaEventSynchronize(e->ev_wait);
+}
+
 int read_ctl(Engine *e, Ctl *c, cudaStream_t s) {
   ECK(cudaMemcpyAsync(e->h_ctl_out, e->S.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s), "read control words");
-  ECK(cudaStreamSynchronize(s), "synchronize");
+  ECK(sync_stream(e, s), "synchronize");
   *c = *e->h_ctl_out;
   return ABYSS_OK;
 }
@@ -1203,11 +1224,22 @@ void engine_destroy(Engine *e) {
   if (e->h_chg) cudaFreeHost(e->h_chg);
   if (e->h_ctl_in) cudaFreeHost(e->h_ctl_in);
   if (e->h_ctl_out) cudaFreeHost(e->h_ctl_out);
+  if (e->ev_wait) cudaEventDestroy(e->ev_wait);
   if (e->stream) cudaStreamDestroy(e->stream);
   delete e;
 }
 
 const char *engine_error(const Engine *e) { return e ? e->err.c_str() : "null engine"; }
+
+int engine_set_wait(Engine *e, int spin_us) {
+  if (!e) return ABYSS_ERR_ARG;
+  if (spin_us >= 0 && !e->ev_wait) {
+    cudaSetDevice(e->device);
+    ECK(cudaEventCreateWithFlags(&e->ev_wait, cudaEventBlockingSync | cudaEventDisableTiming), "wait event");
+  }
+  e->spin_us = spin_us < 0 ? -1 : spin_us;
+  return ABYSS_OK;
+}
 
 namespace {
 constexpr size_t kPoolMax = 16;  // engines kept per process
@@ -1345,10 +1377,11 @@ int engine_upload(Engine *e, int count, long long list_entries) {
   return ABYSS_OK;
 }
 
-int engine_run_levels(Engine *e, const Params &p, RunStats *st) {
+int engine_run_levels(Engine *e, const Params &p, RunStats *st, void *stream) {
   if (!e || e->n <= 0) return ABYSS_ERR_ARG;
   cudaSetDevice(e->device);
-  int rc = reset_ctl(e);
+  cudaStream_t s = stream ? (cudaStream_t)stream : e->stream;
+  int rc = reset_ctl(e, s);
   if (rc != ABYSS_OK) return rc;
   // one block per SM at most (a level's barrier waits on every block), and
   // enough blocks that a slice fits the block's member list
@@ -1359,10 +1392,10 @@ int engine_run_levels(Engine *e, const Params &p, RunStats *st) {
   State S = e->S;
   Params P = p;
   void *args[] = {&S, &P, &slice};
-  ECK(cudaLaunchCooperativeKernel((const void *)irr_levels, dim3(grid), dim3(kThreads), args, 0, e->stream),
+  ECK(cudaLaunchCooperativeKernel((const void *)irr_levels, dim3(grid), dim3(kThreads), args, 0, s),
       "level loop launch");
   Ctl c;
-  rc = read_ctl(e, &c);
+  rc = read_ctl(e, &c, s);
   if (rc != ABYSS_OK) return rc;
   if (st) {
     st->levels = c.levels;
@@ -1383,7 +1416,7 @@ int engine_download(Engine *e) {
   ECK(cudaGetLastError(), "gather launch");
   ECK(cudaMemcpyAsync(e->h_chg, e->S.chg, sizeof(Changed) * (size_t)e->n, cudaMemcpyDeviceToHost, e->stream),
       "D2H changes");
-  ECK(cudaStreamSynchronize(e->stream), "synchronize");
+  ECK(sync_stream(e, e->stream), "synchronize");
   return ABYSS_OK;
 }
 
@@ -1515,7 +1548,7 @@ int engine_download_all(Engine *e) {
       "D2H images");
   ECK(cudaMemcpyAsync(e->h_lists, e->S.nb, sizeof(int) * (size_t)e->n * e->cap, cudaMemcpyDeviceToHost, e->stream),
       "D2H lists");
-  ECK(cudaStreamSynchronize(e->stream), "synchronize");
+  ECK(sync_stream(e, e->stream), "synchronize");
   return ABYSS_OK;
 }
 

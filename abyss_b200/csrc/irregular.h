@@ -89,6 +89,10 @@ struct Engine;
 int engine_create(int device, Engine **out);
 void engine_destroy(Engine *e);
 const char *engine_error(const Engine *e);
+// How the engine's calls wait for the GPU: spin_us < 0 (the default) the
+// stream synchronisation; else poll for spin_us microseconds, then sleep in a
+// blocking event wait (abyss_set_wait of include/abyss_reg.h).
+int engine_set_wait(Engine *e, int spin_us);
 // Size the device state for n particles with lists of capacity cap (keeps
 // the state when the sizes are unchanged; a smaller n with the same capacity
 // reuses the arrays, cleared).
@@ -107,10 +111,11 @@ int *engine_lists(Engine *e);
 // Scatter the first `count` staged images (each carrying its particle index)
 // and their lists (list_entries in all) into the device state.
 int engine_upload(Engine *e, int count, long long list_entries);
-// The level loop up to p.next_reg_block on the device state.  Returns
-// ABYSS_OK, ABYSS_ERR_STATE (a time step out of range: nothing of that level
-// committed), ABYSS_ERR_TIMEOUT or ABYSS_ERR_CUDA.
-int engine_run_levels(Engine *e, const Params &p, RunStats *st);
+// The level loop up to p.next_reg_block on the device state, on `stream` (a
+// cudaStream_t; null: the engine's own).  Returns ABYSS_OK, ABYSS_ERR_STATE (a
+// time step out of range: nothing of that level committed), ABYSS_ERR_TIMEOUT
+// or ABYSS_ERR_CUDA.
+int engine_run_levels(Engine *e, const Params &p, RunStats *st, void *stream = nullptr);
 // Copy the changed fields of every particle into the pinned staging
 // (engine_changed()[i] is particle i, its `touched` flag set when a run since
 // the last download stepped it) and clear the flags.

@@ -101,7 +101,7 @@ class Server:
                  eps2: float = 1e-8, eta_reg: float = 0.02, eta_irr: float = 0.01, host_threads: int = 16,
                  slice_ms: float = 20.0, max_n: int = 16384, chunk_j: int = 256, device_irregular_min_n: int = 0,
                  team_min_n: int = 16384, lane_min_n: int = 0, lane_threads: int = 2, lane_team: int = 4,
-                 device_blocks_min_n: int = 0):
+                 device_blocks_min_n: int = 0, lane_wait_us: int = -1):
         """device_irregular_min_n > 0: integrations of at least that many
         particles run their irregular levels on the GPU (include/abyss_irr.h)
         instead of on their worker thread; the results are the same.
@@ -117,7 +117,10 @@ class Server:
         device_blocks_min_n > 0: a lane's request of at least that many
         particles runs with whole blocks on the GPU and its state kept there
         (abyss_ac_set_device_resident): the host only waits, so many lanes can
-        share the GPU; the results are the same."""
+        share the GPU; the results are the same.
+        lane_wait_us >= 0: a lane thread waiting for the GPU polls that long,
+        then sleeps (include/abyss_reg.h abyss_set_wait), leaving its core to
+        the other lanes; < 0: it spins."""
         self.rf = RegularForce(device)
         self.ens = Ensemble(self.rf, None, list_cap=list_cap, capacity=capacity, max_clusters=max_clusters)
         # short j-chunks: a serving wave is small and latency-bound, so its work
@@ -135,7 +138,10 @@ class Server:
         self.lane_ctx: queue.Queue = queue.Queue()
         if self.lane_min_n > 0:
             for _ in range(max(1, lane_threads)):
-                self.lane_ctx.put(RegularForce(device))
+                rf = RegularForce(device)
+                if lane_wait_us >= 0:
+                    rf.set_wait(int(lane_wait_us))
+                self.lane_ctx.put(rf)
         self.list_cap = list_cap
         nthreads = max(1, host_threads)
         self.host_threads = nthreads
@@ -406,7 +412,7 @@ def poisson_requests(rate: float, duration: float, nmin: int, nmax: int, seed: i
 def serve(rate: float = 200.0, duration: float = 2.0, nmin: int = 256, nmax: int = 2048, t_end: float = 0.0625,
           capacity: int = 1 << 21, seed: int = 5, host_threads: int = 16, serial: bool = False,
           chunk_j: int = 256, slice_ms: float = 20.0, device_irregular_min_n: int = 0, reqs=None,
-          lane_min_n: int = 0, lane_threads: int = 2, device_blocks_min_n: int = 0):
+          lane_min_n: int = 0, lane_threads: int = 2, device_blocks_min_n: int = 0, lane_wait_us: int = -1):
     """Run a Poisson stream through the server (or, with serial=True, one request at
     a time through the same code) and report latency percentiles and throughput.
     `reqs` replaces the generated stream (requests with prebuilt clusters)."""
@@ -422,7 +428,8 @@ def serve(rate: float = 200.0, duration: float = 2.0, nmin: int = 256, nmax: int
     else:
         srv = Server(capacity=capacity, host_threads=host_threads, max_n=max(nmax, max(r.n for r in reqs)),
                      chunk_j=chunk_j, slice_ms=slice_ms, device_irregular_min_n=device_irregular_min_n,
-                     lane_min_n=lane_min_n, lane_threads=lane_threads, device_blocks_min_n=device_blocks_min_n)
+                     lane_min_n=lane_min_n, lane_threads=lane_threads, device_blocks_min_n=device_blocks_min_n,
+                     lane_wait_us=lane_wait_us)
         for r in reqs:
             srv.submit(r)
         srv.run_until_idle()
@@ -447,7 +454,7 @@ def serve(rate: float = 200.0, duration: float = 2.0, nmin: int = 256, nmax: int
                config=dict(rate=rate, duration=duration, nmin=nmin, nmax=nmax, t_end=t_end, capacity=capacity,
                            seed=seed, serial=serial, device_irregular_min_n=device_irregular_min_n,
                            lane_min_n=lane_min_n, lane_threads=lane_threads,
-                           device_blocks_min_n=device_blocks_min_n))
+                           device_blocks_min_n=device_blocks_min_n, lane_wait_us=lane_wait_us))
     return res, done
 
 
@@ -498,9 +505,17 @@ def c4_requests(k: int = 512, t_end: float = 5.0):
             for i, c in enumerate(clusters)]
 
 
+# Server options of the stated configurations (run_config).  Configuration 4
+# runs every integration whole on a lane with its blocks on the GPU: sixteen at
+# once, sharing the GPU.  Configuration 5 sends integrations of 16 384
+# particles and more to four such lanes and serves the rest in waves.
+CONFIG_LANES = {"c4": dict(lane_min_n=1, lane_threads=16, device_blocks_min_n=1),
+                "c5": dict(lane_min_n=16384, lane_threads=4, device_blocks_min_n=1)}
+
+
 def run_config(name: str, duration: float = 1.0, sample: int = 16, device_irregular_min_n: int = 4096,
-               host_threads: int = 16, capacity: int = 1 << 22, lane_min_n: int = 0, lane_threads: int = 2,
-               device_blocks_min_n: int = 0):
+               host_threads: int = 16, capacity: int = 1 << 22, lane_min_n: int | None = None,
+               lane_threads: int | None = None, device_blocks_min_n: int | None = None, lane_wait_us: int = -1):
     """A stated configuration through the continuous server, and the serial
     plain form on an evenly spaced sample of the same requests (the whole
     stream one at a time would take hours): its clusters/s is the sample's
@@ -508,6 +523,10 @@ def run_config(name: str, duration: float = 1.0, sample: int = 16, device_irregu
       c4: the 512 ensemble clusters to t = 5, all arriving at once;
       c5: Poisson 200 requests/s for `duration` s (seed 5), Plummer or King W0
           3/6/9, Kroupa IMF, N log-uniform in [1024, 131072], to t = 1."""
+    lanes = CONFIG_LANES[name]
+    lane_min_n = lanes["lane_min_n"] if lane_min_n is None else lane_min_n
+    lane_threads = lanes["lane_threads"] if lane_threads is None else lane_threads
+    device_blocks_min_n = lanes["device_blocks_min_n"] if device_blocks_min_n is None else device_blocks_min_n
     if name == "c4":
         reqs = c4_requests()
         nmax = 16384
@@ -518,11 +537,12 @@ def run_config(name: str, duration: float = 1.0, sample: int = 16, device_irregu
         r.cluster = r.make_cluster()
     res, done = serve(reqs=reqs, nmax=nmax, capacity=capacity, host_threads=host_threads,
                       device_irregular_min_n=device_irregular_min_n, lane_min_n=lane_min_n,
-                      lane_threads=lane_threads, device_blocks_min_n=device_blocks_min_n)
+                      lane_threads=lane_threads, device_blocks_min_n=device_blocks_min_n, lane_wait_us=lane_wait_us)
     res.pop("phase_s", None)
     res["config"] = dict(
         name=name, requests=len(reqs), device_irregular_min_n=device_irregular_min_n, host_threads=host_threads,
         capacity=capacity, lane_min_n=lane_min_n, lane_threads=lane_threads, device_blocks_min_n=device_blocks_min_n,
+        lane_wait_us=lane_wait_us,
         workload=("512 equal-mass Plummer clusters, N log-uniform in [256, 16384] (seed 4, cluster k seeded "
                   "4000 + k), eps = 1e-4, all arriving at t = 0, each to t = 5" if name == "c4" else
                   f"Poisson 200 requests/s for {duration} s (seed 5), Plummer or King W0 3/6/9, Kroupa IMF, "
@@ -558,13 +578,17 @@ def main():
     ap.add_argument("--config", choices=["c4", "c5"], default=None)
     ap.add_argument("--sample", type=int, default=16)
     ap.add_argument("--device-irregular-min-n", type=int, default=4096)
-    ap.add_argument("--lane-min-n", type=int, default=0,
-                    help="requests of at least this many particles run whole outside the waves (0: none)")
-    ap.add_argument("--lane-threads", type=int, default=2, help="host threads (and contexts) of the lane")
-    ap.add_argument("--device-blocks-min-n", type=int, default=0,
+    ap.add_argument("--lane-min-n", type=int, default=None,
+                    help="requests of at least this many particles run whole outside the waves (0: none; "
+                         "default: 0, or the stated configuration's)")
+    ap.add_argument("--lane-threads", type=int, default=None, help="host threads (and contexts) of the lane")
+    ap.add_argument("--device-blocks-min-n", type=int, default=None,
                     help="lane requests of at least this many particles run whole blocks on the GPU (0: none)")
+    ap.add_argument("--lane-wait-us", type=int, default=-1,
+                    help="a lane thread polls the GPU this long, then sleeps (< 0: spins)")
     ap.add_argument("--rate", type=float, default=2000.0)
-    ap.add_argument("--duration", type=float, default=0.5)
+    ap.add_argument("--duration", type=float, default=None,
+                    help="stream length in s (default 0.5; 1 for the stated configuration 5)")
     ap.add_argument("--nmin", type=int, default=256)
     ap.add_argument("--nmax", type=int, default=2048)
     ap.add_argument("--t-end", type=float, default=0.0625)
@@ -572,15 +596,19 @@ def main():
     ap.add_argument("--threads", type=int, default=16)
     args = ap.parse_args()
     if args.config:
-        print(json.dumps(run_config(args.config, duration=args.duration, sample=args.sample,
+        print(json.dumps(run_config(args.config, duration=1.0 if args.duration is None else args.duration,
+                                    sample=args.sample,
                                     device_irregular_min_n=args.device_irregular_min_n, host_threads=args.threads,
                                     lane_min_n=args.lane_min_n, lane_threads=args.lane_threads,
-                                    device_blocks_min_n=args.device_blocks_min_n)))
+                                    device_blocks_min_n=args.device_blocks_min_n, lane_wait_us=args.lane_wait_us)))
         return
     out = {}
+    duration = 0.5 if args.duration is None else args.duration
     for serial in (False, True):
-        res, _ = serve(args.rate, args.duration, args.nmin, args.nmax, args.t_end, args.capacity,
-                       host_threads=args.threads, serial=serial)
+        res, _ = serve(args.rate, duration, args.nmin, args.nmax, args.t_end, args.capacity,
+                       host_threads=args.threads, serial=serial, lane_min_n=args.lane_min_n or 0,
+                       lane_threads=args.lane_threads or 2, device_blocks_min_n=args.device_blocks_min_n or 0,
+                       lane_wait_us=args.lane_wait_us)
         res["phase_s"].pop("build_thread_s", None)
         out["serial_plain" if serial else "continuous"] = res
     out["speedup"] = out["continuous"]["clusters_per_s"] / out["serial_plain"]["clusters_per_s"]
