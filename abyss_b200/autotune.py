@@ -58,7 +58,7 @@ def _time(rf: RegularForce, tuning, reps=2, list_cap=256, eps2=1e-8):
 def tune(rf: RegularForce, n: int, buckets=BUCKETS, anchor_min: int = 16384, seed: int = 0,
          splits=(0, 2, 4), verbose=False):
     """rf must hold a predicted j-set of n particles.  Returns [(m_max, shape, ms)]."""
-    rf.set_profiling(True)
+    rf.set_profiling("whole")
     rng = np.random.default_rng(seed)
     table = []
     shapes = variants()
@@ -70,8 +70,8 @@ def tune(rf: RegularForce, n: int, buckets=BUCKETS, anchor_min: int = 16384, see
         cands = []
         if m <= 64:
             cands += [dict(kernel=2, ipt=i) for i in (1, 2, 4, 8) if i <= max(1, m)]
-        if 16 <= m <= 256:  # warps sharing targets
-            cands += [dict(kernel=4, ipt=i, j_split=s) for i in (1, 2) for s in (0, 1024, 2048)]
+        if 16 <= m <= 256:  # warps sharing targets, scalar and packed
+            cands += [dict(kernel=k, ipt=i, j_split=s) for k in (4, 5) for i in (1, 2) for s in (0, 1024, 2048)]
         for sh in shapes:
             if sh["mode"] == 1 and m < anchor_min:
                 continue

@@ -122,8 +122,8 @@ struct abyss_ctx {
   abyss_tuning plan{};
   int plan_chunks = 0;
   Table table;
-  // profiling
-  bool profiling = false;
+  // profiling: 0 off, 1 each phase, 2 the whole launch (two events)
+  int profiling = 0;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   // host waits: < 0 stream synchronisation, else spin this long, then block
   int wait_spin_us = -1;
@@ -654,17 +654,30 @@ static abyss_tuning plan_for(abyss_ctx *c, int m, const abyss_tuning *user) {
   // set is dense enough for them to be accurate, double-single offsets below
   // that.
   if (t.kernel == 0) {
-    if (m <= 24) {
+    if (m <= 20) {
       t.kernel = 2;
-    } else if (m <= 96 && t.threads == 0 && t.ipt == 0 && (t.mode == 0 || t.mode == 2)) {
-      // 25-96 targets: the block's 4 warps share 32 targets (64 for 49-64
-      // targets) and split each j-tile, two j per step (measured 384 against
-      // 347 Gpairs/s at m = 32, 502 against 467 at m = 64, 518 at m = 96, for
-      // one target per thread in 32/64/128-thread blocks)
-      t.kernel = 4;
-      t.ipt = (m > 48 && m <= 64) ? 2 : 1;
-      t.unroll = 2;
-      if (t.j_split == 0) t.j_split = m <= 48 ? 2048 : 1024;
+    } else if (m <= 128 && t.threads == 0 && t.ipt == 0 && (t.mode == 0 || t.mode == 2)) {
+      // 21-128 targets: the block's 4 warps share 32 (or 64) targets and
+      // split each j-tile.  Measured whole calls (Gpairs/s): m = 24 packed
+      // over two j 304 (j-major 277); m = 32 the same 406 (scalar with two j
+      // per step 385); m = 48 scalar 346 (packed 333); m = 64 packed over a
+      // thread's two targets 551 (scalar 487); m = 96 scalar 524 (packed
+      // 492); m = 128 packed, two targets 605 (one target per thread on the
+      // 128-thread tile kernel 592)
+      if (m <= 32) {
+        t.kernel = 5;
+        t.ipt = 1;
+        if (t.j_split == 0) t.j_split = 1024;
+      } else if (m <= 48 || (m > 64 && m <= 96)) {
+        t.kernel = 4;
+        t.ipt = 1;
+        t.unroll = 2;
+        if (t.j_split == 0) t.j_split = m <= 48 ? 2048 : 1024;
+      } else {
+        t.kernel = 5;
+        t.ipt = 2;
+        if (t.j_split == 0) t.j_split = 1024;
+      }
     } else if (m <= 128 && (t.threads == 0 || t.threads == (m <= 48 ? 32 : m <= 96 ? 64 : 128)) &&
                (t.ipt == 0 || t.ipt == 1) && (t.mode == 0 || t.mode == 2)) {
       t.kernel = 1;
@@ -703,12 +716,14 @@ static abyss_tuning plan_for(abyss_ctx *c, int m, const abyss_tuning *user) {
         if (t.j_split == 0 && m <= 256) t.j_split = 2048;
       }
     }
-  } else if (t.kernel == 4) {
-    // warps sharing targets: 4 warps, double-single offsets, 32 x ipt targets per block
+  } else if (t.kernel == 4 || t.kernel == 5) {
+    // warps sharing targets: 4 warps, double-single offsets, 32 x ipt targets
+    // per block (kernel 5: packed FP32x2 arithmetic, one j per step for ipt 1
+    // -- its two halves are two j)
     t.mode = 2;
     t.threads = 128;
     if (t.ipt == 0) t.ipt = 1;
-    if (t.unroll == 0) t.unroll = 1;
+    if (t.unroll == 0 || (t.kernel == 5 && t.ipt == 1)) t.unroll = 1;
     t.min_blocks = 1;
   } else {
     if (t.mode == 0) t.mode = (m >= 4096) ? 1 : 2;
@@ -739,10 +754,11 @@ int abyss_launch(abyss_ctx *c, double eps2, int list_cap, const abyss_tuning *tu
     L = (n + want * nw - 1) / (want * nw);
     L = std::max(64, (L + 63) / 64 * 64);
     S = (n + L * nw - 1) / (L * nw);
-  } else if (t.kernel == 1 || t.kernel == 3 || t.kernel == 4) {
-    const int per_block = t.kernel == 4 ? 32 * t.ipt : t.threads * t.ipt;
+  } else if (t.kernel == 1 || t.kernel == 3 || t.kernel == 4 || t.kernel == 5) {
+    const bool split = t.kernel == 4 || t.kernel == 5;
+    const int per_block = split ? 32 * t.ipt : t.threads * t.ipt;
     n_iblocks = (m + per_block - 1) / per_block;
-    const int occ = t.kernel == 4 ? tile_split_occupancy(t.ipt, t.unroll)
+    const int occ = split ? tile_split_occupancy(t.ipt, t.unroll, t.kernel == 5)
                                   : tile_occupancy(t.threads, t.ipt, t.mode == 1, t.kernel == 3, t.unroll, t.min_blocks);
     if (occ <= 0) return fail(c, ABYSS_ERR_ARG, "launch: unsupported tile shape");
     // persistent grid: every SM holds the same number of CTAs, which take
@@ -820,7 +836,7 @@ int abyss_launch(abyss_ctx *c, double eps2, int list_cap, const abyss_tuning *tu
     w.order_t = c->targets.p;
     w.order_o = c->iota.p;
   }
-  if (c->profiling) CK(cudaEventRecord(c->ev[1], c->stream), "event");
+  if (c->profiling == 1) CK(cudaEventRecord(c->ev[1], c->stream), "event");
   Outputs o;
   o.targets = c->targets.p;
   o.acc_reg = c->acc_reg.p;
@@ -831,8 +847,8 @@ int abyss_launch(abyss_ctx *c, double eps2, int list_cap, const abyss_tuning *tu
   o.list = c->list.p;
   o.overflow_rows = c->ovf.p;
   o.ovf_list = c->ovf_list.p;
-  if (t.kernel == 4) {
-    if (launch_tile_split(c->stream, t.ipt, t.unroll, grid, js, w, n_iblocks) != 0)
+  if (t.kernel == 4 || t.kernel == 5) {
+    if (launch_tile_split(c->stream, t.ipt, t.unroll, t.kernel == 5, grid, js, w, n_iblocks) != 0)
       return fail(c, ABYSS_ERR_ARG, "launch: unsupported tile shape");
     t.grid = grid;
   } else if (t.kernel == 1 || t.kernel == 3) {
@@ -846,7 +862,7 @@ int abyss_launch(abyss_ctx *c, double eps2, int list_cap, const abyss_tuning *tu
       return fail(c, ABYSS_ERR_ARG, "launch: unsupported j-major shape");
   }
   CK(cudaGetLastError(), "force kernel launch");
-  if (c->profiling) CK(cudaEventRecord(c->ev[2], c->stream), "event");
+  if (c->profiling == 1) CK(cudaEventRecord(c->ev[2], c->stream), "event");
   if (!(t.kernel == 2 && m <= kFuseRows)) {
     launch_finalize(c->stream, js, w, o, c->sm_count);
     CK(cudaGetLastError(), "finalize launch");
@@ -928,7 +944,7 @@ int abyss_last_order(abyss_ctx *c, int *rows) {
 
 int abyss_set_profiling(abyss_ctx *c, int on) {
   if (!c) return ABYSS_ERR_ARG;
-  c->profiling = on != 0;
+  c->profiling = on == 2 ? 2 : on != 0 ? 1 : 0;
   return ABYSS_OK;
 }
 
@@ -937,6 +953,11 @@ int abyss_last_timing(abyss_ctx *c, float *ms3) {
   if (!c->profiling) return fail(c, ABYSS_ERR_STATE, "last_timing: profiling is off");
   cudaSetDevice(c->device);
   CK(ctx_wait(c), "synchronize");
+  if (c->profiling == 2) {
+    ms3[0] = ms3[2] = 0.0f;
+    CK(cudaEventElapsedTime(&ms3[1], c->ev[0], c->ev[3]), "event time");
+    return ABYSS_OK;
+  }
   for (int i = 0; i < 3; ++i) CK(cudaEventElapsedTime(&ms3[i], c->ev[i], c->ev[i + 1]), "event time");
   return ABYSS_OK;
 }

@@ -478,9 +478,14 @@ struct TileLayout {
 // targets and each takes every JW-th group of 32 j of a tile, so that a small
 // active set still fills the SMs with warps; at the end of an item warp 0 adds
 // the warps' sums in FP64 in warp order.
-template <int NT, int IPT, int TJ, int NST, bool ANCHOR, bool PACK, int UNR, int MINB, int JW = 1>
+//
+// PJ (one target per thread): two j per step as the two halves of the FP32x2
+// operands, so that the pair arithmetic of a single target also runs packed;
+// the halves' tile partials are added at the end of the tile.
+template <int NT, int IPT, int TJ, int NST, bool ANCHOR, bool PACK, int UNR, int MINB, int JW = 1, bool PJ = false>
 __global__ void __launch_bounds__(NT, MINB) reg_force_tile(JSet js, Work w, int n_iblocks) {
   static_assert(JW == 1 || NT == 32 * JW, "warps sharing targets: one target slot per lane");
+  static_assert(!PJ || (IPT == 1 && !PACK), "two j per step: one target per thread, scalar otherwise");
   using LY = TileLayout<NT, IPT, TJ, NST, ANCHOR, PACK>;
   constexpr int TS = JW > 1 ? 32 : NT;  // target slots per k (per lane, or per thread)
   constexpr int TJP = LY::TJP;
@@ -656,6 +661,7 @@ __global__ void __launch_bounds__(NT, MINB) reg_force_tile(JSet js, Work w, int 
 
       float p[IPT][6];  // scalar tile partials
       float2 p2[PP][6]; // packed tile partials
+      float2 pj[6];     // PJ: the two j streams of target 0
 #pragma unroll
       for (int k = 0; k < IPT; ++k)
 #pragma unroll
@@ -664,6 +670,8 @@ __global__ void __launch_bounds__(NT, MINB) reg_force_tile(JSet js, Work w, int 
       for (int q = 0; q < PP; ++q)
 #pragma unroll
         for (int c = 0; c < 6; ++c) p2[q][c] = make_float2(0.0f, 0.0f);
+#pragma unroll
+      for (int c = 0; c < 6; ++c) pj[c] = make_float2(0.0f, 0.0f);
 
       // Fast path, 32 j at a time: every pair is accumulated with candidates
       // (pairs inside the guard band of R_nb) masked to 0, and each thread sets
@@ -674,6 +682,35 @@ __global__ void __launch_bounds__(NT, MINB) reg_force_tile(JSet js, Work w, int 
       for (int g0 = JW > 1 ? 32 * wid : 0; g0 < cnt; g0 += 32 * JW) {
         const int gl = min(32, cnt - g0);
         unsigned cbits = 0u;
+        if constexpr (PJ) {
+          // j = g0 + l and g0 + l + 1 in the two halves (an odd last one pairs
+          // with a pad entry)
+          for (int l = 0; l < gl; l += 2) {
+            const int jl = g0 + l;
+            const float4 P0 = cb[jl], P1 = cb[jl + 1];
+            const float4 V0 = cb[TJP + jl], V1 = cb[TJP + jl + 1];
+            PairGeom2 g;
+            if (ANCHOR) {
+              g = pair_geom2(make_float2(P0.x, P1.x), make_float2(P0.y, P1.y), make_float2(P0.z, P1.z),
+                             make_float2(V0.x, V1.x), make_float2(V0.y, V1.y), make_float2(V0.z, V1.z), dup2(hx[0]),
+                             dup2(hy[0]), dup2(hz[0]), dup2(vx[0]), dup2(vy[0]), dup2(vz[0]), eps2v);
+            } else {
+              const float4 L0 = cb[2 * TJP + jl], L1 = cb[2 * TJP + jl + 1];
+              g = pair_geom2_ds(make_float2(P0.x, P1.x), make_float2(P0.y, P1.y), make_float2(P0.z, P1.z),
+                                make_float2(L0.x, L1.x), make_float2(L0.y, L1.y), make_float2(L0.z, L1.z),
+                                make_float2(V0.x, V1.x), make_float2(V0.y, V1.y), make_float2(V0.z, V1.z), dup2(hx[0]),
+                                dup2(hy[0]), dup2(hz[0]), dup2(lx[0]), dup2(ly[0]), dup2(lz[0]), dup2(vx[0]),
+                                dup2(vy[0]), dup2(vz[0]), eps2v);
+            }
+            const bool c0 = g.r2.x < r2g[0];
+            const bool c1 = g.r2.y < r2g[0];
+            float2 ri;
+            ri.x = c0 ? 0.0f : rsqrtf(g.r2.x);
+            ri.y = c1 ? 0.0f : rsqrtf(g.r2.y);
+            pair_accum2(g, make_float2(P0.w, P1.w), ri, pj);
+            cbits |= ((unsigned)c0 << l) | ((unsigned)c1 << (l + 1));
+          }
+        } else
         for (int l = 0; l < gl; l += UNR) {
 #pragma unroll
           for (int u = 0; u < UNR; ++u) {
@@ -767,6 +804,8 @@ __global__ void __launch_bounds__(NT, MINB) reg_force_tile(JSet js, Work w, int 
           float pv;
           if (k < NPK)
             pv = (k & 1) ? p2[k >> 1][c].y : p2[k >> 1][c].x;
+          else if (PJ)
+            pv = __fadd_rn(__fadd_rn(pj[c].x, pj[c].y), p[k][c]);
           else
             pv = p[k][c];
           float *sp = &ksm[(k * 12 + c) * NT + tid];
@@ -841,6 +880,25 @@ __global__ void __launch_bounds__(32 * kJmWarps, MI <= 2 ? 5 : 1) reg_force_jmaj
   const int jw1 = min(js.n, jw0 + Lw);
   const float2 eps2v = dup2(w.eps2f);
   for (int ig = 0; ig < w.m; ig += MI) {
+    // j records, two per lane a step; a pad is massless and far away: never a
+    // candidate, adds 0.  The next step's records are loaded before this
+    // step's arithmetic, so that a warp keeps two steps of loads in flight;
+    // the first step's are issued before the targets' loads, which they do not
+    // depend on.
+    double nX0 = 1e30, nY0 = 1e30, nZ0 = 1e30, nX1 = 1e30, nY1 = 1e30, nZ1 = 1e30;
+    float4 nV0 = make_float4(0.f, 0.f, 0.f, 0.f), nV1 = nV0;
+    if (jw0 + lane < jw1) {
+      nX0 = js.px[jw0 + lane];
+      nY0 = js.py[jw0 + lane];
+      nZ0 = js.pz[jw0 + lane];
+      nV0 = js.vm[jw0 + lane];
+    }
+    if (jw0 + 32 + lane < jw1) {
+      nX1 = js.px[jw0 + 32 + lane];
+      nY1 = js.py[jw0 + 32 + lane];
+      nZ1 = js.pz[jw0 + 32 + lane];
+      nV1 = js.vm[jw0 + 32 + lane];
+    }
     // targets, held negated as double-single hi/lo; r2g < 0 marks an unused slot
     float nhx[MI], nhy[MI], nhz[MI], nlx[MI], nly[MI], nlz[MI], nvx[MI], nvy[MI], nvz[MI], r2g[MI];
 #pragma unroll
@@ -873,23 +931,6 @@ __global__ void __launch_bounds__(32 * kJmWarps, MI <= 2 ? 5 : 1) reg_force_jmaj
 #pragma unroll
       for (int c = 0; c < 6; ++c) p[k][c] = make_float2(0.0f, 0.0f);
 
-    // j records, two per lane a step; a pad is massless and far away: never a
-    // candidate, adds 0.  The next step's records are loaded before this
-    // step's arithmetic, so that a warp keeps two steps of loads in flight.
-    double nX0 = 1e30, nY0 = 1e30, nZ0 = 1e30, nX1 = 1e30, nY1 = 1e30, nZ1 = 1e30;
-    float4 nV0 = make_float4(0.f, 0.f, 0.f, 0.f), nV1 = nV0;
-    if (jw0 + lane < jw1) {
-      nX0 = js.px[jw0 + lane];
-      nY0 = js.py[jw0 + lane];
-      nZ0 = js.pz[jw0 + lane];
-      nV0 = js.vm[jw0 + lane];
-    }
-    if (jw0 + 32 + lane < jw1) {
-      nX1 = js.px[jw0 + 32 + lane];
-      nY1 = js.py[jw0 + 32 + lane];
-      nZ1 = js.pz[jw0 + 32 + lane];
-      nV1 = js.vm[jw0 + 32 + lane];
-    }
     for (int jb = jw0; jb < jw1; jb += 64) {
       const int ja = jb + lane, jc = jb + 32 + lane;
       const bool ina = ja < jw1, inc = jc < jw1;
@@ -1175,13 +1216,43 @@ __device__ void finalize_row_block(const JSet &js, const Work &w, const Outputs 
                                    int *fin_smem, double (*red)[6], int *s_nl_total) {
   const int nch = w.row_nchunks ? w.row_nchunks[r] : w.n_chunks;
   const int joff = w.row_joff ? w.row_joff[r] : 0;
-  double s[6] = {0, 0, 0, 0, 0, 0};
-  for (int c = threadIdx.x; c < nch; c += NT) {
-    const double *src = w.part + ((size_t)r * w.s_stride + c) * 6;
+  // chunk partials: thread g * 6 + q adds component q of chunks g, g + G, ...
+  // into eight sums by turn (eight independent loads in flight), which it adds
+  // in order; then the G sums of a component are added in g order
+  constexpr int G = NT / 6;
+  constexpr int A = 8;
+  __shared__ double s_part[G * 6];
+  if (threadIdx.x < G * 6) {
+    const int g = threadIdx.x / 6, q = threadIdx.x - 6 * g;
+    const double *src = w.part + (size_t)r * w.s_stride * 6 + q;
+    double acc[A];
 #pragma unroll
-    for (int q = 0; q < 6; ++q) s[q] += __ldcg(&src[q]);
+    for (int k = 0; k < A; ++k) acc[k] = 0.0;
+    int c = g;
+    for (; c + (A - 1) * G < nch; c += A * G) {
+      double v[A];
+#pragma unroll
+      for (int k = 0; k < A; ++k) v[k] = __ldcg(&src[(size_t)(c + k * G) * 6]);
+#pragma unroll
+      for (int k = 0; k < A; ++k) acc[k] += v[k];
+    }
+#pragma unroll
+    for (int k = 0; k < A; ++k)
+      if (c + k * G < nch) acc[k] += __ldcg(&src[(size_t)(c + k * G) * 6]);
+    double t = 0.0;
+#pragma unroll
+    for (int k = 0; k < A; ++k) t += acc[k];
+    s_part[threadIdx.x] = t;
   }
-  block_sum6<NT>(s, red);
+  __syncthreads();
+  double s[6] = {0, 0, 0, 0, 0, 0};
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      double t = 0.0;
+      for (int g = 0; g < G; ++g) t += s_part[6 * g + q];
+      s[q] = t;
+    }
 
   {
     const int total = __ldcg(&w.lcnt[r]);
@@ -1518,43 +1589,56 @@ int launch_tile(cudaStream_t s, int nt, int ipt, bool anchor, bool pack, int unr
   return 0;
 }
 
-// Warps sharing targets (kernel 4): 4 warps, scalar pair arithmetic,
-// double-single offsets; 32 x ipt targets per block; 1 or 2 j per step.
-template <int IPT, int UNR>
+// Warps sharing targets: 4 warps, double-single offsets, 32 x ipt targets per
+// block.  Kernel 4: scalar pair arithmetic, 1 or 2 j per step.  Kernel 5
+// (packed): FP32x2 over the two targets of a thread (ipt 2, 1 or 2 j per
+// step) or over two j (ipt 1).
+template <int IPT, int UNR, bool PK>
 static int split_occ() {
   constexpr int TJ = 128, NST = 3, NT = 128;
-  auto k = reg_force_tile<NT, IPT, TJ, NST, false, false, UNR, 1, 4>;
-  const size_t sm = TileLayout<NT, IPT, TJ, NST, false, false>::bytes;
+  constexpr bool PACK = PK && IPT == 2, PJ = PK && IPT == 1;
+  auto k = reg_force_tile<NT, IPT, TJ, NST, false, PACK, UNR, 1, 4, PJ>;
+  const size_t sm = TileLayout<NT, IPT, TJ, NST, false, PACK>::bytes;
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   int blocks = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k, NT, sm);
   return blocks;
 }
 
-template <int IPT, int UNR>
+template <int IPT, int UNR, bool PK>
 static void split_run(cudaStream_t s, int grid, const JSet &js, const Work &w, int n_iblocks) {
   constexpr int TJ = 128, NST = 3, NT = 128;
-  auto k = reg_force_tile<NT, IPT, TJ, NST, false, false, UNR, 1, 4>;
-  const size_t sm = TileLayout<NT, IPT, TJ, NST, false, false>::bytes;
+  constexpr bool PACK = PK && IPT == 2, PJ = PK && IPT == 1;
+  auto k = reg_force_tile<NT, IPT, TJ, NST, false, PACK, UNR, 1, 4, PJ>;
+  const size_t sm = TileLayout<NT, IPT, TJ, NST, false, PACK>::bytes;
   k<<<grid, NT, sm, s>>>(js, w, n_iblocks);
 }
 
-int tile_split_occupancy(int ipt, int unr) {
+int tile_split_occupancy(int ipt, int unr, bool packed) {
   int occ = -1;
-  if (ipt == 1) occ = unr == 2 ? split_occ<1, 2>() : split_occ<1, 1>();
-  if (ipt == 2) occ = unr == 2 ? split_occ<2, 2>() : split_occ<2, 1>();
+  if (!packed && ipt == 1) occ = unr == 2 ? split_occ<1, 2, false>() : split_occ<1, 1, false>();
+  if (!packed && ipt == 2) occ = unr == 2 ? split_occ<2, 2, false>() : split_occ<2, 1, false>();
+  if (packed && ipt == 1) occ = split_occ<1, 1, true>();
+  if (packed && ipt == 2) occ = unr == 2 ? split_occ<2, 2, true>() : split_occ<2, 1, true>();
   return cudaGetLastError() == cudaSuccess ? occ : -1;
 }
 
-int launch_tile_split(cudaStream_t s, int ipt, int unr, int grid, const JSet &js, const Work &w, int n_iblocks) {
-  if (ipt == 1 && unr == 2)
-    split_run<1, 2>(s, grid, js, w, n_iblocks);
-  else if (ipt == 1 && unr == 1)
-    split_run<1, 1>(s, grid, js, w, n_iblocks);
-  else if (ipt == 2 && unr == 2)
-    split_run<2, 2>(s, grid, js, w, n_iblocks);
-  else if (ipt == 2 && unr == 1)
-    split_run<2, 1>(s, grid, js, w, n_iblocks);
+int launch_tile_split(cudaStream_t s, int ipt, int unr, bool packed, int grid, const JSet &js, const Work &w,
+                      int n_iblocks) {
+  if (!packed && ipt == 1 && unr == 2)
+    split_run<1, 2, false>(s, grid, js, w, n_iblocks);
+  else if (!packed && ipt == 1 && unr == 1)
+    split_run<1, 1, false>(s, grid, js, w, n_iblocks);
+  else if (!packed && ipt == 2 && unr == 2)
+    split_run<2, 2, false>(s, grid, js, w, n_iblocks);
+  else if (!packed && ipt == 2 && unr == 1)
+    split_run<2, 1, false>(s, grid, js, w, n_iblocks);
+  else if (packed && ipt == 1)
+    split_run<1, 1, true>(s, grid, js, w, n_iblocks);
+  else if (packed && ipt == 2 && unr == 2)
+    split_run<2, 2, true>(s, grid, js, w, n_iblocks);
+  else if (packed && ipt == 2 && unr == 1)
+    split_run<2, 1, true>(s, grid, js, w, n_iblocks);
   else
     return -1;
   return 0;

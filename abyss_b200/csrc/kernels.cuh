@@ -31,8 +31,9 @@ int launch_tile(cudaStream_t s, int nt, int ipt, bool anchor, bool pack, int unr
                 const JSet &js, const Work &w, int n_iblocks);
 // Tile kernel whose 4 warps share a block's 32 x ipt targets (ipt 1 or 2) and
 // split each j-tile between them (abyss_tuning.kernel = 4); unr j per step (1, 2).
-int tile_split_occupancy(int ipt, int unr);
-int launch_tile_split(cudaStream_t s, int ipt, int unr, int grid, const JSet &js, const Work &w, int n_iblocks);
+int tile_split_occupancy(int ipt, int unr, bool packed);
+int launch_tile_split(cudaStream_t s, int ipt, int unr, bool packed, int grid, const JSet &js, const Work &w,
+                      int n_iblocks);
 int tile_variant_count();
 int tile_variant_shape(int i, int *shape6);
 // j-major force kernel: w.n_chunks blocks of jmajor_warps() warps, each warp a

@@ -173,8 +173,10 @@ class RegularForce:
         self._check(self._L.abyss_last_order(self._h, ptr(rows, _ip)))
         return rows
 
-    def set_profiling(self, on: bool):
-        self._check(self._L.abyss_set_profiling(self._h, 1 if on else 0))
+    def set_profiling(self, on):
+        """True: time each phase of later launches; "whole": the whole launch
+        with two events (no events between phases); False: off."""
+        self._check(self._L.abyss_set_profiling(self._h, 2 if on == "whole" else 1 if on else 0))
 
     def last_timing(self):
         ms = np.zeros(3, np.float32)

@@ -46,7 +46,9 @@ typedef struct abyss_tuning {
   int kernel;  /* 1 = tile kernel (i in registers, j-tiles by TMA), 2 = j-major kernel,
                   3 = tile kernel with packed FP32x2 pair arithmetic,
                   4 = tile kernel whose 4 warps share 32 x ipt targets (ipt 1 or 2) and
-                      split each j-tile, for small active sets (double-single) */
+                      split each j-tile, for small active sets (double-single),
+                  5 = kernel 4 with packed FP32x2 pair arithmetic (over a thread's two
+                      targets for ipt 2, over two j for ipt 1) */
   int mode;    /* tile kernel: 1 = anchor offsets on spatially ordered targets, 2 = double-single */
   int threads; /* tile kernel: 128 or 256 */
   int ipt;     /* tile: targets per thread 1, 2, 4;  j-major: targets per pass 1, 2, 4, 8 */
@@ -130,10 +132,13 @@ int abyss_last_plan(const abyss_ctx *ctx, abyss_tuning *plan, int *n_chunks);
  * Identity otherwise.
  * Synchronizes the stream.  No reference counterpart (diagnostics). */
 int abyss_last_order(abyss_ctx *ctx, int *rows);
-/* Time each phase of subsequent launches with CUDA events on the context stream. */
+/* Time subsequent launches with CUDA events on the context stream: on == 1
+ * each phase, on == 2 the whole launch with two events (the events between
+ * phases take a few microseconds of the stream themselves), 0 off. */
 int abyss_set_profiling(abyss_ctx *ctx, int on);
 /* Milliseconds of the last profiled launch: [0] target ordering, [1] force
- * kernel, [2] finalize.  Synchronizes the stream. */
+ * kernel, [2] finalize; with on == 2, [1] is the whole launch and [0] = [2] = 0.
+ * Synchronizes the stream. */
 int abyss_last_timing(abyss_ctx *ctx, float *ms3);
 /* Auto-selection table from the autotuner: k entries, each (m_max, tuning);
  * the first entry with m <= m_max wins.  k = 0 restores the built-in rule. */

@@ -28,6 +28,7 @@ TILE_ANCHOR = dict(kernel=1, mode=1)
 JMAJOR = dict(kernel=2)
 PACKED = dict(kernel=3, mode=2)
 SPLIT = dict(kernel=4)
+SPLIT_PACKED = dict(kernel=5)
 SHAPES = [
     ("packed-ds-128x2", dict(kernel=3, mode=2, threads=128, ipt=2)),
     ("packed-ds-256x4", dict(kernel=3, mode=2, threads=256, ipt=4)),
@@ -47,6 +48,9 @@ SHAPES = [
     ("split-ds-128x2", dict(kernel=4, ipt=2)),
     ("split-ds-128x1-u2", dict(kernel=4, ipt=1, unroll=2)),
     ("split-ds-128x2-u2", dict(kernel=4, ipt=2, unroll=2)),
+    ("split-packed-128x1", dict(kernel=5, ipt=1)),
+    ("split-packed-128x2", dict(kernel=5, ipt=2)),
+    ("split-packed-128x2-u2", dict(kernel=5, ipt=2, unroll=2)),
 ]
 
 
@@ -119,7 +123,7 @@ def test_forced_j_splits(rf, split):
     scale = oracle.reg_scale(c.x, c.v, c.m, c.r2nb, 0.0, t)
     for tu in (dict(kernel=1, mode=2, j_split=split), dict(kernel=1, mode=1, j_split=split),
                dict(kernel=2, ipt=8, j_split=split), dict(kernel=3, mode=2, j_split=split),
-               dict(kernel=4, ipt=2, j_split=split)):
+               dict(kernel=4, ipt=2, j_split=split), dict(kernel=5, ipt=1, j_split=split)):
         res = rf.calculate_acceleration(t, eps2=0.0, list_cap=256, tuning=tu)
         check(res, ref, f"split{split}/{tu}", scale)
 
@@ -131,7 +135,7 @@ def test_unsorted_and_repeated_targets(rf):
     rf.send_to_device(c.m, c.x, c.v, c.r2nb)
     ref = oracle.reg_force(c.x, c.v, c.m, c.r2nb, 0.0, t, 256)
     scale = oracle.reg_scale(c.x, c.v, c.m, c.r2nb, 0.0, t)
-    for tu in (TILE_DS, TILE_ANCHOR, JMAJOR, PACKED, SPLIT):
+    for tu in (TILE_DS, TILE_ANCHOR, JMAJOR, PACKED, SPLIT, SPLIT_PACKED):
         res = rf.calculate_acceleration(t, 0.0, 256, tu)
         check(res, ref, f"unsorted/{tu}", scale)
 
@@ -148,7 +152,7 @@ def test_no_neighbours_and_all_neighbours(rf):
     # regular sum, and anchor offsets of a spread-out block of targets are only
     # accurate for pairs wider than the block; the library picks anchor mode only
     # for large active sets ordered along a Hilbert curve)
-    for tu in (TILE_DS, JMAJOR, PACKED, SPLIT):
+    for tu in (TILE_DS, JMAJOR, PACKED, SPLIT, SPLIT_PACKED):
         res = rf.calculate_acceleration(t, 1e-8, 64, tu)
         assert res.nnb.sum() == 0
         check(res, ref, f"R=0/{tu}", scale)
@@ -156,7 +160,7 @@ def test_no_neighbours_and_all_neighbours(rf):
     big = np.full(c.n, 1e6)
     rf.send_to_device(c.m, c.x, c.v, big)
     ref = oracle.reg_force(c.x, c.v, c.m, big, 1e-8, t, 100)
-    for tu in (TILE_DS, TILE_ANCHOR, JMAJOR, PACKED, SPLIT):
+    for tu in (TILE_DS, TILE_ANCHOR, JMAJOR, PACKED, SPLIT, SPLIT_PACKED):
         res = rf.calculate_acceleration(t, 1e-8, 100, tu)
         assert res.overflow_rows == c.n
         assert np.all(res.nnb == c.n - 1)
@@ -177,7 +181,7 @@ def test_overflow_with_few_rows(rf, m):
     big = np.full(c.n, 1e6)
     rf.send_to_device(c.m, c.x, c.v, big)
     ref = oracle.reg_force(c.x, c.v, c.m, big, 1e-8, t, 100)
-    for tu in (TILE_DS, JMAJOR, PACKED, SPLIT):
+    for tu in (TILE_DS, JMAJOR, PACKED, SPLIT, SPLIT_PACKED):
         res = rf.calculate_acceleration(t, 1e-8, 100, tu)
         assert res.overflow_rows == m, tu
         assert np.all(res.nnb == c.n - 1), tu
@@ -194,7 +198,7 @@ def test_tiny_and_ragged_jsets(rf, n):
     rf.send_to_device(c.m, c.x, c.v, c.r2nb)
     ref = oracle.reg_force(c.x, c.v, c.m, c.r2nb, 0.0, t, 32)
     scale = oracle.reg_scale(c.x, c.v, c.m, c.r2nb, 0.0, t)
-    for tu in (TILE_DS, TILE_ANCHOR, JMAJOR, PACKED, SPLIT):
+    for tu in (TILE_DS, TILE_ANCHOR, JMAJOR, PACKED, SPLIT, SPLIT_PACKED):
         res = rf.calculate_acceleration(t, 0.0, 32, tu)
         check(res, ref, f"n={n}/{tu}", scale)
 

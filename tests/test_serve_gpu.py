@@ -72,16 +72,20 @@ def test_device_irregular_levels_in_serving_give_the_same_results():
         assert host[k]["dE_over_E"] == dev[k]["dE_over_E"], k
 
 
-def test_large_requests_run_whole_on_the_lane():
+@pytest.mark.parametrize("device_blocks_min_n", [0, 1])
+def test_large_requests_run_whole_on_the_lane(device_blocks_min_n):
     """Requests above the lane size run whole outside the waves (the plain
-    single-cluster path on a lane context, device irregular levels) while the
-    others are served; a lane result equals the same integration run directly."""
+    single-cluster path on a lane context, device irregular levels; or, with
+    device_blocks_min_n, whole blocks on the GPU with the state kept there)
+    while the others are served; a lane result equals the same integration run
+    directly on the host."""
     from abyss_b200.integrator import ACIntegrator
     from abyss_b200.regforce import RegularForce
 
     reqs = poisson_requests(rate=400.0, duration=0.04, nmin=256, nmax=3000, seed=14, t_end=0.03125, k_nb=16)
     srv = Server(capacity=1 << 17, max_clusters=32, list_cap=64, host_threads=8, max_n=3000,
-                 device_irregular_min_n=1024, lane_min_n=1500)
+                 device_irregular_min_n=1024, lane_min_n=1500, lane_threads=2,
+                 device_blocks_min_n=device_blocks_min_n)
     for r in reqs:
         srv.submit(r)
     srv.run_until_idle(max_seconds=300)
@@ -90,6 +94,7 @@ def test_large_requests_run_whole_on_the_lane():
     assert len(done) == len(reqs)
     lane = [r for r in done.values() if r.result.get("lane")]
     assert lane and len(lane) < len(reqs)
+    assert all(bool(r.result["device_blocks"]) == (device_blocks_min_n > 0) for r in lane)
     probe = lane[0]
     c = Request(probe.rid, 0.0, probe.model, probe.n, probe.seed, t_end=probe.t_end, k_nb=probe.k_nb).make_cluster()
     rf = RegularForce(0)
