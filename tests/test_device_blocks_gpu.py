@@ -158,3 +158,29 @@ def test_split_blocks_refused_while_resident():
     finally:
         ac.close()
         rf.close()
+
+
+def test_pooled_engine_reused_for_a_smaller_cluster(tmp_path):
+    """Device blocks of an N = 1024 integration on the engine an N = 2048 one
+    has just returned to the pool (its arrays reused, cleared): the same state
+    as the host integration, byte for byte."""
+    big = ic.plummer(2048, 5, k_nb=32)
+    rf = RegularForce(0)
+    ac = ACIntegrator(rf, big.x, big.v, big.m, big.r2nb, eps2=EPS2, fix_nb=32, t_end=10.0)
+    try:
+        ac.set_device_resident(True)
+        for _ in range(15):
+            ac.advance_block()
+    finally:
+        ac.close()
+        rf.close()
+    c = ic.plummer(1024, 6, k_nb=32)
+    rfs, acs = _pair(c, 32, 10.0)
+    try:
+        acs[1].set_device_resident(True)
+        for _ in range(30):
+            acs[0].advance_block()
+            acs[1].advance_block()
+        assert _particles(acs[0], tmp_path / "h.ckpt") == _particles(acs[1], tmp_path / "d.ckpt")
+    finally:
+        _close(rfs, acs)

@@ -261,3 +261,21 @@ def test_blocking_wait_policy_gives_the_same_results():
             assert r.energy(c.x, c.v, c.m, 1e-8) == r.energy(c.x, c.v, c.m, 1e-8)
     finally:
         r.close()
+
+
+def test_whole_launch_timing(rf):
+    """abyss_set_profiling(2): one interval around the whole launch, reported as
+    the force time with the other two zero; per-phase timing sums to about it."""
+    c = ic.plummer(4096, 9, k_nb=40)
+    rf.send_to_device(c.m, c.x, c.v, c.r2nb)
+    t = np.arange(0, c.n, 2, dtype=np.int32)
+    rf.set_targets(t)
+    rf.set_profiling("whole")
+    rf.launch(0.0, 256)
+    whole = rf.last_timing()
+    assert whole["order_ms"] == 0.0 and whole["finalize_ms"] == 0.0 and whole["force_ms"] > 0.0
+    rf.set_profiling(True)
+    rf.launch(0.0, 256)
+    parts = rf.last_timing()
+    assert parts["force_ms"] > 0.0 and parts["finalize_ms"] > 0.0
+    rf.set_profiling(False)
