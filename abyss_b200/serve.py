@@ -101,7 +101,7 @@ class Server:
                  eps2: float = 1e-8, eta_reg: float = 0.02, eta_irr: float = 0.01, host_threads: int = 16,
                  slice_ms: float = 20.0, max_n: int = 16384, chunk_j: int = 256, device_irregular_min_n: int = 0,
                  team_min_n: int = 16384, lane_min_n: int = 0, lane_threads: int = 2, lane_team: int = 4,
-                 device_blocks_min_n: int = 0, lane_wait_us: int = -1):
+                 device_blocks_min_n: int = 0, lane_wait_us: int = -1, lane_order: str = "arrival"):
         """device_irregular_min_n > 0: integrations of at least that many
         particles run their irregular levels on the GPU (include/abyss_irr.h)
         instead of on their worker thread; the results are the same.
@@ -120,7 +120,11 @@ class Server:
         share the GPU; the results are the same.
         lane_wait_us >= 0: a lane thread waiting for the GPU polls that long,
         then sleeps (include/abyss_reg.h abyss_set_wait), leaving its core to
-        the other lanes; < 0: it spins."""
+        the other lanes; < 0: it spins.
+        lane_order: which waiting lane request starts when a lane frees up --
+        "arrival" (first come, first served) or "largest" (the most particles
+        first: for a batch that arrives at once, the long integrations do not
+        end up last and alone)."""
         self.rf = RegularForce(device)
         self.ens = Ensemble(self.rf, None, list_cap=list_cap, capacity=capacity, max_clusters=max_clusters)
         # short j-chunks: a serving wave is small and latency-bound, so its work
@@ -134,6 +138,11 @@ class Server:
         self.lane_min_n = int(lane_min_n)
         self.lane_team = max(1, int(lane_team))
         self.lane_jobs: list = []  # (request, future) of large requests run whole
+        self.lane_queue: list = []  # lane requests waiting for a lane
+        self.lane_threads = max(1, lane_threads)
+        if lane_order not in ("arrival", "largest"):
+            raise ValueError("lane_order must be 'arrival' or 'largest'")
+        self.lane_order = lane_order
         self.lane_pool = ThreadPoolExecutor(max_workers=max(1, lane_threads)) if self.lane_min_n > 0 else None
         self.lane_ctx: queue.Queue = queue.Queue()
         if self.lane_min_n > 0:
@@ -247,7 +256,7 @@ class Server:
                 continue
             if self.lane_min_n > 0 and r.n >= self.lane_min_n:
                 r.admitted = self.now()
-                self.lane_jobs.append((r, self.lane_pool.submit(self._run_lane, r)))
+                self.lane_queue.append(r)
                 continue
             slot = self.ens.attach(r.n)
             if slot is None:
@@ -256,6 +265,7 @@ class Server:
             r.slot = slot
             self.building.append((r, self.pool.submit(self._build, r)))
         self.waiting = still
+        self._pump_lanes()
         pending = []
         for r, fut in self.building:
             if fut.done():
@@ -348,15 +358,29 @@ class Server:
             self.lane_ctx.put(rf)
         r.cluster = None
 
-    def _reap_lane(self, wait: bool = False):
-        still = []
-        for r, fut in self.lane_jobs:
-            if wait or fut.done():
-                fut.result()
-                self.done.append(r)
+    def _pump_lanes(self):
+        """Start waiting lane requests while a lane is free, in lane_order."""
+        while self.lane_queue and len(self.lane_jobs) < self.lane_threads:
+            if self.lane_order == "largest":
+                k = max(range(len(self.lane_queue)), key=lambda q: (self.lane_queue[q].n, -q))
             else:
-                still.append((r, fut))
-        self.lane_jobs = still
+                k = 0
+            r = self.lane_queue.pop(k)
+            self.lane_jobs.append((r, self.lane_pool.submit(self._run_lane, r)))
+
+    def _reap_lane(self, wait: bool = False):
+        while True:
+            still = []
+            for r, fut in self.lane_jobs:
+                if wait or fut.done():
+                    fut.result()
+                    self.done.append(r)
+                else:
+                    still.append((r, fut))
+            self.lane_jobs = still
+            self._pump_lanes()
+            if not (wait and (self.lane_jobs or self.lane_queue)):
+                return
 
     def _reap(self, wait: bool = False):
         still = []
@@ -381,12 +405,13 @@ class Server:
         r.ac = None
 
     def run_until_idle(self, max_seconds: float = 1e9):
-        while (self.waiting or self.building or self.active or self.lane_jobs) and self.now() < max_seconds:
+        while (self.waiting or self.building or self.active or self.lane_jobs or self.lane_queue) and \
+                self.now() < max_seconds:
             self._reap_lane()
             if not self.active and not self.building and self.waiting and \
                     all(r.arrival > self.now() for r in self.waiting):
                 time.sleep(max(0.0, min(0.05, min(r.arrival for r in self.waiting) - self.now())))
-            if not self.active and not self.building and not self.waiting and self.lane_jobs:
+            if not self.active and not self.building and not self.waiting and (self.lane_jobs or self.lane_queue):
                 time.sleep(0.01)  # only large requests left: they run on their own threads
             self.round()
         self._reap(wait=True)
@@ -412,7 +437,8 @@ def poisson_requests(rate: float, duration: float, nmin: int, nmax: int, seed: i
 def serve(rate: float = 200.0, duration: float = 2.0, nmin: int = 256, nmax: int = 2048, t_end: float = 0.0625,
           capacity: int = 1 << 21, seed: int = 5, host_threads: int = 16, serial: bool = False,
           chunk_j: int = 256, slice_ms: float = 20.0, device_irregular_min_n: int = 0, reqs=None,
-          lane_min_n: int = 0, lane_threads: int = 2, device_blocks_min_n: int = 0, lane_wait_us: int = -1):
+          lane_min_n: int = 0, lane_threads: int = 2, device_blocks_min_n: int = 0, lane_wait_us: int = -1,
+          lane_order: str = "arrival"):
     """Run a Poisson stream through the server (or, with serial=True, one request at
     a time through the same code) and report latency percentiles and throughput.
     `reqs` replaces the generated stream (requests with prebuilt clusters)."""
@@ -429,7 +455,7 @@ def serve(rate: float = 200.0, duration: float = 2.0, nmin: int = 256, nmax: int
         srv = Server(capacity=capacity, host_threads=host_threads, max_n=max(nmax, max(r.n for r in reqs)),
                      chunk_j=chunk_j, slice_ms=slice_ms, device_irregular_min_n=device_irregular_min_n,
                      lane_min_n=lane_min_n, lane_threads=lane_threads, device_blocks_min_n=device_blocks_min_n,
-                     lane_wait_us=lane_wait_us)
+                     lane_wait_us=lane_wait_us, lane_order=lane_order)
         for r in reqs:
             srv.submit(r)
         srv.run_until_idle()
@@ -454,7 +480,8 @@ def serve(rate: float = 200.0, duration: float = 2.0, nmin: int = 256, nmax: int
                config=dict(rate=rate, duration=duration, nmin=nmin, nmax=nmax, t_end=t_end, capacity=capacity,
                            seed=seed, serial=serial, device_irregular_min_n=device_irregular_min_n,
                            lane_min_n=lane_min_n, lane_threads=lane_threads,
-                           device_blocks_min_n=device_blocks_min_n, lane_wait_us=lane_wait_us))
+                           device_blocks_min_n=device_blocks_min_n, lane_wait_us=lane_wait_us,
+                           lane_order=lane_order))
     return res, done
 
 
@@ -507,15 +534,17 @@ def c4_requests(k: int = 512, t_end: float = 5.0):
 
 # Server options of the stated configurations (run_config).  Configuration 4
 # runs every integration whole on a lane with its blocks on the GPU: sixteen at
-# once, sharing the GPU.  Configuration 5 sends integrations of 16 384
-# particles and more to four such lanes and serves the rest in waves.
-CONFIG_LANES = {"c4": dict(lane_min_n=1, lane_threads=16, device_blocks_min_n=1),
-                "c5": dict(lane_min_n=16384, lane_threads=4, device_blocks_min_n=1)}
+# once, sharing the GPU, the largest clusters first (they all arrive at once).
+# Configuration 5 sends integrations of 16 384 particles and more to four such
+# lanes, in arrival order, and serves the rest in waves.
+CONFIG_LANES = {"c4": dict(lane_min_n=1, lane_threads=16, device_blocks_min_n=1, lane_order="largest"),
+                "c5": dict(lane_min_n=16384, lane_threads=4, device_blocks_min_n=1, lane_order="arrival")}
 
 
 def run_config(name: str, duration: float = 1.0, sample: int = 16, device_irregular_min_n: int = 4096,
                host_threads: int = 16, capacity: int = 1 << 22, lane_min_n: int | None = None,
-               lane_threads: int | None = None, device_blocks_min_n: int | None = None, lane_wait_us: int = -1):
+               lane_threads: int | None = None, device_blocks_min_n: int | None = None, lane_wait_us: int = -1,
+               lane_order: str | None = None):
     """A stated configuration through the continuous server, and the serial
     plain form on an evenly spaced sample of the same requests (the whole
     stream one at a time would take hours): its clusters/s is the sample's
@@ -527,6 +556,7 @@ def run_config(name: str, duration: float = 1.0, sample: int = 16, device_irregu
     lane_min_n = lanes["lane_min_n"] if lane_min_n is None else lane_min_n
     lane_threads = lanes["lane_threads"] if lane_threads is None else lane_threads
     device_blocks_min_n = lanes["device_blocks_min_n"] if device_blocks_min_n is None else device_blocks_min_n
+    lane_order = lanes["lane_order"] if lane_order is None else lane_order
     if name == "c4":
         reqs = c4_requests()
         nmax = 16384
@@ -537,12 +567,13 @@ def run_config(name: str, duration: float = 1.0, sample: int = 16, device_irregu
         r.cluster = r.make_cluster()
     res, done = serve(reqs=reqs, nmax=nmax, capacity=capacity, host_threads=host_threads,
                       device_irregular_min_n=device_irregular_min_n, lane_min_n=lane_min_n,
-                      lane_threads=lane_threads, device_blocks_min_n=device_blocks_min_n, lane_wait_us=lane_wait_us)
+                      lane_threads=lane_threads, device_blocks_min_n=device_blocks_min_n, lane_wait_us=lane_wait_us,
+                      lane_order=lane_order)
     res.pop("phase_s", None)
     res["config"] = dict(
         name=name, requests=len(reqs), device_irregular_min_n=device_irregular_min_n, host_threads=host_threads,
         capacity=capacity, lane_min_n=lane_min_n, lane_threads=lane_threads, device_blocks_min_n=device_blocks_min_n,
-        lane_wait_us=lane_wait_us,
+        lane_wait_us=lane_wait_us, lane_order=lane_order,
         workload=("512 equal-mass Plummer clusters, N log-uniform in [256, 16384] (seed 4, cluster k seeded "
                   "4000 + k), eps = 1e-4, all arriving at t = 0, each to t = 5" if name == "c4" else
                   f"Poisson 200 requests/s for {duration} s (seed 5), Plummer or King W0 3/6/9, Kroupa IMF, "
@@ -586,6 +617,8 @@ def main():
                     help="lane requests of at least this many particles run whole blocks on the GPU (0: none)")
     ap.add_argument("--lane-wait-us", type=int, default=-1,
                     help="a lane thread polls the GPU this long, then sleeps (< 0: spins)")
+    ap.add_argument("--lane-order", choices=["arrival", "largest"], default=None,
+                    help="which waiting lane request starts first (default: arrival, or the configuration's)")
     ap.add_argument("--rate", type=float, default=2000.0)
     ap.add_argument("--duration", type=float, default=None,
                     help="stream length in s (default 0.5; 1 for the stated configuration 5)")
@@ -600,7 +633,8 @@ def main():
                                     sample=args.sample,
                                     device_irregular_min_n=args.device_irregular_min_n, host_threads=args.threads,
                                     lane_min_n=args.lane_min_n, lane_threads=args.lane_threads,
-                                    device_blocks_min_n=args.device_blocks_min_n, lane_wait_us=args.lane_wait_us)))
+                                    device_blocks_min_n=args.device_blocks_min_n, lane_wait_us=args.lane_wait_us,
+                                    lane_order=args.lane_order)))
         return
     out = {}
     duration = 0.5 if args.duration is None else args.duration
@@ -608,7 +642,7 @@ def main():
         res, _ = serve(args.rate, duration, args.nmin, args.nmax, args.t_end, args.capacity,
                        host_threads=args.threads, serial=serial, lane_min_n=args.lane_min_n or 0,
                        lane_threads=args.lane_threads or 2, device_blocks_min_n=args.device_blocks_min_n or 0,
-                       lane_wait_us=args.lane_wait_us)
+                       lane_wait_us=args.lane_wait_us, lane_order=args.lane_order or "arrival")
         res["phase_s"].pop("build_thread_s", None)
         out["serial_plain" if serial else "continuous"] = res
     out["speedup"] = out["continuous"]["clusters_per_s"] / out["serial_plain"]["clusters_per_s"]

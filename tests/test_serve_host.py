@@ -6,6 +6,8 @@
 * A request builds its own cluster from its model and seed (Plummer or King of
   the named W0, Kroupa masses).
 * An autotuning table survives its JSON round trip (autotune.save/load).
+* Lane requests start in the server's lane order (arrival, or the largest
+  first) as lanes free up, never more at once than there are lanes.
 """
 import math
 
@@ -47,3 +49,46 @@ def test_tuning_table_round_trip(tmp_path):
     p = tmp_path / "tuning.json"
     autotune.save(table, p)
     assert autotune.load(p) == table
+
+
+class _Fut:
+    def __init__(self):
+        self.finished = False
+
+    def done(self):
+        return self.finished
+
+    def result(self):
+        return None
+
+
+class _Pool:
+    def submit(self, fn, r):
+        return _Fut()
+
+
+def _lanes(order, sizes, threads):
+    srv = serve.Server.__new__(serve.Server)  # the lane queue alone, no GPU
+    srv.lane_jobs, srv.done = [], []
+    srv.lane_queue = [serve.Request(k, 0.0, "plummer", n, k) for k, n in enumerate(sizes)]
+    srv.lane_threads, srv.lane_order, srv.lane_pool = threads, order, _Pool()
+    return srv
+
+
+def test_lane_order():
+    """Two lanes, five waiting requests; a lane frees up whenever its oldest job
+    finishes.  The start order is the lane order."""
+    sizes = [5000, 90000, 7000, 90000, 1200]
+    for order, want in (("largest", [90000, 90000, 7000, 5000, 1200]),
+                        ("arrival", [5000, 90000, 7000, 90000, 1200])):
+        srv = _lanes(order, sizes, 2)
+        started = []
+        srv._pump_lanes()
+        started += [r.rid for r, _ in srv.lane_jobs]
+        while srv.lane_jobs:
+            assert len(srv.lane_jobs) <= 2
+            srv.lane_jobs[0][1].finished = True
+            srv._reap_lane()
+            started += [r.rid for r, _ in srv.lane_jobs if r.rid not in started]
+        assert [sizes[k] for k in started] == want, order
+        assert sorted(r.n for r in srv.done) == sorted(sizes)
