@@ -545,7 +545,7 @@ CONFIG_LANES = {"c4": dict(lane_min_n=1, lane_threads=16, device_blocks_min_n=1,
 def run_config(name: str, duration: float = 1.0, sample: int = 16, device_irregular_min_n: int = 4096,
                host_threads: int = 16, capacity: int = 1 << 22, lane_min_n: int | None = None,
                lane_threads: int | None = None, device_blocks_min_n: int | None = None, lane_wait_us: int = -1,
-               lane_order: str | None = None):
+               lane_order: str | None = None, k: int = 512):
     """A stated configuration through the continuous server, and the serial
     plain form on an evenly spaced sample of the same requests (the whole
     stream one at a time would take hours): its clusters/s is the sample's
@@ -559,7 +559,7 @@ def run_config(name: str, duration: float = 1.0, sample: int = 16, device_irregu
     device_blocks_min_n = lanes["device_blocks_min_n"] if device_blocks_min_n is None else device_blocks_min_n
     lane_order = lanes["lane_order"] if lane_order is None else lane_order
     if name == "c4":
-        reqs = c4_requests()
+        reqs = c4_requests(k)
         nmax = 16384
     else:
         reqs = poisson_requests(200.0, duration, 1024, 131072, seed=5, t_end=1.0)
@@ -575,8 +575,9 @@ def run_config(name: str, duration: float = 1.0, sample: int = 16, device_irregu
         name=name, requests=len(reqs), device_irregular_min_n=device_irregular_min_n, host_threads=host_threads,
         capacity=capacity, lane_min_n=lane_min_n, lane_threads=lane_threads, device_blocks_min_n=device_blocks_min_n,
         lane_wait_us=lane_wait_us, lane_order=lane_order,
-        workload=("512 equal-mass Plummer clusters, N log-uniform in [256, 16384] (seed 4, cluster k seeded "
-                  "4000 + k), eps = 1e-4, all arriving at t = 0, each to t = 5" if name == "c4" else
+        workload=(f"{k} equal-mass Plummer clusters (the first {k} of the configuration's 512), N log-uniform in "
+                  "[256, 16384] (seed 4, cluster k seeded 4000 + k), eps = 1e-4, all arriving at t = 0, each to t = 5"
+                  if name == "c4" else
                   f"Poisson 200 requests/s for {duration} s (seed 5), Plummer or King W0 3/6/9, Kroupa IMF, "
                   "N log-uniform in [1024, 131072], eps = 1e-4, each to t = 1"))
     de = {r.rid: r.result["dE_over_E"] for r in done}
@@ -585,7 +586,7 @@ def run_config(name: str, duration: float = 1.0, sample: int = 16, device_irregu
     step = max(1, len(reqs) // max(1, sample))
     pick = [r.rid for r in reqs][::step][:sample]
     if name == "c4":
-        fresh = {r.rid: r for r in c4_requests()}
+        fresh = {r.rid: r for r in c4_requests(k)}
     else:
         fresh = {r.rid: r for r in poisson_requests(200.0, duration, 1024, 131072, seed=5, t_end=1.0)}
     sub = [fresh[k] for k in pick]
