@@ -222,3 +222,24 @@ def test_end_block_refuses_bad_results_and_stays_open():
         assert _digest(ac) == want
     finally:
         ac.close()
+
+
+def test_device_modes_need_a_gpu_context():
+    """An integration without a GPU context (a checkpoint loaded for host-side
+    calls) refuses the device irregular levels and device blocks, and stays
+    usable: switching them off is accepted and the state reads back."""
+    from abyss_b200._lib import ABYSS_ERR_STATE, AbyssError
+
+    ac = _load(1)
+    try:
+        before = _digest(ac)
+        for switch in (ac.set_device_irregular, ac.set_device_resident):
+            with pytest.raises(AbyssError) as err:
+                switch(True)
+            assert err.value.code == ABYSS_ERR_STATE
+            switch(False)
+        info = ac.device_resident_info()
+        assert not info["on"] and info["borderline"] == 0
+        assert _digest(ac) == before
+    finally:
+        ac.close()
