@@ -22,6 +22,10 @@
 //     overwrite a_tot while others still predict from it);
 //   * a target whose list overflows nb_max has its radius shrunk and the
 //     regular call re-run, instead of a device assert.
+// The same loop can run with its irregular levels on the GPU
+// (abyss_ac_set_device_irregular, irregular.cu) or with whole blocks there and
+// the state kept on the device (abyss_ac_set_device_resident: resident_block
+// below); both give the host loop's results bit for bit.
 #include <algorithm>
 #include <array>
 #include <chrono>
